@@ -1,0 +1,173 @@
+/*
+ * rigw.h - C ABI of the B200 RI-GW engine (imaginary-frequency G0W0 hot path of MOLGW).
+ *
+ * Every entry point returns an int status: RIGW_OK (0) or a positive error
+ * code; none aborts the caller.  rigw_last_error(ctx) gives the message of the
+ * last failure on that context.  Arrays are plain pointers in C (row-major)
+ * order, which is the memory order of the Fortran column-major arrays named in
+ * each comment; the ``_dev`` flag of a problem says that its pointers are CUDA
+ * device pointers instead of host pointers.
+ *
+ * Reference interfaces replaced (MOLGW 3.4, paths within its source tree):
+ *   rigw_imag_grid              sf_init IMAGINARY_QUAD grid   src/m_spectral_function.f90:286-306
+ *                               + coeffs_gausslegint           src/m_numerical_tools.f90:35-82
+ *   rigw_eri_3center_mo         calculate_eri_3center_mo      src/m_eri_ao_mo.f90:416-582
+ *   rigw_polarizability_imag    polarizability_grid_scalapack src/m_gw_selfenergy_grid.f90:33-209
+ *   rigw_wpol_chi               wpol%chi(:,:,iomega) (the DGEMM at src/m_gw_selfenergy_grid.f90:179-188)
+ *   rigw_gw_selfenergy_imag     gw_selfenergy_imag_scalapack  src/m_gw_selfenergy_grid.f90:213-338
+ *   rigw_qp_solve               se_pade_fit / self_energy_polynomial  src/m_selfenergy_tools.f90:965-1033
+ *                               find_qp_energy_linearization  src/m_selfenergy_tools.f90:202-249
+ *                               find_qp_energy_graphical      src/m_selfenergy_tools.f90:253-420
+ *   rigw_g0w0, rigw_g0w0_batch  the sequence of selfenergy_evaluation for
+ *                               imaginary_axis_pade / _homolumo, src/m_selfenergy_evaluation.f90:214-246,587-611
+ */
+#ifndef RIGW_H
+#define RIGW_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define RIGW_API __attribute__((visibility("default")))
+#else
+#define RIGW_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define RIGW_VERSION 1
+
+enum rigw_status {
+  RIGW_OK = 0,
+  RIGW_ERR_ARG = 1,        /* invalid argument (shape, null pointer, range)            */
+  RIGW_ERR_CUDA = 2,       /* CUDA runtime error                                        */
+  RIGW_ERR_NOMEM = 3,      /* device allocation failed or HBM budget exceeded           */
+  RIGW_ERR_NOT_SPD = 4,    /* eps(iw) not positive definite (a Cholesky pivot <= 0)     */
+  RIGW_ERR_NUMERIC = 5,    /* non-finite QP energy or singular Pade recursion           */
+  RIGW_ERR_TIMEOUT = 6,    /* a bounded wait expired                                    */
+  RIGW_ERR_UNSUPPORTED = 7 /* precision or option not available in this build           */
+};
+
+/* Arithmetic of the chi0 = M D M^T contraction (the eps factorization, Sigma and
+ * the QP solve are FP64 in every mode). */
+enum rigw_precision {
+  RIGW_FP64 = 0,           /* FP64 DMMA tensor cores end to end (the drop-in)            */
+  RIGW_BF16X3 = 1          /* split BF16 hi/lo products on tcgen05, FP32 accumulation    */
+};
+
+enum rigw_technique {
+  RIGW_PADE = 0,           /* imaginary_axis_pade: Thiele continuation                    */
+  RIGW_HOMOLUMO = 1        /* imaginary_axis_homolumo: quadratic fit in the gap          */
+};
+
+#define RIGW_PROBLEM_DEVICE_POINTERS 1
+
+typedef struct rigw_ctx rigw_ctx;
+typedef struct rigw_wpol rigw_wpol;
+
+/* One closed-shell (nspin = 1) G0W0 problem on the imaginary axis. */
+typedef struct rigw_problem {
+  int naux;                  /* auxiliary functions kept (nauxil_global)                  */
+  int nocc, nvirt;           /* W window: occupied ncore_W+1..nhomo_W, virtual nlumo_W..nvirtual_W-1 */
+  int nomega;                /* nomega_chi_imag                                           */
+  const double* omega;       /* [nomega] imaginary parts of wpol%omega; NULL: built here   */
+  const double* weight;      /* [nomega] wpol%weight_quad; NULL: built here               */
+  const double* m_ia;        /* [nocc][nvirt][naux] = eri_3center_mo(naux, a, i)           */
+  const double* e_occ;       /* [nocc]  energy(i)  (Ha)                                   */
+  const double* e_virt;      /* [nvirt] energy(a)                                         */
+  const double* occ_occ;     /* [nocc]  occupation(i)                                     */
+  const double* occ_virt;    /* [nvirt] occupation(a)                                     */
+  int nstate_p;              /* p = ncore_G+1 .. nvirtual_G-1                              */
+  int nsig;                  /* Sigma states nsemin..nsemax                               */
+  const double* m_pm;        /* [nsig][nstate_p][naux] = eri_3center_mo(naux, p, m)        */
+  const double* e_p;         /* [nstate_p] energy(p)                                      */
+  const double* e_sig;       /* [nsig] energy0 of the Sigma states                        */
+  const double* occ_sig;     /* [nsig] occupation of the Sigma states (HOMO/LUMO output)   */
+  const double* exchange_m_vxc; /* [nsig] Sigma_x - V_xc; NULL: zero (G0W0@HF)             */
+  int technique;             /* rigw_technique                                            */
+  int nomega_sigma_calc;     /* Sigma evaluation points (<= 128)                          */
+  double step_sigma_calc;
+  const double* omega_calc;  /* [nomega_sigma_calc][2] complex points; NULL: efermi + i*step*(k-1) */
+  int nomega_sigma;          /* real grid has 2*(nomega_sigma/2)+1 points                 */
+  double step_sigma;
+  double eta;
+  double efermi;             /* se_init efermi (mid-gap or mu_origin)                      */
+  int precision;             /* rigw_precision                                            */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS                               */
+} rigw_problem;
+
+/* Outputs of one problem; every array is caller-owned host memory (or device
+ * memory under RIGW_PROBLEM_DEVICE_POINTERS) and may be NULL when not wanted. */
+typedef struct rigw_result {
+  double erpa, egw;          /* 'RPA correlation energy (Ha)', 'GW  correlation energy (Ha)' */
+  double* sigma_calc;        /* [nsig][nomega_sigma_calc][2] se%sigma_calc                 */
+  double* sigma;             /* [nsig][2*(nomega_sigma/2)+1][2] se%sigma on the real grid   */
+  double* energy_qp_g;       /* [nsig] graphical QP energies (the reported ones)           */
+  double* energy_qp_z;       /* [nsig] linearized QP energies                              */
+  double* zz;                /* [nsig] Z of the graphical solution                         */
+  double ehomo, elumo;       /* output_homolumo over the Sigma range (Ha)                   */
+  double device_ms;          /* GPU time of the solve (CUDA events)                        */
+} rigw_result;
+
+/* Per-call statistics of the last solve on a context (the device-side analogue of
+ * MOLGW's stage timers timer_rpa_dynamic / timer_gw_self, src/m_timing.f90:268-284). */
+typedef struct rigw_stats {
+  double stage_ms[4];        /* CUDA-event times: input packing, chi0 contraction,
+                                eps factorization + triangular solves, energies + Sigma + QP */
+  double total_ms;
+  int kernel_launches;       /* kernels launched by the last solve                        */
+  int graph_replayed;        /* 1 when the launch sequence was a CUDA-graph replay        */
+  size_t device_bytes_in_use, device_bytes_peak;
+} rigw_stats;
+
+/* ---- context ---------------------------------------------------------------- */
+RIGW_API int rigw_create(rigw_ctx** ctx, int device, size_t hbm_budget_bytes);
+RIGW_API int rigw_destroy(rigw_ctx* ctx);
+RIGW_API const char* rigw_last_error(const rigw_ctx* ctx);
+RIGW_API int rigw_version(void);
+RIGW_API int rigw_last_stats(const rigw_ctx* ctx, rigw_stats* stats);
+/* Bytes of device memory a problem of these sizes needs (admission by footprint). */
+RIGW_API size_t rigw_footprint_bytes(int naux, int nocc, int nvirt, int nomega, int nstate_p, int nsig,
+                            int precision);
+
+/* ---- building blocks -------------------------------------------------------- */
+/* Gauss-Legendre imaginary grid: omega_k = 2x/(1-x), weight_k = 2w/(1-x)^2. */
+RIGW_API int rigw_imag_grid(int nomega, double* omega, double* weight);
+
+/* AO->MO: out[n][m][P] = sum_{mu,nu} C[m][mu] C[n][nu] B(mu nu, P) for
+ * m in [mstate_min, mstate_max], n in [nstate_min, nstate_max] (1-based).
+ * eri3 is [naux][npair] (eri_3center(npair, naux)), index_basis [npair][2]
+ * 1-based, diagonal pairs stored x0.5; c_matrix is [nstate][nbf]
+ * (c_matrix(nbf, nstate)); out is [n_count][m_count][naux]. Host pointers. */
+RIGW_API int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux,
+                        const int* index_basis, const double* eri3, const double* c_matrix,
+                        int mstate_min, int mstate_max, int nstate_min, int nstate_max,
+                        double* out);
+
+/* chi0, eps(iw) = 1 - chi0 and its factorization for every frequency; keeps the
+ * factors resident on the device in *wpol.  Uses the W-window fields of
+ * ``prob`` (naux..occ_virt, nomega, omega, weight, precision, flags). */
+RIGW_API int rigw_polarizability_imag(rigw_ctx* ctx, const rigw_problem* prob, double* erpa, double* egw,
+                             rigw_wpol** wpol);
+/* wpol%chi(:,:,iomega) = (1-chi0)^-1 chi0 for all frequencies, [nomega][naux][naux]. */
+RIGW_API int rigw_wpol_chi(rigw_ctx* ctx, const rigw_wpol* wpol, double* chi);
+/* Sigma_c on the evaluation points from resident factors; uses the Sigma fields
+ * of ``prob``; writes result->sigma_calc. */
+RIGW_API int rigw_gw_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_problem* prob,
+                            rigw_result* result);
+RIGW_API int rigw_wpol_release(rigw_ctx* ctx, rigw_wpol* wpol);
+/* Continuation + QP equation from sigma_calc (host arrays of ``result``). */
+RIGW_API int rigw_qp_solve(rigw_ctx* ctx, const rigw_problem* prob, const double* sigma_calc,
+                  rigw_result* result);
+
+/* ---- fused solves ----------------------------------------------------------- */
+RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result);
+/* Many problems of different sizes in one launch sequence (one CUDA graph). */
+RIGW_API int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_result* results);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RIGW_H */

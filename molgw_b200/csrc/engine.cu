@@ -1,0 +1,695 @@
+// Host engine of the RI-GW library: plans, device memory, launch sequences.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <tuple>
+
+#include "engine.cuh"
+
+namespace rigw {
+
+namespace {
+constexpr size_t kAlign = 256;
+inline size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
+}  // namespace
+
+// ---------------------------------------------------------------------------
+bool Shape::operator<(const Shape& o) const {
+  return std::tie(naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision) <
+         std::tie(o.naux, o.nocc, o.nvirt, o.nomega, o.nstate_p, o.nsig, o.nc, o.nsigma_half, o.technique,
+                  o.precision);
+}
+
+Status make_shape(const rigw_problem& p, Shape* sh) {
+  if (p.naux <= 0 || p.nocc < 0 || p.nvirt < 0 || p.nomega <= 0)
+    return Status::fail(RIGW_ERR_ARG, "invalid W-window sizes naux=%d nocc=%d nvirt=%d nomega=%d", p.naux,
+                        p.nocc, p.nvirt, p.nomega);
+  if (p.nsig < 0 || p.nstate_p < 0)
+    return Status::fail(RIGW_ERR_ARG, "invalid Sigma sizes nsig=%d nstate_p=%d", p.nsig, p.nstate_p);
+  if (p.nomega_sigma_calc < 0 || p.nomega_sigma_calc > 128)
+    return Status::fail(RIGW_ERR_ARG, "nomega_sigma_calc=%d outside [0,128]", p.nomega_sigma_calc);
+  if (p.technique != RIGW_PADE && p.technique != RIGW_HOMOLUMO)
+    return Status::fail(RIGW_ERR_ARG, "unknown technique %d", p.technique);
+  if (p.precision != RIGW_FP64 && p.precision != RIGW_BF16X3)
+    return Status::fail(RIGW_ERR_ARG, "unknown precision %d", p.precision);
+  sh->naux = p.naux;
+  sh->nocc = p.nocc;
+  sh->nvirt = p.nvirt;
+  sh->nomega = p.nomega;
+  sh->nstate_p = p.nstate_p;
+  sh->nsig = p.nsig;
+  sh->nc = p.nomega_sigma_calc;
+  sh->nsigma_half = p.nomega_sigma / 2;
+  sh->technique = p.technique;
+  sh->precision = p.precision;
+  return Status::ok();
+}
+
+// ---------------------------------------------------------------------------
+DeviceBuffer::~DeviceBuffer() { release(); }
+
+Status DeviceBuffer::allocate(Context* ctx, size_t bytes, const char* name) {
+  release();
+  if (bytes == 0) return Status::ok();
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget)
+    return Status::fail(RIGW_ERR_NOMEM, "%s: %zu bytes exceed the HBM budget (%zu in use of %zu)", name, bytes,
+                        ctx->in_use, ctx->budget);
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), bytes);
+  if (e != cudaSuccess) {
+    ptr_ = nullptr;
+    cudaGetLastError();
+    return Status::fail(RIGW_ERR_NOMEM, "%s: cudaMalloc(%zu) failed: %s", name, bytes, cudaGetErrorString(e));
+  }
+  ctx_ = ctx;
+  bytes_ = bytes;
+  ctx->in_use += bytes;
+  ctx->peak = std::max(ctx->peak, ctx->in_use);
+  return Status::ok();
+}
+
+void DeviceBuffer::release() {
+  if (ptr_) {
+    cudaFree(ptr_);
+    ctx_->in_use -= bytes_;
+  }
+  ptr_ = nullptr;
+  bytes_ = 0;
+}
+
+// ---------------------------------------------------------------------------
+Status Context::init(int dev, size_t budget_bytes) {
+  device = dev;
+  budget = budget_bytes;
+  RIGW_CUDA_TRY(cudaSetDevice(dev));
+  RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  RIGW_CUDA_TRY(prepare_dgemm_kernels());
+  return Status::ok();
+}
+
+Context::~Context() {
+  fused_cache.clear();
+  if (stream) cudaStreamDestroy(stream);
+}
+
+// ---------------------------------------------------------------------------
+namespace {
+
+struct Dims {
+  int npad, npanel, nia, nia_pad, want_identity, moff, ncm, ldb, nreal;
+};
+
+Dims dims_of(const Shape& sh, PlanMode mode) {
+  Dims d;
+  d.npad = round_up(sh.naux, kPanel);
+  d.npanel = d.npad / kPanel;
+  d.nia = sh.nocc * sh.nvirt;
+  d.nia_pad = round_up(std::max(d.nia, 1), 16);
+  d.want_identity = (mode == kPlanFused || mode == kPlanPolar) ? 1 : 0;
+  d.moff = d.want_identity ? d.npad : 0;
+  d.ncm = (mode == kPlanFused || mode == kPlanSigma) ? round_up(sh.nsig * sh.nstate_p, 8) : 0;
+  d.ldb = d.moff + d.ncm;
+  d.nreal = 2 * sh.nsigma_half + 1;
+  return d;
+}
+
+// Bump allocator over one arena; first pass measures, second pass assigns.
+struct Layout {
+  size_t cur = 0;
+  size_t take(size_t bytes) {
+    const size_t o = cur;
+    cur = align_up(cur + std::max<size_t>(bytes, 1), kAlign);
+    return o;
+  }
+};
+
+}  // namespace
+
+size_t footprint(const Shape& sh, PlanMode mode) {
+  const Dims d = dims_of(sh, mode);
+  const size_t D = sizeof(double);
+  size_t b = 0;
+  const bool factor = (mode == kPlanFused || mode == kPlanPolar);
+  const bool sigma = (mode == kPlanFused || mode == kPlanSigma);
+  if (factor) {
+    b += size_t(d.nia) * sh.naux * D;                    // staged M
+    b += size_t(d.nia_pad) * d.npad * D;                 // packed M
+    b += size_t(sh.nomega) * d.nia_pad * D;              // D_w(t)
+    b += size_t(sh.nomega) * d.npad * d.npad * D;        // eps / U
+    b += size_t(sh.nomega) * d.npanel * kPanel * kPanel * D;
+  }
+  if (sigma) b += size_t(sh.nsig) * sh.nstate_p * sh.naux * D;
+  b += size_t(sh.nomega) * d.npad * d.ldb * D;           // rhs
+  b += size_t(sh.nomega) * d.npanel * d.ldb * D;         // colsq
+  b += size_t(sh.nomega) * d.ncm * D * 2;
+  return b + (1u << 20);
+}
+
+Plan::~Plan() {
+  if (exec_) cudaGraphExecDestroy(exec_);
+  if (graph_) cudaGraphDestroy(graph_);
+  if (ev0_) cudaEventDestroy(ev0_);
+  if (ev1_) cudaEventDestroy(ev1_);
+  for (auto& e : stage_ev_)
+    if (e) cudaEventDestroy(e);
+}
+
+Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
+                   const std::vector<const ProbDev*>& factors) {
+  ctx_ = ctx;
+  mode_ = mode;
+  shapes_ = shapes;
+  const int np = int(shapes.size());
+  probs_.assign(np, PlanProblem{});
+  const bool factor = (mode == kPlanFused || mode == kPlanPolar);
+  const bool sigma = (mode == kPlanFused || mode == kPlanSigma);
+  const bool qp = (mode == kPlanFused || mode == kPlanQP);
+  if (mode == kPlanSigma && int(factors.size()) != np)
+    return Status::fail(RIGW_ERR_ARG, "sigma plan needs resident factors");
+  const size_t D = sizeof(double);
+
+  // ---- memory layout
+  Layout L;
+  struct Off {
+    size_t mp, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, en, sc, sr, qp;
+  };
+  std::vector<Off> off(np);
+  for (int i = 0; i < np; ++i) {
+    const Shape& sh = shapes[i];
+    const Dims d = dims_of(sh, mode);
+    PlanProblem& pp = probs_[i];
+    pp.sh = sh;
+    if (factor) {
+      pp.off_in_m = L.take(size_t(d.nia) * sh.naux * D);
+      pp.off_in_eocc = L.take(size_t(sh.nocc) * D);
+      pp.off_in_evirt = L.take(size_t(sh.nvirt) * D);
+      pp.off_in_oocc = L.take(size_t(sh.nocc) * D);
+      pp.off_in_ovirt = L.take(size_t(sh.nvirt) * D);
+      pp.off_in_omega = L.take(size_t(sh.nomega) * D);
+      pp.off_in_weight = L.take(size_t(sh.nomega) * D);
+      off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
+      off[i].tnorm = L.take(size_t(d.nia_pad) * D);
+      off[i].dscale = L.take(size_t(sh.nomega) * d.nia_pad * D);
+      off[i].eps = L.take(size_t(sh.nomega) * d.npad * d.npad * D);
+      off[i].winv = L.take(size_t(sh.nomega) * d.npanel * kPanel * kPanel * D);
+      off[i].logdet = L.take(size_t(sh.nomega) * d.npanel * D);
+      off[i].ew = L.take(size_t(sh.nomega) * 2 * D);
+      off[i].en = L.take(2 * D);
+    }
+    if (sigma) {
+      pp.off_in_msig = L.take(size_t(sh.nsig) * sh.nstate_p * sh.naux * D);
+      pp.off_in_ep = L.take(size_t(sh.nstate_p) * D);
+      off[i].mnorm = L.take(size_t(d.ncm) * D);
+      off[i].vchiv = L.take(size_t(sh.nomega) * d.ncm * D);
+      if (mode == kPlanSigma) {
+        pp.off_in_omega = L.take(size_t(sh.nomega) * D);
+        pp.off_in_weight = L.take(size_t(sh.nomega) * D);
+      }
+    }
+    if (d.ldb > 0) {
+      off[i].rhs = L.take(size_t(sh.nomega) * d.npad * d.ldb * D);
+      off[i].colsq = L.take(size_t(sh.nomega) * d.npanel * d.ldb * D);
+    }
+    if (sigma || qp) {
+      pp.off_in_zcalc = L.take(size_t(2) * sh.nc * D);
+      off[i].sc = L.take(size_t(2) * sh.nsig * sh.nc * D);
+    }
+    if (qp) {
+      pp.off_in_esig = L.take(size_t(sh.nsig) * D);
+      pp.off_in_xc = L.take(size_t(sh.nsig) * D);
+      off[i].sr = L.take(size_t(2) * sh.nsig * d.nreal * D);
+      off[i].qp = L.take(size_t(4) * sh.nsig * D);
+    }
+  }
+  const size_t table_off = L.take(sizeof(ProbDev) * np);
+  const size_t err_off = L.take(sizeof(int));
+  RIGW_TRY(arena_.allocate(ctx, L.cur, "plan arena"));
+  char* base = arena_.data();
+  probs_dev_ = reinterpret_cast<ProbDev*>(base + table_off);
+  err_dev_ = reinterpret_cast<int*>(base + err_off);
+  auto dp = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
+
+  // ---- device descriptors
+  for (int i = 0; i < np; ++i) {
+    const Shape& sh = shapes[i];
+    const Dims d = dims_of(sh, mode);
+    ProbDev& p = probs_[i].dev;
+    std::memset(&p, 0, sizeof(p));
+    p.naux = sh.naux;
+    p.npad = d.npad;
+    p.nocc = sh.nocc;
+    p.nvirt = sh.nvirt;
+    p.nia = d.nia;
+    p.nia_pad = d.nia_pad;
+    p.nomega = sh.nomega;
+    p.npanel = d.npanel;
+    p.nsig = sh.nsig;
+    p.nstate_p = sh.nstate_p;
+    p.ncm = d.ncm;
+    p.moff = d.moff;
+    p.ldb = d.ldb;
+    p.nc = sh.nc;
+    p.nsigma_half = sh.nsigma_half;
+    p.technique = sh.technique;
+    p.want_identity = d.want_identity;
+    if (factor) {
+      p.mp = dp(off[i].mp);
+      p.tnorm = dp(off[i].tnorm);
+      p.dscale = dp(off[i].dscale);
+      p.eps = dp(off[i].eps);
+      p.winv = dp(off[i].winv);
+      p.logdet = dp(off[i].logdet);
+      p.ew = dp(off[i].ew);
+      p.out_energies = dp(off[i].en);
+    } else if (mode == kPlanSigma) {
+      const ProbDev& f = *factors[i];
+      p.eps = f.eps;
+      p.winv = f.winv;
+      p.npad = f.npad;
+      p.npanel = f.npanel;
+    }
+    if (d.ldb > 0) {
+      p.rhs = dp(off[i].rhs);
+      p.colsq = dp(off[i].colsq);
+    }
+    if (sigma) {
+      p.mnorm = dp(off[i].mnorm);
+      p.vchiv = dp(off[i].vchiv);
+    }
+    if (sigma || qp) p.sigma_calc = dp(off[i].sc);
+    if (qp) {
+      p.sigma_real = dp(off[i].sr);
+      p.qp = dp(off[i].qp);
+    }
+    p.err = err_dev_;
+  }
+
+  // ---- work lists
+  const int BMN = 128;
+  int max_panels = 0;
+  for (int i = 0; i < np; ++i) max_panels = std::max(max_panels, probs_[i].dev.npanel);
+  wl_diag_.assign(max_panels, {});
+  gl_k2_.assign(max_panels, {});
+  gl_k3_.assign(max_panels, {});
+  for (int i = 0; i < np; ++i) {
+    const Shape& sh = shapes[i];
+    const ProbDev& p = probs_[i].dev;
+    const int npad = p.npad, ldb = p.ldb;
+    if (factor) {
+      for (int t0 = 0; t0 < p.nia_pad; t0 += 8) wl_pack_.push_back({i, t0, 0, 0});
+      for (int w = 0; w < sh.nomega; ++w) {
+        double* E = p.eps + size_t(w) * npad * npad;
+        for (int ti = 0; ti < npad; ti += BMN)
+          for (int tj = ti; tj < npad; tj += BMN) {
+            GemmItem g{};
+            g.A = p.mp + ti;
+            g.B = p.mp + tj;
+            g.lda = g.ldb = npad;
+            g.C = E + size_t(ti) * npad + tj;
+            g.ldc = npad;
+            g.kscale = p.dscale + size_t(w) * p.nia_pad;
+            g.m = std::min(BMN, npad - ti);
+            g.n = std::min(BMN, npad - tj);
+            g.k = p.nia_pad;
+            g.flags = kAddIdentity;
+            g.diag = ti - tj;
+            g.alpha = 1.0;
+            g.beta = 0.0;
+            gl_syrk_.push_back(g);
+          }
+      }
+    }
+    if (ldb > 0) {
+      for (int i0 = 0; i0 < npad; i0 += 32)
+        for (int c0 = 0; c0 < ldb; c0 += 32) wl_rhs_.push_back({i, i0, c0, 0});
+    }
+    if (sigma)
+      for (int c0 = 0; c0 < p.ncm; c0 += 8) wl_mnorm_.push_back({i, c0, 0, 0});
+    for (int k = 0; k < p.npanel; ++k) {
+      const int r0 = (k + 1) * kPanel;
+      for (int w = 0; w < sh.nomega; ++w) {
+        double* E = p.eps + size_t(w) * npad * npad;
+        double* R = p.rhs + size_t(w) * npad * ldb;
+        const double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
+        double* cs = p.colsq ? p.colsq + (size_t(w) * p.npanel + k) * ldb : nullptr;
+        if (factor) wl_diag_[k].push_back({i, w, 0, 0});
+        auto k2 = [&](double* X, int ldx, int c0, int n, double* colsq) {
+          GemmItem g{};
+          g.A = W;
+          g.lda = kPanel;
+          g.B = X + size_t(k) * kPanel * ldx + c0;
+          g.ldb = ldx;
+          g.C = X + size_t(k) * kPanel * ldx + c0;
+          g.ldc = ldx;
+          g.colsq = colsq;
+          g.m = kPanel;
+          g.n = n;
+          g.k = kPanel;
+          g.alpha = 1.0;
+          gl_k2_[k].push_back(g);
+        };
+        if (factor)
+          for (int c0 = r0; c0 < npad; c0 += BMN) k2(E, npad, c0, std::min(BMN, npad - c0), nullptr);
+        if (p.want_identity)
+          for (int c0 = 0; c0 < r0; c0 += BMN) k2(R, ldb, c0, std::min(BMN, r0 - c0), cs + c0);
+        for (int c0 = p.moff; c0 < ldb; c0 += BMN) k2(R, ldb, c0, std::min(BMN, ldb - c0), cs + c0);
+        // trailing update of panel k
+        auto k3 = [&](const double* Bsrc, int ldbs, double* Cdst, int ldc, int i0, int c0, int m, int n) {
+          GemmItem g{};
+          g.A = E + size_t(k) * kPanel * npad + i0;
+          g.lda = npad;
+          g.B = Bsrc + size_t(k) * kPanel * ldbs + c0;
+          g.ldb = ldbs;
+          g.C = Cdst + size_t(i0) * ldc + c0;
+          g.Cin = g.C;
+          g.ldc = ldc;
+          g.m = m;
+          g.n = n;
+          g.k = kPanel;
+          g.alpha = -1.0;
+          g.beta = 1.0;
+          gl_k3_[k].push_back(g);
+        };
+        for (int i0 = r0; i0 < npad; i0 += BMN) {
+          const int m = std::min(BMN, npad - i0);
+          if (factor)
+            for (int j0 = i0; j0 < npad; j0 += BMN) k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0));
+          if (p.want_identity)
+            for (int c0 = 0; c0 < r0; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, r0 - c0));
+          for (int c0 = p.moff; c0 < ldb; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, ldb - c0));
+        }
+      }
+    }
+    if (factor)
+      for (int w = 0; w < sh.nomega; ++w) wl_energy_.push_back({i, w, 0, 0});
+    if (sigma) {
+      for (int w = 0; w < sh.nomega; ++w)
+        for (int c0 = 0; c0 < p.ncm; c0 += 256) wl_vchiv_.push_back({i, w, c0, 0});
+      for (int s = 0; s < sh.nsig; ++s)
+        for (int kz = 0; kz < sh.nc; ++kz) wl_sigma_.push_back({i, s, kz, 0});
+    }
+    if (qp)
+      for (int s = 0; s < sh.nsig; ++s) wl_pade_.push_back({i, s, 0, 0});
+  }
+
+  // ---- upload the lists and the launch sequence
+  size_t lbytes = 0;
+  auto reserve = [&](size_t n) {
+    const size_t o = lbytes;
+    lbytes = align_up(lbytes + n, kAlign);
+    return o;
+  };
+  struct Pending {
+    int kind;
+    const void* src;
+    size_t bytes;
+    int count;
+    int arg;
+  };
+  std::vector<Pending> pend;
+  auto add = [&](int kind, const void* src, size_t elem, size_t n, int arg) {
+    if (n == 0) return;
+    pend.push_back({kind, src, elem * n, int(n), arg});
+  };
+  add(0, wl_pack_.data(), sizeof(WorkItem), wl_pack_.size(), 0);
+  add(2, wl_rhs_.data(), sizeof(WorkItem), wl_rhs_.size(), 0);
+  add(3, wl_mnorm_.data(), sizeof(WorkItem), wl_mnorm_.size(), 0);
+  add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
+  for (int k = 0; k < max_panels; ++k) {
+    add(4, wl_diag_[k].data(), sizeof(WorkItem), wl_diag_[k].size(), k);
+    add(5, gl_k2_[k].data(), sizeof(GemmItem), gl_k2_[k].size(), k);
+    add(6, gl_k3_[k].data(), sizeof(GemmItem), gl_k3_[k].size(), k);
+  }
+  add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0);
+  if (factor) pend.push_back({8, nullptr, 0, np, 0});
+  add(9, wl_vchiv_.data(), sizeof(WorkItem), wl_vchiv_.size(), 0);
+  add(10, wl_sigma_.data(), sizeof(WorkItem), wl_sigma_.size(), 0);
+  add(11, wl_pade_.data(), sizeof(WorkItem), wl_pade_.size(), 0);
+  std::vector<size_t> offs;
+  for (auto& pd : pend) offs.push_back(pd.bytes ? reserve(pd.bytes) : 0);
+  RIGW_TRY(lists_.allocate(ctx, std::max<size_t>(lbytes, kAlign), "plan work lists"));
+  std::vector<char> host(lbytes);
+  for (size_t j = 0; j < pend.size(); ++j) {
+    if (pend[j].bytes) std::memcpy(host.data() + offs[j], pend[j].src, pend[j].bytes);
+    seq_.push_back({pend[j].kind, offs[j], pend[j].count, pend[j].arg});
+  }
+  RIGW_CUDA_TRY(cudaMemcpy(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice));
+  RIGW_CUDA_TRY(cudaEventCreate(&ev0_));
+  RIGW_CUDA_TRY(cudaEventCreate(&ev1_));
+  for (auto& e : stage_ev_) RIGW_CUDA_TRY(cudaEventCreate(&e));
+  host_table_.resize(np);
+  n_launches_ = int(seq_.size());
+  return Status::ok();
+}
+
+// Stage of a launch kind: 0 input packing, 1 chi0, 2 eps factorization and
+// solves, 3 energies / Sigma / QP.  Stage boundaries carry CUDA events that are
+// captured into the graph, so every replay reports its own stage times.
+static int stage_of(int kind) {
+  switch (kind) {
+    case 0: case 2: case 3: return 0;
+    case 1: return 1;
+    case 4: case 5: case 6: return 2;
+    default: return 3;
+  }
+}
+
+void Plan::record(cudaStream_t s) {
+  char* lb = lists_.data();
+  int phase = 0;
+  cudaEventRecord(stage_ev_[0], s);
+  for (const Launch& L : seq_) {
+    const int st = stage_of(L.kind);
+    while (phase < st) cudaEventRecord(stage_ev_[++phase], s);
+    const WorkItem* wl = reinterpret_cast<const WorkItem*>(lb + L.off);
+    const GemmItem* gl = reinterpret_cast<const GemmItem*>(lb + L.off);
+    switch (L.kind) {
+      case 0: pack_m_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 1: launch_dgemm_128x128(gl, L.count, s); break;
+      case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 4: chol_diag_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl, L.arg); break;
+      case 5: launch_dgemm_64x128(gl, L.count, s); break;
+      case 6: launch_dgemm_128x128(gl, L.count, s); break;
+      case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 8: energy_sum_kernel<<<(L.count + 127) / 128, 128, 0, s>>>(probs_dev_, L.count); break;
+      case 9: vchiv_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 10: sigma_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 11: pade_qp_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      default: break;
+    }
+  }
+  while (phase < 4) cudaEventRecord(stage_ev_[++phase], s);
+}
+
+// Gauss-Legendre imaginary grid (coeffs_gausslegint + the [0,1) -> [0,inf) map).
+void imag_grid(int n, double* omega, double* weight) {
+  const double pi = 3.14159265358979323;
+  std::vector<double> x(n), w(n);
+  const double tol = 1.0e-13, xl = 0.5, xmean = 0.5;
+  for (int i = 1; i <= (n + 1) / 2; ++i) {
+    double z = std::cos(pi * (i - 0.25) / (n + 0.5)), z1, pp, p1, p2, p3;
+    do {
+      p1 = 1.0;
+      p2 = 0.0;
+      for (int j = 1; j <= n; ++j) {
+        p3 = p2;
+        p2 = p1;
+        p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j;
+      }
+      pp = n * (p2 - z * p1) / (1.0 - z * z);
+      z1 = z;
+      z = z1 - p1 / pp;
+    } while (std::fabs(z - z1) >= tol);
+    x[i - 1] = xmean - xl * z;
+    x[n - i] = xmean + xl * z;
+    w[i - 1] = 2.0 * xl / ((1.0 - z * z) * pp * pp);
+    w[n - i] = w[i - 1];
+  }
+  const double alpha = 1.0, beta = 2.0;
+  for (int k = 0; k < n; ++k) {
+    weight[k] = w[k] / (std::pow(2.0, alpha) - 1.0) * alpha * std::pow(1.0 - x[k], -alpha - 1.0) * beta;
+    omega[k] = 1.0 / (std::pow(2.0, alpha) - 1.0) * (1.0 / std::pow(1.0 - x[k], alpha) - 1.0) * beta;
+  }
+}
+
+Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
+  char* base = arena_.data();
+  auto dp = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
+  const bool factor = (mode_ == kPlanFused || mode_ == kPlanPolar);
+  const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma);
+  const bool qp = (mode_ == kPlanFused || mode_ == kPlanQP);
+  for (size_t i = 0; i < probs_.size(); ++i) {
+    const rigw_problem& q = probs[i];
+    PlanProblem& pp = probs_[i];
+    ProbDev& p = pp.dev;
+    const Shape& sh = pp.sh;
+    const bool on_dev = (q.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
+    auto bind = [&](const double* user, size_t off, size_t n, const char* what, const double** slot) -> Status {
+      if (n == 0) {
+        *slot = dp(off);
+        return Status::ok();
+      }
+      if (!user) return Status::fail(RIGW_ERR_ARG, "problem %zu: %s is NULL", i, what);
+      if (on_dev) {
+        *slot = user;
+      } else {
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(off), user, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        *slot = dp(off);
+      }
+      return Status::ok();
+    };
+    if (factor || sigma) {
+      // frequency grid: caller's or Gauss-Legendre
+      if (q.omega && q.weight) {
+        RIGW_TRY(bind(q.omega, pp.off_in_omega, sh.nomega, "omega", &p.omega));
+        RIGW_TRY(bind(q.weight, pp.off_in_weight, sh.nomega, "weight", &p.weight));
+      } else {
+        std::vector<double> om(sh.nomega), wt(sh.nomega);
+        imag_grid(sh.nomega, om.data(), wt.data());
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_omega), om.data(), om.size() * 8, cudaMemcpyHostToDevice, s));
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_weight), wt.data(), wt.size() * 8, cudaMemcpyHostToDevice, s));
+        RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+        p.omega = dp(pp.off_in_omega);
+        p.weight = dp(pp.off_in_weight);
+      }
+    }
+    if (factor) {
+      const size_t nia = size_t(sh.nocc) * sh.nvirt;
+      RIGW_TRY(bind(q.m_ia, pp.off_in_m, nia * sh.naux, "m_ia", &p.m_in));
+      RIGW_TRY(bind(q.e_occ, pp.off_in_eocc, sh.nocc, "e_occ", &p.e_occ));
+      RIGW_TRY(bind(q.e_virt, pp.off_in_evirt, sh.nvirt, "e_virt", &p.e_virt));
+      RIGW_TRY(bind(q.occ_occ, pp.off_in_oocc, sh.nocc, "occ_occ", &p.occ_occ));
+      RIGW_TRY(bind(q.occ_virt, pp.off_in_ovirt, sh.nvirt, "occ_virt", &p.occ_virt));
+    }
+    if (sigma) {
+      RIGW_TRY(bind(q.m_pm, pp.off_in_msig, size_t(sh.nsig) * sh.nstate_p * sh.naux, "m_pm", &p.msig_in));
+      RIGW_TRY(bind(q.e_p, pp.off_in_ep, sh.nstate_p, "e_p", &p.e_p));
+    }
+    if (sigma || qp) {
+      if (q.omega_calc) {
+        RIGW_TRY(bind(q.omega_calc, pp.off_in_zcalc, size_t(2) * sh.nc, "omega_calc", &p.zcalc));
+      } else {
+        if (sh.technique != RIGW_PADE)
+          return Status::fail(RIGW_ERR_ARG, "problem %zu: homolumo technique needs omega_calc", i);
+        std::vector<double> z(2 * sh.nc);
+        for (int k = 0; k < sh.nc; ++k) {
+          z[2 * k] = q.efermi;
+          z[2 * k + 1] = q.step_sigma_calc * k;
+        }
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_zcalc), z.data(), z.size() * 8, cudaMemcpyHostToDevice, s));
+        RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+        p.zcalc = dp(pp.off_in_zcalc);
+      }
+    }
+    if (qp) {
+      RIGW_TRY(bind(q.e_sig, pp.off_in_esig, sh.nsig, "e_sig", &p.e_sig));
+      if (q.exchange_m_vxc) {
+        RIGW_TRY(bind(q.exchange_m_vxc, pp.off_in_xc, sh.nsig, "exchange_m_vxc", &p.xc_sig));
+      } else {
+        p.xc_sig = nullptr;
+      }
+      p.efermi = q.efermi;
+      p.step_sigma = q.step_sigma;
+      p.eta = q.eta;
+    }
+    host_table_[i] = p;
+  }
+  RIGW_CUDA_TRY(cudaMemcpyAsync(probs_dev_, host_table_.data(), sizeof(ProbDev) * host_table_.size(),
+                                cudaMemcpyHostToDevice, s));
+  return Status::ok();
+}
+
+Status Plan::stage_sigma_calc(int i, const double* sc, cudaStream_t s) {
+  ProbDev& p = probs_[i].dev;
+  RIGW_CUDA_TRY(cudaMemcpyAsync(p.sigma_calc, sc, sizeof(double) * 2 * p.nsig * p.nc, cudaMemcpyDefault, s));
+  return Status::ok();
+}
+
+Status Plan::launch(cudaStream_t s) {
+  RIGW_CUDA_TRY(cudaMemsetAsync(err_dev_, 0, sizeof(int), s));
+  if (ctx_->use_graphs) {
+    if (!exec_) {
+      RIGW_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      record(s);
+      cudaGraph_t g = nullptr;
+      cudaError_t e = cudaStreamEndCapture(s, &g);
+      if (e != cudaSuccess)
+        return Status::fail(RIGW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
+      graph_ = g;
+      RIGW_CUDA_TRY(cudaGraphInstantiate(&exec_, graph_, 0));
+    }
+    RIGW_CUDA_TRY(cudaEventRecord(ev0_, s));
+    RIGW_CUDA_TRY(cudaGraphLaunch(exec_, s));
+    RIGW_CUDA_TRY(cudaEventRecord(ev1_, s));
+    replayed_ = true;
+  } else {
+    replayed_ = false;
+    RIGW_CUDA_TRY(cudaEventRecord(ev0_, s));
+    record(s);
+    RIGW_CUDA_TRY(cudaGetLastError());
+    RIGW_CUDA_TRY(cudaEventRecord(ev1_, s));
+  }
+  return Status::ok();
+}
+
+Status Plan::check_errors(cudaStream_t s) {
+  int err = 0;
+  RIGW_CUDA_TRY(cudaMemcpyAsync(&err, err_dev_, sizeof(int), cudaMemcpyDeviceToHost, s));
+  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  RIGW_CUDA_TRY(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+  for (int k = 0; k < 4; ++k) RIGW_CUDA_TRY(cudaEventElapsedTime(&stage_ms_[k], stage_ev_[k], stage_ev_[k + 1]));
+  if (err & kErrNotSPD) return Status::fail(RIGW_ERR_NOT_SPD, "eps(iw) is not positive definite");
+  if (err & (kErrNonFinite | kErrPade))
+    return Status::fail(RIGW_ERR_NUMERIC, "non-finite QP energy or singular Pade recursion (flags %d)", err);
+  return Status::ok();
+}
+
+Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStream_t s) {
+  for (size_t i = 0; i < probs_.size(); ++i) {
+    const ProbDev& p = probs_[i].dev;
+    rigw_result& r = res[i];
+    const int nreal = 2 * p.nsigma_half + 1;
+    if (p.out_energies) {
+      double en[2];
+      RIGW_CUDA_TRY(cudaMemcpyAsync(en, p.out_energies, sizeof(en), cudaMemcpyDeviceToHost, s));
+      RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+      r.erpa = en[0];
+      r.egw = en[1];
+    }
+    if (r.sigma_calc && p.sigma_calc && mode_ != kPlanQP)
+      RIGW_CUDA_TRY(cudaMemcpyAsync(r.sigma_calc, p.sigma_calc, sizeof(double) * 2 * p.nsig * p.nc,
+                                    cudaMemcpyDefault, s));
+    if (r.sigma && p.sigma_real)
+      RIGW_CUDA_TRY(
+          cudaMemcpyAsync(r.sigma, p.sigma_real, sizeof(double) * 2 * p.nsig * nreal, cudaMemcpyDefault, s));
+    if (p.qp) {
+      std::vector<double> q(4 * p.nsig);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(q.data(), p.qp, q.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
+      RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+      std::vector<double> occ(p.nsig, 0.0);
+      if (probs[i].occ_sig)
+        RIGW_CUDA_TRY(cudaMemcpy(occ.data(), probs[i].occ_sig, p.nsig * sizeof(double), cudaMemcpyDefault));
+      std::vector<double> g(p.nsig), z(p.nsig), zz(p.nsig);
+      double eh = -HUGE_VAL, el = HUGE_VAL;
+      for (int k = 0; k < p.nsig; ++k) {
+        g[k] = q[4 * k];
+        z[k] = q[4 * k + 1];
+        zz[k] = q[4 * k + 2];
+        // output_homolumo, src/m_hamiltonian_tools.f90:564-612 (spin_fact = 2)
+        if (occ[k] / 2.0 > 1.0e-5) eh = std::max(eh, g[k]);
+        if (occ[k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[k]);
+      }
+      r.ehomo = eh;
+      r.elumo = el;
+      if (r.energy_qp_g) RIGW_CUDA_TRY(cudaMemcpy(r.energy_qp_g, g.data(), g.size() * 8, cudaMemcpyDefault));
+      if (r.energy_qp_z) RIGW_CUDA_TRY(cudaMemcpy(r.energy_qp_z, z.data(), z.size() * 8, cudaMemcpyDefault));
+      if (r.zz) RIGW_CUDA_TRY(cudaMemcpy(r.zz, zz.data(), zz.size() * 8, cudaMemcpyDefault));
+    }
+    r.device_ms = last_ms_;
+  }
+  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  return Status::ok();
+}
+
+}  // namespace rigw

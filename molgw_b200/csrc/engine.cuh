@@ -1,0 +1,184 @@
+// Host-side engine: device memory accounting, batch plans (problem table +
+// work lists + launch sequence), CUDA-graph replay.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdarg>
+#include <cstdio>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/rigw.h"
+#include "kernels.cuh"
+
+namespace rigw {
+
+struct Status {
+  int code = RIGW_OK;
+  std::string msg;
+  static Status ok() { return {}; }
+  static Status fail(int c, const char* fmt, ...) {
+    Status s;
+    s.code = c;
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    s.msg = buf;
+    return s;
+  }
+  bool good() const { return code == RIGW_OK; }
+};
+
+#define RIGW_CUDA_TRY(expr)                                                                      \
+  do {                                                                                           \
+    cudaError_t e__ = (expr);                                                                    \
+    if (e__ != cudaSuccess)                                                                      \
+      return ::rigw::Status::fail(RIGW_ERR_CUDA, "%s failed: %s (%s:%d)", #expr,                 \
+                                  cudaGetErrorString(e__), __FILE__, __LINE__);                  \
+  } while (0)
+
+#define RIGW_TRY(expr)             \
+  do {                             \
+    ::rigw::Status s__ = (expr);   \
+    if (!s__.good()) return s__;   \
+  } while (0)
+
+class Context;
+
+// Device allocation with named accounting against the context's HBM budget
+// (the pattern of MOLGW's clean_allocate, src/m_memory.f90:16-92).
+class DeviceBuffer {
+ public:
+  DeviceBuffer() = default;
+  ~DeviceBuffer();
+  DeviceBuffer(const DeviceBuffer&) = delete;
+  DeviceBuffer& operator=(const DeviceBuffer&) = delete;
+  Status allocate(Context* ctx, size_t bytes, const char* name);
+  void release();
+  char* data() const { return ptr_; }
+  size_t size() const { return bytes_; }
+
+ private:
+  Context* ctx_ = nullptr;
+  char* ptr_ = nullptr;
+  size_t bytes_ = 0;
+};
+
+// Shapes of one problem of a plan (derived from rigw_problem).
+struct Shape {
+  int naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision;
+  bool operator<(const Shape& o) const;
+};
+
+enum PlanMode : int {
+  kPlanFused = 0,      // chi0 -> eps -> factor -> [I | M_sigma] solve -> Sigma -> QP
+  kPlanPolar = 1,      // chi0 -> eps -> factor -> I solve -> energies (factors stay resident)
+  kPlanSigma = 2,      // M_sigma solve with resident factors -> Sigma
+  kPlanQP = 3,         // continuation + QP from given sigma_calc
+};
+
+struct PlanProblem {
+  Shape sh;
+  ProbDev dev;                 // device descriptor (input pointers patched per call)
+  size_t off_in_m = 0, off_in_eocc = 0, off_in_evirt = 0, off_in_oocc = 0, off_in_ovirt = 0;
+  size_t off_in_omega = 0, off_in_weight = 0, off_in_msig = 0, off_in_ep = 0, off_in_esig = 0;
+  size_t off_in_xc = 0, off_in_zcalc = 0, off_out = 0, off_sigma_in = 0;
+};
+
+// A batch plan: all device memory, the problem table, the work lists and the
+// launch sequence of one group of problems.
+class Plan {
+ public:
+  Status build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
+               const std::vector<const ProbDev*>& factors);
+  // Copy inputs (host or device pointers) and run; results stay on the device.
+  Status stage_inputs(const rigw_problem* probs, cudaStream_t s);
+  Status stage_sigma_calc(int i, const double* sigma_calc_host, cudaStream_t s);
+  Status launch(cudaStream_t s);
+  Status fetch_results(const rigw_problem* probs, rigw_result* res, cudaStream_t s);
+  Status check_errors(cudaStream_t s);
+  float last_ms() const { return last_ms_; }
+  std::vector<PlanProblem>& problems() { return probs_; }
+  size_t bytes() const { return arena_.size(); }
+  PlanMode mode() const { return mode_; }
+  const std::vector<Shape>& shapes() const { return shapes_; }
+  ~Plan();
+
+  // launch statistics (kernels per launch sequence)
+  int kernel_launches() const { return n_launches_; }
+
+ private:
+  void record(cudaStream_t s);
+  Context* ctx_ = nullptr;
+  PlanMode mode_ = kPlanFused;
+  std::vector<Shape> shapes_;
+  std::vector<PlanProblem> probs_;
+  DeviceBuffer arena_;
+  DeviceBuffer lists_;
+  ProbDev* probs_dev_ = nullptr;
+  int* err_dev_ = nullptr;
+  // work lists (host copies + device offsets)
+  std::vector<WorkItem> wl_pack_, wl_rhs_, wl_mnorm_, wl_energy_, wl_vchiv_, wl_sigma_, wl_pade_;
+  std::vector<std::vector<WorkItem>> wl_diag_;
+  std::vector<GemmItem> gl_syrk_;
+  std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_;
+  struct Launch {
+    int kind;        // see Plan::record
+    size_t off;      // byte offset of the list in lists_
+    int count;
+    int arg;
+  };
+  std::vector<Launch> seq_;
+  cudaGraph_t graph_ = nullptr;
+  cudaGraphExec_t exec_ = nullptr;
+  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaEvent_t stage_ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  float last_ms_ = 0.0f;
+  float stage_ms_[4] = {0, 0, 0, 0};
+  bool replayed_ = false;
+
+ public:
+  const float* stage_ms() const { return stage_ms_; }
+  bool replayed() const { return replayed_; }
+
+ private:
+  int n_launches_ = 0;
+  std::vector<ProbDev> host_table_;
+};
+
+class Context {
+ public:
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  size_t budget = 0;
+  size_t in_use = 0, peak = 0;
+  std::string last_error;
+  std::mutex mu;
+  std::map<std::vector<Shape>, std::unique_ptr<Plan>> fused_cache;
+  bool use_graphs = true;
+  rigw_stats last_stats{};
+  Status init(int dev, size_t budget_bytes);
+  ~Context();
+};
+
+struct Wpol {
+  Context* ctx = nullptr;
+  std::unique_ptr<Plan> plan;     // the kPlanPolar plan that owns eps/U, winv and U^-T
+  Shape sh;
+};
+
+Status make_shape(const rigw_problem& p, Shape* sh);
+size_t footprint(const Shape& sh, PlanMode mode);
+void imag_grid(int n, double* omega, double* weight);
+Status wpol_chi(Context& c, const Wpol& w, double* chi);
+Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
+                      const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
+                      int nstate_min, int nstate_max, double* out);
+bool bf16x3_available();
+
+}  // namespace rigw

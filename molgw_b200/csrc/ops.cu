@@ -1,0 +1,167 @@
+// Stand-alone operations of the C ABI: explicit chi(iw) from resident factors
+// and the AO -> MO transform.
+#include <algorithm>
+#include <cstring>
+
+#include "engine.cuh"
+
+namespace rigw {
+
+namespace {
+inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
+
+Status run_gemm_items(Context& c, const std::vector<GemmItem>& items, bool wide) {
+  if (items.empty()) return Status::ok();
+  DeviceBuffer buf;
+  RIGW_TRY(buf.allocate(&c, items.size() * sizeof(GemmItem), "gemm items"));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(buf.data(), items.data(), items.size() * sizeof(GemmItem), cudaMemcpyHostToDevice,
+                                c.stream));
+  const GemmItem* d = reinterpret_cast<const GemmItem*>(buf.data());
+  if (wide) launch_dgemm_128x128(d, int(items.size()), c.stream);
+  else launch_dgemm_64x128(d, int(items.size()), c.stream);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  RIGW_CUDA_TRY(cudaStreamSynchronize(c.stream));
+  return Status::ok();
+}
+}  // namespace
+
+// chi(iw) = eps^-1 - 1 = (U^-T)^T (U^-T) - 1, from the I-part of the resident solve.
+Status wpol_chi(Context& c, const Wpol& w, double* chi) {
+  Plan& plan = *w.plan;
+  const ProbDev& p = plan.problems()[0].dev;
+  const int npad = p.npad, naux = p.naux;
+  DeviceBuffer out;
+  RIGW_TRY(out.allocate(&c, size_t(npad) * npad * sizeof(double), "chi"));
+  double* X = reinterpret_cast<double*>(out.data());
+  for (int iw = 0; iw < p.nomega; ++iw) {
+    const double* Y = p.rhs + size_t(iw) * npad * p.ldb;   // U^-T in columns [0, npad)
+    std::vector<GemmItem> items;
+    for (int i0 = 0; i0 < npad; i0 += 128)
+      for (int j0 = 0; j0 < npad; j0 += 128) {
+        GemmItem g{};
+        g.A = Y + i0;
+        g.lda = p.ldb;
+        g.B = Y + j0;
+        g.ldb = p.ldb;
+        g.C = X + size_t(i0) * npad + j0;
+        g.ldc = npad;
+        g.m = std::min(128, npad - i0);
+        g.n = std::min(128, npad - j0);
+        g.k = npad;
+        g.flags = kSubIdentity;
+        g.diag = i0 - j0;
+        g.alpha = 1.0;
+        items.push_back(g);
+      }
+    RIGW_TRY(run_gemm_items(c, items, true));
+    RIGW_CUDA_TRY(cudaMemcpy2D(chi + size_t(iw) * naux * naux, naux * sizeof(double), X, npad * sizeof(double),
+                               naux * sizeof(double), naux, cudaMemcpyDeviceToHost));
+  }
+  return Status::ok();
+}
+
+// out[n][m][P] = sum_{mu,nu} C[m][mu] C[n][nu] B(mu nu, P)  (src/m_eri_ao_mo.f90:416-582).
+Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
+                      const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
+                      int nstate_min, int nstate_max, double* out) {
+  if (nbf <= 0 || nstate <= 0 || npair <= 0 || naux <= 0 || !index_basis || !eri3 || !c_matrix || !out)
+    return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: invalid arguments");
+  if (mstate_min < 1 || mstate_max > nstate || mstate_min > mstate_max || nstate_min < 1 ||
+      nstate_max > nstate || nstate_min > nstate_max)
+    return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: state ranges outside [1, %d]", nstate);
+  for (int q = 0; q < 2 * npair; ++q)
+    if (index_basis[q] < 1 || index_basis[q] > nbf)
+      return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: index_basis entry %d out of [1, %d]", q, nbf);
+  const int mc = mstate_max - mstate_min + 1, nc = nstate_max - nstate_min + 1;
+  const int mcp = round_up(mc, 2), ncp = round_up(nc, 2);
+  // C^T restricted to the two ranges: ctm[mu][m], ctn[nu][n] (m, n contiguous, even widths)
+  std::vector<double> ctm(size_t(nbf) * mcp, 0.0), ctn(size_t(nbf) * ncp, 0.0);
+  for (int mu = 0; mu < nbf; ++mu) {
+    for (int m = 0; m < mc; ++m) ctm[size_t(mu) * mcp + m] = c_matrix[size_t(mstate_min - 1 + m) * nbf + mu];
+    for (int n = 0; n < nc; ++n) ctn[size_t(mu) * ncp + n] = c_matrix[size_t(nstate_min - 1 + n) * nbf + mu];
+  }
+  // auxiliary chunk so that the unpacked (nu, mu, P) block stays below ~2 GB
+  const size_t per_aux = size_t(nbf) * nbf * sizeof(double);
+  int pc = int(std::max<size_t>(8, (size_t(2) << 30) / per_aux / 8 * 8));
+  pc = std::min(pc, round_up(naux, 8));
+  const int pcp = round_up(pc, 8);
+  DeviceBuffer b_ctm, b_ctn, b_idx, b_eri, b_full, b_t, b_out, b_item;
+  RIGW_TRY(b_ctm.allocate(&c, ctm.size() * 8, "aomo ctm"));
+  RIGW_TRY(b_ctn.allocate(&c, ctn.size() * 8, "aomo ctn"));
+  RIGW_TRY(b_idx.allocate(&c, size_t(2) * npair * sizeof(int), "aomo index"));
+  RIGW_TRY(b_eri.allocate(&c, size_t(pc) * npair * 8, "aomo eri3 chunk"));
+  RIGW_TRY(b_full.allocate(&c, size_t(nbf) * nbf * pcp * 8, "aomo unpacked"));
+  RIGW_TRY(b_t.allocate(&c, size_t(ncp) * nbf * pcp * 8, "aomo half"));
+  RIGW_TRY(b_out.allocate(&c, size_t(ncp) * mcp * pcp * 8, "aomo out chunk"));
+  RIGW_TRY(b_item.allocate(&c, sizeof(AomoUnpackItem), "aomo item"));
+  cudaStream_t s = c.stream;
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_ctm.data(), ctm.data(), ctm.size() * 8, cudaMemcpyHostToDevice, s));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_ctn.data(), ctn.data(), ctn.size() * 8, cudaMemcpyHostToDevice, s));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_idx.data(), index_basis, size_t(2) * npair * sizeof(int), cudaMemcpyHostToDevice, s));
+  double* dctm = reinterpret_cast<double*>(b_ctm.data());
+  double* dctn = reinterpret_cast<double*>(b_ctn.data());
+  double* dfull = reinterpret_cast<double*>(b_full.data());
+  double* dt = reinterpret_cast<double*>(b_t.data());
+  double* dout = reinterpret_cast<double*>(b_out.data());
+  for (int p0 = 0; p0 < naux; p0 += pc) {
+    const int cnt = std::min(pc, naux - p0);
+    RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), eri3 + size_t(p0) * npair, size_t(cnt) * npair * 8,
+                                  cudaMemcpyHostToDevice, s));
+    RIGW_CUDA_TRY(cudaMemsetAsync(dfull, 0, size_t(nbf) * nbf * pcp * 8, s));
+    AomoUnpackItem it{reinterpret_cast<const double*>(b_eri.data()), reinterpret_cast<const int*>(b_idx.data()),
+                      dfull, cnt, pcp, npair, nbf, 0};
+    RIGW_CUDA_TRY(cudaMemcpyAsync(b_item.data(), &it, sizeof(it), cudaMemcpyHostToDevice, s));
+    dim3 grid((npair + 31) / 32, (cnt + 31) / 32);
+    aomo_unpack_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const AomoUnpackItem*>(b_item.data()));
+    RIGW_CUDA_TRY(cudaGetLastError());
+    // step 1: T[n][(mu,P)] = sum_nu ctn[nu][n] B[nu][(mu,P)]
+    std::vector<GemmItem> g1;
+    const int wide = nbf * pcp;
+    for (int i0 = 0; i0 < ncp; i0 += 128)
+      for (int j0 = 0; j0 < wide; j0 += 128) {
+        GemmItem g{};
+        g.A = dctn + i0;
+        g.lda = ncp;
+        g.B = dfull + j0;
+        g.ldb = wide;
+        g.C = dt + size_t(i0) * wide + j0;
+        g.ldc = wide;
+        g.m = std::min(128, ncp - i0);
+        g.n = std::min(128, wide - j0);
+        g.k = nbf;
+        g.alpha = 1.0;
+        g1.push_back(g);
+      }
+    RIGW_TRY(run_gemm_items(c, g1, true));
+    // step 2: O[n][m][P] = sum_mu ctm[mu][m] T[n][mu][P]
+    std::vector<GemmItem> g2;
+    for (int n = 0; n < nc; ++n)
+      for (int i0 = 0; i0 < mcp; i0 += 128)
+        for (int j0 = 0; j0 < pcp; j0 += 128) {
+          GemmItem g{};
+          g.A = dctm + i0;
+          g.lda = mcp;
+          g.B = dt + size_t(n) * wide + j0;
+          g.ldb = pcp;
+          g.C = dout + (size_t(n) * mcp + i0) * pcp + j0;
+          g.ldc = pcp;
+          g.m = std::min(128, mcp - i0);
+          g.n = std::min(128, pcp - j0);
+          g.k = nbf;
+          g.alpha = 1.0;
+          g2.push_back(g);
+        }
+    RIGW_TRY(run_gemm_items(c, g2, true));
+    // out[n][m][p0 : p0+cnt]
+    for (int n = 0; n < nc; ++n)
+      RIGW_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t(n) * mc) * naux + p0, size_t(naux) * 8,
+                                      dout + size_t(n) * mcp * pcp, size_t(pcp) * 8, size_t(cnt) * 8, mc,
+                                      cudaMemcpyDeviceToHost, s));
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  return Status::ok();
+}
+
+bool bf16x3_available() { return false; }
+
+}  // namespace rigw

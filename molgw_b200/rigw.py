@@ -1,0 +1,330 @@
+"""Python host mirror of MOLGW's imaginary-axis GW interface over librigw (ctypes).
+
+The names follow the reference routines the library replaces:
+
+* ``polarizability_grid_scalapack``  src/m_gw_selfenergy_grid.f90:33-209
+* ``gw_selfenergy_imag_scalapack``   src/m_gw_selfenergy_grid.f90:213-338
+* ``calculate_eri_3center_mo``       src/m_eri_ao_mo.f90:416-582
+* ``qp_solve`` (se_pade_fit + find_qp_energy_linearization/graphical)
+                                     src/m_selfenergy_tools.f90:202-420, 965-1033
+* ``g0w0`` / ``g0w0_batch``          selfenergy_evaluation for imaginary_axis_pade,
+                                     src/m_selfenergy_evaluation.f90:214-246, 587-611
+
+Errors: the library returns a status and never aborts; this module raises
+``RigwError`` with the library's message, the analogue of MOLGW's ``die()``
+(src/m_warning.f90:78-89).  There is no CPU fallback: importing this module
+without the built library, or calling it without a CUDA device, raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().parent / "librigw.so"
+
+RIGW_FP64 = 0
+RIGW_BF16X3 = 1
+RIGW_PADE = 0
+RIGW_HOMOLUMO = 1
+RIGW_PROBLEM_DEVICE_POINTERS = 1
+STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_NOT_SPD", 5: "ERR_NUMERIC",
+                6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED"}
+
+_dp = C.POINTER(C.c_double)
+
+
+class RigwError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"rigw: {STATUS_NAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class Problem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nocc", C.c_int), ("nvirt", C.c_int), ("nomega", C.c_int),
+        ("omega", _dp), ("weight", _dp), ("m_ia", _dp), ("e_occ", _dp), ("e_virt", _dp),
+        ("occ_occ", _dp), ("occ_virt", _dp),
+        ("nstate_p", C.c_int), ("nsig", C.c_int),
+        ("m_pm", _dp), ("e_p", _dp), ("e_sig", _dp), ("occ_sig", _dp), ("exchange_m_vxc", _dp),
+        ("technique", C.c_int), ("nomega_sigma_calc", C.c_int), ("step_sigma_calc", C.c_double),
+        ("omega_calc", _dp), ("nomega_sigma", C.c_int), ("step_sigma", C.c_double), ("eta", C.c_double),
+        ("efermi", C.c_double), ("precision", C.c_int), ("flags", C.c_int),
+    ]
+
+
+class Result(C.Structure):
+    _fields_ = [
+        ("erpa", C.c_double), ("egw", C.c_double),
+        ("sigma_calc", _dp), ("sigma", _dp), ("energy_qp_g", _dp), ("energy_qp_z", _dp), ("zz", _dp),
+        ("ehomo", C.c_double), ("elumo", C.c_double), ("device_ms", C.c_double),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("stage_ms", C.c_double * 4), ("total_ms", C.c_double), ("kernel_launches", C.c_int),
+        ("graph_replayed", C.c_int), ("device_bytes_in_use", C.c_size_t), ("device_bytes_peak", C.c_size_t),
+    ]
+
+
+def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
+    path = Path(path)
+    if not path.exists():
+        raise RigwError(7, f"{path} is not built (run python -m molgw_b200.build)")
+    lib = C.CDLL(str(path))
+    lib.rigw_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_size_t]
+    lib.rigw_destroy.argtypes = [C.c_void_p]
+    lib.rigw_last_error.argtypes = [C.c_void_p]
+    lib.rigw_last_error.restype = C.c_char_p
+    lib.rigw_version.restype = C.c_int
+    lib.rigw_last_stats.argtypes = [C.c_void_p, C.POINTER(Stats)]
+    lib.rigw_footprint_bytes.argtypes = [C.c_int] * 7
+    lib.rigw_footprint_bytes.restype = C.c_size_t
+    lib.rigw_imag_grid.argtypes = [C.c_int, _dp, _dp]
+    lib.rigw_eri_3center_mo.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                        _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+    lib.rigw_polarizability_imag.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, _dp, C.POINTER(C.c_void_p)]
+    lib.rigw_wpol_chi.argtypes = [C.c_void_p, C.c_void_p, _dp]
+    lib.rigw_gw_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
+    lib.rigw_wpol_release.argtypes = [C.c_void_p, C.c_void_p]
+    lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
+    lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
+    lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
+    return lib
+
+
+_LIB: C.CDLL | None = None
+
+
+def lib() -> C.CDLL:
+    global _LIB
+    if _LIB is None:
+        _LIB = load_library()
+    return _LIB
+
+
+def _ptr(a) -> _dp:
+    """Pointer to a C-contiguous float64 numpy array, or to a CUDA tensor (data_ptr)."""
+    if a is None:
+        return _dp()
+    if hasattr(a, "data_ptr"):
+        return C.cast(C.c_void_p(a.data_ptr()), _dp)
+    if not (a.flags["C_CONTIGUOUS"] and a.dtype == np.float64):
+        raise ValueError("arrays passed to librigw must be C-contiguous float64")
+    return a.ctypes.data_as(_dp)
+
+
+def imag_grid(nomega: int):
+    """sf_init IMAGINARY_QUAD grid (omega_k imaginary parts, weights)."""
+    om = np.zeros(nomega)
+    wt = np.zeros(nomega)
+    rc = lib().rigw_imag_grid(nomega, _ptr(om), _ptr(wt))
+    if rc:
+        raise RigwError(rc, "rigw_imag_grid")
+    return om, wt
+
+
+@dataclass
+class G0W0Output:
+    erpa: float
+    egw: float
+    sigma_calc: np.ndarray      # [nsig, nc] complex
+    sigma: np.ndarray           # [nsig, nreal] complex
+    energy_qp_g: np.ndarray
+    energy_qp_z: np.ndarray
+    zz: np.ndarray
+    ehomo: float
+    elumo: float
+    device_ms: float
+
+
+class Engine:
+    """One library context on one CUDA device."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self._lib = lib()
+        h = C.c_void_p()
+        rc = self._lib.rigw_create(C.byref(h), device, hbm_budget_bytes)
+        if rc:
+            raise RigwError(rc, f"rigw_create(device={device})")
+        self._h = h
+        self._keep = []
+
+    def close(self):
+        if self._h:
+            self._lib.rigw_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def last_stats(self) -> dict:
+        st = Stats()
+        self._check(self._lib.rigw_last_stats(self._h, C.byref(st)), "rigw_last_stats")
+        return dict(stage_ms=list(st.stage_ms), total_ms=st.total_ms, kernel_launches=st.kernel_launches,
+                    graph_replayed=bool(st.graph_replayed), device_bytes_in_use=st.device_bytes_in_use,
+                    device_bytes_peak=st.device_bytes_peak)
+
+    def _check(self, rc: int, what: str):
+        if rc:
+            raise RigwError(rc, f"{what}: {self._lib.rigw_last_error(self._h).decode()}")
+
+    # ---------------------------------------------------------------- problems
+    def make_problem(self, inst, precision: int = RIGW_FP64, device_arrays: dict | None = None,
+                     technique: int = RIGW_PADE) -> tuple[Problem, list]:
+        """Problem descriptor for a ``molgw_b200.synth.GWInstance``-like object.
+
+        ``device_arrays`` maps field names to CUDA tensors that replace the host
+        arrays (all W/Sigma inputs must then be device tensors)."""
+        nocc, nvirt = inst.nocc, inst.nvirt
+        e = np.ascontiguousarray(inst.energy, dtype=np.float64)
+        occ = np.ascontiguousarray(inst.occupation, dtype=np.float64)
+        nsemin, nsemax = inst.nsemin, inst.nsemax
+        host = {
+            "m_ia": np.ascontiguousarray(inst.m_ia), "e_occ": e[:nocc].copy(), "e_virt": e[nocc:nocc + nvirt].copy(),
+            "occ_occ": occ[:nocc].copy(), "occ_virt": occ[nocc:nocc + nvirt].copy(),
+            "m_pm": np.ascontiguousarray(inst.m_sigma), "e_p": e.copy(),
+            "e_sig": e[nsemin - 1:nsemax].copy(),
+        }
+        occ_sig = occ[nsemin - 1:nsemax].copy()
+        arrs = dict(host)
+        flags = 0
+        if device_arrays:
+            arrs.update(device_arrays)
+            flags = RIGW_PROBLEM_DEVICE_POINTERS
+            occ_sig = device_arrays.get("occ_sig", occ_sig)
+        efermi = 0.5 * (e[nocc - 1] + e[nocc])
+        p = Problem()
+        p.naux = inst.naux
+        p.nocc, p.nvirt = nocc, nvirt
+        p.nomega = inst.nomega
+        for k in ("m_ia", "e_occ", "e_virt", "occ_occ", "occ_virt", "m_pm", "e_p", "e_sig"):
+            setattr(p, k, _ptr(arrs[k]))
+        p.occ_sig = _ptr(occ_sig)
+        p.nstate_p = e.shape[0]
+        p.nsig = nsemax - nsemin + 1
+        p.technique = technique
+        p.nomega_sigma_calc = inst.nomega_sigma_calc
+        p.step_sigma_calc = inst.step_sigma_calc
+        p.nomega_sigma = inst.nomega_sigma
+        p.step_sigma = inst.step_sigma
+        p.eta = inst.eta
+        p.efermi = efermi
+        p.precision = precision
+        p.flags = flags
+        keep = [arrs, occ_sig]
+        return p, keep
+
+    def _alloc_result(self, p: Problem):
+        nreal = 2 * (p.nomega_sigma // 2) + 1
+        bufs = {
+            "sigma_calc": np.zeros((p.nsig, p.nomega_sigma_calc, 2)),
+            "sigma": np.zeros((p.nsig, nreal, 2)),
+            "energy_qp_g": np.zeros(p.nsig), "energy_qp_z": np.zeros(p.nsig), "zz": np.zeros(p.nsig),
+        }
+        r = Result()
+        for k, v in bufs.items():
+            setattr(r, k, _ptr(v))
+        return r, bufs
+
+    @staticmethod
+    def _output(r: Result, bufs) -> G0W0Output:
+        sc = bufs["sigma_calc"]
+        sg = bufs["sigma"]
+        return G0W0Output(r.erpa, r.egw, sc[..., 0] + 1j * sc[..., 1], sg[..., 0] + 1j * sg[..., 1],
+                          bufs["energy_qp_g"].copy(), bufs["energy_qp_z"].copy(), bufs["zz"].copy(),
+                          r.ehomo, r.elumo, r.device_ms)
+
+    # ---------------------------------------------------------------- fused
+    def g0w0_batch(self, insts, precision: int = RIGW_FP64, device_arrays=None) -> list[G0W0Output]:
+        n = len(insts)
+        probs = (Problem * n)()
+        ress = (Result * n)()
+        keep, bufs = [], []
+        for i, inst in enumerate(insts):
+            p, k = self.make_problem(inst, precision, device_arrays[i] if device_arrays else None)
+            probs[i] = p
+            keep.append(k)
+            r, b = self._alloc_result(p)
+            ress[i] = r
+            bufs.append(b)
+        self._check(self._lib.rigw_g0w0_batch(self._h, n, probs, ress), "rigw_g0w0_batch")
+        return [self._output(ress[i], bufs[i]) for i in range(n)]
+
+    def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None) -> G0W0Output:
+        return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None)[0]
+
+    # ---------------------------------------------------------------- drop-in pieces
+    def polarizability_grid_scalapack(self, inst, precision: int = RIGW_FP64):
+        """Returns (erpa, egw, wpol handle)."""
+        p, keep = self.make_problem(inst, precision)
+        erpa, egw = C.c_double(), C.c_double()
+        w = C.c_void_p()
+        self._check(self._lib.rigw_polarizability_imag(self._h, C.byref(p), C.byref(erpa), C.byref(egw),
+                                                       C.byref(w)), "rigw_polarizability_imag")
+        return erpa.value, egw.value, WPol(self, w, inst.naux, inst.nomega)
+
+    def gw_selfenergy_imag_scalapack(self, wpol: "WPol", inst) -> np.ndarray:
+        p, keep = self.make_problem(inst)
+        r, bufs = self._alloc_result(p)
+        self._check(self._lib.rigw_gw_selfenergy_imag(self._h, wpol.handle, C.byref(p), C.byref(r)),
+                    "rigw_gw_selfenergy_imag")
+        sc = bufs["sigma_calc"]
+        return sc[..., 0] + 1j * sc[..., 1]
+
+    def qp_solve(self, inst, sigma_calc: np.ndarray, technique: int = RIGW_PADE, omega_calc=None) -> G0W0Output:
+        p, keep = self.make_problem(inst, technique=technique)
+        if omega_calc is not None:
+            oc = np.ascontiguousarray(np.stack([omega_calc.real, omega_calc.imag], -1))
+            p.omega_calc = _ptr(oc)
+            keep.append(oc)
+        sc = np.ascontiguousarray(np.stack([sigma_calc.real, sigma_calc.imag], -1))
+        r, bufs = self._alloc_result(p)
+        self._check(self._lib.rigw_qp_solve(self._h, C.byref(p), _ptr(sc), C.byref(r)), "rigw_qp_solve")
+        out = self._output(r, bufs)
+        out.sigma_calc = sigma_calc
+        return out
+
+    def calculate_eri_3center_mo(self, eri3: np.ndarray, index_basis: np.ndarray, c_matrix: np.ndarray,
+                                 m_min: int, m_max: int, n_min: int, n_max: int) -> np.ndarray:
+        naux, npair = eri3.shape
+        nstate, nbf = c_matrix.shape
+        idx = np.ascontiguousarray(index_basis, dtype=np.int32)
+        out = np.zeros((n_max - n_min + 1, m_max - m_min + 1, naux))
+        self._check(self._lib.rigw_eri_3center_mo(
+            self._h, nbf, nstate, npair, naux, idx.ctypes.data_as(C.POINTER(C.c_int)),
+            _ptr(np.ascontiguousarray(eri3)), _ptr(np.ascontiguousarray(c_matrix)), m_min, m_max, n_min, n_max,
+            _ptr(out)), "rigw_eri_3center_mo")
+        return out
+
+
+class WPol:
+    """Resident screened interaction (the device-side wpol of the reference)."""
+
+    def __init__(self, eng: Engine, handle: C.c_void_p, naux: int, nomega: int):
+        self.eng = eng
+        self.handle = handle
+        self.naux = naux
+        self.nomega = nomega
+
+    def chi(self) -> np.ndarray:
+        out = np.zeros((self.nomega, self.naux, self.naux))
+        self.eng._check(self.eng._lib.rigw_wpol_chi(self.eng._h, self.handle, _ptr(out)), "rigw_wpol_chi")
+        return out
+
+    def release(self):
+        if self.handle:
+            self.eng._lib.rigw_wpol_release(self.eng._h, self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.release()
+        except Exception:
+            pass

@@ -1,0 +1,140 @@
+"""Seeded synthetic RI-GW instances with the shapes and value distributions of the
+benchmark workloads (no public dataset exists for this path).
+
+One instance is a closed-shell (nspin=1) G0W0@HF problem on the imaginary axis:
+
+* occupied energies ~ U[-30, -8] eV, virtual energies ~ U[0.5, 40] eV, sorted,
+  stored in Hartree (eV / 27.21138505, src/m_definitions.f90:43);
+* occupation 2 for occupied states, 0 for virtual ones;
+* the W-window tensor M[P, a, i] ~ N(0, s^2), where s = sqrt(0.8 / lmax) and
+  lmax is the largest eigenvalue of -chi0(i0) = sum_t 4/de_t M_t M_t^T built
+  with the unscaled N(0,1) draw, so that eig(eps(i0)) lies in [1, 1.8];
+* the Sigma tensor M[P, p, m] for p over all states and m in {HOMO, LUMO}
+  (S = 2): its occupied-virtual entries coincide with the W tensor (M is
+  symmetric in its two state indices), the other entries are fresh draws from
+  the same N(0, s^2);
+* Sigma_x - V_xc = 0 (G0W0@HF), Sigma grid of tests/inputs/h2o_gw_pade.in:
+  nomega_sigma_calc=50, step_sigma_calc=0.075, nomega_sigma=101,
+  step_sigma=0.025, eta=0.01 Ha.
+
+State indices follow MOLGW: states 1..nocc are occupied, HOMO = nocc,
+LUMO = nocc+1; the Sigma range is nsemin..nsemax = HOMO..LUMO.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+HA_EV = 27.21138505
+
+
+@dataclass
+class GWInstance:
+    """One G0W0 problem in the library's host layout (C order, float64)."""
+    nocc: int
+    nvirt: int
+    naux: int
+    nomega: int
+    energy: np.ndarray        # [nstate] Ha, sorted occupied then virtual
+    occupation: np.ndarray    # [nstate]
+    m_ia: np.ndarray          # [nocc, nvirt, naux]   (Fortran eri_3center_mo(P, a, i))
+    m_sigma: np.ndarray       # [nsig, nstate, naux]  (Fortran eri_3center_mo(P, p, m))
+    nsemin: int = 0           # 1-based Sigma state range
+    nsemax: int = 0
+    nomega_sigma_calc: int = 50
+    step_sigma_calc: float = 0.075
+    nomega_sigma: int = 101
+    step_sigma: float = 0.025
+    eta: float = 0.01
+    seed: int = 0
+
+    @property
+    def nstate(self) -> int:
+        return self.nocc + self.nvirt
+
+    @property
+    def nsig(self) -> int:
+        return self.nsemax - self.nsemin + 1
+
+
+def _energies(rng: np.random.Generator, nocc: int, nvirt: int) -> np.ndarray:
+    e_occ = np.sort(rng.uniform(-30.0, -8.0, nocc))
+    e_virt = np.sort(rng.uniform(0.5, 40.0, nvirt))
+    return np.concatenate([e_occ, e_virt]) / HA_EV
+
+
+def _lambda_max(m_t: np.ndarray, de: np.ndarray) -> float:
+    """Largest eigenvalue of sum_t (4/de_t) m_t m_t^T, m_t rows of ``m_t``."""
+    w = np.sqrt(4.0 / de)
+    a = m_t * w[:, None]                    # [Nia, naux]
+    if a.shape[1] <= 2500:
+        g = a.T @ a
+        return float(np.linalg.eigvalsh(g)[-1])
+    # large instances: power iteration on a^T a (converges to ~1e-10 quickly
+    # because the top of the spectrum of a Wishart-like matrix is separated)
+    v = np.ones(a.shape[1]) / np.sqrt(a.shape[1])
+    lam = 0.0
+    for _ in range(300):
+        u = a.T @ (a @ v)
+        lam_new = float(np.linalg.norm(u))
+        v = u / lam_new
+        if abs(lam_new - lam) < 1e-12 * lam_new:
+            break
+        lam = lam_new
+    return lam_new
+
+
+def make_instance(nocc: int, nvirt: int, naux: int, nomega: int, seed: int,
+                  with_sigma: bool = True) -> GWInstance:
+    """Build one seeded instance (numpy Generator(PCG64(seed)))."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    energy = _energies(rng, nocc, nvirt)
+    occupation = np.concatenate([np.full(nocc, 2.0), np.zeros(nvirt)])
+    m_raw = rng.standard_normal((nocc, nvirt, naux))
+    de = (energy[nocc:][None, :] - energy[:nocc][:, None]).reshape(-1)
+    lmax = _lambda_max(m_raw.reshape(-1, naux), de)
+    s = np.sqrt(0.8 / lmax)
+    m_ia = m_raw * s
+    nstate = nocc + nvirt
+    homo, lumo = nocc, nocc + 1                    # 1-based
+    if with_sigma:
+        m_sigma = np.empty((2, nstate, naux))
+        # column m = HOMO: p occupied -> fresh, p virtual -> M[P, a, HOMO]
+        m_sigma[0, :nocc] = rng.standard_normal((nocc, naux)) * s
+        m_sigma[0, nocc:] = m_ia[homo - 1]
+        # column m = LUMO: p occupied -> M[P, LUMO, i], p virtual -> fresh
+        m_sigma[1, :nocc] = m_ia[:, lumo - nocc - 1]
+        m_sigma[1, nocc:] = rng.standard_normal((nvirt, naux)) * s
+    else:
+        m_sigma = np.zeros((0, nstate, naux))
+    return GWInstance(nocc=nocc, nvirt=nvirt, naux=naux, nomega=nomega, energy=energy,
+                      occupation=occupation, m_ia=m_ia, m_sigma=m_sigma,
+                      nsemin=homo, nsemax=lumo, seed=seed)
+
+
+# Workloads of the benchmark table --------------------------------------------
+def single_instance_840(seed: int = 2) -> GWInstance:
+    """Nocc=21, Nvirt=207, Naux=840, 32 imaginary frequencies."""
+    return make_instance(21, 207, 840, 32, seed)
+
+
+def large_instance_4000(seed: int = 3) -> GWInstance:
+    """Nocc=100, Nvirt=1100, Naux=4000, 48 imaginary frequencies."""
+    return make_instance(100, 1100, 4000, 48, seed)
+
+
+def batch_sizes(count: int = 256, base_seed: int = 4):
+    """Ragged molecule sizes: Nocc ~ U{5..60}, Nvirt = round(Nocc*U[8,10]),
+    Naux = 4*(Nocc+Nvirt), 32 frequencies; molecule k uses seed base_seed+k."""
+    out = []
+    for k in range(count):
+        rng = np.random.Generator(np.random.PCG64(base_seed + k))
+        nocc = int(rng.integers(5, 61))
+        nvirt = int(round(nocc * rng.uniform(8.0, 10.0)))
+        out.append((nocc, nvirt, 4 * (nocc + nvirt), 32, base_seed + k))
+    return out
+
+
+def batch_instances(count: int = 256, base_seed: int = 4):
+    return [make_instance(no, nv, na, nw, sd) for (no, nv, na, nw, sd) in batch_sizes(count, base_seed)]

@@ -1,0 +1,563 @@
+"""CPU restatement of MOLGW's imaginary-frequency RI-GW path (test infrastructure).
+
+This module is the ORACLE: only the test suite, ``__graft_entry__.smoke()`` and
+the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` import it, and
+only as the checker or as the timed CPU baseline.  The product path (the CUDA
+library under ``molgw_b200/csrc``) never calls into it.
+
+Every function follows a routine of MOLGW 3.4 statement by statement and issues
+the same BLAS/LAPACK call sequence (through SciPy's bundled OpenBLAS):
+
+* ``coeffs_gausslegint``      src/m_numerical_tools.f90:35-82
+* ``imaginary_quad_grid``     src/m_spectral_function.f90:286-306 (alpha=1, beta=2)
+* ``transition_table``        src/m_spectral_function.f90:239-266, 359-378
+* ``calculate_eri_3center_mo`` src/m_eri_ao_mo.f90:416-582
+* ``polarizability_grid``     src/m_gw_selfenergy_grid.f90:33-209
+                              (DSYRK('L','N') -> negate -> symmetrize -> 1-chi0 ->
+                               DSYEV('N') -> LU inverse -> DGEMM)
+* ``gw_selfenergy_imag``      src/m_gw_selfenergy_grid.f90:213-338
+* ``selfenergy_set_state_range`` src/m_selfenergy_tools.f90:67-122
+* ``se_init_imaginary_axis``  src/m_selfenergy_tools.f90:557-699
+* ``pade`` / ``calculate_pade_a`` src/m_numerical_tools.f90:86-146
+* ``se_pade_fit``             src/m_selfenergy_tools.f90:965-999
+* ``self_energy_polynomial``  src/m_selfenergy_tools.f90:1005-1033
+* ``find_qp_energy_linearization`` src/m_selfenergy_tools.f90:202-249
+* ``find_qp_energy_graphical`` / ``find_fixed_point`` src/m_selfenergy_tools.f90:253-420
+* ``output_homolumo``         src/m_hamiltonian_tools.f90:564-612
+
+Pinning: the reference's own known answer that needs no Gaussian integrals is
+the analytic RPA correlation energy of bulk LiH from the shipped CC4S tensor
+(tests/inputs/testsuite:1206-1207, -0.1152301335 Ha, tol 1e-7).  The analytic
+RPA of this module reproduces it to 1e-7, and the imaginary-axis RPA of
+``polarizability_grid`` converges to it with the number of frequencies (see
+tests/test_oracle.py).  The H2O GW values of the reference suite need an SCF with
+Gaussian integrals and are not reproducible here.
+
+Units: Hartree.  Arrays are numpy, with the Fortran index order kept in the
+shapes (``m_ia`` is ``[nocc, nvirt, naux]`` in C order, i.e. the Fortran
+``eri_3center_mo(naux, a, i)`` column-major array).
+"""
+from __future__ import annotations
+
+import math
+from dataclasses import dataclass, field
+
+import numpy as np
+import scipy.linalg as sla
+from scipy.linalg import blas as sblas
+from scipy.linalg import lapack as slapack
+
+HA_EV = 27.21138505            # src/m_definitions.f90:43
+PI = 3.14159265358979323       # src/m_definitions.f90:50
+COMPLETELY_EMPTY = 1.0e-5      # src/m_definitions.f90:66
+
+
+# ---------------------------------------------------------------------------
+# Frequency grids
+# ---------------------------------------------------------------------------
+def coeffs_gausslegint(xmin: float, xmax: float, n: int):
+    """Gauss-Legendre nodes/weights by Newton iteration, tol 1e-13.
+
+    Follows src/m_numerical_tools.f90:35-82 (Rybicki's routine) literally.
+    """
+    x = np.zeros(n)
+    w = np.zeros(n)
+    tol = 1.0e-13
+    xl = (xmax - xmin) * 0.5
+    xmean = (xmax + xmin) * 0.5
+    for i in range(1, (n + 1) // 2 + 1):
+        z = math.cos(PI * (i - 0.25) / (n + 0.5))
+        while True:
+            p1 = 1.0
+            p2 = 0.0
+            for j in range(1, n + 1):
+                p3 = p2
+                p2 = p1
+                p1 = ((2.0 * j - 1.0) * z * p2 - (j - 1.0) * p3) / j
+            pp = n * (p2 - z * p1) / (1.0 - z * z)
+            z1 = z
+            z = z1 - p1 / pp
+            if abs(z - z1) < tol:
+                break
+        x[i - 1] = xmean - xl * z
+        x[n - i] = xmean + xl * z
+        w[i - 1] = 2.0 * xl / ((1.0 - z * z) * pp * pp)
+        w[n - i] = w[i - 1]
+    return x, w
+
+
+def imaginary_quad_grid(nomega: int):
+    """Imaginary-frequency grid of sf_init(IMAGINARY_QUAD).
+
+    src/m_spectral_function.f90:286-306 with alpha=1, beta=2 (:155-156):
+    w_k <- w_k/(2^a-1)*a*(1-x_k)^(-a-1)*b ;  omega_k = 1/(2^a-1)*((1-x_k)^-a - 1)*b.
+    Returns (omega_imag, weight); the frequencies are i*omega_imag.
+    """
+    alpha, beta = 1.0, 2.0
+    x, w = coeffs_gausslegint(0.0, 1.0, nomega)
+    weight = w / (2.0 ** alpha - 1.0) * alpha * (1.0 - x) ** (-alpha - 1.0) * beta
+    omega = 1.0 / (2.0 ** alpha - 1.0) * (1.0 / (1.0 - x) ** alpha - 1.0) * beta
+    return omega, weight
+
+
+# ---------------------------------------------------------------------------
+# Transition space
+# ---------------------------------------------------------------------------
+def transition_table(occupation: np.ndarray, ncore_w: int = 0, nvirtual_w: int | None = None,
+                     spin_fact: float = 2.0):
+    """Resonant transitions (i, a), i outer / a inner, 1-based state indices.
+
+    src/m_spectral_function.f90:239-266 with skip_transition :359-378 (nspin=1).
+    """
+    nstate = occupation.shape[0]
+    if nvirtual_w is None:
+        nvirtual_w = nstate + 1
+    table = []
+    for istate in range(1, nstate + 1):
+        for jstate in range(1, nstate + 1):
+            o1 = occupation[jstate - 1]
+            o2 = occupation[istate - 1]
+            skip = False
+            if jstate <= ncore_w or istate <= ncore_w:
+                skip = True
+            if jstate >= nvirtual_w or istate >= nvirtual_w:
+                skip = True
+            if o1 < COMPLETELY_EMPTY and o2 < COMPLETELY_EMPTY:
+                skip = True
+            if o1 > spin_fact - COMPLETELY_EMPTY and o2 > spin_fact - COMPLETELY_EMPTY:
+                skip = True
+            if skip:
+                continue
+            if o1 - o2 > 0.0:
+                continue
+            table.append((istate, jstate))
+    return np.array(table, dtype=np.int64).reshape(-1, 2)
+
+
+# ---------------------------------------------------------------------------
+# AO -> MO transform of the RI 3-center integrals
+# ---------------------------------------------------------------------------
+def calculate_eri_3center_mo(eri3: np.ndarray, index_basis: np.ndarray, c: np.ndarray,
+                             m_min: int, m_max: int, n_min: int, n_max: int) -> np.ndarray:
+    """M(P, m, n) = sum_{mu nu} C_{mu m} C_{nu n} B(mu nu, P).
+
+    src/m_eri_ao_mo.f90:416-582.  ``eri3`` is ``[naux, npair]`` (the Fortran
+    ``eri_3center(npair, naux)`` column-major array), ``index_basis`` is
+    ``[npair, 2]`` 1-based basis indices (src/m_eri.f90:252-320), diagonal pairs
+    carry the x0.5 convention of src/m_eri_calculate.f90:1841,1854.  ``c`` is
+    ``[nstate, nbf]`` (Fortran ``c_matrix(nbf, nstate)``).  State ranges are
+    1-based inclusive.  Returns ``[n_count, m_count, naux]`` (Fortran
+    ``eri_3center_mo(naux, m, n)``).
+    """
+    naux, npair = eri3.shape
+    nbf = c.shape[1]
+    ms = slice(m_min - 1, m_max)
+    ns = slice(n_min - 1, n_max)
+    c_t = c[ns, :]                       # c_t(n, nbf) = TRANSPOSE(c_matrix(:, n))
+    kbf = index_basis[:, 0] - 1
+    lbf = index_basis[:, 1] - 1
+    out = np.zeros((n_max - n_min + 1, m_max - m_min + 1, naux))
+    for p in range(naux):
+        # pair loop (OpenMP reduction in the reference), :515-524
+        tmp1 = np.zeros((c_t.shape[0], nbf))
+        b = eri3[p]
+        np.add.at(tmp1.T, kbf, (c_t[:, lbf] * b).T)
+        np.add.at(tmp1.T, lbf, (c_t[:, kbf] * b).T)
+        # DGEMM('T','T') :527-530 -> tmp2(m, n) = C(:,m)^T tmp1(n,:)^T
+        tmp2 = c[ms, :] @ tmp1.T
+        out[:, :, p] = tmp2.T
+    return out
+
+
+# ---------------------------------------------------------------------------
+# chi0 / epsilon / chi on the imaginary axis
+# ---------------------------------------------------------------------------
+@dataclass
+class SpectralFunction:
+    """Container of src/m_spectral_function.f90:48-91 (the fields the path uses)."""
+    omega: np.ndarray            # imaginary parts
+    weight_quad: np.ndarray
+    chi: np.ndarray | None = None   # [nomega, naux, naux]
+    erpa: float = 0.0
+    egw: float = 0.0
+    eigval: list = field(default_factory=list)
+
+
+def polarizability_grid(m_ia: np.ndarray, e_occ: np.ndarray, e_virt: np.ndarray,
+                        occ_occ: np.ndarray, occ_virt: np.ndarray,
+                        omega: np.ndarray, weight: np.ndarray, keep_chi: bool = True,
+                        keep_eigval: bool = False) -> SpectralFunction:
+    """RPA polarizability on the imaginary grid, src/m_gw_selfenergy_grid.f90:33-209.
+
+    ``m_ia`` is ``[nocc, nvirt, naux]`` (transition t = (i, a), a fastest, as the
+    transition table orders them).  Per frequency: scale M by
+    sqrt(2*docc*de/(w^2+de^2)) (:126-137), DSYRK('L','N') (:145-149), chi0 = -chi0,
+    symmetrize lower->upper (src/m_scalapack.f90:2461-2551 serial branch), 1-chi0,
+    DSYEV('N') eigenvalues -> E_RPA, E_GW (:171-173), DGETRF/DGETRI inverse
+    (src/m_linear_algebra.f90:179-205), DGEMM chi = (1-chi0)^-1 chi0 (:179-188).
+    """
+    nocc, nvirt, naux = m_ia.shape
+    docc = (occ_occ[:, None] - occ_virt[None, :]).reshape(-1)
+    de = (e_virt[None, :] - e_occ[:, None]).reshape(-1)
+    m_t = np.ascontiguousarray(m_ia.reshape(nocc * nvirt, naux).T)   # eri3(naux, t), Fortran order
+    sf = SpectralFunction(omega=omega.copy(), weight_quad=weight.copy())
+    if keep_chi:
+        sf.chi = np.zeros((len(omega), naux, naux))
+    erpa = 0.0
+    egw = 0.0
+    for iw, w in enumerate(omega):
+        factor_sqrt = np.sqrt(2.0 * docc * de / (w * w + de * de))
+        eri3_t = np.asfortranarray(m_t * factor_sqrt[None, :])
+        chi0 = sblas.dsyrk(1.0, eri3_t, lower=1, trans=0)          # lower triangle
+        chi0 = -chi0
+        il = np.tril_indices(naux, -1)
+        chi0 = np.tril(chi0)
+        chi0[il[1], il[0]] = chi0[il]                              # symmetrize_matrix_sca('L')
+        one_m_chi0 = -chi0
+        one_m_chi0[np.diag_indices(naux)] += 1.0
+        eigval = sla.eigvalsh(one_m_chi0, driver="ev")             # DSYEV('N')
+        if keep_eigval:
+            sf.eigval.append(eigval)
+        erpa += np.sum(np.log(eigval) + 1.0 - eigval) / (2.0 * PI) * weight[iw]
+        egw += np.sum(-(1.0 - eigval) / eigval + 1.0 - eigval) / (2.0 * PI) * weight[iw]
+        if keep_chi:
+            lu, piv, info = slapack.dgetrf(one_m_chi0)
+            if info != 0:
+                raise ArithmeticError(f"dgetrf info={info}")
+            inv, info = slapack.dgetri(lu, piv)
+            if info != 0:
+                raise ArithmeticError(f"dgetri info={info}")
+            sf.chi[iw] = sblas.dgemm(1.0, inv, chi0)
+    sf.erpa = erpa
+    sf.egw = egw
+    return sf
+
+
+def analytic_rpa_correlation(m_ia: np.ndarray, e_occ: np.ndarray, e_virt: np.ndarray) -> float:
+    """Closed-shell direct-RPA correlation energy from the Casida problem.
+
+    MOLGW's analytic RPA (postscf='RPA', src/m_acfd.f90:104-107 ->
+    src/m_linear_response.f90 polarizability, get_rpa_correlation
+    src/m_build_bse.f90:287-314) is E_c = 1/2 sum_n Omega_n - 1/4 tr(A+B) - 1/4 tr(A-B)
+    with A+B = de + 4K, A-B = de (singlet), K_{ia,jb} = sum_P M_Pia M_Pjb.
+    Omega^2 are the eigenvalues of (A-B)^1/2 (A+B) (A-B)^1/2.
+    """
+    nocc, nvirt, naux = m_ia.shape
+    de = (e_virt[None, :] - e_occ[:, None]).reshape(-1)
+    m = m_ia.reshape(nocc * nvirt, naux)
+    k = m @ m.T
+    apb = np.diag(de) + 4.0 * k
+    amb = np.diag(de)
+    sq = np.sqrt(de)
+    c = sq[:, None] * apb * sq[None, :]
+    omega2 = sla.eigvalsh(c)
+    omega_n = np.sqrt(omega2)
+    return 0.5 * np.sum(omega_n) - 0.25 * np.trace(apb) - 0.25 * np.trace(amb)
+
+
+# ---------------------------------------------------------------------------
+# Self-energy on the imaginary axis
+# ---------------------------------------------------------------------------
+@dataclass
+class StateRange:
+    """Module variables set by selfenergy_set_state_range (1-based)."""
+    ncore_g: int
+    nvirtual_g: int
+    nhomo_g: int
+    nlumo_g: int
+    nsemin: int
+    nsemax: int
+
+
+def selfenergy_set_state_range(nstate: int, occupation: np.ndarray, ncoreg: int = 0,
+                               nvirtualg: int = 100000, selfenergy_state_min: int = 1,
+                               selfenergy_state_max: int = 100000,
+                               selfenergy_state_range: int = 100000) -> StateRange:
+    """src/m_selfenergy_tools.f90:67-122 (no frozen-core atom tables: ncoreg given)."""
+    ncore_g = ncoreg
+    nvirtual_g = min(nvirtualg, nstate + 1)
+    nhomo_g = 1
+    for p in range(1, nstate + 1):
+        if not occupation[p - 1] < COMPLETELY_EMPTY:
+            nhomo_g = max(nhomo_g, p)
+    nlumo_g = 100000
+    for p in range(1, nstate + 1):
+        if not occupation[p - 1] > COMPLETELY_EMPTY:
+            nlumo_g = min(nlumo_g, p)
+    nsemin = max(ncore_g + 1, selfenergy_state_min, 1, nhomo_g - selfenergy_state_range)
+    nsemax = min(nvirtual_g - 1, selfenergy_state_max, nstate, nhomo_g + selfenergy_state_range)
+    return StateRange(ncore_g, nvirtual_g, nhomo_g, nlumo_g, nsemin, nsemax)
+
+
+@dataclass
+class SelfEnergyGrid:
+    """selfenergy_grid type, src/m_selfenergy_tools.f90:45-60 (one spin)."""
+    omega: np.ndarray            # real grid, index -nomega..nomega -> [0..2*nomega]
+    omega_calc: np.ndarray       # complex evaluation points
+    energy0: np.ndarray          # per state of the range
+    sigma: np.ndarray | None = None        # [2*nomega+1, nstate_range] complex
+    sigma_calc: np.ndarray | None = None   # [nomega_calc, nstate_range] complex
+
+    @property
+    def nomega(self) -> int:
+        return (len(self.omega) - 1) // 2
+
+
+def fermi_level(energy0: np.ndarray, nhomo_g: int, mu_origin: float = -100.0) -> float:
+    """efermi of se_init, src/m_selfenergy_tools.f90:573-596."""
+    if mu_origin > -99.0:
+        if mu_origin < energy0[nhomo_g - 1] or mu_origin > energy0[nhomo_g]:
+            raise ValueError("se_init: efermi needs to be in the HOMO-LUMO gap")
+        return mu_origin
+    return 0.5 * (energy0[nhomo_g - 1] + energy0[nhomo_g])
+
+
+def se_init_imaginary_axis(energy0: np.ndarray, rng: StateRange, technique: str = "pade",
+                           nomega_sigma: int = 51, step_sigma: float = 0.01,
+                           nomega_sigma_calc: int = 1, step_sigma_calc: float = 0.03,
+                           mu_origin: float = -100.0) -> SelfEnergyGrid:
+    """se_init for imaginary_axis_pade / imaginary_axis_homolumo, :557-699."""
+    efermi = fermi_level(energy0, rng.nhomo_g, mu_origin)
+    nom = nomega_sigma // 2
+    omega = efermi + step_sigma * np.arange(-nom, nom + 1, dtype=np.float64)
+    if technique == "pade":
+        omega_calc = efermi + step_sigma_calc * np.arange(nomega_sigma_calc) * 1j
+    elif technique == "homolumo":
+        eh = energy0[rng.nhomo_g - 1]
+        el = energy0[rng.nhomo_g]
+        omega_calc = (eh + 0.01 + np.arange(nomega_sigma_calc) / (nomega_sigma_calc - 1.0)
+                      * (el - eh - 0.02)).astype(np.complex128)
+    else:
+        raise ValueError(technique)
+    ns = rng.nsemax - rng.nsemin + 1
+    return SelfEnergyGrid(omega=omega, omega_calc=omega_calc, energy0=np.zeros(ns),
+                          sigma=np.zeros((2 * nom + 1, ns), dtype=np.complex128),
+                          sigma_calc=np.zeros((nomega_sigma_calc, ns), dtype=np.complex128))
+
+
+def gw_selfenergy_imag(energy: np.ndarray, m_sigma: np.ndarray, sf: SpectralFunction,
+                       omega_calc: np.ndarray, pstate_first: int) -> np.ndarray:
+    """Sigma_c on the evaluation points, src/m_gw_selfenergy_grid.f90:213-338.
+
+    ``m_sigma`` is ``[nsig, prange, naux]`` (Fortran ``eri_3center_mo(naux, p, m)``
+    for p = ncore_G+1..nvirtual_G-1, m = nsemin..nsemax).  ``pstate_first`` is
+    ncore_G+1 (1-based).  Returns sigma_calc ``[nomega_calc, nsig]``.
+    """
+    nsig, prange, naux = m_sigma.shape
+    sig = np.zeros((len(omega_calc), nsig), dtype=np.complex128)
+    e_p = energy[pstate_first - 1: pstate_first - 1 + prange]
+    for m in range(nsig):
+        eri3 = np.asfortranarray(m_sigma[m].T)                  # (naux, prange)
+        for iw in range(len(sf.omega)):
+            chi_eri3 = sblas.dgemm(1.0, sf.chi[iw], eri3)       # DGEMM('N','N') :297-300
+            v_chi_v = np.einsum("ij,ij->j", eri3, chi_eri3)     # DOT_PRODUCT per p :307
+            om = 1j * sf.omega[iw]
+            a = omega_calc[:, None] - e_p[None, :]
+            fac = 1.0 / (a + om) + 1.0 / (a - om)
+            sig[:, m] -= sf.weight_quad[iw] * (fac * v_chi_v[None, :]).sum(axis=1) / (2.0 * PI)
+    return sig
+
+
+# ---------------------------------------------------------------------------
+# Analytic continuation
+# ---------------------------------------------------------------------------
+def calculate_pade_a(z_in: np.ndarray, f_in: np.ndarray) -> np.ndarray:
+    """Thiele continued-fraction coefficients, src/m_numerical_tools.f90:120-146."""
+    n = len(z_in)
+    g = np.zeros((n, n), dtype=np.complex128)
+    g[0, :] = f_in
+    for ip in range(1, n):
+        for jp in range(ip, n):
+            g[ip, jp] = (g[ip - 1, ip - 1] - g[ip - 1, jp]) / ((z_in[jp] - z_in[ip - 1]) * g[ip - 1, jp])
+    return np.diag(g).copy()
+
+
+def pade_eval(aa: np.ndarray, z_in: np.ndarray, z_out: complex) -> complex:
+    """Continued-fraction evaluation of src/m_numerical_tools.f90:86-116."""
+    n = len(z_in)
+    az_m1, az = 0.0 + 0.0j, aa[0]
+    bz_m1, bz = 1.0 + 0.0j, 1.0 + 0.0j
+    for ip in range(1, n):
+        az_new = az + (z_out - z_in[ip - 1]) * aa[ip] * az_m1
+        bz_new = bz + (z_out - z_in[ip - 1]) * aa[ip] * bz_m1
+        az_m1, az = az, az_new
+        bz_m1, bz = bz, bz_new
+    return az / bz
+
+
+def pade(z_in: np.ndarray, f_in: np.ndarray, z_out: complex) -> complex:
+    """pade(), src/m_numerical_tools.f90:86-116 (coefficients are recomputed per call,
+    exactly as the reference does; they depend on z_in, f_in only)."""
+    return pade_eval(calculate_pade_a(z_in, f_in), z_in, z_out)
+
+
+def se_pade_fit(se: SelfEnergyGrid, eta: float) -> None:
+    """src/m_selfenergy_tools.f90:965-999: symmetric data on 2*Nc-1 points, then
+    Thiele continuation to omega_j + i*eta*sign with sign = -sgn(omega_j - Re z_1)."""
+    nc = len(se.omega_calc)
+    for s in range(se.sigma_calc.shape[1]):
+        omega_sym = np.zeros(2 * nc - 1, dtype=np.complex128)
+        sigma_sym = np.zeros(2 * nc - 1, dtype=np.complex128)
+        omega_sym[nc - 1] = se.omega_calc[0]
+        sigma_sym[nc - 1] = se.sigma_calc[0, s]
+        for k in range(2, nc + 1):
+            omega_sym[nc + k - 2] = se.omega_calc[k - 1]
+            sigma_sym[nc + k - 2] = se.sigma_calc[k - 1, s]
+            omega_sym[nc - k] = np.conj(se.omega_calc[k - 1])
+            sigma_sym[nc - k] = np.conj(se.sigma_calc[k - 1, s])
+        aa = calculate_pade_a(omega_sym, sigma_sym)
+        for j, w in enumerate(se.omega):
+            sign_eta = -math.copysign(1.0, w - se.omega_calc[0].real)
+            se.sigma[j, s] = pade_eval(aa, omega_sym, w + 1j * eta * sign_eta)
+
+
+def self_energy_polynomial(se: SelfEnergyGrid) -> None:
+    """Quadratic fit for imaginary_axis_homolumo, src/m_selfenergy_tools.f90:1005-1033."""
+    nc = len(se.omega_calc)
+    mid = nc // 2          # Fortran nomega_calc/2+1, 1-based
+    for s in range(se.sigma_calc.shape[1]):
+        sc = se.sigma_calc[:, s]
+        a0 = sc[mid].real
+        a1 = (sc[nc - 1].real - sc[0].real) / (se.omega_calc[nc - 1].real - se.omega_calc[0].real)
+        a2 = (sc[nc - 1].real + sc[0].real - 2.0 * sc[mid].real) \
+            / (se.omega_calc[nc - 1].real - se.omega_calc[0].real) ** 2 * 2.0
+        d = se.omega - se.omega_calc[mid]
+        se.sigma[:, s] = a0 + a1 * d + a2 * d * d
+
+
+# ---------------------------------------------------------------------------
+# Quasiparticle equation
+# ---------------------------------------------------------------------------
+def find_fixed_point(xx: np.ndarray, fx: np.ndarray, nfpmx: int = 4):
+    """Sign changes of f(x)-x with Z weights, src/m_selfenergy_tools.f90:367-420."""
+    z_weight = -np.ones(nfpmx)
+    efp = np.zeros(nfpmx)
+    gx = fx - xx
+    for ix in range(len(xx) - 1):
+        if gx[ix] * gx[ix + 1] < 0.0:
+            z_zero = 1.0 / (1.0 - (fx[ix + 1] - fx[ix]) / (xx[ix + 1] - xx[ix]))
+            if z_zero < 0.00001:
+                continue
+            if z_zero > z_weight[nfpmx - 1]:
+                cand = [k for k in range(nfpmx) if z_zero > z_weight[k]]
+                jf = min(cand)
+                z_weight[jf + 1:] = z_weight[jf:nfpmx - 1].copy()
+                efp[jf + 1:] = efp[jf:nfpmx - 1].copy()
+                z_weight[jf] = z_zero
+                gpxi = (gx[ix + 1] - gx[ix]) / (xx[ix + 1] - xx[ix])
+                efp[jf] = xx[ix] - gx[ix] / gpxi
+    return efp, z_weight
+
+
+def find_qp_energy_linearization(se: SelfEnergyGrid, exchange_m_vxc: np.ndarray,
+                                 energy0: np.ndarray):
+    """src/m_selfenergy_tools.f90:202-249 (range states; zz present)."""
+    nom = se.nomega
+    if nom > 0:
+        zz = (se.sigma[nom + 1].real - se.sigma[nom - 1].real) / (se.omega[nom + 1] - se.omega[nom - 1]).real
+        zz = 1.0 / (1.0 - zz)
+        zz = np.minimum(np.maximum(zz, 0.0), 1.0)
+        eqp = se.energy0 + zz * (energy0 - se.energy0 + se.sigma[nom].real + exchange_m_vxc)
+    else:
+        zz = np.ones_like(energy0)
+        eqp = energy0 + se.sigma[nom].real + exchange_m_vxc
+    return eqp, zz
+
+
+def find_qp_energy_graphical(se: SelfEnergyGrid, exchange_m_vxc: np.ndarray, energy0: np.ndarray):
+    """src/m_selfenergy_tools.f90:253-363 for the states of the range.
+
+    Returns (energy_qp_g, zz, fixed_points, z_weights).
+    """
+    ns = len(energy0)
+    nom = se.nomega
+    eqp = np.zeros(ns)
+    zz = np.zeros(ns)
+    efps = np.zeros((ns, 4))
+    zws = np.zeros((ns, 4))
+    if nom > 0:
+        for s in range(ns):
+            lhs = se.omega.real + se.energy0[s]
+            rhs = se.sigma[:, s].real + exchange_m_vxc[s] + energy0[s]
+            efp, zw = find_fixed_point(lhs, rhs)
+            efps[s], zws[s] = efp, zw
+            if zw.max() > 1.0e-6:
+                iqp = int(np.argmax(zw))
+                eqp[s] = efp[iqp]
+                zz[s] = zw[iqp]
+            else:
+                eqp[s] = energy0[s]
+                zz[s] = 1.0
+            if np.count_nonzero(zw > 0.0) == 0:
+                eqp[s] = energy0[s] + se.sigma[nom, s].real + exchange_m_vxc[s]
+    else:
+        eqp = energy0 + se.sigma[nom].real + exchange_m_vxc
+        zz[:] = 1.0
+    return eqp, zz, efps, zws
+
+
+def output_homolumo(occupation: np.ndarray, energy: np.ndarray, istate_min: int, istate_max: int,
+                    spin_fact: float = 2.0):
+    """HOMO/LUMO over a state range, src/m_hamiltonian_tools.f90:564-612 (nspin=1)."""
+    ehomo, elumo = -np.inf, np.inf
+    for s in range(istate_min, istate_max + 1):
+        if occupation[s - 1] / spin_fact > COMPLETELY_EMPTY:
+            ehomo = max(ehomo, energy[s - 1])
+        if occupation[s - 1] / spin_fact < 1.0 - COMPLETELY_EMPTY:
+            elumo = min(elumo, energy[s - 1])
+    return ehomo, elumo
+
+
+# ---------------------------------------------------------------------------
+# One-shot G0W0 on the imaginary axis (the path of selfenergy_evaluation)
+# ---------------------------------------------------------------------------
+@dataclass
+class G0W0Result:
+    erpa: float
+    egw: float
+    sigma_calc: np.ndarray       # [Nc, nsig] complex
+    sigma: np.ndarray            # [Nsigma, nsig] complex (real grid)
+    energy_qp_g: np.ndarray      # graphical, per range state
+    energy_qp_z: np.ndarray      # linearized
+    zz: np.ndarray
+    ehomo: float
+    elumo: float
+    nsemin: int
+    nsemax: int
+
+
+def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_sigma: np.ndarray,
+              nomega_chi_imag: int, rng: StateRange, nomega_sigma: int = 51,
+              step_sigma: float = 0.01, nomega_sigma_calc: int = 50,
+              step_sigma_calc: float = 0.075, eta: float = 0.01,
+              exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
+              ncore_w: int = 0) -> G0W0Result:
+    """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
+    (src/m_selfenergy_evaluation.f90:214-246, 587-611).
+
+    ``m_ia`` is the W-window tensor ``[nocc_w, nvirt_w, naux]``; ``m_sigma`` is
+    ``[nsig, prange, naux]`` with p = ncore_G+1.. nvirtual_G-1.
+    """
+    occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
+    e_occ = energy[ncore_w:ncore_w + m_ia.shape[0]]
+    nlumo = ncore_w + m_ia.shape[0]
+    e_virt = energy[nlumo:nlumo + m_ia.shape[1]]
+    occ_v = occupation[nlumo:nlumo + m_ia.shape[1]]
+    omega, weight = imaginary_quad_grid(nomega_chi_imag)
+    sf = polarizability_grid(m_ia, e_occ, e_virt, occ_w, occ_v, omega, weight)
+    se = se_init_imaginary_axis(energy, rng, technique, nomega_sigma, step_sigma,
+                                nomega_sigma_calc, step_sigma_calc)
+    se.sigma_calc[:] = gw_selfenergy_imag(energy, m_sigma, sf, se.omega_calc, rng.ncore_g + 1)
+    if technique == "pade":
+        se_pade_fit(se, eta)
+    else:
+        self_energy_polynomial(se)
+    e0 = energy[rng.nsemin - 1: rng.nsemax]
+    xc = np.zeros_like(e0) if exchange_m_vxc is None else exchange_m_vxc
+    eqp_z, zz = find_qp_energy_linearization(se, xc, e0)
+    eqp_g, zz_g, _, _ = find_qp_energy_graphical(se, xc, e0)
+    full = energy.copy()
+    full[rng.nsemin - 1: rng.nsemax] = eqp_g
+    ehomo, elumo = output_homolumo(occupation, full, rng.nsemin, rng.nsemax)
+    return G0W0Result(sf.erpa, sf.egw, se.sigma_calc.copy(), se.sigma.copy(), eqp_g, eqp_z, zz_g,
+                      ehomo, elumo, rng.nsemin, rng.nsemax)
