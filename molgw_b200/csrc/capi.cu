@@ -29,6 +29,10 @@ Status run_batch(Context& c, rigw::PlanMode mode, int n, const rigw_problem* pro
                  const double* const* sigma_in) {
   std::vector<Shape> shapes(n);
   for (int i = 0; i < n; ++i) RIGW_TRY(rigw::make_shape(probs[i], &shapes[i]));
+  if (mode != rigw::kPlanPolar)
+    for (int i = 0; i < n; ++i)
+      if (shapes[i].nc < 1 || shapes[i].nsig < 1 || shapes[i].nstate_p < 1)
+        return Status::fail(RIGW_ERR_ARG, "problem %d: Sigma needs nomega_sigma_calc, nsig, nstate_p >= 1", i);
   for (int i = 0; i < n; ++i)
     if (probs[i].precision != RIGW_FP64 && !rigw::bf16x3_available())
       return Status::fail(RIGW_ERR_UNSUPPORTED, "precision %d not available", probs[i].precision);

@@ -146,10 +146,10 @@ size_t footprint(const Shape& sh, PlanMode mode) {
 }
 
 Plan::~Plan() {
-  if (exec_) cudaGraphExecDestroy(exec_);
-  if (graph_) cudaGraphDestroy(graph_);
-  if (ev0_) cudaEventDestroy(ev0_);
-  if (ev1_) cudaEventDestroy(ev1_);
+  for (int st = 0; st < 4; ++st) {
+    if (stage_exec_[st]) cudaGraphExecDestroy(stage_exec_[st]);
+    if (stage_graph_[st]) cudaGraphDestroy(stage_graph_[st]);
+  }
   for (auto& e : stage_ev_)
     if (e) cudaEventDestroy(e);
 }
@@ -434,8 +434,6 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     seq_.push_back({pend[j].kind, offs[j], pend[j].count, pend[j].arg});
   }
   RIGW_CUDA_TRY(cudaMemcpy(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice));
-  RIGW_CUDA_TRY(cudaEventCreate(&ev0_));
-  RIGW_CUDA_TRY(cudaEventCreate(&ev1_));
   for (auto& e : stage_ev_) RIGW_CUDA_TRY(cudaEventCreate(&e));
   host_table_.resize(np);
   n_launches_ = int(seq_.size());
@@ -443,8 +441,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 }
 
 // Stage of a launch kind: 0 input packing, 1 chi0, 2 eps factorization and
-// solves, 3 energies / Sigma / QP.  Stage boundaries carry CUDA events that are
-// captured into the graph, so every replay reports its own stage times.
+// solves, 3 energies / Sigma / QP.  Each stage is its own CUDA graph; CUDA
+// events between the stage graphs time every replay stage by stage.
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
@@ -454,13 +452,10 @@ static int stage_of(int kind) {
   }
 }
 
-void Plan::record(cudaStream_t s) {
+void Plan::record(cudaStream_t s, int stage) {
   char* lb = lists_.data();
-  int phase = 0;
-  cudaEventRecord(stage_ev_[0], s);
   for (const Launch& L : seq_) {
-    const int st = stage_of(L.kind);
-    while (phase < st) cudaEventRecord(stage_ev_[++phase], s);
+    if (stage >= 0 && stage_of(L.kind) != stage) continue;
     const WorkItem* wl = reinterpret_cast<const WorkItem*>(lb + L.off);
     const GemmItem* gl = reinterpret_cast<const GemmItem*>(lb + L.off);
     switch (L.kind) {
@@ -479,7 +474,6 @@ void Plan::record(cudaStream_t s) {
       default: break;
     }
   }
-  while (phase < 4) cudaEventRecord(stage_ev_[++phase], s);
 }
 
 // Gauss-Legendre imaginary grid (coeffs_gausslegint + the [0,1) -> [0,inf) map).
@@ -609,26 +603,37 @@ Status Plan::stage_sigma_calc(int i, const double* sc, cudaStream_t s) {
 Status Plan::launch(cudaStream_t s) {
   RIGW_CUDA_TRY(cudaMemsetAsync(err_dev_, 0, sizeof(int), s));
   if (ctx_->use_graphs) {
-    if (!exec_) {
+    for (int st = 0; st < 4; ++st) {
+      if (stage_exec_[st] || stage_empty_[st]) continue;
+      bool any = false;
+      for (const Launch& L : seq_) any |= stage_of(L.kind) == st;
+      if (!any) {
+        stage_empty_[st] = true;
+        continue;
+      }
       RIGW_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      record(s);
+      record(s, st);
       cudaGraph_t g = nullptr;
       cudaError_t e = cudaStreamEndCapture(s, &g);
       if (e != cudaSuccess)
         return Status::fail(RIGW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
-      graph_ = g;
-      RIGW_CUDA_TRY(cudaGraphInstantiate(&exec_, graph_, 0));
+      stage_graph_[st] = g;
+      RIGW_CUDA_TRY(cudaGraphInstantiate(&stage_exec_[st], g, 0));
     }
-    RIGW_CUDA_TRY(cudaEventRecord(ev0_, s));
-    RIGW_CUDA_TRY(cudaGraphLaunch(exec_, s));
-    RIGW_CUDA_TRY(cudaEventRecord(ev1_, s));
+    for (int st = 0; st < 4; ++st) {
+      RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[st], s));
+      if (stage_exec_[st]) RIGW_CUDA_TRY(cudaGraphLaunch(stage_exec_[st], s));
+    }
+    RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[4], s));
     replayed_ = true;
   } else {
     replayed_ = false;
-    RIGW_CUDA_TRY(cudaEventRecord(ev0_, s));
-    record(s);
-    RIGW_CUDA_TRY(cudaGetLastError());
-    RIGW_CUDA_TRY(cudaEventRecord(ev1_, s));
+    for (int st = 0; st < 4; ++st) {
+      RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[st], s));
+      record(s, st);
+      RIGW_CUDA_TRY(cudaGetLastError());
+    }
+    RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[4], s));
   }
   return Status::ok();
 }
@@ -637,7 +642,7 @@ Status Plan::check_errors(cudaStream_t s) {
   int err = 0;
   RIGW_CUDA_TRY(cudaMemcpyAsync(&err, err_dev_, sizeof(int), cudaMemcpyDeviceToHost, s));
   RIGW_CUDA_TRY(cudaStreamSynchronize(s));
-  RIGW_CUDA_TRY(cudaEventElapsedTime(&last_ms_, ev0_, ev1_));
+  RIGW_CUDA_TRY(cudaEventElapsedTime(&last_ms_, stage_ev_[0], stage_ev_[4]));
   for (int k = 0; k < 4; ++k) RIGW_CUDA_TRY(cudaEventElapsedTime(&stage_ms_[k], stage_ev_[k], stage_ev_[k + 1]));
   if (err & kErrNotSPD) return Status::fail(RIGW_ERR_NOT_SPD, "eps(iw) is not positive definite");
   if (err & (kErrNonFinite | kErrPade))

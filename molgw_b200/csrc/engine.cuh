@@ -113,7 +113,7 @@ class Plan {
   int kernel_launches() const { return n_launches_; }
 
  private:
-  void record(cudaStream_t s);
+  void record(cudaStream_t s, int stage);
   Context* ctx_ = nullptr;
   PlanMode mode_ = kPlanFused;
   std::vector<Shape> shapes_;
@@ -134,9 +134,9 @@ class Plan {
     int arg;
   };
   std::vector<Launch> seq_;
-  cudaGraph_t graph_ = nullptr;
-  cudaGraphExec_t exec_ = nullptr;
-  cudaEvent_t ev0_ = nullptr, ev1_ = nullptr;
+  cudaGraph_t stage_graph_[4] = {nullptr, nullptr, nullptr, nullptr};
+  cudaGraphExec_t stage_exec_[4] = {nullptr, nullptr, nullptr, nullptr};
+  bool stage_empty_[4] = {false, false, false, false};
   cudaEvent_t stage_ev_[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   float last_ms_ = 0.0f;
   float stage_ms_[4] = {0, 0, 0, 0};

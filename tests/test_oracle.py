@@ -80,6 +80,31 @@ def test_pade_exact_for_rational_function():
         assert abs(o.pade_eval(aa, z, x + 0.01j) - (2.0 / (x + 0.01j - 1.5) - 1.0 / (x + 0.01j + 0.8))) < 1e-8
 
 
+def test_pade_continuation_sensitivity_bounds_the_parity_tolerance(golden_lih):
+    """The reference's continuation (se_pade_fit on 2*50-1 points) turns 1e-15
+    relative changes of sigma_calc into ~1e-6 changes of Sigma on the real grid,
+    while the graphical QP energies move by < 1e-7 eV.  This fixes the tolerances
+    of the GPU parity tests for the real-grid Sigma and the QP energies."""
+    d = golden_lih
+    e = d["energy"]
+    nsemin, nsemax = int(d["nsemin"]), int(d["nsemax"])
+    rng = o.selfenergy_set_state_range(len(e), d["occupation"], selfenergy_state_min=nsemin,
+                                       selfenergy_state_max=nsemax)
+    sc = d["sigma_calc"].T.copy()
+    outs = []
+    for trial in range(3):
+        se = o.se_init_imaginary_axis(e, rng, "pade", 101, 0.025, 50, 0.075)
+        noise = 1.0 + (1e-15 * np.random.default_rng(trial).standard_normal(sc.shape) if trial else 0.0)
+        se.sigma_calc[:] = sc * noise
+        o.se_pade_fit(se, 0.01)
+        eqp, _, _, _ = o.find_qp_energy_graphical(se, np.zeros(2), e[nsemin - 1:nsemax])
+        outs.append((se.sigma.copy(), eqp))
+    dsig = max(np.abs(outs[k][0] - outs[0][0]).max() for k in (1, 2)) / np.abs(outs[0][0]).max()
+    dqp = max(np.abs(outs[k][1] - outs[0][1]).max() for k in (1, 2)) * 27.21138505
+    assert 1e-8 < dsig < 2e-5
+    assert dqp < 1e-7
+
+
 def test_find_fixed_point_linear():
     x = np.linspace(-1, 1, 21)
     fx = 0.2 + 0.5 * x           # fixed point at x = 0.4, Z = 1/(1-0.5) = 2
