@@ -10,7 +10,7 @@
 namespace rigw {
 
 constexpr double kPi = 3.14159265358979323;   // src/m_definitions.f90:50
-constexpr int kPanel = 64;                     // Cholesky panel width (rows of one U block row)
+constexpr int kPanel = 128;                    // Cholesky panel width (rows of one U block row)
 
 // Device-side error flags (bitmask written with atomicOr, read by the host after a stage).
 enum DeviceError : int {
@@ -18,6 +18,7 @@ enum DeviceError : int {
   kErrNotSPD = 1,        // a pivot of eps(iw) was <= 0 (eps must be SPD with eigenvalues >= 1)
   kErrNonFinite = 2,     // NaN/Inf met in an output sentinel
   kErrPade = 4,          // zero denominator in the Thiele recursion
+  kErrTimeout = 8,       // a bounded mbarrier wait gave up
 };
 
 RIGW_DEVICE_INLINE uint32_t smem_u32(const void* p) {

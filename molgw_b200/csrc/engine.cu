@@ -84,6 +84,7 @@ Status Context::init(int dev, size_t budget_bytes) {
   RIGW_CUDA_TRY(cudaSetDevice(dev));
   RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
   RIGW_CUDA_TRY(prepare_dgemm_kernels());
+  RIGW_CUDA_TRY(prepare_tc_kernels());
   return Status::ok();
 }
 
@@ -104,7 +105,7 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   d.npad = round_up(sh.naux, kPanel);
   d.npanel = d.npad / kPanel;
   d.nia = sh.nocc * sh.nvirt;
-  d.nia_pad = round_up(std::max(d.nia, 1), 16);
+  d.nia_pad = round_up(std::max(d.nia, 1), 64);
   d.want_identity = (mode == kPlanFused || mode == kPlanPolar) ? 1 : 0;
   d.moff = d.want_identity ? d.npad : 0;
   d.ncm = (mode == kPlanFused || mode == kPlanSigma) ? round_up(sh.nsig * sh.nstate_p, 8) : 0;
@@ -171,7 +172,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // ---- memory layout
   Layout L;
   struct Off {
-    size_t mp, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, en, sc, sr, qp;
+    size_t mp, xs, tmap, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, en, sc, sr, qp;
   };
   std::vector<Off> off(np);
   for (int i = 0; i < np; ++i) {
@@ -188,6 +189,10 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       pp.off_in_omega = L.take(size_t(sh.nomega) * D);
       pp.off_in_weight = L.take(size_t(sh.nomega) * D);
       off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
+      if (sh.precision == RIGW_BF16X3) {
+        off[i].xs = L.take(size_t(sh.nomega) * 2 * d.npad * d.nia_pad * 2);
+        off[i].tmap = L.take(128);
+      }
       off[i].tnorm = L.take(size_t(d.nia_pad) * D);
       off[i].dscale = L.take(size_t(sh.nomega) * d.nia_pad * D);
       off[i].eps = L.take(size_t(sh.nomega) * d.npad * d.npad * D);
@@ -254,6 +259,13 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     p.want_identity = d.want_identity;
     if (factor) {
       p.mp = dp(off[i].mp);
+      p.kpad = d.nia_pad;
+      if (sh.precision == RIGW_BF16X3) {
+        p.xs = base + off[i].xs;
+        alignas(64) unsigned char map[128];
+        RIGW_TRY(make_split_tmap(map, p.xs, d.nia_pad, (long long)sh.nomega * 2 * d.npad));
+        RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
+      }
       p.tnorm = dp(off[i].tnorm);
       p.dscale = dp(off[i].dscale);
       p.eps = dp(off[i].eps);
@@ -297,7 +309,26 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     const int npad = p.npad, ldb = p.ldb;
     if (factor) {
       for (int t0 = 0; t0 < p.nia_pad; t0 += 8) wl_pack_.push_back({i, t0, 0, 0});
-      for (int w = 0; w < sh.nomega; ++w) {
+      if (sh.precision == RIGW_BF16X3) {
+        for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+          for (int p0 = 0; p0 < npad; p0 += 64) wl_split_.push_back({i, t0, p0, 0});
+        for (int w = 0; w < sh.nomega; ++w)
+          for (int ti = 0; ti < npad; ti += BMN)
+            for (int tj = ti; tj < npad; tj += BMN) {
+              TcItem t{};
+              t.tmap = base + off[i].tmap;
+              t.C = p.eps + size_t(w) * npad * npad + size_t(ti) * npad + tj;
+              t.err = err_dev_;
+              t.row_a = w * 2 * npad + ti;
+              t.row_b = w * 2 * npad + tj;
+              t.lo_off = npad;
+              t.ktiles = p.kpad / 64;
+              t.ldc = npad;
+              t.diag = ti - tj;
+              tl_syrk_.push_back(t);
+            }
+      }
+      for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
         double* E = p.eps + size_t(w) * npad * npad;
         for (int ti = 0; ti < npad; ti += BMN)
           for (int tj = ti; tj < npad; tj += BMN) {
@@ -415,6 +446,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(2, wl_rhs_.data(), sizeof(WorkItem), wl_rhs_.size(), 0);
   add(3, wl_mnorm_.data(), sizeof(WorkItem), wl_mnorm_.size(), 0);
   add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
+  add(12, wl_split_.data(), sizeof(WorkItem), wl_split_.size(), 0);
+  add(13, tl_syrk_.data(), sizeof(TcItem), tl_syrk_.size(), 0);
   for (int k = 0; k < max_panels; ++k) {
     add(4, wl_diag_[k].data(), sizeof(WorkItem), wl_diag_[k].size(), k);
     add(5, gl_k2_[k].data(), sizeof(GemmItem), gl_k2_[k].size(), k);
@@ -446,7 +479,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: return 1;
+    case 1: case 12: case 13: return 1;
     case 4: case 5: case 6: return 2;
     default: return 3;
   }
@@ -461,10 +494,12 @@ void Plan::record(cudaStream_t s, int stage) {
     switch (L.kind) {
       case 0: pack_m_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 1: launch_dgemm_128x128(gl, L.count, s); break;
+      case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
+      case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
-      case 4: chol_diag_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl, L.arg); break;
-      case 5: launch_dgemm_64x128(gl, L.count, s); break;
+      case 4: chol_diag_kernel<<<L.count, kDiagThreads, 0, s>>>(probs_dev_, wl, L.arg); break;
+      case 5: launch_dgemm_128x128(gl, L.count, s); break;
       case 6: launch_dgemm_128x128(gl, L.count, s); break;
       case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 8: energy_sum_kernel<<<(L.count + 127) / 128, 128, 0, s>>>(probs_dev_, L.count); break;
@@ -645,6 +680,7 @@ Status Plan::check_errors(cudaStream_t s) {
   RIGW_CUDA_TRY(cudaEventElapsedTime(&last_ms_, stage_ev_[0], stage_ev_[4]));
   for (int k = 0; k < 4; ++k) RIGW_CUDA_TRY(cudaEventElapsedTime(&stage_ms_[k], stage_ev_[k], stage_ev_[k + 1]));
   if (err & kErrNotSPD) return Status::fail(RIGW_ERR_NOT_SPD, "eps(iw) is not positive definite");
+  if (err & kErrTimeout) return Status::fail(RIGW_ERR_TIMEOUT, "a bounded device wait expired");
   if (err & (kErrNonFinite | kErrPade))
     return Status::fail(RIGW_ERR_NUMERIC, "non-finite QP energy or singular Pade recursion (flags %d)", err);
   return Status::ok();

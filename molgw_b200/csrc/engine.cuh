@@ -126,6 +126,8 @@ class Plan {
   std::vector<WorkItem> wl_pack_, wl_rhs_, wl_mnorm_, wl_energy_, wl_vchiv_, wl_sigma_, wl_pade_;
   std::vector<std::vector<WorkItem>> wl_diag_;
   std::vector<GemmItem> gl_syrk_;
+  std::vector<WorkItem> wl_split_;
+  std::vector<TcItem> tl_syrk_;
   std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_;
   struct Launch {
     int kind;        // see Plan::record
@@ -180,5 +182,6 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                       int nstate_min, int nstate_max, double* out);
 bool bf16x3_available();
+Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
 
 }  // namespace rigw

@@ -15,6 +15,7 @@ struct WorkItem {
 __global__ void pack_m_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void init_rhs_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void mnorm_kernel(const ProbDev* probs, const WorkItem* items);
+constexpr int kDiagThreads = 512;  // threads of chol_diag_kernel (kPanel columns x 4 row groups)
 __global__ void chol_diag_kernel(const ProbDev* probs, const WorkItem* items, int k);
 __global__ void energy_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void vchiv_kernel(const ProbDev* probs, const WorkItem* items);
@@ -30,6 +31,21 @@ struct AomoUnpackItem {
   int naux, naux_pad, npair, nbf, p0;
 };
 __global__ void aomo_unpack_kernel(const AomoUnpackItem* items);
+
+// Split-precision chi0 (syrk_bf16x3.cu): one 128x128 upper tile of eps(iw).
+struct TcItem {
+  const void* tmap;   // CUtensorMap of the problem's hi/lo tensor (rows: [nomega][2][npad], cols: kpad)
+  double* C;          // &eps[w][i0][j0]
+  int* err;
+  int row_a, row_b;   // tensor rows of the hi blocks of the A (i0) and B (j0) operands
+  int lo_off;         // rows from a hi block to its lo block (npad)
+  int ktiles;         // kpad / 64
+  int ldc;            // npad
+  int diag;           // i0 - j0: identity where (col - row) == diag
+};
+void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
+void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s);
+cudaError_t prepare_tc_kernels();
 
 // Host-side launchers of the DMMA tile engine (gemm_f64.cu).
 void launch_dgemm_128x128(const GemmItem* items, int n, cudaStream_t s);

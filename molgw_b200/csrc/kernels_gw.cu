@@ -133,85 +133,73 @@ __global__ void __launch_bounds__(256) mnorm_kernel(const ProbDev* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block of panel k: A_kk = U_kk^T U_kk (upper Cholesky) and W = U_kk^-1.
-// One CTA (256 threads) per (prob, frequency).  Thread t owns column l = t & 63
-// and rows i = (t >> 6) + 4r (r < 16) of the block in registers.
-__global__ void __launch_bounds__(256) chol_diag_kernel(const ProbDev* __restrict__ probs,
-                                                        const WorkItem* __restrict__ items, int k) {
+// Diagonal block of panel k: A_kk = U^T U (upper Cholesky) and W = U^-1 in one
+// sweep.  Gaussian elimination of the symmetric block, with the same row
+// operations applied to an identity block stored in the (initially zero)
+// strictly lower triangle, leaves D L^T in the upper triangle and L^-1 (unit
+// diagonal implicit) in the lower one, where A = L D L^T.  Then U = D^-1/2 (D L^T)
+// and W = U^-1 = L^-T D^-1/2, i.e. W[l][m] = (L^-1)[m][l] / sqrt(d_m).
+// One CTA of kDiagThreads threads per (prob, frequency); thread t owns column
+// l = t % kPanel and rows i = t / kPanel + kDiagGroups * r of the block.
+constexpr int kDiagGroups = kDiagThreads / kPanel;        // 4
+constexpr int kDiagRows = kPanel / kDiagGroups;           // 32 rows per thread
+
+__global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* __restrict__ probs,
+                                                                 const WorkItem* __restrict__ items, int k) {
   const WorkItem wi = items[blockIdx.x];
   const ProbDev& p = probs[wi.prob];
   const int w = wi.a;
   const int ld = p.npad;
   double* A = p.eps + size_t(w) * ld * ld + size_t(k) * kPanel * ld + size_t(k) * kPanel;
-  __shared__ double rowbuf[2][64];
-  __shared__ double piv[64];
-  __shared__ double invd[64];
-  __shared__ double u[64][65];   // U, then overwritten row by row with W = U^-1
-  __shared__ double red[4][64];
+  __shared__ double rowbuf[2][kPanel];
+  __shared__ double piv[kPanel];
+  __shared__ double invd[kPanel];
   const int t = threadIdx.x;
-  const int l = t & 63;
-  const int i0 = t >> 6;
-  double v[16];
+  const int l = t % kPanel;
+  const int i0 = t / kPanel;
+  double v[kDiagRows];
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int i = i0 + 4 * r;
+  for (int r = 0; r < kDiagRows; ++r) {
+    const int i = i0 + kDiagGroups * r;
     v[r] = (l >= i) ? A[size_t(i) * ld + l] : 0.0;
   }
 #pragma unroll
-  for (int j = 0; j < 64; ++j) {
-    if (i0 == (j & 3)) rowbuf[j & 1][l] = v[j >> 2];
-    __syncthreads();
-    const double pj = rowbuf[j & 1][j];
-    if (t == 0) piv[j] = pj;
-    const double ajl = rowbuf[j & 1][l] / pj;
+  for (int r = 0; r < kDiagRows; ++r) {
 #pragma unroll
-    for (int r = 0; r < 16; ++r) {
-      const int i = i0 + 4 * r;
-      if (i > j && l >= i) v[r] -= rowbuf[j & 1][i] * ajl;
+    for (int q = 0; q < kDiagGroups; ++q) {
+      const int j = kDiagGroups * r + q;
+      if (i0 == q) rowbuf[j & 1][l] = v[r];
+      __syncthreads();
+      const double pj = rowbuf[j & 1][j];
+      if (t == 0) piv[j] = pj;
+      // multiplier row: A part (l > j) or the L^-1 part (l < j); the implicit unit diagonal at l == j
+      const double xj = (l == j ? 1.0 : rowbuf[j & 1][l]) / pj;
+#pragma unroll
+      for (int rr = r; rr < kDiagRows; ++rr) {
+        const int i = i0 + kDiagGroups * rr;
+        if (i > j && (l >= i || l <= j)) v[rr] -= rowbuf[j & 1][i] * xj;
+      }
     }
   }
   __syncthreads();
-  if (t < 64) {
+  if (t < kPanel) {
     const double pv = piv[t];
     if (!(pv > 0.0)) atomicOr(p.err, kErrNotSPD);
     invd[t] = 1.0 / sqrt(pv);
   }
   __syncthreads();
-#pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int i = i0 + 4 * r;
-    const double uv = (l >= i) ? v[r] * invd[i] : 0.0;
-    u[i][l] = uv;
-    if (l >= i) A[size_t(i) * ld + l] = uv;
-  }
-  if (t < 32) {
-    double s = log(piv[t]) + log(piv[t + 32]);
-    s = warp_sum(s);
-    if (t == 0) p.logdet[size_t(w) * p.npanel + k] = s;
-  }
-  __syncthreads();
-  // W = U^-1 by rows, bottom-up, in place of U:
-  //   W_ii = 1/U_ii,  W_ic = -(1/U_ii) sum_{m=i+1..c} U_im W_mc  (rows m > i already hold W).
-  const int c = l, qpart = i0;
-  for (int i = 63; i >= 0; --i) {
-    const double di = 1.0 / u[i][i];
-    if (c > i) {
-      double s = 0.0;
-      for (int m = i + 1 + qpart; m <= c; m += 4) s += u[i][m] * u[m][c];
-      red[qpart][c] = s;
-    }
-    __syncthreads();
-    if (qpart == 0) {
-      if (c == i) u[i][i] = di;
-      else if (c > i) u[i][c] = -(red[0][c] + red[1][c] + red[2][c] + red[3][c]) * di;
-    }
-    __syncthreads();
-  }
   double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
 #pragma unroll
-  for (int r = 0; r < 16; ++r) {
-    const int i = i0 + 4 * r;
-    W[i * kPanel + l] = (l >= i) ? u[i][l] : 0.0;
+  for (int r = 0; r < kDiagRows; ++r) {
+    const int i = i0 + kDiagGroups * r;
+    if (l >= i) A[size_t(i) * ld + l] = v[r] * invd[i];
+    W[l * kPanel + i] = (l < i) ? v[r] * invd[i] : (l == i ? invd[i] : 0.0);
+  }
+  if (t < 32) {
+    double s = 0.0;
+    for (int m = t; m < kPanel; m += 32) s += log(piv[m]);
+    s = warp_sum(s);
+    if (t == 0) p.logdet[size_t(w) * p.npanel + k] = s;
   }
 }
 

@@ -162,6 +162,4 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   return Status::ok();
 }
 
-bool bf16x3_available() { return false; }
-
 }  // namespace rigw

@@ -45,6 +45,8 @@ struct ProbDev {
   const double* zcalc;       // [nc] complex (re, im) evaluation points
   // ---- workspace (device)
   double* mp;
+  void* xs;                  // split precision: [nomega][2][npad][kpad] bf16 hi/lo of M sqrt(D_w)
+  int kpad;                  // transitions padded to the 64-wide tensor-core K tile (== nia_pad)
   double* tnorm;
   double* dscale;
   double* eps;

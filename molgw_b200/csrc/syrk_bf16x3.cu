@@ -1,0 +1,207 @@
+// Split-precision chi0 contraction on the 5th-generation tensor cores.
+//
+//   eps(iw) = 1 + S S^T,   S = M diag(sqrt(D_w)),   S = S_hi + S_lo  (bf16 hi/lo split)
+//   S S^T  ~=  S_hi S_hi^T + S_hi S_lo^T + S_lo S_hi^T     (fp32 accumulation in TMEM)
+//
+// split_bf16x3_kernel: per 64x64 tile of the packed FP64 tensor, scales by
+//   sqrt(D_w(t)) for every frequency and writes the hi/lo bf16 pair in the
+//   K-major (transition-contiguous) layout the tensor cores read.
+// syrk_bf16x3_kernel: one 128x128 upper tile of eps(iw) per CTA.  One thread
+//   issues TMA loads (4 tiles of 128 rows x 64 bf16 per stage, 128-byte
+//   swizzle) into a 3-stage ring, one thread issues tcgen05.mma (M=128, N=128,
+//   K=16; 12 per stage), the four warps then read the fp32 accumulator out of
+//   TMEM, add the identity and store FP64.  All mbarrier waits are bounded.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cudaTypedefs.h>
+
+#include "engine.cuh"
+#include "tc_common.cuh"
+
+namespace rigw {
+
+constexpr int kTcStages = 3;
+constexpr int kTcTileBytes = 128 * 64 * 2;
+constexpr int kTcStageBytes = 4 * kTcTileBytes;
+constexpr size_t kTcSmemBytes = size_t(kTcStages) * kTcStageBytes + 1024 + 256;
+
+// item: (prob, t0, p0); 256 threads.
+__global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __restrict__ probs,
+                                                           const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  const int t0 = wi.a, p0 = wi.b;
+  __shared__ double tile[64][65];   // [P][t]
+  __shared__ double sc[64];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int tt = idx >> 6, pp = idx & 63;
+    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
+  }
+  __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(p.xs);
+  for (int w = 0; w < p.nomega; ++w) {
+    __syncthreads();
+    if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+    __syncthreads();
+    const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
+#pragma unroll
+    for (int pr = 0; pr < 8; ++pr) {
+      const int pp = warp * 8 + pr;
+      const double v0 = tile[pp][2 * lane] * s0, v1 = tile[pp][2 * lane + 1] * s1;
+      const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
+      const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
+      const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
+      const size_t hi_row = (size_t(2 * w) * p.npad + p0 + pp) * p.kpad + t0;
+      const size_t lo_row = (size_t(2 * w + 1) * p.npad + p0 + pp) * p.kpad + t0;
+      reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
+      reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(128, 1) syrk_bf16x3_kernel(const TcItem* __restrict__ items) {
+  const TcItem it = items[blockIdx.x];
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTcStages * kTcStageBytes);
+  uint64_t* empty = full + kTcStages;
+  uint64_t* accum = empty + kTcStages;
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(accum + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto tile = [&](int s, int which) { return smem + s * kTcStageBytes + which * kTcTileBytes; };
+
+  if (tid == 0) {
+    for (int s = 0; s < kTcStages; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    tc::mbar_init(accum, 1);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tslot, 128);
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const int nk = it.ktiles;
+
+  if (tid == 0) {
+    // ---- TMA producer
+    tc::tmap_acquire(it.tmap);
+    int issued[kTcStages] = {0, 0, 0};
+    bool ok = true;
+    for (int kt = 0; kt < nk && ok; ++kt) {
+      const int s = kt % kTcStages;
+      if (kt >= kTcStages && !tc::mbar_wait(&empty[s], ((kt / kTcStages) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      tc::mbar_arrive_expect_tx(&full[s], kTcStageBytes);
+      const int k0 = kt * 64;
+      tc::tma_load_2d(tile(s, 0), it.tmap, &full[s], k0, it.row_a);
+      tc::tma_load_2d(tile(s, 1), it.tmap, &full[s], k0, it.row_a + it.lo_off);
+      tc::tma_load_2d(tile(s, 2), it.tmap, &full[s], k0, it.row_b);
+      tc::tma_load_2d(tile(s, 3), it.tmap, &full[s], k0, it.row_b + it.lo_off);
+      ++issued[s];
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+    // every issued copy has landed before the CTA may exit
+    for (int s = 0; s < kTcStages; ++s)
+      if (issued[s] > 0 && !tc::mbar_wait(&full[s], (issued[s] - 1) & 1)) atomicOr(it.err, kErrTimeout);
+  } else if (tid == 32) {
+    // ---- MMA issuer
+    constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 128);
+    bool ok = true;
+    for (int kt = 0; kt < nk; ++kt) {
+      const int s = kt % kTcStages;
+      if (!tc::mbar_wait(&full[s], (kt / kTcStages) & 1)) {
+        ok = false;
+        break;
+      }
+      tc::tc_fence_after();
+      const uint64_t ah = tc::desc_kmajor_sw128(tile(s, 0)), al = tc::desc_kmajor_sw128(tile(s, 1));
+      const uint64_t bh = tc::desc_kmajor_sw128(tile(s, 2)), bl = tc::desc_kmajor_sw128(tile(s, 3));
+#pragma unroll
+      for (int sub = 0; sub < 4; ++sub) {
+        const uint64_t o = uint64_t(sub * 2);   // 16 bf16 = 32 bytes along K
+        tc::mma_bf16(tmem, ah + o, bh + o, idesc, (kt > 0 || sub > 0) ? 1u : 0u);
+        tc::mma_bf16(tmem, ah + o, bl + o, idesc, 1u);
+        tc::mma_bf16(tmem, al + o, bh + o, idesc, 1u);
+      }
+      tc::mma_commit(&empty[s]);
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+    tc::mma_commit(accum);
+  }
+  __syncwarp();
+  // ---- epilogue: TMEM -> registers -> FP64 eps tile
+  const bool got = __all_sync(0xffffffffu, tc::mbar_wait(accum, 0));
+  tc::tc_fence_after();
+  if (got) {
+    const int row = warp * 32 + lane;
+#pragma unroll 1
+    for (int c0 = 0; c0 < 128; c0 += 32) {
+      uint32_t r[32];
+      tc::tmem_ld_32x32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), r);
+      double* dst = it.C + size_t(row) * it.ldc + c0;
+#pragma unroll
+      for (int j = 0; j < 32; j += 2) {
+        double v0 = double(__uint_as_float(r[j])), v1 = double(__uint_as_float(r[j + 1]));
+        if (c0 + j - row == it.diag) v0 += 1.0;
+        if (c0 + j + 1 - row == it.diag) v1 += 1.0;
+        *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
+      }
+    }
+  } else if (lane == 0) {
+    atomicOr(it.err, kErrTimeout);
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 128);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+namespace {
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
+}
+
+bool bf16x3_available() {
+  if (g_encode) return true;
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return false;
+  }
+  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  return true;
+}
+
+Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows) {
+  if (!bf16x3_available()) return Status::fail(RIGW_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
+  CUtensorMap* m = reinterpret_cast<CUtensorMap*>(host_map);
+  cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
+  cuuint64_t strides[1] = {cuuint64_t(kpad) * 2};
+  cuuint32_t box[2] = {64, 128};
+  cuuint32_t estr[2] = {1, 1};
+  CUresult r = g_encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(xs), dims, strides, box, estr,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) return Status::fail(RIGW_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
+  return Status::ok();
+}
+
+void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
+  if (n > 0) split_bf16x3_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+
+void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s) {
+  if (n > 0) syrk_bf16x3_kernel<<<n, 128, kTcSmemBytes, s>>>(items);
+}
+
+cudaError_t prepare_tc_kernels() {
+  return cudaFuncSetAttribute(syrk_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kTcSmemBytes));
+}
+
+}  // namespace rigw

@@ -262,7 +262,7 @@ class Engine:
 
     # ---------------------------------------------------------------- drop-in pieces
     def polarizability_grid_scalapack(self, inst, precision: int = RIGW_FP64):
-        """Returns (erpa, egw, wpol handle)."""
+        """Returns (erpa, egw, wpol handle) for the W window of ``inst``."""
         p, keep = self.make_problem(inst, precision)
         erpa, egw = C.c_double(), C.c_double()
         w = C.c_void_p()

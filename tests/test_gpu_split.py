@@ -1,0 +1,56 @@
+"""Split-precision chi0 (bf16 hi/lo products on tcgen05, fp32 accumulation) against
+the FP64 path and the oracle.  The eps factorization, Sigma and the QP solve stay
+FP64.  Tolerances:
+  HOMO/LUMO QP energies   |d| <= 1 meV against FP64 (the stated accuracy bar)
+  E_RPA                   |d| <= 1e-4 * |E_RPA|
+  chi(iw)                 |d| <= 1e-4 * max|chi|
+"""
+import numpy as np
+import pytest
+
+from molgw_b200 import synth
+from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64
+from tests.conftest import HA_EV, instance_from_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(engine, inst):
+    a = engine.g0w0(inst, RIGW_FP64)
+    b = engine.g0w0(inst, RIGW_BF16X3)
+    dqp = np.abs(a.energy_qp_g - b.energy_qp_g).max() * HA_EV * 1e3
+    assert dqp <= 1.0, dqp
+    assert abs(a.erpa - b.erpa) <= 1e-4 * abs(a.erpa)
+    return dqp
+
+
+def test_split_precision_synthetic_small(engine, golden_synth):
+    compare(engine, instance_from_golden(golden_synth))
+
+
+def test_split_precision_lih_cc4s(engine, golden_lih):
+    compare(engine, instance_from_golden(golden_lih))
+
+
+def test_split_precision_single_instance_840(engine):
+    dqp = compare(engine, synth.single_instance_840())
+    assert dqp < 0.1      # expected ~1e-3 meV: fp32 accumulation of the 3 bf16 products
+
+
+def test_split_precision_chi_matches_fp64(engine, golden_synth):
+    inst = instance_from_golden(golden_synth)
+    _, _, w64 = engine.polarizability_grid_scalapack(inst, RIGW_FP64)
+    _, _, w16 = engine.polarizability_grid_scalapack(inst, RIGW_BF16X3)
+    c64, c16 = w64.chi(), w16.chi()
+    assert np.abs(c64 - c16).max() <= 1e-4 * np.abs(c64).max()
+    w64.release()
+    w16.release()
+
+
+def test_split_precision_ragged_batch(engine):
+    insts = [synth.make_instance(4, 30, 70, 8, seed=41), synth.make_instance(9, 80, 200, 16, seed=42),
+             synth.make_instance(6, 50, 130, 12, seed=43)]
+    outs = engine.g0w0_batch(insts, RIGW_BF16X3)
+    for inst, o in zip(insts, outs):
+        ref = engine.g0w0(inst, RIGW_FP64)
+        assert np.abs(o.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3 <= 1.0
