@@ -108,6 +108,13 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
     if (s < ktiles) load_stage(s, s);
     cp_async_commit();
   }
+  // Pull the tile read by the epilogue into L2 while the mainloop runs.
+  if (it.Cin != nullptr) {
+    for (int rr = tid; rr < it.m * 2; rr += NT) {
+      const double* line = it.Cin + size_t(rr >> 1) * it.ldc + (rr & 1) * 64;
+      if ((rr & 1) * 64 < it.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+    }
+  }
 
   const int q = lane >> 2;   // fragment row (A) / column (B) within the 8-wide tile
   const int r = lane & 3;    // fragment k index
