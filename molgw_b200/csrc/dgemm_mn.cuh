@@ -110,9 +110,11 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
   }
   // Pull the tile read by the epilogue into L2 while the mainloop runs.
   if (it.Cin != nullptr) {
-    for (int rr = tid; rr < it.m * 2; rr += NT) {
-      const double* line = it.Cin + size_t(rr >> 1) * it.ldc + (rr & 1) * 64;
-      if ((rr & 1) * 64 < it.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
+    constexpr int kLines = BN / 16;   // 128-byte lines per tile row
+    for (int rr = tid; rr < it.m * kLines; rr += NT) {
+      const int col = (rr % kLines) * 16;
+      const double* line = it.Cin + size_t(rr / kLines) * it.ldc + col;
+      if (col < it.n) asm volatile("prefetch.global.L2 [%0];" ::"l"(line));
     }
   }
 
