@@ -167,6 +167,30 @@ RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* res
 /* Many problems of different sizes in one launch sequence (one CUDA graph). */
 RIGW_API int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_result* results);
 
+/* ---- allocation-free variant -------------------------------------------------
+ * No counterpart in the reference.  The continuation + QP equation of
+ * rigw_qp_solve for callers that may not allocate device memory: a host code
+ * with its own device memory pool, an application whose caching allocator owns
+ * the GPU, or a request loop whose memory is reserved up front (cudaMalloc
+ * would also synchronize the device).  Every array is a CUDA device pointer
+ * owned by the caller: sigma_calc [nsig][nomega_sigma_calc][2], e_sig [nsig],
+ * exchange_m_vxc [nsig] or NULL, omega_calc [nomega_sigma_calc][2] or NULL
+ * (then efermi + i*step_sigma_calc*(k-1)); outputs energy_qp_g, energy_qp_z
+ * (or NULL), zz (or NULL) [nsig] and sigma [nsig][2*(nomega_sigma/2)+1][2] (or
+ * NULL).  ``stream`` is a cudaStream_t (NULL: default stream); the call returns
+ * after the work on it is done.  Intermediates live in a fixed 1.06 MiB
+ * device-resident scratch array that every GPU loading the library keeps until
+ * exit; limits: nsig <= 64, nomega_sigma_calc <= 128, 2*(nomega_sigma/2)+1 <=
+ * 1025 (larger sizes return RIGW_ERR_ARG).  The first call on a device looks up
+ * the scratch address (make it before any stream capture).  Calls share the
+ * scratch: calls that overlap on the GPU race.  The message of a failure is
+ * written to errbuf (errlen bytes, may be NULL). */
+RIGW_API int rigw_qp_solve_noalloc(int device, int nsig, int nomega_sigma_calc, const double* omega_calc,
+                                   const double* sigma_calc, const double* e_sig, const double* exchange_m_vxc,
+                                   int technique, int nomega_sigma, double step_sigma, double step_sigma_calc,
+                                   double eta, double efermi, double* energy_qp_g, double* energy_qp_z, double* zz,
+                                   double* sigma, void* stream, char* errbuf, size_t errlen);
+
 #ifdef __cplusplus
 }
 #endif

@@ -93,7 +93,26 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
+    lib.rigw_qp_solve_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_int,
+                                          C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
+                                          C.c_void_p, C.c_char_p, C.c_size_t]
     return lib
+
+
+def qp_solve_noalloc(sigma_calc, e_sig, energy_qp_g, energy_qp_z=None, zz=None, sigma=None, *, device=0,
+                     omega_calc=None, exchange_m_vxc=None, technique=RIGW_PADE, nomega_sigma=101,
+                     step_sigma=0.025, step_sigma_calc=0.075, eta=0.01, efermi=0.0, stream=0):
+    """Continuation + QP equation on caller-owned CUDA tensors, with no device
+    allocation inside the library (``rigw_qp_solve_noalloc``).  ``sigma_calc`` is a
+    [nsig, nc, 2] float64 CUDA tensor; outputs are written in place."""
+    nsig, nc = int(sigma_calc.shape[0]), int(sigma_calc.shape[1])
+    buf = C.create_string_buffer(512)
+    rc = lib().rigw_qp_solve_noalloc(device, nsig, nc, _ptr(omega_calc), _ptr(sigma_calc), _ptr(e_sig),
+                                     _ptr(exchange_m_vxc), technique, nomega_sigma, step_sigma, step_sigma_calc,
+                                     eta, efermi, _ptr(energy_qp_g), _ptr(energy_qp_z), _ptr(zz), _ptr(sigma),
+                                     C.c_void_p(stream), buf, 512)
+    if rc:
+        raise RigwError(rc, buf.value.decode())
 
 
 _LIB: C.CDLL | None = None
