@@ -63,6 +63,9 @@ enum rigw_technique {
 };
 
 #define RIGW_PROBLEM_DEVICE_POINTERS 1
+/* Compute only what the QP energies need: skips the tr eps^-1 solve behind
+ * 'GW  correlation energy' (egw is returned as NaN); E_RPA is still computed. */
+#define RIGW_PROBLEM_QP_ONLY 2
 
 typedef struct rigw_ctx rigw_ctx;
 typedef struct rigw_wpol rigw_wpol;

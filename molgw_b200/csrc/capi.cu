@@ -112,7 +112,7 @@ const char* rigw_last_error(const rigw_ctx* ctx) {
 }
 
 size_t rigw_footprint_bytes(int naux, int nocc, int nvirt, int nomega, int nstate_p, int nsig, int precision) {
-  Shape sh{naux, nocc, nvirt, nomega, nstate_p, nsig, 0, 0, 0, precision};
+  Shape sh{naux, nocc, nvirt, nomega, nstate_p, nsig, 0, 0, 0, precision, 0};
   return rigw::footprint(sh, rigw::kPlanFused);
 }
 

@@ -32,23 +32,23 @@ struct GemmItem {
   double alpha, beta;
 };
 
-template <int BM, int BN>
+template <int BM, int BN, int ST = 3>
 struct DgemmCfg {
   static constexpr int kWarpsM = BM / 64;
   static constexpr int kWarpsN = BN / 32;
   static constexpr int kThreads = kWarpsM * kWarpsN * 32;
   static constexpr int kBK = 16;
-  static constexpr int kStages = 3;
+  static constexpr int kStages = ST;
   static constexpr int kLdaS = BM + 2;   // == 2 (mod 16): conflict-free 128-bit A fragment loads
   static constexpr int kLdbS = BN + 4;   // == 4 (mod 16): conflict-free 64-bit B fragment loads
   static constexpr int kStageDoubles = kBK * kLdaS + kBK * kLdbS + kBK;
   static constexpr size_t kSmemBytes = size_t(kStages) * kStageDoubles * sizeof(double);
 };
 
-template <int BM, int BN>
-__global__ void __launch_bounds__(DgemmCfg<BM, BN>::kThreads, 1)
+template <int BM, int BN, int STAGES = 3>
+__global__ void __launch_bounds__(DgemmCfg<BM, BN, STAGES>::kThreads, 1)
 dgemm_mn_kernel(const GemmItem* __restrict__ items) {
-  using Cfg = DgemmCfg<BM, BN>;
+  using Cfg = DgemmCfg<BM, BN, STAGES>;
   constexpr int BK = Cfg::kBK;
   constexpr int ST = Cfg::kStages;
   constexpr int NT = Cfg::kThreads;

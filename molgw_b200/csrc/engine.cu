@@ -16,9 +16,9 @@ inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
 
 // ---------------------------------------------------------------------------
 bool Shape::operator<(const Shape& o) const {
-  return std::tie(naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision) <
+  return std::tie(naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision, qp_only) <
          std::tie(o.naux, o.nocc, o.nvirt, o.nomega, o.nstate_p, o.nsig, o.nc, o.nsigma_half, o.technique,
-                  o.precision);
+                  o.precision, o.qp_only);
 }
 
 Status make_shape(const rigw_problem& p, Shape* sh) {
@@ -43,6 +43,7 @@ Status make_shape(const rigw_problem& p, Shape* sh) {
   sh->nsigma_half = p.nomega_sigma / 2;
   sh->technique = p.technique;
   sh->precision = p.precision;
+  sh->qp_only = (p.flags & RIGW_PROBLEM_QP_ONLY) ? 1 : 0;
   return Status::ok();
 }
 
@@ -106,7 +107,7 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   d.npanel = d.npad / kPanel;
   d.nia = sh.nocc * sh.nvirt;
   d.nia_pad = round_up(std::max(d.nia, 1), 64);
-  d.want_identity = (mode == kPlanFused || mode == kPlanPolar) ? 1 : 0;
+  d.want_identity = (mode == kPlanPolar || (mode == kPlanFused && !sh.qp_only)) ? 1 : 0;
   d.moff = d.want_identity ? d.npad : 0;
   d.ncm = (mode == kPlanFused || mode == kPlanSigma) ? round_up(sh.nsig * sh.nstate_p, 8) : 0;
   d.ldb = d.moff + d.ncm;
@@ -153,6 +154,9 @@ Plan::~Plan() {
   }
   for (auto& e : stage_ev_)
     if (e) cudaEventDestroy(e);
+  for (auto& e : la_ev_)
+    if (e) cudaEventDestroy(e);
+  if (aux_stream_) cudaStreamDestroy(aux_stream_);
 }
 
 Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
@@ -172,7 +176,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // ---- memory layout
   Layout L;
   struct Off {
-    size_t mp, xs, tmap, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, en, sc, sr, qp;
+    size_t mp, xs, tmap, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, tr, en, sc, sr, qp;
   };
   std::vector<Off> off(np);
   for (int i = 0; i < np; ++i) {
@@ -199,6 +203,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       off[i].winv = L.take(size_t(sh.nomega) * d.npanel * kPanel * kPanel * D);
       off[i].logdet = L.take(size_t(sh.nomega) * d.npanel * D);
       off[i].ew = L.take(size_t(sh.nomega) * 2 * D);
+      off[i].tr = L.take(size_t(sh.nomega) * D);
       off[i].en = L.take(2 * D);
     }
     if (sigma) {
@@ -272,6 +277,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       p.winv = dp(off[i].winv);
       p.logdet = dp(off[i].logdet);
       p.ew = dp(off[i].ew);
+      p.treps = dp(off[i].tr);
       p.out_energies = dp(off[i].en);
     } else if (mode == kPlanSigma) {
       const ProbDev& f = *factors[i];
@@ -297,12 +303,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   }
 
   // ---- work lists
-  const int BMN = 128;
+  const int BMN = 128;   // column width of every DMMA item
+  const int BM = 64;     // row height of the chi0 and trailing-update items
   int max_panels = 0;
   for (int i = 0; i < np; ++i) max_panels = std::max(max_panels, probs_[i].dev.npanel);
   wl_diag_.assign(max_panels, {});
   gl_k2_.assign(max_panels, {});
   gl_k3_.assign(max_panels, {});
+  gl_k3d_.assign(max_panels, {});
   for (int i = 0; i < np; ++i) {
     const Shape& sh = shapes[i];
     const ProbDev& p = probs_[i].dev;
@@ -328,10 +336,11 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
               tl_syrk_.push_back(t);
             }
       }
+      // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM)
       for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
         double* E = p.eps + size_t(w) * npad * npad;
-        for (int ti = 0; ti < npad; ti += BMN)
-          for (int tj = ti; tj < npad; tj += BMN) {
+        for (int ti = 0; ti < npad; ti += BM)
+          for (int tj = ti / BMN * BMN; tj < npad; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
             g.B = p.mp + tj;
@@ -339,7 +348,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             g.C = E + size_t(ti) * npad + tj;
             g.ldc = npad;
             g.kscale = p.dscale + size_t(w) * p.nia_pad;
-            g.m = std::min(BMN, npad - ti);
+            g.m = std::min(BM, npad - ti);
             g.n = std::min(BMN, npad - tj);
             g.k = p.nia_pad;
             g.flags = kAddIdentity;
@@ -349,6 +358,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             gl_syrk_.push_back(g);
           }
       }
+      for (int w = 0; w < sh.nomega; ++w) wl_trace_.push_back({i, w, 0, 0});
     }
     if (ldb > 0) {
       for (int i0 = 0; i0 < npad; i0 += 32)
@@ -384,8 +394,11 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         if (p.want_identity)
           for (int c0 = 0; c0 < r0; c0 += BMN) k2(R, ldb, c0, std::min(BMN, r0 - c0), cs + c0);
         for (int c0 = p.moff; c0 < ldb; c0 += BMN) k2(R, ldb, c0, std::min(BMN, ldb - c0), cs + c0);
-        // trailing update of panel k
-        auto k3 = [&](const double* Bsrc, int ldbs, double* Cdst, int ldc, int i0, int c0, int m, int n) {
+        // trailing update of panel k, in 64-row items; the items of the next
+        // diagonal block go to their own list so that its factorization can start
+        // while the rest of the update runs (lookahead)
+        auto k3 = [&](const double* Bsrc, int ldbs, double* Cdst, int ldc, int i0, int c0, int m, int n,
+                      bool next_diag) {
           GemmItem g{};
           g.A = E + size_t(k) * kPanel * npad + i0;
           g.lda = npad;
@@ -399,15 +412,17 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.k = kPanel;
           g.alpha = -1.0;
           g.beta = 1.0;
-          gl_k3_[k].push_back(g);
+          (next_diag ? gl_k3d_[k] : gl_k3_[k]).push_back(g);
         };
-        for (int i0 = r0; i0 < npad; i0 += BMN) {
-          const int m = std::min(BMN, npad - i0);
+        for (int i0 = r0; i0 < npad; i0 += BM) {
+          const int m = std::min(BM, npad - i0);
           if (factor)
-            for (int j0 = i0; j0 < npad; j0 += BMN) k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0));
+            for (int j0 = i0 / BMN * BMN; j0 < npad; j0 += BMN)
+              k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0), i0 < r0 + kPanel && j0 == r0);
           if (p.want_identity)
-            for (int c0 = 0; c0 < r0; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, r0 - c0));
-          for (int c0 = p.moff; c0 < ldb; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, ldb - c0));
+            for (int c0 = 0; c0 < r0; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, r0 - c0), false);
+          for (int c0 = p.moff; c0 < ldb; c0 += BMN)
+            k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, ldb - c0), false);
         }
       }
     }
@@ -436,11 +451,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     size_t bytes;
     int count;
     int arg;
+    int stream, wait_ev, rec_ev;
   };
   std::vector<Pending> pend;
-  auto add = [&](int kind, const void* src, size_t elem, size_t n, int arg) {
-    if (n == 0) return;
-    pend.push_back({kind, src, elem * n, int(n), arg});
+  auto add = [&](int kind, const void* src, size_t elem, size_t n, int arg, int stream = 0, int wait_ev = -1,
+                 int rec_ev = -1) {
+    if (n == 0) return false;
+    pend.push_back({kind, src, elem * n, int(n), arg, stream, wait_ev, rec_ev});
+    return true;
   };
   add(0, wl_pack_.data(), sizeof(WorkItem), wl_pack_.size(), 0);
   add(2, wl_rhs_.data(), sizeof(WorkItem), wl_rhs_.size(), 0);
@@ -448,13 +466,23 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
   add(12, wl_split_.data(), sizeof(WorkItem), wl_split_.size(), 0);
   add(13, tl_syrk_.data(), sizeof(TcItem), tl_syrk_.size(), 0);
+  add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
+  // Panel loop with a one-panel lookahead: the update of the next diagonal block
+  // (K3d) goes first, then its factorization runs on the second stream while the
+  // rest of the trailing update (K3) runs on the first.
+  int pending_join = -1;
   for (int k = 0; k < max_panels; ++k) {
-    add(4, wl_diag_[k].data(), sizeof(WorkItem), wl_diag_[k].size(), k);
-    add(5, gl_k2_[k].data(), sizeof(GemmItem), gl_k2_[k].size(), k);
+    if (k == 0) add(4, wl_diag_[0].data(), sizeof(WorkItem), wl_diag_[0].size(), 0);
+    add(5, gl_k2_[k].data(), sizeof(GemmItem), gl_k2_[k].size(), k, 0, pending_join);
+    pending_join = -1;
+    const bool next = k + 1 < max_panels && !wl_diag_[k + 1].empty();
+    add(14, gl_k3d_[k].data(), sizeof(GemmItem), gl_k3d_[k].size(), k, 0, -1, next ? 2 * k : -1);
+    if (next && add(4, wl_diag_[k + 1].data(), sizeof(WorkItem), wl_diag_[k + 1].size(), k + 1, 1, 2 * k, 2 * k + 1))
+      pending_join = 2 * k + 1;
     add(6, gl_k3_[k].data(), sizeof(GemmItem), gl_k3_[k].size(), k);
   }
-  add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0);
-  if (factor) pend.push_back({8, nullptr, 0, np, 0});
+  add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0, 0, pending_join);
+  if (factor) pend.push_back({8, nullptr, 0, np, 0, 0, -1, -1});
   add(9, wl_vchiv_.data(), sizeof(WorkItem), wl_vchiv_.size(), 0);
   add(10, wl_sigma_.data(), sizeof(WorkItem), wl_sigma_.size(), 0);
   add(11, wl_pade_.data(), sizeof(WorkItem), wl_pade_.size(), 0);
@@ -464,10 +492,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   std::vector<char> host(lbytes);
   for (size_t j = 0; j < pend.size(); ++j) {
     if (pend[j].bytes) std::memcpy(host.data() + offs[j], pend[j].src, pend[j].bytes);
-    seq_.push_back({pend[j].kind, offs[j], pend[j].count, pend[j].arg});
+    seq_.push_back({pend[j].kind, offs[j], pend[j].count, pend[j].arg, pend[j].stream, pend[j].wait_ev,
+                    pend[j].rec_ev});
   }
   RIGW_CUDA_TRY(cudaMemcpy(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice));
   for (auto& e : stage_ev_) RIGW_CUDA_TRY(cudaEventCreate(&e));
+  la_ev_.assign(2 * std::max(max_panels, 1), nullptr);
+  for (auto& e : la_ev_) RIGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+  RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking));
   host_table_.resize(np);
   n_launches_ = int(seq_.size());
   return Status::ok();
@@ -479,28 +511,32 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: case 12: case 13: return 1;
-    case 4: case 5: case 6: return 2;
+    case 1: case 12: case 13: case 15: return 1;
+    case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
 }
 
-void Plan::record(cudaStream_t s, int stage) {
+void Plan::record(cudaStream_t s0, int stage) {
   char* lb = lists_.data();
   for (const Launch& L : seq_) {
     if (stage >= 0 && stage_of(L.kind) != stage) continue;
+    cudaStream_t s = L.stream ? aux_stream_ : s0;
+    if (L.wait_ev >= 0) cudaStreamWaitEvent(s, la_ev_[L.wait_ev], 0);
     const WorkItem* wl = reinterpret_cast<const WorkItem*>(lb + L.off);
     const GemmItem* gl = reinterpret_cast<const GemmItem*>(lb + L.off);
     switch (L.kind) {
       case 0: pack_m_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
-      case 1: launch_dgemm_128x128(gl, L.count, s); break;
+      case 1: launch_dgemm_64x128(gl, L.count, s); break;
+      case 14: launch_dgemm_64x128(gl, L.count, s); break;
+      case 15: trace_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
       case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 4: chol_diag_kernel<<<L.count, kDiagThreads, 0, s>>>(probs_dev_, wl, L.arg); break;
       case 5: launch_dgemm_128x128(gl, L.count, s); break;
-      case 6: launch_dgemm_128x128(gl, L.count, s); break;
+      case 6: launch_dgemm_64x128(gl, L.count, s); break;
       case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 8: energy_sum_kernel<<<(L.count + 127) / 128, 128, 0, s>>>(probs_dev_, L.count); break;
       case 9: vchiv_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
@@ -508,6 +544,7 @@ void Plan::record(cudaStream_t s, int stage) {
       case 11: pade_qp_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       default: break;
     }
+    if (L.rec_ev >= 0) cudaEventRecord(la_ev_[L.rec_ev], s);
   }
 }
 

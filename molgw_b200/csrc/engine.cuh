@@ -72,6 +72,7 @@ class DeviceBuffer {
 // Shapes of one problem of a plan (derived from rigw_problem).
 struct Shape {
   int naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision;
+  int qp_only;
   bool operator<(const Shape& o) const;
 };
 
@@ -128,13 +129,19 @@ class Plan {
   std::vector<GemmItem> gl_syrk_;
   std::vector<WorkItem> wl_split_;
   std::vector<TcItem> tl_syrk_;
-  std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_;
+  std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_;
+  std::vector<WorkItem> wl_trace_;
   struct Launch {
     int kind;        // see Plan::record
     size_t off;      // byte offset of the list in lists_
     int count;
     int arg;
+    int stream;      // 0: the plan's stream, 1: the lookahead stream
+    int wait_ev;     // lookahead event to wait for before the launch (-1: none)
+    int rec_ev;      // lookahead event to record after the launch (-1: none)
   };
+  std::vector<cudaEvent_t> la_ev_;
+  cudaStream_t aux_stream_ = nullptr;
   std::vector<Launch> seq_;
   cudaGraph_t stage_graph_[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaGraphExec_t stage_exec_[4] = {nullptr, nullptr, nullptr, nullptr};

@@ -18,6 +18,7 @@ __global__ void mnorm_kernel(const ProbDev* probs, const WorkItem* items);
 constexpr int kDiagThreads = 512;  // threads of chol_diag_kernel (kPanel columns x 4 row groups)
 __global__ void chol_diag_kernel(const ProbDev* probs, const WorkItem* items, int k);
 __global__ void energy_kernel(const ProbDev* probs, const WorkItem* items);
+__global__ void trace_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void vchiv_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void sigma_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void pade_qp_kernel(const ProbDev* probs, const WorkItem* items);

@@ -214,10 +214,9 @@ __global__ void __launch_bounds__(256) energy_kernel(const ProbDev* __restrict__
   const ProbDev& p = probs[wi.prob];
   const int w = wi.a;
   __shared__ double red[8];
-  double s = 0.0;
-  const double* ds = p.dscale + size_t(w) * p.nia_pad;
-  for (int t = threadIdx.x; t < p.nia_pad; t += 256) s += ds[t] * p.tnorm[t];
-  const double treps = p.npad + block_sum_256(s, red);
+  // tr eps from the matrix that was factorized (so that ln det and tr use the
+  // same eps in the split-precision mode; in FP64 this equals npad + sum_t D |M_t|^2)
+  const double treps = p.treps[w];
   double trinv = 0.0;
   if (p.want_identity) {
     double q = 0.0;
@@ -232,8 +231,23 @@ __global__ void __launch_bounds__(256) energy_kernel(const ProbDev* __restrict__
     double ld = 0.0;
     for (int k = 0; k < p.npanel; ++k) ld += p.logdet[size_t(w) * p.npanel + k];
     p.ew[2 * w + 0] = ld + p.npad - treps;
-    p.ew[2 * w + 1] = p.want_identity ? (2.0 * p.npad - trinv - treps) : 0.0;
+    p.ew[2 * w + 1] = p.want_identity ? (2.0 * p.npad - trinv - treps) : __longlong_as_double(0x7ff8000000000000ll);
   }
+}
+
+// tr eps(iw) = sum of the diagonal of eps as built by the chi0 stage, before the
+// factorization overwrites it.  item: (prob, w).
+__global__ void __launch_bounds__(256) trace_kernel(const ProbDev* __restrict__ probs,
+                                                    const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  const int w = wi.a;
+  __shared__ double red[8];
+  const double* E = p.eps + size_t(w) * p.npad * p.npad;
+  double s = 0.0;
+  for (int i = threadIdx.x; i < p.npad; i += 256) s += E[size_t(i) * p.npad + i];
+  s = block_sum_256(s, red);
+  if (threadIdx.x == 0) p.treps[w] = s;
 }
 
 // v(p, m, w) = M_pm^T chi(iw) M_pm = |U^-T M_pm|^2 - |M_pm|^2  (chi = eps^-1 - 1).

@@ -57,6 +57,7 @@ struct ProbDev {
   double* mnorm;
   double* vchiv;
   double* ew;
+  double* treps;             // [nomega] tr eps(iw), summed from the matrix that is factorized
   // ---- outputs (device)
   double* out_energies;      // [2]  erpa, egw
   double* sigma_calc;        // [nsig][nc] complex

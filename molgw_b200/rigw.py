@@ -30,6 +30,7 @@ RIGW_BF16X3 = 1
 RIGW_PADE = 0
 RIGW_HOMOLUMO = 1
 RIGW_PROBLEM_DEVICE_POINTERS = 1
+RIGW_PROBLEM_QP_ONLY = 2
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_NOT_SPD", 5: "ERR_NUMERIC",
                 6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED"}
 
@@ -196,7 +197,7 @@ class Engine:
 
     # ---------------------------------------------------------------- problems
     def make_problem(self, inst, precision: int = RIGW_FP64, device_arrays: dict | None = None,
-                     technique: int = RIGW_PADE) -> tuple[Problem, list]:
+                     technique: int = RIGW_PADE, qp_only: bool = False) -> tuple[Problem, list]:
         """Problem descriptor for a ``molgw_b200.synth.GWInstance``-like object.
 
         ``device_arrays`` maps field names to CUDA tensors that replace the host
@@ -236,7 +237,7 @@ class Engine:
         p.eta = inst.eta
         p.efermi = efermi
         p.precision = precision
-        p.flags = flags
+        p.flags = flags | (RIGW_PROBLEM_QP_ONLY if qp_only else 0)
         keep = [arrs, occ_sig]
         return p, keep
 
@@ -261,13 +262,15 @@ class Engine:
                           r.ehomo, r.elumo, r.device_ms)
 
     # ---------------------------------------------------------------- fused
-    def g0w0_batch(self, insts, precision: int = RIGW_FP64, device_arrays=None) -> list[G0W0Output]:
+    def g0w0_batch(self, insts, precision: int = RIGW_FP64, device_arrays=None,
+                   qp_only: bool = False) -> list[G0W0Output]:
         n = len(insts)
         probs = (Problem * n)()
         ress = (Result * n)()
         keep, bufs = [], []
         for i, inst in enumerate(insts):
-            p, k = self.make_problem(inst, precision, device_arrays[i] if device_arrays else None)
+            p, k = self.make_problem(inst, precision, device_arrays[i] if device_arrays else None,
+                                     qp_only=qp_only)
             probs[i] = p
             keep.append(k)
             r, b = self._alloc_result(p)
@@ -276,8 +279,8 @@ class Engine:
         self._check(self._lib.rigw_g0w0_batch(self._h, n, probs, ress), "rigw_g0w0_batch")
         return [self._output(ress[i], bufs[i]) for i in range(n)]
 
-    def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None) -> G0W0Output:
-        return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None)[0]
+    def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False) -> G0W0Output:
+        return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None, qp_only)[0]
 
     # ---------------------------------------------------------------- drop-in pieces
     def polarizability_grid_scalapack(self, inst, precision: int = RIGW_FP64):

@@ -102,6 +102,16 @@ def test_ragged_batch_equals_single_solves(engine):
         assert np.abs(b.energy_qp_g - s.energy_qp_g).max() < 1e-13
 
 
+def test_qp_only_mode_gives_the_same_qp_energies(engine, golden_synth):
+    """RIGW_PROBLEM_QP_ONLY skips the tr eps^-1 solve (E_GW); every other output is unchanged."""
+    inst = instance_from_golden(golden_synth)
+    full = engine.g0w0(inst)
+    lean = engine.g0w0(inst, qp_only=True)
+    assert np.isnan(lean.egw) and lean.erpa == full.erpa
+    assert np.array_equal(lean.sigma_calc, full.sigma_calc)
+    assert np.array_equal(lean.energy_qp_g, full.energy_qp_g)
+
+
 def test_repeat_runs_are_bitwise_identical(engine, golden_synth):
     inst = instance_from_golden(golden_synth)
     a = engine.g0w0(inst)
