@@ -336,11 +336,13 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
               tl_syrk_.push_back(t);
             }
       }
-      // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM)
+      // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM),
+      // over the naux x naux block only; the identity pads are written afterwards
       for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
         double* E = p.eps + size_t(w) * npad * npad;
-        for (int ti = 0; ti < npad; ti += BM)
-          for (int tj = ti / BMN * BMN; tj < npad; tj += BMN) {
+        if (npad > sh.naux) wl_pad_.push_back({i, w, 0, 0});
+        for (int ti = 0; ti < sh.naux; ti += BM)
+          for (int tj = ti / BMN * BMN; tj < sh.naux; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
             g.B = p.mp + tj;
@@ -348,8 +350,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             g.C = E + size_t(ti) * npad + tj;
             g.ldc = npad;
             g.kscale = p.dscale + size_t(w) * p.nia_pad;
-            g.m = std::min(BM, npad - ti);
-            g.n = std::min(BMN, npad - tj);
+            g.m = std::min(BM, sh.naux - ti);
+            g.n = std::min(BMN, sh.naux - tj);
             g.k = p.nia_pad;
             g.flags = kAddIdentity;
             g.diag = ti - tj;
@@ -466,6 +468,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
   add(12, wl_split_.data(), sizeof(WorkItem), wl_split_.size(), 0);
   add(13, tl_syrk_.data(), sizeof(TcItem), tl_syrk_.size(), 0);
+  add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
   // Panel loop with a one-panel lookahead: the update of the next diagonal block
   // (K3d) goes first, then its factorization runs on the second stream while the
@@ -511,7 +514,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: case 12: case 13: case 15: return 1;
+    case 1: case 12: case 13: case 15: case 16: return 1;
     case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
@@ -530,6 +533,7 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 1: launch_dgemm_64x128(gl, L.count, s); break;
       case 14: launch_dgemm_64x128(gl, L.count, s); break;
       case 15: trace_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
+      case 16: pad_eps_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
       case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;

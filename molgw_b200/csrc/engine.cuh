@@ -130,7 +130,7 @@ class Plan {
   std::vector<WorkItem> wl_split_;
   std::vector<TcItem> tl_syrk_;
   std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_;
-  std::vector<WorkItem> wl_trace_;
+  std::vector<WorkItem> wl_trace_, wl_pad_;
   struct Launch {
     int kind;        // see Plan::record
     size_t off;      // byte offset of the list in lists_

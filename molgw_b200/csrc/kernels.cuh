@@ -19,6 +19,7 @@ constexpr int kDiagThreads = 512;  // threads of chol_diag_kernel (kPanel column
 __global__ void chol_diag_kernel(const ProbDev* probs, const WorkItem* items, int k);
 __global__ void energy_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void trace_kernel(const ProbDev* probs, const WorkItem* items);
+__global__ void pad_eps_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void vchiv_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void sigma_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void pade_qp_kernel(const ProbDev* probs, const WorkItem* items);

@@ -235,6 +235,20 @@ __global__ void __launch_bounds__(256) energy_kernel(const ProbDev* __restrict__
   }
 }
 
+// Identity in the padded rows/columns of eps(iw) (upper part, columns >= naux):
+// the FP64 chi0 items cover the naux x naux block only.  item: (prob, w).
+__global__ void __launch_bounds__(256) pad_eps_kernel(const ProbDev* __restrict__ probs,
+                                                      const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  double* E = p.eps + size_t(wi.a) * p.npad * p.npad;
+  const int npadc = p.npad - p.naux;
+  for (int idx = threadIdx.x; idx < npadc * p.npad; idx += 256) {
+    const int j = p.naux + idx / p.npad, i = idx % p.npad;
+    if (i <= j) E[size_t(i) * p.npad + j] = (i == j) ? 1.0 : 0.0;
+  }
+}
+
 // tr eps(iw) = sum of the diagonal of eps as built by the chi0 stage, before the
 // factorization overwrites it.  item: (prob, w).
 __global__ void __launch_bounds__(256) trace_kernel(const ProbDev* __restrict__ probs,
