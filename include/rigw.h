@@ -123,6 +123,8 @@ typedef struct rigw_stats {
   int kernel_launches;       /* kernels launched by the last solve                        */
   int graph_replayed;        /* 1 when the launch sequence was a CUDA-graph replay        */
   size_t device_bytes_in_use, device_bytes_peak;
+  int chunks;                /* problem-frequency chunks the batch was split into      */
+  int waves;                 /* plans run one after the other under the memory budget  */
 } rigw_stats;
 
 /* ---- context ---------------------------------------------------------------- */

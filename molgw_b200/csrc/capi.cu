@@ -36,24 +36,15 @@ Status run_batch(Context& c, rigw::PlanMode mode, int n, const rigw_problem* pro
   for (int i = 0; i < n; ++i)
     if (probs[i].precision != RIGW_FP64 && !rigw::bf16x3_available())
       return Status::fail(RIGW_ERR_UNSUPPORTED, "precision %d not available", probs[i].precision);
-  Plan* plan = nullptr;
-  std::unique_ptr<Plan> fresh;
-  if (mode == rigw::kPlanFused && !owned_plan) {
-    auto it = c.fused_cache.find(shapes);
-    if (it == c.fused_cache.end()) {
-      if (c.fused_cache.size() >= 4) c.fused_cache.clear();
-      fresh.reset(new Plan());
-      RIGW_TRY(fresh->build(&c, mode, shapes, factors));
-      plan = fresh.get();
-      c.fused_cache.emplace(shapes, std::move(fresh));
-    } else {
-      plan = it->second.get();
-    }
-  } else {
+  std::unique_ptr<Plan> fresh(new Plan());
+  Status bs = fresh->build(&c, mode, shapes, factors);
+  if (bs.code == RIGW_ERR_NOMEM && !c.plan_cache.empty()) {   // cached plans hold memory: drop them, retry once
+    c.plan_cache.clear();
     fresh.reset(new Plan());
-    RIGW_TRY(fresh->build(&c, mode, shapes, factors));
-    plan = fresh.get();
+    bs = fresh->build(&c, mode, shapes, factors);
   }
+  RIGW_TRY(bs);
+  Plan* plan = fresh.get();
   RIGW_TRY(plan->stage_inputs(probs, c.stream));
   if (sigma_in)
     for (int i = 0; i < n; ++i) RIGW_TRY(plan->stage_sigma_calc(i, sigma_in[i], c.stream));
@@ -66,6 +57,8 @@ Status run_batch(Context& c, rigw::PlanMode mode, int n, const rigw_problem* pro
   st.graph_replayed = plan->replayed() ? 1 : 0;
   st.device_bytes_in_use = c.in_use;
   st.device_bytes_peak = c.peak;
+  st.chunks = n;
+  st.waves = 1;
   RIGW_TRY(err);
   if (res) RIGW_TRY(plan->fetch_results(probs, res, c.stream));
   if (owned_plan) *owned_plan = std::move(fresh);
@@ -127,7 +120,7 @@ int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_re
   if (nprob <= 0 || !probs || !results) return finish(ctx, Status::fail(RIGW_ERR_ARG, "empty batch"));
   std::lock_guard<std::mutex> lock(ctx->impl.mu);
   cudaSetDevice(ctx->impl.device);
-  return finish(ctx, run_batch(ctx->impl, rigw::kPlanFused, nprob, probs, results, nullptr, {}, nullptr));
+  return finish(ctx, rigw::solve_batch(ctx->impl, nprob, probs, results));
 }
 
 int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result) {

@@ -90,7 +90,7 @@ Status Context::init(int dev, size_t budget_bytes) {
 }
 
 Context::~Context() {
-  fused_cache.clear();
+  plan_cache.clear();
   if (stream) cudaStreamDestroy(stream);
 }
 
@@ -107,9 +107,11 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   d.npanel = d.npad / kPanel;
   d.nia = sh.nocc * sh.nvirt;
   d.nia_pad = round_up(std::max(d.nia, 1), 64);
-  d.want_identity = (mode == kPlanPolar || (mode == kPlanFused && !sh.qp_only)) ? 1 : 0;
+  d.want_identity =
+      (mode == kPlanPolar || ((mode == kPlanFused || mode == kPlanPartial) && !sh.qp_only)) ? 1 : 0;
   d.moff = d.want_identity ? d.npad : 0;
-  d.ncm = (mode == kPlanFused || mode == kPlanSigma) ? round_up(sh.nsig * sh.nstate_p, 8) : 0;
+  d.ncm = (mode == kPlanFused || mode == kPlanSigma || mode == kPlanPartial) ? round_up(sh.nsig * sh.nstate_p, 8)
+                                                                               : 0;
   d.ldb = d.moff + d.ncm;
   d.nreal = 2 * sh.nsigma_half + 1;
   return d;
@@ -127,25 +129,7 @@ struct Layout {
 
 }  // namespace
 
-size_t footprint(const Shape& sh, PlanMode mode) {
-  const Dims d = dims_of(sh, mode);
-  const size_t D = sizeof(double);
-  size_t b = 0;
-  const bool factor = (mode == kPlanFused || mode == kPlanPolar);
-  const bool sigma = (mode == kPlanFused || mode == kPlanSigma);
-  if (factor) {
-    b += size_t(d.nia) * sh.naux * D;                    // staged M
-    b += size_t(d.nia_pad) * d.npad * D;                 // packed M
-    b += size_t(sh.nomega) * d.nia_pad * D;              // D_w(t)
-    b += size_t(sh.nomega) * d.npad * d.npad * D;        // eps / U
-    b += size_t(sh.nomega) * d.npanel * kPanel * kPanel * D;
-  }
-  if (sigma) b += size_t(sh.nsig) * sh.nstate_p * sh.naux * D;
-  b += size_t(sh.nomega) * d.npad * d.ldb * D;           // rhs
-  b += size_t(sh.nomega) * d.npanel * d.ldb * D;         // colsq
-  b += size_t(sh.nomega) * d.ncm * D * 2;
-  return b + (1u << 20);
-}
+size_t footprint(const Shape& sh, PlanMode mode) { return Plan::measure({sh}, mode); }
 
 Plan::~Plan() {
   for (int st = 0; st < 4; ++st) {
@@ -159,17 +143,24 @@ Plan::~Plan() {
   if (aux_stream_) cudaStreamDestroy(aux_stream_);
 }
 
+size_t Plan::measure(const std::vector<Shape>& shapes, PlanMode mode) {
+  Plan p;
+  size_t bytes = 0;
+  Status s = p.build(nullptr, mode, shapes, {}, &bytes);
+  return s.good() ? bytes : size_t(-1);
+}
+
 Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
-                   const std::vector<const ProbDev*>& factors) {
+                   const std::vector<const ProbDev*>& factors, size_t* measure_only) {
   ctx_ = ctx;
   mode_ = mode;
   shapes_ = shapes;
   const int np = int(shapes.size());
   probs_.assign(np, PlanProblem{});
-  const bool factor = (mode == kPlanFused || mode == kPlanPolar);
-  const bool sigma = (mode == kPlanFused || mode == kPlanSigma);
+  const bool factor = (mode == kPlanFused || mode == kPlanPolar || mode == kPlanPartial);
+  const bool sigma = (mode == kPlanFused || mode == kPlanSigma || mode == kPlanPartial);
   const bool qp = (mode == kPlanFused || mode == kPlanQP);
-  if (mode == kPlanSigma && int(factors.size()) != np)
+  if (mode == kPlanSigma && int(factors.size()) != np && !measure_only)
     return Status::fail(RIGW_ERR_ARG, "sigma plan needs resident factors");
   const size_t D = sizeof(double);
 
@@ -233,6 +224,17 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   }
   const size_t table_off = L.take(sizeof(ProbDev) * np);
   const size_t err_off = L.take(sizeof(int));
+  if (measure_only) {
+    // arena + a bound on the work lists (tiles of every stage, all frequencies)
+    size_t lists = 0;
+    for (const Shape& sh : shapes) {
+      const Dims d = dims_of(sh, mode);
+      const size_t t = size_t(d.npanel + 2) * (d.npanel + 2 + (d.ldb + 127) / 128) * 4;
+      lists += size_t(sh.nomega) * t * sizeof(GemmItem) + size_t(d.nia_pad / 8 + d.npad * d.ldb / 1024 + 64) * 16;
+    }
+    *measure_only = L.cur + lists + (size_t(1) << 20);
+    return Status::ok();
+  }
   RIGW_TRY(arena_.allocate(ctx, L.cur, "plan arena"));
   char* base = arena_.data();
   probs_dev_ = reinterpret_cast<ProbDev*>(base + table_off);
@@ -586,8 +588,8 @@ void imag_grid(int n, double* omega, double* weight) {
 Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   char* base = arena_.data();
   auto dp = [&](size_t o) { return reinterpret_cast<double*>(base + o); };
-  const bool factor = (mode_ == kPlanFused || mode_ == kPlanPolar);
-  const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma);
+  const bool factor = (mode_ == kPlanFused || mode_ == kPlanPolar || mode_ == kPlanPartial);
+  const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma || mode_ == kPlanPartial);
   const bool qp = (mode_ == kPlanFused || mode_ == kPlanQP);
   for (size_t i = 0; i < probs_.size(); ++i) {
     const rigw_problem& q = probs[i];
@@ -612,8 +614,12 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
     if (factor || sigma) {
       // frequency grid: caller's or Gauss-Legendre
       if (q.omega && q.weight) {
-        RIGW_TRY(bind(q.omega, pp.off_in_omega, sh.nomega, "omega", &p.omega));
-        RIGW_TRY(bind(q.weight, pp.off_in_weight, sh.nomega, "weight", &p.weight));
+        // small arrays: always copied (host or device source), so that a frequency
+        // chunk may pass host subsets of the grid beside device-resident tensors
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_omega), q.omega, sh.nomega * 8, cudaMemcpyDefault, s));
+        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_weight), q.weight, sh.nomega * 8, cudaMemcpyDefault, s));
+        p.omega = dp(pp.off_in_omega);
+        p.weight = dp(pp.off_in_weight);
       } else {
         std::vector<double> om(sh.nomega), wt(sh.nomega);
         imag_grid(sh.nomega, om.data(), wt.data());

@@ -81,6 +81,8 @@ enum PlanMode : int {
   kPlanPolar = 1,      // chi0 -> eps -> factor -> I solve -> energies (factors stay resident)
   kPlanSigma = 2,      // M_sigma solve with resident factors -> Sigma
   kPlanQP = 3,         // continuation + QP from given sigma_calc
+  kPlanPartial = 4,    // chi0 -> eps -> factor -> solves -> partial Sigma and energies (no QP):
+                       // one frequency chunk of a problem, summed over chunks by the scheduler
 };
 
 struct PlanProblem {
@@ -96,7 +98,9 @@ struct PlanProblem {
 class Plan {
  public:
   Status build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
-               const std::vector<const ProbDev*>& factors);
+               const std::vector<const ProbDev*>& factors, size_t* measure_only = nullptr);
+  // Device bytes a plan of these shapes allocates (arena + work lists).
+  static size_t measure(const std::vector<Shape>& shapes, PlanMode mode);
   // Copy inputs (host or device pointers) and run; results stay on the device.
   Status stage_inputs(const rigw_problem* probs, cudaStream_t s);
   Status stage_sigma_calc(int i, const double* sigma_calc_host, cudaStream_t s);
@@ -168,7 +172,8 @@ class Context {
   size_t in_use = 0, peak = 0;
   std::string last_error;
   std::mutex mu;
-  std::map<std::vector<Shape>, std::unique_ptr<Plan>> fused_cache;
+  // plans by (mode, shapes); a repeated batch replays its CUDA graphs
+  std::map<std::pair<int, std::vector<Shape>>, std::unique_ptr<Plan>> plan_cache;
   bool use_graphs = true;
   rigw_stats last_stats{};
   Status init(int dev, size_t budget_bytes);
@@ -189,6 +194,8 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                       int nstate_min, int nstate_max, double* out);
 bool bf16x3_available();
+Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes);
+Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res);
 Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
 
 }  // namespace rigw

@@ -1,0 +1,206 @@
+// Memory-bounded execution of a batch of G0W0 problems.
+//
+// A batch whose fused plan fits the device runs as one plan (four CUDA graphs).
+// Otherwise every problem is split into frequency chunks that fit, the chunks of
+// all problems are packed into waves under the memory budget, each wave runs as
+// one partial plan (chi0, factorization, solves, partial Sigma_c and energies),
+// the partial sums are accumulated in chunk order (deterministic), and one QP
+// plan finishes all problems.  The frequency sum is the only coupling between
+// chunks: Sigma_c(z) and both energies are sums over omega
+// (src/m_gw_selfenergy_grid.f90:118-191, 290-321), which is also what makes the
+// poorman frequency split of the reference (:626,658) exact.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace rigw {
+
+namespace {
+
+size_t available_bytes(Context& c) {
+  size_t free_b = 0, total_b = 0;
+  if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+    cudaGetLastError();
+    free_b = 0;
+  }
+  size_t avail = size_t(double(free_b) * 0.9);
+  if (c.budget) avail = std::min(avail, c.budget > c.in_use ? c.budget - c.in_use : 0);
+  return avail;
+}
+
+Status get_plan(Context& c, PlanMode mode, const std::vector<Shape>& shapes, Plan** out) {
+  auto key = std::make_pair(int(mode), shapes);
+  auto it = c.plan_cache.find(key);
+  if (it != c.plan_cache.end()) {
+    *out = it->second.get();
+    return Status::ok();
+  }
+  if (c.plan_cache.size() >= 8) c.plan_cache.clear();
+  std::unique_ptr<Plan> p(new Plan());
+  Status s = p->build(&c, mode, shapes, {});
+  if (s.code == RIGW_ERR_NOMEM && !c.plan_cache.empty()) {   // cached plans hold memory: drop them, retry once
+    c.plan_cache.clear();
+    p.reset(new Plan());
+    s = p->build(&c, mode, shapes, {});
+  }
+  RIGW_TRY(s);
+  *out = p.get();
+  c.plan_cache.emplace(key, std::move(p));
+  return Status::ok();
+}
+
+void add_stats(Context& c, const Plan& p, bool first) {
+  rigw_stats& st = c.last_stats;
+  if (first) {
+    std::memset(&st, 0, sizeof(st));
+  }
+  for (int k = 0; k < 4; ++k) st.stage_ms[k] += p.stage_ms()[k];
+  st.total_ms += p.last_ms();
+  st.kernel_launches += p.kernel_launches();
+  st.graph_replayed = p.replayed() ? 1 : 0;
+  st.device_bytes_in_use = c.in_use;
+  st.device_bytes_peak = c.peak;
+}
+
+Status run_plan(Context& c, Plan* plan, const rigw_problem* probs, rigw_result* res,
+                const std::vector<const double*>* sigma_in, bool first) {
+  RIGW_TRY(plan->stage_inputs(probs, c.stream));
+  if (sigma_in)
+    for (size_t i = 0; i < sigma_in->size(); ++i) RIGW_TRY(plan->stage_sigma_calc(int(i), (*sigma_in)[i], c.stream));
+  RIGW_TRY(plan->launch(c.stream));
+  Status err = plan->check_errors(c.stream);
+  add_stats(c, *plan, first);
+  RIGW_TRY(err);
+  return plan->fetch_results(probs, res, c.stream);
+}
+
+}  // namespace
+
+Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes) {
+  shapes->resize(n);
+  for (int i = 0; i < n; ++i) {
+    RIGW_TRY(make_shape(probs[i], &(*shapes)[i]));
+    const Shape& s = (*shapes)[i];
+    if (s.nc < 1 || s.nsig < 1 || s.nstate_p < 1)
+      return Status::fail(RIGW_ERR_ARG, "problem %d: Sigma needs nomega_sigma_calc, nsig, nstate_p >= 1", i);
+    if (probs[i].precision != RIGW_FP64 && !bf16x3_available())
+      return Status::fail(RIGW_ERR_UNSUPPORTED, "precision %d not available", probs[i].precision);
+  }
+  return Status::ok();
+}
+
+Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res) {
+  std::vector<Shape> shapes;
+  RIGW_TRY(validate_batch(n, probs, &shapes));
+  size_t avail = available_bytes(c);
+  // plans cached for other shapes count as free memory for this decision
+  size_t cached = 0;
+  for (auto& kv : c.plan_cache) cached += kv.second->bytes();
+  const size_t usable = avail + cached;
+
+  // ---- fits: one fused plan
+  if (Plan::measure(shapes, kPlanFused) <= usable) {
+    Plan* plan = nullptr;
+    RIGW_TRY(get_plan(c, kPlanFused, shapes, &plan));
+    RIGW_TRY(run_plan(c, plan, probs, res, nullptr, true));
+    c.last_stats.chunks = n;
+    c.last_stats.waves = 1;
+    return Status::ok();
+  }
+
+  // ---- frequency chunks and waves
+  c.plan_cache.clear();
+  avail = available_bytes(c);
+  struct Unit {
+    int prob, w0, nw;
+  };
+  std::vector<Unit> units;
+  std::vector<std::vector<double>> om(n), wt(n);
+  for (int i = 0; i < n; ++i) {
+    const Shape& sh = shapes[i];
+    int wc = sh.nomega;
+    for (; wc >= 1; --wc) {
+      Shape s2 = sh;
+      s2.nomega = wc;
+      if (Plan::measure({s2}, kPlanPartial) <= avail) break;
+    }
+    if (wc < 1)
+      return Status::fail(RIGW_ERR_NOMEM, "problem %d (naux=%d, nocc=%d, nvirt=%d) does not fit in %zu bytes even "
+                          "one frequency at a time", i, sh.naux, sh.nocc, sh.nvirt, avail);
+    om[i].resize(sh.nomega);
+    wt[i].resize(sh.nomega);
+    if (probs[i].omega && probs[i].weight) {
+      RIGW_CUDA_TRY(cudaMemcpy(om[i].data(), probs[i].omega, sh.nomega * 8, cudaMemcpyDefault));
+      RIGW_CUDA_TRY(cudaMemcpy(wt[i].data(), probs[i].weight, sh.nomega * 8, cudaMemcpyDefault));
+    } else {
+      imag_grid(sh.nomega, om[i].data(), wt[i].data());
+    }
+    for (int w0 = 0; w0 < sh.nomega; w0 += wc) units.push_back({i, w0, std::min(wc, sh.nomega - w0)});
+  }
+  std::vector<std::vector<double>> acc_sig(n);
+  std::vector<double> acc_en(2 * size_t(n), 0.0);
+  for (int i = 0; i < n; ++i) acc_sig[i].assign(size_t(2) * shapes[i].nsig * shapes[i].nc, 0.0);
+
+  bool first = true;
+  int waves = 0;
+  for (size_t u0 = 0; u0 < units.size();) {
+    // greedy wave: units in order while the sum of their footprints fits
+    size_t u1 = u0, used = 0;
+    std::vector<Shape> wsh;
+    while (u1 < units.size()) {
+      Shape s2 = shapes[units[u1].prob];
+      s2.nomega = units[u1].nw;
+      const size_t b = Plan::measure({s2}, kPlanPartial);
+      if (u1 > u0 && used + b > avail) break;
+      used += b;
+      wsh.push_back(s2);
+      ++u1;
+    }
+    const int nu = int(u1 - u0);
+    std::vector<rigw_problem> up(nu);
+    std::vector<rigw_result> ur(nu);
+    std::vector<std::vector<double>> usig(nu);
+    for (int k = 0; k < nu; ++k) {
+      const Unit& u = units[u0 + k];
+      up[k] = probs[u.prob];
+      up[k].nomega = u.nw;
+      up[k].omega = om[u.prob].data() + u.w0;
+      up[k].weight = wt[u.prob].data() + u.w0;
+      usig[k].assign(size_t(2) * shapes[u.prob].nsig * shapes[u.prob].nc, 0.0);
+      std::memset(&ur[k], 0, sizeof(rigw_result));
+      ur[k].sigma_calc = usig[k].data();
+    }
+    Plan* plan = nullptr;
+    RIGW_TRY(get_plan(c, kPlanPartial, wsh, &plan));
+    RIGW_TRY(run_plan(c, plan, up.data(), ur.data(), nullptr, first));
+    first = false;
+    ++waves;
+    for (int k = 0; k < nu; ++k) {
+      const int i = units[u0 + k].prob;
+      for (size_t q = 0; q < acc_sig[i].size(); ++q) acc_sig[i][q] += usig[k][q];
+      acc_en[2 * i] += ur[k].erpa;
+      acc_en[2 * i + 1] += ur[k].egw;
+    }
+    u0 = u1;
+  }
+  // ---- QP for every problem from the summed Sigma_c
+  Plan* qplan = nullptr;
+  RIGW_TRY(get_plan(c, kPlanQP, shapes, &qplan));
+  std::vector<const double*> sin(n);
+  for (int i = 0; i < n; ++i) sin[i] = acc_sig[i].data();
+  RIGW_TRY(run_plan(c, qplan, probs, res, &sin, false));
+  for (int i = 0; i < n; ++i) {
+    res[i].erpa = acc_en[2 * i];
+    res[i].egw = acc_en[2 * i + 1];
+    if (res[i].sigma_calc)
+      RIGW_CUDA_TRY(cudaMemcpy(res[i].sigma_calc, acc_sig[i].data(), acc_sig[i].size() * 8, cudaMemcpyDefault));
+    res[i].device_ms = c.last_stats.total_ms;
+  }
+  c.last_stats.chunks = int(units.size());
+  c.last_stats.waves = waves;
+  return Status::ok();
+}
+
+}  // namespace rigw

@@ -68,6 +68,7 @@ class Stats(C.Structure):
     _fields_ = [
         ("stage_ms", C.c_double * 4), ("total_ms", C.c_double), ("kernel_launches", C.c_int),
         ("graph_replayed", C.c_int), ("device_bytes_in_use", C.c_size_t), ("device_bytes_peak", C.c_size_t),
+        ("chunks", C.c_int), ("waves", C.c_int),
     ]
 
 
@@ -189,7 +190,7 @@ class Engine:
         self._check(self._lib.rigw_last_stats(self._h, C.byref(st)), "rigw_last_stats")
         return dict(stage_ms=list(st.stage_ms), total_ms=st.total_ms, kernel_launches=st.kernel_launches,
                     graph_replayed=bool(st.graph_replayed), device_bytes_in_use=st.device_bytes_in_use,
-                    device_bytes_peak=st.device_bytes_peak)
+                    device_bytes_peak=st.device_bytes_peak, chunks=st.chunks, waves=st.waves)
 
     def _check(self, rc: int, what: str):
         if rc:

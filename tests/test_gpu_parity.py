@@ -91,6 +91,13 @@ def test_qp_solve_polynomial_technique(engine, golden_synth):
     assert np.abs(out.energy_qp_g - eqp).max() * HA_EV < 1e-9
 
 
+@pytest.mark.parametrize("nocc,nvirt,naux,nomega", [(5, 37, 85, 8), (3, 29, 129, 6), (7, 64, 256, 4)])
+def test_edge_shapes_match_oracle(engine, nocc, nvirt, naux, nomega):
+    """Odd auxiliary count, one past a 128-panel, exactly two panels."""
+    inst = synth.make_instance(nocc, nvirt, naux, nomega, seed=naux)
+    assert_matches(engine.g0w0(inst), oracle_outputs(inst))
+
+
 def test_ragged_batch_equals_single_solves(engine):
     insts = [synth.make_instance(4, 30, 70, 8, seed=21), synth.make_instance(7, 60, 150, 12, seed=22),
              synth.make_instance(5, 41, 130, 16, seed=23)]
