@@ -172,6 +172,29 @@ RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* res
 /* Many problems of different sizes in one launch sequence (one CUDA graph). */
 RIGW_API int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_result* results);
 
+/* ---- request loop (continuous batching) --------------------------------------
+ * No routine of the reference corresponds to this (MOLGW runs one molecule per
+ * process); it serves many G0W0 solves on one GPU.  `workers` threads each own a
+ * context with hbm_budget_bytes/workers of device memory (0: 85% of the free
+ * memory); a free worker takes the queued requests in arrival order while their
+ * footprints fit its share (at most max_batch) and solves them as one batch, so
+ * requests that arrive while others run are admitted as workers and memory free
+ * up, and batches of different workers overlap on the GPU.  The caller keeps the
+ * arrays of a submitted problem and its result buffers alive until
+ * rigw_server_wait returned for its ticket. */
+typedef struct rigw_server rigw_server;
+RIGW_API int rigw_server_create(rigw_server** srv, int device, size_t hbm_budget_bytes, int workers,
+                                int max_batch);
+RIGW_API int rigw_server_submit(rigw_server* srv, const rigw_problem* prob, rigw_result* result,
+                                uint64_t* ticket);
+RIGW_API int rigw_server_poll(rigw_server* srv, uint64_t ticket, int* done);
+/* Waits at most timeout_ns; returns the request's status (RIGW_ERR_TIMEOUT if not
+ * done yet, the ticket stays valid), releases the ticket otherwise. */
+RIGW_API int rigw_server_wait(rigw_server* srv, uint64_t ticket, int64_t timeout_ns, char* errbuf, size_t errlen);
+RIGW_API int rigw_server_counters(rigw_server* srv, long long* completed, long long* batches, long long* queued);
+/* Finishes the queued requests, then stops the workers. */
+RIGW_API int rigw_server_destroy(rigw_server* srv);
+
 /* ---- allocation-free variant -------------------------------------------------
  * No counterpart in the reference.  The continuation + QP equation of
  * rigw_qp_solve for callers that may not allocate device memory: a host code

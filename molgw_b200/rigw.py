@@ -208,11 +208,13 @@ class Engine:
         occ = np.ascontiguousarray(inst.occupation, dtype=np.float64)
         nsemin, nsemax = inst.nsemin, inst.nsemax
         host = {
-            "m_ia": np.ascontiguousarray(inst.m_ia), "e_occ": e[:nocc].copy(), "e_virt": e[nocc:nocc + nvirt].copy(),
+            "e_occ": e[:nocc].copy(), "e_virt": e[nocc:nocc + nvirt].copy(),
             "occ_occ": occ[:nocc].copy(), "occ_virt": occ[nocc:nocc + nvirt].copy(),
-            "m_pm": np.ascontiguousarray(inst.m_sigma), "e_p": e.copy(),
-            "e_sig": e[nsemin - 1:nsemax].copy(),
+            "e_p": e.copy(), "e_sig": e[nsemin - 1:nsemax].copy(),
         }
+        if inst.m_ia is not None:
+            host["m_ia"] = np.ascontiguousarray(inst.m_ia)
+            host["m_pm"] = np.ascontiguousarray(inst.m_sigma)
         occ_sig = occ[nsemin - 1:nsemax].copy()
         arrs = dict(host)
         flags = 0
@@ -349,5 +351,70 @@ class WPol:
     def __del__(self):
         try:
             self.release()
+        except Exception:
+            pass
+
+
+class Server:
+    """Continuous-batching request loop (rigw_server_*): submit G0W0 problems from
+    any thread, wait for their results by ticket."""
+
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, workers: int = 2, max_batch: int = 64):
+        self._lib = lib()
+        L = self._lib
+        L.rigw_server_create.argtypes = [C.POINTER(C.c_void_p), C.c_int, C.c_size_t, C.c_int, C.c_int]
+        L.rigw_server_submit.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result), C.POINTER(C.c_uint64)]
+        L.rigw_server_poll.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_int)]
+        L.rigw_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, C.c_char_p, C.c_size_t]
+        L.rigw_server_counters.argtypes = [C.c_void_p] + [C.POINTER(C.c_longlong)] * 3
+        L.rigw_server_destroy.argtypes = [C.c_void_p]
+        h = C.c_void_p()
+        rc = L.rigw_server_create(C.byref(h), device, hbm_budget_bytes, workers, max_batch)
+        if rc:
+            raise RigwError(rc, "rigw_server_create")
+        self._h = h
+        self._helper = Engine.__new__(Engine)      # problem/result builders only (no context)
+        self._pending = {}
+
+    def submit(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False) -> int:
+        p, keep = Engine.make_problem(self._helper, inst, precision, device_arrays, qp_only=qp_only)
+        r, bufs = Engine._alloc_result(self._helper, p)
+        pp = Problem()
+        C.pointer(pp)[0] = p
+        t = C.c_uint64()
+        rc = self._lib.rigw_server_submit(self._h, C.byref(pp), C.byref(r), C.byref(t))
+        if rc:
+            raise RigwError(rc, "rigw_server_submit")
+        self._pending[t.value] = (pp, r, bufs, keep)
+        return t.value
+
+    def done(self, ticket: int) -> bool:
+        d = C.c_int()
+        self._lib.rigw_server_poll(self._h, ticket, C.byref(d))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_s: float = 600.0) -> G0W0Output:
+        buf = C.create_string_buffer(512)
+        rc = self._lib.rigw_server_wait(self._h, ticket, int(timeout_s * 1e9), buf, 512)
+        if rc == 6:
+            raise RigwError(rc, f"ticket {ticket} not done after {timeout_s} s")
+        pp, r, bufs, keep = self._pending.pop(ticket)
+        if rc:
+            raise RigwError(rc, buf.value.decode())
+        return Engine._output(r, bufs)
+
+    def counters(self) -> dict:
+        a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()
+        self._lib.rigw_server_counters(self._h, C.byref(a), C.byref(b), C.byref(c))
+        return {"completed": a.value, "batches": b.value, "queued": c.value}
+
+    def close(self):
+        if self._h:
+            self._lib.rigw_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
         except Exception:
             pass

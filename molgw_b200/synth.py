@@ -86,14 +86,17 @@ def _lambda_max(m_t: np.ndarray, de: np.ndarray) -> float:
 
 
 def make_instance(nocc: int, nvirt: int, naux: int, nomega: int, seed: int,
-                  with_sigma: bool = True) -> GWInstance:
-    """Build one seeded instance (numpy Generator(PCG64(seed)))."""
+                  with_sigma: bool = True, lambda_max=None) -> GWInstance:
+    """Build one seeded instance (numpy Generator(PCG64(seed))).
+
+    ``lambda_max(m_t, de)`` may replace the host eigenvalue computation of the
+    scaling (same quantity, e.g. evaluated on a GPU for large batches)."""
     rng = np.random.Generator(np.random.PCG64(seed))
     energy = _energies(rng, nocc, nvirt)
     occupation = np.concatenate([np.full(nocc, 2.0), np.zeros(nvirt)])
     m_raw = rng.standard_normal((nocc, nvirt, naux))
     de = (energy[nocc:][None, :] - energy[:nocc][:, None]).reshape(-1)
-    lmax = _lambda_max(m_raw.reshape(-1, naux), de)
+    lmax = (lambda_max or _lambda_max)(m_raw.reshape(-1, naux), de)
     s = np.sqrt(0.8 / lmax)
     m_ia = m_raw * s
     nstate = nocc + nvirt
@@ -136,5 +139,76 @@ def batch_sizes(count: int = 256, base_seed: int = 4):
     return out
 
 
-def batch_instances(count: int = 256, base_seed: int = 4):
-    return [make_instance(no, nv, na, nw, sd) for (no, nv, na, nw, sd) in batch_sizes(count, base_seed)]
+def batch_instances(count: int = 256, base_seed: int = 4, lambda_max=None):
+    return [make_instance(no, nv, na, nw, sd, lambda_max=lambda_max)
+            for (no, nv, na, nw, sd) in batch_sizes(count, base_seed)]
+
+
+def serving_sizes(rate: float = 200.0, duration: float = 60.0, seed: int = 5, large_fraction: float = 0.05):
+    """Poisson arrivals and request sizes: 95% drawn like the ragged batch, 5%
+    large (Nocc=150, Nvirt=1500, Naux=6000, 48 frequencies).  Returns a list of
+    (arrival_time_s, (nocc, nvirt, naux, nomega, seed))."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    t = 0.0
+    k = 0
+    while True:
+        t += rng.exponential(1.0 / rate)
+        if t >= duration:
+            break
+        if rng.random() < large_fraction:
+            size = (150, 1500, 6000, 48, 100000 + k)
+        else:
+            r2 = np.random.Generator(np.random.PCG64(1000 + k))
+            nocc = int(r2.integers(5, 61))
+            nvirt = int(round(nocc * r2.uniform(8.0, 10.0)))
+            size = (nocc, nvirt, 4 * (nocc + nvirt), 32, 1000 + k)
+        out.append((t, size))
+        k += 1
+    return out
+
+
+def make_instance_device(nocc: int, nvirt: int, naux: int, nomega: int, seed: int, device: str = "cuda"):
+    """The same distributions generated directly in device memory (torch, float64,
+    seeded torch.Generator), for batches too large to draw on the host.
+
+    Returns (GWInstance with m_ia = m_sigma = None, dict of device tensors in the
+    layout of ``Engine.make_problem``'s ``device_arrays``)."""
+    import torch
+    rng = np.random.Generator(np.random.PCG64(seed))
+    energy = _energies(rng, nocc, nvirt)
+    occupation = np.concatenate([np.full(nocc, 2.0), np.zeros(nvirt)])
+    g = torch.Generator(device=device)
+    g.manual_seed(int(seed))
+    m = torch.randn((nocc, nvirt, naux), generator=g, dtype=torch.float64, device=device)
+    de = torch.from_numpy((energy[nocc:][None, :] - energy[:nocc][:, None]).reshape(-1)).to(device)
+    a = m.reshape(-1, naux) * torch.sqrt(4.0 / de)[:, None]
+    lmax = float(torch.linalg.eigvalsh(a.T @ a)[-1].item())
+    del a
+    s = float(np.sqrt(0.8 / lmax))
+    m.mul_(s)
+    nstate = nocc + nvirt
+    ms = torch.empty((2, nstate, naux), dtype=torch.float64, device=device)
+    ms[0, :nocc] = torch.randn((nocc, naux), generator=g, dtype=torch.float64, device=device) * s
+    ms[0, nocc:] = m[nocc - 1]
+    ms[1, :nocc] = m[:, 0]
+    ms[1, nocc:] = torch.randn((nvirt, naux), generator=g, dtype=torch.float64, device=device) * s
+    inst = GWInstance(nocc=nocc, nvirt=nvirt, naux=naux, nomega=nomega, energy=energy, occupation=occupation,
+                      m_ia=None, m_sigma=None, nsemin=nocc, nsemax=nocc + 1, seed=seed)
+    t = lambda x: torch.from_numpy(np.ascontiguousarray(x)).to(device)
+    dev = {"m_ia": m, "m_pm": ms, "e_occ": t(energy[:nocc]), "e_virt": t(energy[nocc:]),
+           "occ_occ": t(occupation[:nocc]), "occ_virt": t(occupation[nocc:]), "e_p": t(energy),
+           "e_sig": t(energy[nocc - 1:nocc + 1]), "occ_sig": t(occupation[nocc - 1:nocc + 1])}
+    return inst, dev
+
+
+def torch_lambda_max(device: str = "cuda"):
+    """lambda_max hook evaluating max eig of sum_t (4/de_t) m_t m_t^T with torch
+    (float64) on ``device``; used to generate large batches quickly."""
+    import torch
+
+    def f(m_t: np.ndarray, de: np.ndarray) -> float:
+        a = torch.from_numpy(m_t).to(device) * torch.from_numpy(np.sqrt(4.0 / de)).to(device)[:, None]
+        g = a.T @ a
+        return float(torch.linalg.eigvalsh(g)[-1].item())
+    return f
