@@ -50,6 +50,12 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=32,
                     help="molecules of the ragged batch measured beside the single instance (0: skip)")
     ap.add_argument("--batch-reps", type=int, default=2)
+    ap.add_argument("--workload", default="single", choices=["single", "serve"])
+    ap.add_argument("--serve-rate", type=float, default=200.0)
+    ap.add_argument("--serve-duration", type=float, default=60.0)
+    ap.add_argument("--serve-workers", type=int, default=2)
+    ap.add_argument("--serve-batch", type=int, default=32)
+    ap.add_argument("--serve-fp64", action="store_true", help="also serve the same arrivals in FP64")
     return ap.parse_args()
 
 
@@ -183,6 +189,110 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
     return res
 
 
+def run_serving(rate: float, duration: float, precision: int, workers: int, max_batch: int) -> dict:
+    """Poisson arrivals (rate req/s for `duration` s; 95% ragged sizes, 5% large
+    Nocc=150/Nvirt=1500/Naux=6000/48 frequencies) submitted in real time to the
+    request loop; latency = completion - arrival on the host clock.  Request
+    inputs come from a device-resident pool: one instance per Nocc class
+    (Nvirt = 9 Nocc, Naux = 40 Nocc) and one large instance."""
+    import threading
+    import torch
+    from molgw_b200 import synth
+    from molgw_b200.rigw import Server
+    sched = synth.serving_sizes(rate=rate, duration=duration)
+    pool = {}
+    for _, (no, nv, na, nw, sd) in sched:
+        key = (no, nw)
+        if key not in pool:
+            nv2 = nv if no == 150 else 9 * no
+            pool[key] = synth.make_instance_device(no, nv2, 4 * (no + nv2), nw, 7000 + no)
+    torch.cuda.synchronize()
+    srv = Server(0, workers=workers, max_batch=max_batch)
+    # warm the worker plans on one request of each kind
+    for key in list(pool)[:2]:
+        srv.wait(srv.submit(pool[key][0], precision, pool[key][1], qp_only=True))
+    arrive, submit_t, done_t = {}, {}, {}
+    lock = threading.Lock()
+    finished = threading.Event()
+
+    def poller():
+        while not finished.is_set() or len(done_t) < len(submit_t):
+            with lock:
+                pend = [t for t in submit_t if t not in done_t]
+            for t in pend:
+                if srv.done(t):
+                    done_t[t] = time.perf_counter()
+            time.sleep(0.0005)
+
+    th = threading.Thread(target=poller)
+    th.start()
+    t0 = time.perf_counter()
+    tickets = []
+    for at, (no, nv, na, nw, sd) in sched:
+        now = time.perf_counter() - t0
+        if at > now:
+            time.sleep(at - now)
+        inst, dev = pool[(no, nw)]
+        with lock:
+            tk = srv.submit(inst, precision, dev, qp_only=True)
+            submit_t[tk] = time.perf_counter()
+            arrive[tk] = t0 + at
+        tickets.append(tk)
+    finished.set()
+    th.join()
+    outs = [srv.wait(t) for t in tickets]
+    srv.close()
+    lat = np.array([done_t[t] - arrive[t] for t in tickets]) * 1e3
+    span = max(done_t.values()) - t0
+    n_large = sum(1 for _, s in sched if s[0] == 150)
+    return {"requests": len(tickets), "large_requests": n_large, "offered_rate": rate, "duration_s": duration,
+            "solves_per_s": len(tickets) / span, "p50_ms": float(np.percentile(lat, 50)),
+            "p99_ms": float(np.percentile(lat, 99)), "max_ms": float(lat.max()), "span_s": span,
+            "workers": workers, "max_batch": max_batch, "outputs": outs, "pool": pool}
+
+
+def run_serve_line(args):
+    """`--workload serve`: the request loop under Poisson arrivals, split precision
+    (and FP64 with --serve-fp64), one JSON line."""
+    import torch
+    from molgw_b200 import build
+    build.build()
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64, Engine
+    torch.cuda.set_device(0)
+    res = {}
+    split = run_serving(args.serve_rate, args.serve_duration, RIGW_BF16X3, args.serve_workers, args.serve_batch)
+    pool, outs = split.pop("pool"), split.pop("outputs")
+    res["bf16x3"] = split
+    # accuracy: every distinct instance of the pool once in FP64 (single context)
+    eng = Engine(0)
+    sched = None
+    worst = 0.0
+    seen = {}
+    from molgw_b200 import synth
+    sched = synth.serving_sizes(rate=args.serve_rate, duration=args.serve_duration)
+    for (at, (no, nv, na, nw, sd)), o in zip(sched, outs):
+        key = (no, nw)
+        if key not in seen:
+            inst, dev = pool[key]
+            seen[key] = eng.g0w0(inst, RIGW_FP64, dev, qp_only=True)
+        worst = max(worst, float(np.abs(o.energy_qp_g - seen[key].energy_qp_g).max() * HA_EV * 1e3))
+    eng.close()
+    res["bf16x3"]["qp_max_diff_mev_vs_fp64"] = worst
+    if args.serve_fp64:
+        f64 = run_serving(args.serve_rate, args.serve_duration, RIGW_FP64, args.serve_workers, args.serve_batch)
+        f64.pop("pool")
+        f64.pop("outputs")
+        res["fp64"] = f64
+        res["speedup_split_vs_fp64"] = res["bf16x3"]["solves_per_s"] / f64["solves_per_s"]
+    line = {"metric": "G0W0 solves/s + p50/p99 latency (request loop)", "unit": "solves/s",
+            "value": res["bf16x3"]["solves_per_s"], "n_gpus": 1, "higher_is_better": True, "dtype": "bf16x3+f64",
+            "data": "synthetic (Poisson arrivals, seed 5; sizes snapped to Nocc classes)",
+            "config": {"workload": "serving: Poisson arrivals, 95% ragged sizes / 5% Nocc=150 Nvirt=1500 Naux=6000 "
+                                   "48 frequencies", "rate": args.serve_rate, "duration_s": args.serve_duration},
+            "serving": res}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the MOLGW path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -222,6 +332,9 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "serve":
+        run_serve_line(args)
         return
 
     import torch
