@@ -9,8 +9,9 @@
 // syrk_bf16x3_kernel: one 128x128 upper tile of eps(iw) per CTA.  One thread
 //   issues TMA loads (4 tiles of 128 rows x 64 bf16 per stage, 128-byte
 //   swizzle) into a 3-stage ring, one thread issues tcgen05.mma (M=128, N=128,
-//   K=16; 12 per stage), the four warps then read the fp32 accumulator out of
-//   TMEM, add the identity and store FP64.  All mbarrier waits are bounded.
+//   K=16; 12 per stage) into two ping-pong TMEM accumulators, eight warps drain
+//   them chunk by chunk into FP64, add the identity and store.  All mbarrier
+//   waits are bounded.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -59,14 +60,23 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
   }
 }
 
-__global__ void __launch_bounds__(128, 1) syrk_bf16x3_kernel(const TcItem* __restrict__ items) {
+// K is consumed in chunks of kTcChunk k-tiles (512 transitions).  Each chunk
+// accumulates in fp32 in one of two TMEM accumulators (128 columns each); eight
+// epilogue warps drain a finished chunk into FP64 registers while the MMA warp
+// fills the other accumulator.  The fp32 accumulation length is therefore
+// bounded by the chunk, whatever the number of transitions.
+constexpr int kTcChunk = 8;
+constexpr int kTcThreads = 320;    // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
+
+__global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem* __restrict__ items) {
   const TcItem it = items[blockIdx.x];
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTcStages * kTcStageBytes);
   uint64_t* empty = full + kTcStages;
-  uint64_t* accum = empty + kTcStages;
-  uint32_t* tslot = reinterpret_cast<uint32_t*>(accum + 1);
+  uint64_t* accf = empty + kTcStages;     // [2] chunk accumulated
+  uint64_t* acce = accf + 2;              // [2] chunk drained
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 2);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   auto tile = [&](int s, int which) { return smem + s * kTcStageBytes + which * kTcTileBytes; };
 
@@ -75,14 +85,18 @@ __global__ void __launch_bounds__(128, 1) syrk_bf16x3_kernel(const TcItem* __res
       tc::mbar_init(&full[s], 1);
       tc::mbar_init(&empty[s], 1);
     }
-    tc::mbar_init(accum, 1);
+    for (int b = 0; b < 2; ++b) {
+      tc::mbar_init(&accf[b], 1);
+      tc::mbar_init(&acce[b], 8);
+    }
     tc::fence_mbar_init();
   }
-  if (warp == 0) tc::tmem_alloc(tslot, 128);
+  if (warp == 0) tc::tmem_alloc(tslot, 256);
   __syncthreads();
   tc::tc_fence_after();
   const uint32_t tmem = *tslot;
   const int nk = it.ktiles;
+  const int nchunks = (nk + kTcChunk - 1) / kTcChunk;
 
   if (tid == 0) {
     // ---- TMA producer
@@ -104,59 +118,82 @@ __global__ void __launch_bounds__(128, 1) syrk_bf16x3_kernel(const TcItem* __res
       ++issued[s];
     }
     if (!ok) atomicOr(it.err, kErrTimeout);
-    // every issued copy has landed before the CTA may exit
     for (int s = 0; s < kTcStages; ++s)
       if (issued[s] > 0 && !tc::mbar_wait(&full[s], (issued[s] - 1) & 1)) atomicOr(it.err, kErrTimeout);
   } else if (tid == 32) {
     // ---- MMA issuer
     constexpr uint32_t idesc = tc::idesc_bf16_f32(128, 128);
     bool ok = true;
-    for (int kt = 0; kt < nk; ++kt) {
+    for (int kt = 0; kt < nk && ok; ++kt) {
+      const int c = kt / kTcChunk, b = c & 1;
+      const bool first = (kt % kTcChunk) == 0;
+      if (first && c >= 2 && !tc::mbar_wait(&acce[b], ((c >> 1) - 1) & 1)) {
+        ok = false;
+        break;
+      }
       const int s = kt % kTcStages;
       if (!tc::mbar_wait(&full[s], (kt / kTcStages) & 1)) {
         ok = false;
         break;
       }
       tc::tc_fence_after();
+      const uint32_t d = tmem + uint32_t(b * 128);
       const uint64_t ah = tc::desc_kmajor_sw128(tile(s, 0)), al = tc::desc_kmajor_sw128(tile(s, 1));
       const uint64_t bh = tc::desc_kmajor_sw128(tile(s, 2)), bl = tc::desc_kmajor_sw128(tile(s, 3));
 #pragma unroll
       for (int sub = 0; sub < 4; ++sub) {
         const uint64_t o = uint64_t(sub * 2);   // 16 bf16 = 32 bytes along K
-        tc::mma_bf16(tmem, ah + o, bh + o, idesc, (kt > 0 || sub > 0) ? 1u : 0u);
-        tc::mma_bf16(tmem, ah + o, bl + o, idesc, 1u);
-        tc::mma_bf16(tmem, al + o, bh + o, idesc, 1u);
+        tc::mma_bf16(d, ah + o, bh + o, idesc, (first && sub == 0) ? 0u : 1u);
+        tc::mma_bf16(d, ah + o, bl + o, idesc, 1u);
+        tc::mma_bf16(d, al + o, bh + o, idesc, 1u);
       }
       tc::mma_commit(&empty[s]);
+      if ((kt % kTcChunk) == kTcChunk - 1 || kt == nk - 1) tc::mma_commit(&accf[b]);
     }
     if (!ok) atomicOr(it.err, kErrTimeout);
-    tc::mma_commit(accum);
-  }
-  __syncwarp();
-  // ---- epilogue: TMEM -> registers -> FP64 eps tile
-  const bool got = __all_sync(0xffffffffu, tc::mbar_wait(accum, 0));
-  tc::tc_fence_after();
-  if (got) {
-    const int row = warp * 32 + lane;
-#pragma unroll 1
-    for (int c0 = 0; c0 < 128; c0 += 32) {
-      uint32_t r[32];
-      tc::tmem_ld_32x32(tmem + (uint32_t(warp * 32) << 16) + uint32_t(c0), r);
-      double* dst = it.C + size_t(row) * it.ldc + c0;
+  } else if (warp >= 2) {
+    // ---- epilogue: drain each chunk into FP64 registers, then store the tile
+    const int quad = warp & 3;                 // TMEM lanes 32*quad .. 32*quad+31 (rows)
+    const int half = (warp - 2) >> 2;          // columns 64*half .. 64*half+63
+    const int row = quad * 32 + lane;
+    double acc[64];
 #pragma unroll
-      for (int j = 0; j < 32; j += 2) {
-        double v0 = double(__uint_as_float(r[j])), v1 = double(__uint_as_float(r[j + 1]));
-        if (c0 + j - row == it.diag) v0 += 1.0;
-        if (c0 + j + 1 - row == it.diag) v1 += 1.0;
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    bool ok = true;
+    for (int c = 0; c < nchunks; ++c) {
+      const int b = c & 1;
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[b], (c >> 1) & 1));
+      if (!ok) break;
+      tc::tc_fence_after();
+      const uint32_t base = tmem + uint32_t(b * 128 + half * 64) + (uint32_t(quad * 32) << 16);
+      uint32_t r[32];
+      tc::tmem_ld_32x32(base, r);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] += double(__uint_as_float(r[j]));
+      tc::tmem_ld_32x32(base + 32, r);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[32 + j] += double(__uint_as_float(r[j]));
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(&acce[b]);
+    }
+    if (ok) {
+      double* dst = it.C + size_t(row) * it.ldc + half * 64;
+#pragma unroll
+      for (int j = 0; j < 64; j += 2) {
+        const int col = half * 64 + j;
+        double v0 = acc[j], v1 = acc[j + 1];
+        if (col - row == it.diag) v0 += 1.0;
+        if (col + 1 - row == it.diag) v1 += 1.0;
         *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
       }
+    } else if (lane == 0) {
+      atomicOr(it.err, kErrTimeout);
     }
-  } else if (lane == 0) {
-    atomicOr(it.err, kErrTimeout);
   }
   tc::tc_fence_before();
   __syncthreads();
-  if (warp == 0) tc::tmem_dealloc(tmem, 128);
+  if (warp == 0) tc::tmem_dealloc(tmem, 256);
 }
 
 // ---------------------------------------------------------------------------
@@ -197,7 +234,7 @@ void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cud
 }
 
 void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s) {
-  if (n > 0) syrk_bf16x3_kernel<<<n, 128, kTcSmemBytes, s>>>(items);
+  if (n > 0) syrk_bf16x3_kernel<<<n, kTcThreads, kTcSmemBytes, s>>>(items);
 }
 
 cudaError_t prepare_tc_kernels() {
