@@ -140,7 +140,8 @@ Plan::~Plan() {
     if (e) cudaEventDestroy(e);
   for (auto& e : la_ev_)
     if (e) cudaEventDestroy(e);
-  if (aux_stream_) cudaStreamDestroy(aux_stream_);
+  for (auto& s : aux_streams_)
+    if (s) cudaStreamDestroy(s);
 }
 
 size_t Plan::measure(const std::vector<Shape>& shapes, PlanMode mode) {
@@ -307,12 +308,21 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // ---- work lists
   const int BMN = 128;   // column width of every DMMA item
   const int BM = 64;     // row height of the chi0 and trailing-update items
-  int max_panels = 0;
-  for (int i = 0; i < np; ++i) max_panels = std::max(max_panels, probs_[i].dev.npanel);
-  wl_diag_.assign(max_panels, {});
-  gl_k2_.assign(max_panels, {});
-  gl_k3_.assign(max_panels, {});
-  gl_k3d_.assign(max_panels, {});
+  int max_panels = 0, npairs = 0;
+  for (int i = 0; i < np; ++i) {
+    max_panels = std::max(max_panels, probs_[i].dev.npanel);
+    npairs += shapes[i].nomega;
+  }
+  // The factorization and solves of independent (problem, frequency) pairs run
+  // as two chains on their own streams, each with its own one-panel lookahead,
+  // so that one chain's launch tails and diagonal blocks overlap the other's GEMMs.
+  nchains_ = npairs >= 8 ? 2 : 1;
+  const int nlists = nchains_ * std::max(max_panels, 1);
+  wl_diag_.assign(nlists, {});
+  gl_k2_.assign(nlists, {});
+  gl_k3_.assign(nlists, {});
+  gl_k3d_.assign(nlists, {});
+  int pair = 0;
   for (int i = 0; i < np; ++i) {
     const Shape& sh = shapes[i];
     const ProbDev& p = probs_[i].dev;
@@ -377,7 +387,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         double* R = p.rhs + size_t(w) * npad * ldb;
         const double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
         double* cs = p.colsq ? p.colsq + (size_t(w) * p.npanel + k) * ldb : nullptr;
-        if (factor) wl_diag_[k].push_back({i, w, 0, 0});
+        const int li = ((pair + w) % nchains_) * max_panels + k;   // list of (chain, panel)
+        if (factor) wl_diag_[li].push_back({i, w, 0, 0});
         auto k2 = [&](double* X, int ldx, int c0, int n, double* colsq) {
           GemmItem g{};
           g.A = W;
@@ -391,7 +402,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.n = n;
           g.k = kPanel;
           g.alpha = 1.0;
-          gl_k2_[k].push_back(g);
+          gl_k2_[li].push_back(g);
         };
         if (factor)
           for (int c0 = r0; c0 < npad; c0 += BMN) k2(E, npad, c0, std::min(BMN, npad - c0), nullptr);
@@ -416,7 +427,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.k = kPanel;
           g.alpha = -1.0;
           g.beta = 1.0;
-          (next_diag ? gl_k3d_[k] : gl_k3_[k]).push_back(g);
+          (next_diag ? gl_k3d_[li] : gl_k3_[li]).push_back(g);
         };
         for (int i0 = r0; i0 < npad; i0 += BM) {
           const int m = std::min(BM, npad - i0);
@@ -440,6 +451,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     }
     if (qp)
       for (int s = 0; s < sh.nsig; ++s) wl_pade_.push_back({i, s, 0, 0});
+    pair += sh.nomega;
   }
 
   // ---- upload the lists and the launch sequence
@@ -472,21 +484,44 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(13, tl_syrk_.data(), sizeof(TcItem), tl_syrk_.size(), 0);
   add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
-  // Panel loop with a one-panel lookahead: the update of the next diagonal block
-  // (K3d) goes first, then its factorization runs on the second stream while the
-  // rest of the trailing update (K3) runs on the first.
-  int pending_join = -1;
-  for (int k = 0; k < max_panels; ++k) {
-    if (k == 0) add(4, wl_diag_[0].data(), sizeof(WorkItem), wl_diag_[0].size(), 0);
-    add(5, gl_k2_[k].data(), sizeof(GemmItem), gl_k2_[k].size(), k, 0, pending_join);
-    pending_join = -1;
-    const bool next = k + 1 < max_panels && !wl_diag_[k + 1].empty();
-    add(14, gl_k3d_[k].data(), sizeof(GemmItem), gl_k3d_[k].size(), k, 0, -1, next ? 2 * k : -1);
-    if (next && add(4, wl_diag_[k + 1].data(), sizeof(WorkItem), wl_diag_[k + 1].size(), k + 1, 1, 2 * k, 2 * k + 1))
-      pending_join = 2 * k + 1;
-    add(6, gl_k3_[k].data(), sizeof(GemmItem), gl_k3_[k].size(), k);
+  // Panel loop of each chain with a one-panel lookahead: the update of the next
+  // diagonal block (K3d) goes first, then its factorization runs on the chain's
+  // lookahead stream while the rest of the trailing update (K3) runs on the
+  // chain's main stream.  Streams: chain c uses 2c (main) and 2c+1 (lookahead);
+  // stream 0 is the plan's own stream.  Kind -1 launches nothing (event marker).
+  int nev = 0;
+  const int fork_ev = nchains_ > 1 ? nev++ : -1;
+  if (fork_ev >= 0) pend.push_back({-1, nullptr, 0, 0, 0, 0, -1, fork_ev});
+  std::vector<int> chain_end;
+  for (int ch = 0; ch < nchains_; ++ch) {
+    const int sm = 2 * ch, sl = 2 * ch + 1;
+    int pending = ch > 0 ? fork_ev : -1;
+    auto L = [&](int k) { return ch * max_panels + k; };
+    for (int k = 0; k < max_panels; ++k) {
+      if (k == 0 && add(4, wl_diag_[L(0)].data(), sizeof(WorkItem), wl_diag_[L(0)].size(), 0, sm, pending))
+        pending = -1;
+      if (add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm, pending)) pending = -1;
+      const bool next = k + 1 < max_panels && !wl_diag_[L(k + 1)].empty();
+      const int ea = next ? nev++ : -1, eb = next ? nev++ : -1;
+      if (next && !gl_k3d_[L(k)].empty()) {
+        add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm, -1, ea);
+        add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sl, ea, eb);
+        pending = eb;
+      } else {
+        add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm);
+      }
+      add(6, gl_k3_[L(k)].data(), sizeof(GemmItem), gl_k3_[L(k)].size(), k, sm);
+    }
+    if (ch > 0) {
+      const int ej = nev++;
+      pend.push_back({-1, nullptr, 0, 0, 0, sm, pending, ej});   // joins the lookahead, marks the chain's end
+      chain_end.push_back(ej);
+    } else if (pending >= 0) {
+      pend.push_back({-1, nullptr, 0, 0, 0, 0, pending, -1});
+    }
   }
-  add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0, 0, pending_join);
+  for (int ej : chain_end) pend.push_back({-1, nullptr, 0, 0, 0, 0, ej, -1});
+  add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0);
   if (factor) pend.push_back({8, nullptr, 0, np, 0, 0, -1, -1});
   add(9, wl_vchiv_.data(), sizeof(WorkItem), wl_vchiv_.size(), 0);
   add(10, wl_sigma_.data(), sizeof(WorkItem), wl_sigma_.size(), 0);
@@ -502,9 +537,10 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   }
   RIGW_CUDA_TRY(cudaMemcpy(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice));
   for (auto& e : stage_ev_) RIGW_CUDA_TRY(cudaEventCreate(&e));
-  la_ev_.assign(2 * std::max(max_panels, 1), nullptr);
+  la_ev_.assign(std::max(nev, 1), nullptr);
   for (auto& e : la_ev_) RIGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&aux_stream_, cudaStreamNonBlocking));
+  aux_streams_.assign(2 * nchains_ - 1, nullptr);
+  for (auto& s : aux_streams_) RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
   host_table_.resize(np);
   n_launches_ = int(seq_.size());
   return Status::ok();
@@ -517,7 +553,7 @@ static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
     case 1: case 12: case 13: case 15: case 16: return 1;
-    case 4: case 5: case 6: case 14: return 2;
+    case -1: case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
 }
@@ -526,8 +562,12 @@ void Plan::record(cudaStream_t s0, int stage) {
   char* lb = lists_.data();
   for (const Launch& L : seq_) {
     if (stage >= 0 && stage_of(L.kind) != stage) continue;
-    cudaStream_t s = L.stream ? aux_stream_ : s0;
+    cudaStream_t s = L.stream ? aux_streams_[L.stream - 1] : s0;
     if (L.wait_ev >= 0) cudaStreamWaitEvent(s, la_ev_[L.wait_ev], 0);
+    if (L.kind < 0) {
+      if (L.rec_ev >= 0) cudaEventRecord(la_ev_[L.rec_ev], s);
+      continue;
+    }
     const WorkItem* wl = reinterpret_cast<const WorkItem*>(lb + L.off);
     const GemmItem* gl = reinterpret_cast<const GemmItem*>(lb + L.off);
     switch (L.kind) {

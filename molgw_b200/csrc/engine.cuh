@@ -145,7 +145,8 @@ class Plan {
     int rec_ev;      // lookahead event to record after the launch (-1: none)
   };
   std::vector<cudaEvent_t> la_ev_;
-  cudaStream_t aux_stream_ = nullptr;
+  std::vector<cudaStream_t> aux_streams_;   // streams 1.. of the launch sequence (0 is the plan's stream)
+  int nchains_ = 1;
   std::vector<Launch> seq_;
   cudaGraph_t stage_graph_[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaGraphExec_t stage_exec_[4] = {nullptr, nullptr, nullptr, nullptr};
