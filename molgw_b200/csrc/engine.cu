@@ -56,11 +56,14 @@ Status DeviceBuffer::allocate(Context* ctx, size_t bytes, const char* name) {
   if (ctx->budget && ctx->in_use + bytes > ctx->budget)
     return Status::fail(RIGW_ERR_NOMEM, "%s: %zu bytes exceed the HBM budget (%zu in use of %zu)", name, bytes,
                         ctx->in_use, ctx->budget);
-  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&ptr_), bytes);
+  // Stream-ordered allocation from the device pool: memory released by a plan
+  // stays mapped in the pool and is handed to the next plan without remapping.
+  cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ptr_), bytes, ctx->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
   if (e != cudaSuccess) {
     ptr_ = nullptr;
     cudaGetLastError();
-    return Status::fail(RIGW_ERR_NOMEM, "%s: cudaMalloc(%zu) failed: %s", name, bytes, cudaGetErrorString(e));
+    return Status::fail(RIGW_ERR_NOMEM, "%s: cudaMallocAsync(%zu) failed: %s", name, bytes, cudaGetErrorString(e));
   }
   ctx_ = ctx;
   bytes_ = bytes;
@@ -71,7 +74,8 @@ Status DeviceBuffer::allocate(Context* ctx, size_t bytes, const char* name) {
 
 void DeviceBuffer::release() {
   if (ptr_) {
-    cudaFree(ptr_);
+    cudaStreamSynchronize(ctx_->stream);
+    cudaFreeAsync(ptr_, ctx_->stream);
     ctx_->in_use -= bytes_;
   }
   ptr_ = nullptr;
@@ -84,6 +88,10 @@ Status Context::init(int dev, size_t budget_bytes) {
   budget = budget_bytes;
   RIGW_CUDA_TRY(cudaSetDevice(dev));
   RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  cudaMemPool_t pool;
+  RIGW_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
+  uint64_t keep = ~uint64_t(0);
+  RIGW_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   RIGW_CUDA_TRY(prepare_dgemm_kernels());
   RIGW_CUDA_TRY(prepare_tc_kernels());
   return Status::ok();
@@ -91,7 +99,10 @@ Status Context::init(int dev, size_t budget_bytes) {
 
 Context::~Context() {
   plan_cache.clear();
-  if (stream) cudaStreamDestroy(stream);
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
 }
 
 // ---------------------------------------------------------------------------

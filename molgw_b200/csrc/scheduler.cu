@@ -25,6 +25,15 @@ size_t available_bytes(Context& c) {
     cudaGetLastError();
     free_b = 0;
   }
+  // memory held by the stream-ordered pool but not in use is available as well
+  cudaMemPool_t pool;
+  uint64_t reserved = 0, used = 0;
+  if (cudaDeviceGetDefaultMemPool(&pool, c.device) == cudaSuccess) {
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+  }
+  cudaGetLastError();
+  free_b += size_t(reserved > used ? reserved - used : 0);
   size_t avail = size_t(double(free_b) * 0.9);
   if (c.budget) avail = std::min(avail, c.budget > c.in_use ? c.budget - c.in_use : 0);
   return avail;
