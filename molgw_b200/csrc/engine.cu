@@ -197,7 +197,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       pp.off_in_weight = L.take(size_t(sh.nomega) * D);
       off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
       if (sh.precision == RIGW_BF16X3) {
-        off[i].xs = L.take(size_t(sh.nomega) * 2 * d.npad * d.nia_pad * 2);
+        off[i].xs = L.take(size_t(std::min(sh.nomega, kSplitGroup)) * 2 * d.npad * d.nia_pad * 2);
         off[i].tmap = L.take(128);
       }
       off[i].tnorm = L.take(size_t(d.nia_pad) * D);
@@ -243,6 +243,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       const Dims d = dims_of(sh, mode);
       const size_t t = size_t(d.npanel + 2) * (d.npanel + 2 + (d.ldb + 127) / 128) * 4;
       lists += size_t(sh.nomega) * t * sizeof(GemmItem) + size_t(d.nia_pad / 8 + d.npad * d.ldb / 1024 + 64) * 16;
+      if (sh.precision == RIGW_BF16X3)   // split items: one per (group, 64 transitions, 64 aux)
+        lists += size_t((sh.nomega + kSplitGroup - 1) / kSplitGroup) * (d.nia_pad / 64) * (d.npad / 64) *
+                 sizeof(WorkItem);
     }
     *measure_only = L.cur + lists + (size_t(1) << 20);
     return Status::ok();
@@ -279,10 +282,11 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     if (factor) {
       p.mp = dp(off[i].mp);
       p.kpad = d.nia_pad;
+      p.wgroup = std::max(1, std::min(sh.nomega, kSplitGroup));
       if (sh.precision == RIGW_BF16X3) {
         p.xs = base + off[i].xs;
         alignas(64) unsigned char map[128];
-        RIGW_TRY(make_split_tmap(map, p.xs, d.nia_pad, (long long)sh.nomega * 2 * d.npad));
+        RIGW_TRY(make_split_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * 2 * d.npad));
         RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
       }
       p.tnorm = dp(off[i].tnorm);
@@ -341,22 +345,30 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     if (factor) {
       for (int t0 = 0; t0 < p.nia_pad; t0 += 8) wl_pack_.push_back({i, t0, 0, 0});
       if (sh.precision == RIGW_BF16X3) {
-        for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
-          for (int p0 = 0; p0 < npad; p0 += 64) wl_split_.push_back({i, t0, p0, 0});
+        // frequencies in groups of p.wgroup sharing one hi/lo buffer: split(g), then chi0(g)
+        for (int w0 = 0, g = 0; w0 < sh.nomega; w0 += p.wgroup, ++g) {
+          if (int(wl_split_.size()) <= g) {
+            wl_split_.resize(g + 1);
+            tl_syrk_.resize(g + 1);
+          }
+          for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+            for (int p0 = 0; p0 < npad; p0 += 64) wl_split_[g].push_back({i, t0, p0, w0});
+        }
         for (int w = 0; w < sh.nomega; ++w)
           for (int ti = 0; ti < npad; ti += BMN)
             for (int tj = ti; tj < npad; tj += BMN) {
+              const int wl = w % p.wgroup;
               TcItem t{};
               t.tmap = base + off[i].tmap;
               t.C = p.eps + size_t(w) * npad * npad + size_t(ti) * npad + tj;
               t.err = err_dev_;
-              t.row_a = w * 2 * npad + ti;
-              t.row_b = w * 2 * npad + tj;
+              t.row_a = wl * 2 * npad + ti;
+              t.row_b = wl * 2 * npad + tj;
               t.lo_off = npad;
               t.ktiles = p.kpad / 64;
               t.ldc = npad;
               t.diag = ti - tj;
-              tl_syrk_.push_back(t);
+              tl_syrk_[w / p.wgroup].push_back(t);
             }
       }
       // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM),
@@ -491,8 +503,10 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(2, wl_rhs_.data(), sizeof(WorkItem), wl_rhs_.size(), 0);
   add(3, wl_mnorm_.data(), sizeof(WorkItem), wl_mnorm_.size(), 0);
   add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
-  add(12, wl_split_.data(), sizeof(WorkItem), wl_split_.size(), 0);
-  add(13, tl_syrk_.data(), sizeof(TcItem), tl_syrk_.size(), 0);
+  for (size_t g = 0; g < wl_split_.size(); ++g) {
+    add(12, wl_split_[g].data(), sizeof(WorkItem), wl_split_[g].size(), 0);
+    add(13, tl_syrk_[g].data(), sizeof(TcItem), tl_syrk_[g].size(), 0);
+  }
   add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
   // Panel loop of each chain with a one-panel lookahead: the update of the next

@@ -131,8 +131,8 @@ class Plan {
   std::vector<WorkItem> wl_pack_, wl_rhs_, wl_mnorm_, wl_energy_, wl_vchiv_, wl_sigma_, wl_pade_;
   std::vector<std::vector<WorkItem>> wl_diag_;
   std::vector<GemmItem> gl_syrk_;
-  std::vector<WorkItem> wl_split_;
-  std::vector<TcItem> tl_syrk_;
+  std::vector<std::vector<WorkItem>> wl_split_;   // per frequency group
+  std::vector<std::vector<TcItem>> tl_syrk_;
   std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_;
   std::vector<WorkItem> wl_trace_, wl_pad_;
   struct Launch {

@@ -36,7 +36,7 @@ __global__ void aomo_unpack_kernel(const AomoUnpackItem* items);
 
 // Split-precision chi0 (syrk_bf16x3.cu): one 128x128 upper tile of eps(iw).
 struct TcItem {
-  const void* tmap;   // CUtensorMap of the problem's hi/lo tensor (rows: [nomega][2][npad], cols: kpad)
+  const void* tmap;   // CUtensorMap of the problem's hi/lo tensor (rows: [wgroup][2][npad], cols: kpad)
   double* C;          // &eps[w][i0][j0]
   int* err;
   int row_a, row_b;   // tensor rows of the hi blocks of the A (i0) and B (j0) operands

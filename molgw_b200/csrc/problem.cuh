@@ -45,8 +45,9 @@ struct ProbDev {
   const double* zcalc;       // [nc] complex (re, im) evaluation points
   // ---- workspace (device)
   double* mp;
-  void* xs;                  // split precision: [nomega][2][npad][kpad] bf16 hi/lo of M sqrt(D_w)
+  void* xs;                  // split precision: [wgroup][2][npad][kpad] bf16 hi/lo of M sqrt(D_w)
   int kpad;                  // transitions padded to the 64-wide tensor-core K tile (== nia_pad)
+  int wgroup;                // frequencies per split group (one hi/lo buffer, reused group by group)
   double* tnorm;
   double* dscale;
   double* eps;

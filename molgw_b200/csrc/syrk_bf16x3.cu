@@ -40,7 +40,9 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
     tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
   }
   __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(p.xs);
-  for (int w = 0; w < p.nomega; ++w) {
+  const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);   // this item's frequency group
+  for (int w = w0; w < w1; ++w) {
+    const int wl = w - w0;
     __syncthreads();
     if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
     __syncthreads();
@@ -52,8 +54,8 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
       const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
       const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
       const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
-      const size_t hi_row = (size_t(2 * w) * p.npad + p0 + pp) * p.kpad + t0;
-      const size_t lo_row = (size_t(2 * w + 1) * p.npad + p0 + pp) * p.kpad + t0;
+      const size_t hi_row = (size_t(2 * wl) * p.npad + p0 + pp) * p.kpad + t0;
+      const size_t lo_row = (size_t(2 * wl + 1) * p.npad + p0 + pp) * p.kpad + t0;
       reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
       reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
     }
