@@ -458,7 +458,7 @@ def main():
         chi0_avg = float(np.mean(chi0_ms))
         achieved = chi0_flops(inst) / (chi0_avg * 1e-3) / 1e12
         traffic = profile_traffic("chi0_syrk_fp64_naux840.txt")
-        roofline = {"kernel": "chi0 contraction M D M^T (dgemm_mn_kernel<128,128>, FP64 DMMA)",
+        roofline = {"kernel": "chi0 contraction M D M^T (dgemm_mn_kernel<64,128>, FP64 DMMA)",
                     "bound": "tensor", "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                     "frac": achieved / fp64_peak, "traffic": traffic,
                     "peak_source": "measured cuBLAS DGEMM 8192^3 on this GPU (torch.matmul float64, best of 6); "

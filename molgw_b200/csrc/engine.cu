@@ -176,6 +176,20 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     return Status::fail(RIGW_ERR_ARG, "sigma plan needs resident factors");
   const size_t D = sizeof(double);
 
+  // Split precision: when the hi/lo buffers of every frequency of the batch are
+  // small, one group holds all frequencies (one split and one tensor-core launch
+  // with a full grid); otherwise groups of kSplitGroup frequencies share a buffer.
+  size_t split_all = 0;
+  for (const Shape& sh : shapes)
+    if (factor && sh.precision == RIGW_BF16X3) {
+      const Dims d = dims_of(sh, mode);
+      split_all += size_t(sh.nomega) * 2 * d.npad * d.nia_pad * 2;
+    }
+  const bool split_whole = split_all <= kSplitWholeBytes;
+  auto split_group = [&](const Shape& sh) {
+    return split_whole ? std::max(1, sh.nomega) : std::max(1, std::min(sh.nomega, kSplitGroup));
+  };
+
   // ---- memory layout
   Layout L;
   struct Off {
@@ -197,7 +211,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       pp.off_in_weight = L.take(size_t(sh.nomega) * D);
       off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
       if (sh.precision == RIGW_BF16X3) {
-        off[i].xs = L.take(size_t(std::min(sh.nomega, kSplitGroup)) * 2 * d.npad * d.nia_pad * 2);
+        off[i].xs = L.take(size_t(split_group(sh)) * 2 * d.npad * d.nia_pad * 2);
         off[i].tmap = L.take(128);
       }
       off[i].tnorm = L.take(size_t(d.nia_pad) * D);
@@ -282,7 +296,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     if (factor) {
       p.mp = dp(off[i].mp);
       p.kpad = d.nia_pad;
-      p.wgroup = std::max(1, std::min(sh.nomega, kSplitGroup));
+      p.wgroup = split_group(sh);
       if (sh.precision == RIGW_BF16X3) {
         p.xs = base + off[i].xs;
         alignas(64) unsigned char map[128];
