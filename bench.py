@@ -50,7 +50,8 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=32,
                     help="molecules of the ragged batch measured beside the single instance (0: skip)")
     ap.add_argument("--batch-reps", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "serve"])
+    ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep"])
+    ap.add_argument("--sweep-reps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-duration", type=float, default=60.0)
     ap.add_argument("--serve-workers", type=int, default=2)
@@ -293,6 +294,64 @@ def run_serve_line(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sweep_line(args):
+    """`--workload sweep`: the precision sweep on one large instance (Nocc=100,
+    Nvirt=1100, Naux=4000, 48 frequencies, seed 3, generated in device memory):
+    FP64, BF16x3 and Ozaki INT8 with 3..7 slices.  chi0 runs in the named
+    arithmetic, the eps factorization, Sigma and the QP solve in FP64; QP energies
+    are reported in meV against the FP64 solve of the same run.  One JSON line."""
+    import torch
+    from molgw_b200 import build, synth
+    build.build()
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64, RIGW_OZAKI, Engine
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    fp64_peak = measured_fp64_peak(torch)
+    no, nv, na, nw = 100, 1100, 4000, 48
+    inst, dev = synth.make_instance_device(no, nv, na, nw, 3)
+    torch.cuda.synchronize()
+    f_chi0 = float(nw) * na * (na + 1) * (no * nv)
+    clocks = ClockSampler(0)
+    clocks.start()
+    out, ref = {}, None
+    plan = [("fp64", RIGW_FP64, 1, fp64_peak, "measured cuBLAS DGEMM"),
+            ("bf16x3", RIGW_BF16X3, 3, bf16_peak, "MEASURED_PEAKS.json bf16_tflops")]
+    plan += [(f"ozaki{k}", RIGW_OZAKI(k), k * (k + 1) // 2, 2.0 * bf16_peak,
+              "2 x MEASURED_PEAKS.json bf16_tflops (dense int8 rate = 2 x bf16 on B200)") for k in range(3, 8)]
+    for name, prec, products, peak, peak_src in plan:
+        eng = Engine(0)                 # one context per precision: its plan is freed before the next
+        eng.g0w0(inst, prec, dev, qp_only=True)
+        tot, chi = [], []
+        for _ in range(args.sweep_reps):
+            o = eng.g0w0(inst, prec, dev, qp_only=True)
+            st = eng.last_stats()
+            tot.append(st["total_ms"])
+            chi.append(st["stage_ms"][1])
+        eng.close()
+        if ref is None:
+            ref = o
+        chi_ms = float(np.mean(chi))
+        achieved = f_chi0 / (chi_ms * 1e-3) / 1e12
+        out[name] = {"solves_per_s": 1e3 / float(np.mean(tot)), "ms_per_solve": float(np.mean(tot)),
+                     "chi0_ms": chi_ms, "stage_ms": st["stage_ms"],
+                     "chi0_tflops_algorithmic": achieved,
+                     "chi0_tensor_ops_per_s": achieved * products, "tensor_products": products,
+                     "chi0_frac_of_peak": achieved * products / peak, "peak": peak, "peak_source": peak_src,
+                     "qp_diff_mev_vs_fp64": float(np.abs(o.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3),
+                     "erpa_rel_diff_vs_fp64": float(abs(o.erpa - ref.erpa) / abs(ref.erpa))}
+    clk = clocks.stop()
+    line = {"metric": METRIC, "value": out["fp64"]["solves_per_s"], "unit": "solves/s", "n_gpus": 1,
+            "steps": args.sweep_reps, "warmup": 1, "ms_per_step": out["fp64"]["ms_per_solve"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded torch.Generator in device memory; energies U[-30,-8]/U[0.5,40] eV, "
+                    "M ~ N(0,s^2) scaled so max eig eps(i0) = 1.8)",
+            "config": {"workload": "precision sweep: Nocc=100 Nvirt=1100 Naux=4000, 48 imaginary frequencies, "
+                                   "QP-only outputs (HOMO/LUMO); value = the FP64 solve",
+                       "chi0_flops_algorithmic": f_chi0, "l2": "inputs larger than L2 (M is 3.5 GB)"},
+            "precisions": out, "clocks": clk}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the MOLGW path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -332,6 +391,13 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload == "sweep":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the CPU restatement of one Naux=4000 solve "
+                              "(84 TFLOP of chi0) does not finish in minutes"}), flush=True)
+            return
+        run_sweep_line(args)
         return
     if args.workload == "serve":
         run_serve_line(args)

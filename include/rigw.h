@@ -54,8 +54,14 @@ enum rigw_status {
  * the QP solve are FP64 in every mode). */
 enum rigw_precision {
   RIGW_FP64 = 0,           /* FP64 DMMA tensor cores end to end (the drop-in)            */
-  RIGW_BF16X3 = 1          /* split BF16 hi/lo products on tcgen05, FP32 accumulation    */
+  RIGW_BF16X3 = 1,         /* split BF16 hi/lo products on tcgen05, FP32 accumulation    */
+  RIGW_OZAKI_INT8 = 16     /* + s (3 <= s <= 7): Ozaki-sliced INT8 products on tcgen05,
+                              s signed 7-bit slices per row, exact INT32 accumulation,
+                              FP64 recombination; use RIGW_OZAKI(s)                      */
 };
+#define RIGW_OZAKI(s) (RIGW_OZAKI_INT8 + (s))
+#define RIGW_OZAKI_MIN_SLICES 3
+#define RIGW_OZAKI_MAX_SLICES 7
 
 enum rigw_technique {
   RIGW_PADE = 0,           /* imaginary_axis_pade: Thiele continuation                    */

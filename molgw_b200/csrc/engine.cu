@@ -31,7 +31,7 @@ Status make_shape(const rigw_problem& p, Shape* sh) {
     return Status::fail(RIGW_ERR_ARG, "nomega_sigma_calc=%d outside [0,128]", p.nomega_sigma_calc);
   if (p.technique != RIGW_PADE && p.technique != RIGW_HOMOLUMO)
     return Status::fail(RIGW_ERR_ARG, "unknown technique %d", p.technique);
-  if (p.precision != RIGW_FP64 && p.precision != RIGW_BF16X3)
+  if (p.precision != RIGW_FP64 && p.precision != RIGW_BF16X3 && !is_ozaki(p.precision))
     return Status::fail(RIGW_ERR_ARG, "unknown precision %d", p.precision);
   sh->naux = p.naux;
   sh->nocc = p.nocc;
@@ -94,6 +94,7 @@ Status Context::init(int dev, size_t budget_bytes) {
   RIGW_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   RIGW_CUDA_TRY(prepare_dgemm_kernels());
   RIGW_CUDA_TRY(prepare_tc_kernels());
+  RIGW_CUDA_TRY(prepare_ozaki_kernels());
   return Status::ok();
 }
 
@@ -117,7 +118,8 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   d.npad = round_up(sh.naux, kPanel);
   d.npanel = d.npad / kPanel;
   d.nia = sh.nocc * sh.nvirt;
-  d.nia_pad = round_up(std::max(d.nia, 1), 64);
+  // the int8 tensor-core K tile is 128 transitions (128 bytes), the bf16 one 64
+  d.nia_pad = round_up(std::max(d.nia, 1), is_ozaki(sh.precision) ? 128 : 64);
   d.want_identity =
       (mode == kPlanPolar || ((mode == kPlanFused || mode == kPlanPartial) && !sh.qp_only)) ? 1 : 0;
   d.moff = d.want_identity ? d.npad : 0;
@@ -181,9 +183,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // with a full grid); otherwise groups of kSplitGroup frequencies share a buffer.
   size_t split_all = 0;
   for (const Shape& sh : shapes)
-    if (factor && sh.precision == RIGW_BF16X3) {
+    if (factor && sh.precision != RIGW_FP64) {
       const Dims d = dims_of(sh, mode);
-      split_all += size_t(sh.nomega) * 2 * d.npad * d.nia_pad * 2;
+      split_all += size_t(sh.nomega) * d.npad * d.nia_pad * (is_ozaki(sh.precision) ? ozaki_slices(sh.precision) : 4);
     }
   const bool split_whole = split_all <= kSplitWholeBytes;
   auto split_group = [&](const Shape& sh) {
@@ -193,7 +195,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // ---- memory layout
   Layout L;
   struct Off {
-    size_t mp, xs, tmap, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, tr, en, sc, sr, qp;
+    size_t mp, xs, tmap, rmax, xexp, tnorm, dscale, eps, winv, logdet, rhs, colsq, mnorm, vchiv, ew, tr, en, sc, sr, qp;
   };
   std::vector<Off> off(np);
   for (int i = 0; i < np; ++i) {
@@ -213,6 +215,11 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       if (sh.precision == RIGW_BF16X3) {
         off[i].xs = L.take(size_t(split_group(sh)) * 2 * d.npad * d.nia_pad * 2);
         off[i].tmap = L.take(128);
+      } else if (is_ozaki(sh.precision)) {
+        off[i].xs = L.take(size_t(split_group(sh)) * ozaki_slices(sh.precision) * d.npad * d.nia_pad);
+        off[i].tmap = L.take(128);
+        off[i].rmax = L.take(size_t(sh.nomega) * d.npad * sizeof(unsigned long long));
+        off[i].xexp = L.take(size_t(sh.nomega) * d.npad * sizeof(int));
       }
       off[i].tnorm = L.take(size_t(d.nia_pad) * D);
       off[i].dscale = L.take(size_t(sh.nomega) * d.nia_pad * D);
@@ -257,9 +264,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       const Dims d = dims_of(sh, mode);
       const size_t t = size_t(d.npanel + 2) * (d.npanel + 2 + (d.ldb + 127) / 128) * 4;
       lists += size_t(sh.nomega) * t * sizeof(GemmItem) + size_t(d.nia_pad / 8 + d.npad * d.ldb / 1024 + 64) * 16;
-      if (sh.precision == RIGW_BF16X3)   // split items: one per (group, 64 transitions, 64 aux)
-        lists += size_t((sh.nomega + kSplitGroup - 1) / kSplitGroup) * (d.nia_pad / 64) * (d.npad / 64) *
-                 sizeof(WorkItem);
+      if (sh.precision != RIGW_FP64)   // split items: one per (group, 64 transitions, 64 aux), + row maxima
+        lists += size_t((sh.nomega + kSplitGroup - 1) / kSplitGroup + 1) * (d.nia_pad / 64) * (d.npad / 64) *
+                     sizeof(WorkItem) + size_t(sh.nomega) * d.npad / 4096 * sizeof(WorkItem) + 64;
     }
     *measure_only = L.cur + lists + (size_t(1) << 20);
     return Status::ok();
@@ -301,6 +308,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         p.xs = base + off[i].xs;
         alignas(64) unsigned char map[128];
         RIGW_TRY(make_split_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * 2 * d.npad));
+        RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
+      } else if (is_ozaki(sh.precision)) {
+        p.slices = ozaki_slices(sh.precision);
+        p.xs = base + off[i].xs;
+        p.rmax = reinterpret_cast<unsigned long long*>(base + off[i].rmax);
+        p.xexp = reinterpret_cast<int*>(base + off[i].xexp);
+        alignas(64) unsigned char map[128];
+        RIGW_TRY(make_ozaki_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * p.slices * d.npad));
         RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
       }
       p.tnorm = dp(off[i].tnorm);
@@ -387,6 +402,39 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       }
       // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM),
       // over the naux x naux block only; the identity pads are written afterwards
+      if (is_ozaki(sh.precision)) {
+        // row maxima of S over every frequency, then per frequency group: slices, chi0
+        for (size_t e = 0; e < size_t(sh.nomega) * npad; e += 4096) wl_ozzero_.push_back({i, int(e), 0, 0});
+        for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+          for (int p0 = 0; p0 < npad; p0 += 64) wl_rowmax_.push_back({i, t0, p0, 0});
+        for (int w0 = 0, g = 0; w0 < sh.nomega; w0 += p.wgroup, ++g) {
+          if (int(wl_slice_.size()) <= g) {
+            wl_slice_.resize(g + 1);
+            tl_ozaki_.resize(g + 1);
+          }
+          for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+            for (int p0 = 0; p0 < npad; p0 += 64) wl_slice_[g].push_back({i, t0, p0, w0});
+        }
+        for (int w = 0; w < sh.nomega; ++w)
+          for (int ti = 0; ti < npad; ti += BMN)
+            for (int tj = ti; tj < npad; tj += BMN) {
+              const int wl = w % p.wgroup;
+              TcItem t{};
+              t.tmap = base + off[i].tmap;
+              t.C = p.eps + size_t(w) * npad * npad + size_t(ti) * npad + tj;
+              t.err = err_dev_;
+              t.row_a = wl * p.slices * npad + ti;
+              t.row_b = wl * p.slices * npad + tj;
+              t.lo_off = npad;
+              t.ktiles = p.kpad / 128;
+              t.ldc = npad;
+              t.diag = ti - tj;
+              t.ea = p.xexp + size_t(w) * npad + ti;
+              t.eb = p.xexp + size_t(w) * npad + tj;
+              t.slices = p.slices;
+              tl_ozaki_[w / p.wgroup].push_back(t);
+            }
+      }
       for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
         double* E = p.eps + size_t(w) * npad * npad;
         if (npad > sh.naux) wl_pad_.push_back({i, w, 0, 0});
@@ -521,6 +569,12 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     add(12, wl_split_[g].data(), sizeof(WorkItem), wl_split_[g].size(), 0);
     add(13, tl_syrk_[g].data(), sizeof(TcItem), tl_syrk_[g].size(), 0);
   }
+  add(17, wl_ozzero_.data(), sizeof(WorkItem), wl_ozzero_.size(), 0);
+  add(18, wl_rowmax_.data(), sizeof(WorkItem), wl_rowmax_.size(), 0);
+  for (size_t g = 0; g < wl_slice_.size(); ++g) {
+    add(19, wl_slice_[g].data(), sizeof(WorkItem), wl_slice_[g].size(), 0);
+    add(20, tl_ozaki_[g].data(), sizeof(TcItem), tl_ozaki_[g].size(), 0);
+  }
   add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
   // Panel loop of each chain with a one-panel lookahead: the update of the next
@@ -591,7 +645,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: case 12: case 13: case 15: case 16: return 1;
+    case 1: case 12: case 13: case 15: case 16: case 17: case 18: case 19: case 20: return 1;
     case -1: case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
@@ -617,6 +671,10 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 16: pad_eps_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
       case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
+      case 17: launch_ozaki_zero(probs_dev_, wl, L.count, s); break;
+      case 18: launch_ozaki_rowmax(probs_dev_, wl, L.count, s); break;
+      case 19: launch_ozaki_slice(probs_dev_, wl, L.count, s); break;
+      case 20: launch_syrk_ozaki(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 4: chol_diag_kernel<<<L.count, kDiagThreads, 0, s>>>(probs_dev_, wl, L.arg); break;

@@ -69,6 +69,11 @@ class DeviceBuffer {
   size_t bytes_ = 0;
 };
 
+inline bool is_ozaki(int precision) {
+  return precision >= RIGW_OZAKI(RIGW_OZAKI_MIN_SLICES) && precision <= RIGW_OZAKI(RIGW_OZAKI_MAX_SLICES);
+}
+inline int ozaki_slices(int precision) { return is_ozaki(precision) ? precision - RIGW_OZAKI_INT8 : 0; }
+
 // Shapes of one problem of a plan (derived from rigw_problem).
 struct Shape {
   int naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision;
@@ -133,6 +138,9 @@ class Plan {
   std::vector<GemmItem> gl_syrk_;
   std::vector<std::vector<WorkItem>> wl_split_;   // per frequency group
   std::vector<std::vector<TcItem>> tl_syrk_;
+  std::vector<WorkItem> wl_ozzero_, wl_rowmax_;    // Ozaki: row maxima over every frequency
+  std::vector<std::vector<WorkItem>> wl_slice_;   // Ozaki: per frequency group
+  std::vector<std::vector<TcItem>> tl_ozaki_;
   std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_;
   std::vector<WorkItem> wl_trace_, wl_pad_;
   struct Launch {
@@ -198,5 +206,6 @@ bool bf16x3_available();
 Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes);
 Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res);
 Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
+Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows);
 
 }  // namespace rigw

@@ -44,9 +44,19 @@ struct TcItem {
   int ktiles;         // kpad / 64
   int ldc;            // npad
   int diag;           // i0 - j0: identity where (col - row) == diag
+  // Ozaki INT8 (syrk_ozaki.cu): row_a/row_b address slice 1, lo_off is the row
+  // distance between slices, ktiles = kpad / 128
+  const int* ea;      // row exponents of the A rows (e_p, p = i0 ..)
+  const int* eb;      // row exponents of the B rows (e_q, q = j0 ..)
+  int slices;
 };
 void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s);
+void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
+void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
+void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
+void launch_syrk_ozaki(const TcItem* items, int n, cudaStream_t s);
+cudaError_t prepare_ozaki_kernels();
 cudaError_t prepare_tc_kernels();
 
 // Host-side launchers of the DMMA tile engine (gemm_f64.cu).

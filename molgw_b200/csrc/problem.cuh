@@ -45,9 +45,13 @@ struct ProbDev {
   const double* zcalc;       // [nc] complex (re, im) evaluation points
   // ---- workspace (device)
   double* mp;
-  void* xs;                  // split precision: [wgroup][2][npad][kpad] bf16 hi/lo of M sqrt(D_w)
-  int kpad;                  // transitions padded to the 64-wide tensor-core K tile (== nia_pad)
-  int wgroup;                // frequencies per split group (one hi/lo buffer, reused group by group)
+  void* xs;                  // split precision: [wgroup][2][npad][kpad] bf16 hi/lo of M sqrt(D_w);
+                             // Ozaki: [wgroup][slices][npad][kpad] int8 slices of M sqrt(D_w) 2^-e
+  int kpad;                  // transitions padded to the tensor-core K tile (== nia_pad)
+  int wgroup;                // frequencies per split group (one buffer, reused group by group)
+  int slices;                // Ozaki slices (0: not Ozaki)
+  unsigned long long* rmax;  // Ozaki: [nomega][npad] max_t |S_pt| as double bits (atomicMax)
+  int* xexp;                 // Ozaki: [nomega][npad] row exponents e_p
   double* tnorm;
   double* dscale;
   double* eps;

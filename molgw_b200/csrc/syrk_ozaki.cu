@@ -1,0 +1,295 @@
+// Ozaki-sliced INT8 chi0 contraction on the 5th-generation tensor cores.
+//
+//   eps(iw) = 1 + S S^T,  S = M diag(sqrt(D_w))
+//   row p of S is scaled by 2^-e_p, e_p the exponent of max_t |S_pt| (so |x| < 1):
+//     x_pt = S_pt 2^-e_p = sum_{k=1..s} q_k(p,t) 2^-7k + r,  q_k integers in [-127, 127],
+//   each q_k the truncated integer part of the residual times 128 (exact in FP64).
+//   (S S^T)_pq ~= 2^(e_p+e_q) sum_{d=2..s+1} 2^-7d L_d(p,q),   L_d = sum_{i+j=d} Q_i Q_j^T
+//   (the products of level i+j > s+1 are dropped, as in the Ozaki scheme).
+//
+// L_d is an exact INT32 sum (tcgen05.mma kind::i8).  K is consumed in chunks of
+// kOzChunk k-tiles (4096 transitions): |L_d| <= s * 4096 * 127^2 < 2^31 on one
+// chunk, so no sum can overflow; every (chunk, level) accumulator is drained
+// into FP64 registers with its weight 2^-7d while the MMA warp fills another of
+// the four TMEM accumulators.
+//
+// ozaki_zero_kernel:   clears the per-row maxima of a problem.
+// ozaki_rowmax_kernel: max_t |S_pt| for every frequency and row (atomicMax on the
+//                      bit pattern of a non-negative double: order independent).
+// ozaki_slice_kernel:  row exponents and the s int8 slices of one frequency group,
+//                      K-major (transition-contiguous) for TMA.
+// syrk_ozaki_kernel:   one 128x128 upper tile of eps(iw) per CTA; warp 0 issues
+//                      TMA loads (one A and one B slice tile of 128 rows x 128
+//                      transitions per stage, 128-byte swizzle, 6 stages), warp 1
+//                      issues the MMAs, warps 2..9 drain.  All waits are bounded.
+#include "engine.cuh"
+#include "tc_common.cuh"
+
+namespace rigw {
+
+// ---------------------------------------------------------------------------
+// item: (prob, first entry); 256 threads clear 4096 entries.
+__global__ void __launch_bounds__(256) ozaki_zero_kernel(const ProbDev* __restrict__ probs,
+                                                         const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  const size_t n = size_t(p.nomega) * p.npad;
+  for (int k = threadIdx.x; k < 4096; k += 256) {
+    const size_t e = size_t(wi.a) + k;
+    if (e < n) p.rmax[e] = 0ull;
+  }
+}
+
+// item: (prob, t0, p0): a 64 (transitions) x 64 (rows) tile, every frequency.
+__global__ void __launch_bounds__(256) ozaki_rowmax_kernel(const ProbDev* __restrict__ probs,
+                                                           const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  const int t0 = wi.a, p0 = wi.b;
+  __shared__ double tile[64][65];   // [row p][transition t]
+  __shared__ double sc[64];
+  __shared__ double part[4][64];
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int tt = idx >> 6, pp = idx & 63;
+    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
+  }
+  const int pp = tid & 63, tq = tid >> 6;
+  for (int w = 0; w < p.nomega; ++w) {
+    __syncthreads();
+    if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+    __syncthreads();
+    double m = 0.0;
+#pragma unroll
+    for (int t = tq * 16; t < tq * 16 + 16; ++t) m = fmax(m, fabs(tile[pp][t] * sc[t]));
+    part[tq][pp] = m;
+    __syncthreads();
+    if (tid < 64) {
+      m = fmax(fmax(part[0][tid], part[1][tid]), fmax(part[2][tid], part[3][tid]));
+      if (m > 0.0) atomicMax(p.rmax + size_t(w) * p.npad + p0 + tid, (unsigned long long)__double_as_longlong(m));
+    }
+  }
+}
+
+// item: (prob, t0, p0, w0): the same tile for the frequencies w0 .. w0+wgroup-1.
+__global__ void __launch_bounds__(256) ozaki_slice_kernel(const ProbDev* __restrict__ probs,
+                                                          const WorkItem* __restrict__ items) {
+  const WorkItem wi = items[blockIdx.x];
+  const ProbDev& p = probs[wi.prob];
+  const int t0 = wi.a, p0 = wi.b;
+  __shared__ double tile[64][65];   // [row p][transition t]
+  __shared__ double sc[64];         // sqrt(D_w(t0 + t))
+  __shared__ double rs[64];         // 2^-e_p
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int tt = idx >> 6, pp = idx & 63;
+    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
+  }
+  int8_t* xq = reinterpret_cast<int8_t*>(p.xs);
+  const int ns = p.slices;
+  const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);
+  for (int w = w0; w < w1; ++w) {
+    const int wl = w - w0;
+    __syncthreads();
+    if (tid < 64) {
+      sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+    } else if (tid < 128) {
+      const int pp = tid - 64;
+      const double m = __longlong_as_double((long long)p.rmax[size_t(w) * p.npad + p0 + pp]);
+      int e = 0;
+      if (m > 0.0) frexp(m, &e);    // m = f 2^e, f in [0.5, 1): every |S_pt| of the row is < 2^e
+      rs[pp] = ldexp(1.0, -e);
+      if (t0 == 0) p.xexp[size_t(w) * p.npad + p0 + pp] = e;
+    }
+    __syncthreads();
+    const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
+#pragma unroll 1
+    for (int pr = 0; pr < 8; ++pr) {
+      const int pp = warp * 8 + pr;
+      double x0 = tile[pp][2 * lane] * s0 * rs[pp];
+      double x1 = tile[pp][2 * lane + 1] * s1 * rs[pp];
+      for (int k = 0; k < ns; ++k) {
+        const double v0 = x0 * 128.0, v1 = x1 * 128.0;
+        const double q0 = trunc(v0), q1 = trunc(v1);
+        x0 = v0 - q0;
+        x1 = v1 - q1;
+        const size_t row = (size_t(wl * ns + k) * p.npad + p0 + pp) * p.kpad + t0;
+        reinterpret_cast<char2*>(xq + row)[lane] = make_char2(char(int(q0)), char(int(q1)));
+      }
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+constexpr int kOzStages = 6;
+constexpr int kOzTileBytes = 128 * 128;                 // 128 rows x 128 int8 transitions
+constexpr int kOzStageBytes = 2 * kOzTileBytes;
+constexpr size_t kOzSmemBytes = size_t(kOzStages) * kOzStageBytes + 1024 + 256;
+constexpr int kOzChunk = 32;                            // k-tiles per exact INT32 accumulation
+constexpr int kOzAcc = 4;                               // TMEM accumulators of 128 columns
+constexpr int kOzThreads = 320;                         // warp 0 TMA, warp 1 MMA, warps 2..9 drain
+
+__global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem* __restrict__ items) {
+  const TcItem it = items[blockIdx.x];
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOzStages * kOzStageBytes);
+  uint64_t* empty = full + kOzStages;
+  uint64_t* accf = empty + kOzStages;     // [kOzAcc] unit accumulated
+  uint64_t* acce = accf + kOzAcc;         // [kOzAcc] unit drained
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + kOzAcc);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto tile = [&](int s, int which) { return smem + s * kOzStageBytes + which * kOzTileBytes; };
+
+  if (tid == 0) {
+    for (int s = 0; s < kOzStages; ++s) {
+      tc::mbar_init(&full[s], 1);
+      tc::mbar_init(&empty[s], 1);
+    }
+    for (int b = 0; b < kOzAcc; ++b) {
+      tc::mbar_init(&accf[b], 1);
+      tc::mbar_init(&acce[b], 8);
+    }
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tslot, 128 * kOzAcc);
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const int nk = it.ktiles;
+  const int ns = it.slices;
+  const int nchunks = (nk + kOzChunk - 1) / kOzChunk;
+  // Work order (identical in the producer and the MMA issuer): chunk c, level
+  // d = 2..ns+1, slice pair (i, d-i), k-tile of the chunk.  One unit = (c, d).
+
+  if (tid == 0) {
+    // ---- TMA producer
+    tc::tmap_acquire(it.tmap);
+    int issued[kOzStages] = {0, 0, 0, 0, 0, 0};
+    bool ok = true;
+    int step = 0;
+    for (int c = 0; c < nchunks && ok; ++c) {
+      const int k0 = c * kOzChunk, k1 = min(nk, k0 + kOzChunk);
+      for (int d = 2; d <= ns + 1 && ok; ++d)
+        for (int i = max(1, d - ns); i <= min(ns, d - 1) && ok; ++i)
+          for (int kt = k0; kt < k1; ++kt, ++step) {
+            const int s = step % kOzStages;
+            if (step >= kOzStages && !tc::mbar_wait(&empty[s], ((step / kOzStages) - 1) & 1)) {
+              ok = false;
+              break;
+            }
+            tc::mbar_arrive_expect_tx(&full[s], kOzStageBytes);
+            tc::tma_load_2d(tile(s, 0), it.tmap, &full[s], kt * 128, it.row_a + (i - 1) * it.lo_off);
+            tc::tma_load_2d(tile(s, 1), it.tmap, &full[s], kt * 128, it.row_b + (d - i - 1) * it.lo_off);
+            ++issued[s];
+          }
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+    for (int s = 0; s < kOzStages; ++s)
+      if (issued[s] > 0 && !tc::mbar_wait(&full[s], (issued[s] - 1) & 1)) atomicOr(it.err, kErrTimeout);
+  } else if (tid == 32) {
+    // ---- MMA issuer
+    constexpr uint32_t idesc = tc::idesc_s8_s32(128, 128);
+    bool ok = true;
+    int step = 0, u = 0;
+    for (int c = 0; c < nchunks && ok; ++c) {
+      const int k0 = c * kOzChunk, k1 = min(nk, k0 + kOzChunk);
+      for (int d = 2; d <= ns + 1 && ok; ++d, ++u) {
+        const int b = u % kOzAcc;
+        if (u >= kOzAcc && !tc::mbar_wait(&acce[b], ((u / kOzAcc) - 1) & 1)) {
+          ok = false;
+          break;
+        }
+        tc::tc_fence_after();
+        const uint32_t dt = tmem + uint32_t(b * 128);
+        bool first = true;
+        for (int i = max(1, d - ns); i <= min(ns, d - 1) && ok; ++i)
+          for (int kt = k0; kt < k1; ++kt, ++step) {
+            const int s = step % kOzStages;
+            if (!tc::mbar_wait(&full[s], (step / kOzStages) & 1)) {
+              ok = false;
+              break;
+            }
+            tc::tc_fence_after();
+            const uint64_t ad = tc::desc_kmajor_sw128(tile(s, 0)), bd = tc::desc_kmajor_sw128(tile(s, 1));
+#pragma unroll
+            for (int sub = 0; sub < 4; ++sub) {
+              const uint64_t o = uint64_t(sub * 2);   // 32 int8 = 32 bytes along K
+              tc::mma_s8(dt, ad + o, bd + o, idesc, (first && sub == 0) ? 0u : 1u);
+            }
+            first = false;
+            tc::mma_commit(&empty[s]);
+          }
+        if (ok) tc::mma_commit(&accf[b]);
+      }
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+  } else if (warp >= 2) {
+    // ---- drain: every (chunk, level) accumulator into FP64 with weight 2^-7d
+    const int quad = warp & 3;                 // TMEM lanes 32*quad .. 32*quad+31 (rows)
+    const int half = (warp - 2) >> 2;          // columns 64*half .. 64*half+63
+    const int row = quad * 32 + lane;
+    double acc[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    bool ok = true;
+    int u = 0;
+    for (int c = 0; c < nchunks && ok; ++c)
+      for (int d = 2; d <= ns + 1; ++d, ++u) {
+        const int b = u % kOzAcc;
+        ok = __all_sync(0xffffffffu, tc::mbar_wait(&accf[b], (u / kOzAcc) & 1));
+        if (!ok) break;
+        tc::tc_fence_after();
+        const double wd = ldexp(1.0, -7 * d);
+        const uint32_t base = tmem + uint32_t(b * 128 + half * 64) + (uint32_t(quad * 32) << 16);
+        uint32_t r[32];
+        tc::tmem_ld_32x32(base, r);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += double(int(r[j])) * wd;
+        tc::tmem_ld_32x32(base + 32, r);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[32 + j] += double(int(r[j])) * wd;
+        tc::tc_fence_before();
+        __syncwarp();
+        if (lane == 0) tc::mbar_arrive(&acce[b]);
+      }
+    if (ok) {
+      const int er = it.ea[row];
+      double* dst = it.C + size_t(row) * it.ldc + half * 64;
+#pragma unroll
+      for (int j = 0; j < 64; j += 2) {
+        const int col = half * 64 + j;
+        double v0 = ldexp(acc[j], er + it.eb[col]), v1 = ldexp(acc[j + 1], er + it.eb[col + 1]);
+        if (col - row == it.diag) v0 += 1.0;
+        if (col + 1 - row == it.diag) v1 += 1.0;
+        *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
+      }
+    } else if (lane == 0) {
+      atomicOr(it.err, kErrTimeout);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 128 * kOzAcc);
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
+  if (n > 0) ozaki_zero_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
+  if (n > 0) ozaki_rowmax_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
+  if (n > 0) ozaki_slice_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+void launch_syrk_ozaki(const TcItem* items, int n, cudaStream_t s) {
+  if (n > 0) syrk_ozaki_kernel<<<n, kOzThreads, kOzSmemBytes, s>>>(items);
+}
+
+cudaError_t prepare_ozaki_kernels() {
+  return cudaFuncSetAttribute(syrk_ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kOzSmemBytes));
+}
+
+}  // namespace rigw

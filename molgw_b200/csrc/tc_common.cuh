@@ -85,6 +85,14 @@ RIGW_DEVICE_INLINE void mma_bf16(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc
       "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
       "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
 }
+// D[tmem] (+)= A[smem] * B[smem]^T, kind::i8 (signed 8-bit inputs, exact INT32 accumulation).
+RIGW_DEVICE_INLINE void mma_s8(uint32_t d_tmem, uint64_t adesc, uint64_t bdesc, uint32_t idesc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(acc));
+}
 // Arrive on an mbarrier when all previously issued MMAs of this thread are done.
 RIGW_DEVICE_INLINE void mma_commit(uint64_t* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
@@ -117,6 +125,11 @@ RIGW_DEVICE_INLINE uint64_t desc_kmajor_sw128(const void* smem) {
   d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
   d |= uint64_t(2) << 61;                  // SWIZZLE_128B
   return d;
+}
+
+// Instruction descriptor, kind::i8: signed 8-bit A/B (K-major), s32 D, shape M x N.
+constexpr uint32_t idesc_s8_s32(int M, int N) {
+  return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 
 // Instruction descriptor, kind::f16: bf16 A/B (K-major), fp32 D, shape M x N.

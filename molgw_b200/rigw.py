@@ -27,6 +27,16 @@ LIB_PATH = Path(__file__).resolve().parent / "librigw.so"
 
 RIGW_FP64 = 0
 RIGW_BF16X3 = 1
+RIGW_OZAKI_INT8 = 16
+
+
+def RIGW_OZAKI(slices: int) -> int:
+    """Precision code of the Ozaki-sliced INT8 chi0 with ``slices`` 7-bit slices (3..7)."""
+    if not 3 <= slices <= 7:
+        raise ValueError(f"Ozaki slices must be in [3, 7], got {slices}")
+    return RIGW_OZAKI_INT8 + slices
+
+
 RIGW_PADE = 0
 RIGW_HOMOLUMO = 1
 RIGW_PROBLEM_DEVICE_POINTERS = 1
@@ -265,14 +275,16 @@ class Engine:
                           r.ehomo, r.elumo, r.device_ms)
 
     # ---------------------------------------------------------------- fused
-    def g0w0_batch(self, insts, precision: int = RIGW_FP64, device_arrays=None,
+    def g0w0_batch(self, insts, precision=RIGW_FP64, device_arrays=None,
                    qp_only: bool = False) -> list[G0W0Output]:
+        """One call for many molecules; ``precision`` is one code for all or one per molecule."""
         n = len(insts)
+        precs = list(precision) if isinstance(precision, (list, tuple)) else [precision] * n
         probs = (Problem * n)()
         ress = (Result * n)()
         keep, bufs = [], []
         for i, inst in enumerate(insts):
-            p, k = self.make_problem(inst, precision, device_arrays[i] if device_arrays else None,
+            p, k = self.make_problem(inst, precs[i], device_arrays[i] if device_arrays else None,
                                      qp_only=qp_only)
             probs[i] = p
             keep.append(k)
