@@ -95,6 +95,8 @@ Status Context::init(int dev, size_t budget_bytes) {
   RIGW_CUDA_TRY(prepare_dgemm_kernels());
   RIGW_CUDA_TRY(prepare_tc_kernels());
   RIGW_CUDA_TRY(prepare_ozaki_kernels());
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(chol_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(chol_diag_smem_bytes())));
   return Status::ok();
 }
 
@@ -360,7 +362,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // The factorization and solves of independent (problem, frequency) pairs run
   // as two chains on their own streams, each with its own one-panel lookahead,
   // so that one chain's launch tails and diagonal blocks overlap the other's GEMMs.
-  nchains_ = npairs >= 8 ? 2 : 1;
+  // frequency chains: independent factorization sequences on their own streams,
+  // at least kChainPairs (problem, frequency) pairs each
+  nchains_ = std::max(1, std::min(kMaxChains, npairs / kChainPairs));
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});
@@ -677,7 +681,7 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 20: launch_syrk_ozaki(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
-      case 4: chol_diag_kernel<<<L.count, kDiagThreads, 0, s>>>(probs_dev_, wl, L.arg); break;
+      case 4: chol_diag_kernel<<<L.count, kDiagThreads, chol_diag_smem_bytes(), s>>>(probs_dev_, wl, L.arg); break;
       case 5: launch_dgemm_128x128(gl, L.count, s); break;
       case 6: launch_dgemm_64x128(gl, L.count, s); break;
       case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;

@@ -15,8 +15,9 @@ struct WorkItem {
 __global__ void pack_m_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void init_rhs_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void mnorm_kernel(const ProbDev* probs, const WorkItem* items);
-constexpr int kDiagThreads = 512;  // threads of chol_diag_kernel (kPanel columns x 4 row groups)
+constexpr int kDiagThreads = 256;  // threads of chol_diag_kernel
 __global__ void chol_diag_kernel(const ProbDev* probs, const WorkItem* items, int k);
+size_t chol_diag_smem_bytes();   // dynamic shared memory of chol_diag_kernel
 __global__ void energy_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void trace_kernel(const ProbDev* probs, const WorkItem* items);
 __global__ void pad_eps_kernel(const ProbDev* probs, const WorkItem* items);

@@ -133,16 +133,70 @@ __global__ void __launch_bounds__(256) mnorm_kernel(const ProbDev* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------
-// Diagonal block of panel k: A_kk = U^T U (upper Cholesky) and W = U^-1 in one
-// sweep.  Gaussian elimination of the symmetric block, with the same row
-// operations applied to an identity block stored in the (initially zero)
-// strictly lower triangle, leaves D L^T in the upper triangle and L^-1 (unit
-// diagonal implicit) in the lower one, where A = L D L^T.  Then U = D^-1/2 (D L^T)
-// and W = U^-1 = L^-T D^-1/2, i.e. W[l][m] = (L^-1)[m][l] / sqrt(d_m).
-// One CTA of kDiagThreads threads per (prob, frequency); thread t owns column
-// l = t % kPanel and rows i = t / kPanel + kDiagGroups * r of the block.
-constexpr int kDiagGroups = kDiagThreads / kPanel;        // 4
-constexpr int kDiagRows = kPanel / kDiagGroups;           // 32 rows per thread
+// Diagonal block of panel k: A_kk = U^T U (upper Cholesky, in place) and
+// W = U^-1 (to winv), blocked in shared memory.  One CTA of kDiagThreads threads
+// per (prob, frequency).  Shared memory holds the block (U in its upper
+// triangle, W^T in its strictly lower triangle), 1/U(i,i), dense copies of the
+// four 32x32 diagonal blocks of W^T and a scratch for the W products.
+// For each 32-row block j (right-looking):
+//   a. one warp factors and inverts A_jj in registers: Gaussian elimination of
+//      [A_jj | I] (lane l owns column l; the identity part lives in the strictly
+//      lower triangle) leaves D L^T above and L^-1 below the diagonal,
+//      A_jj = L D L^T; U_jj = D^-1/2 (D L^T), W_jj = U_jj^-1 = L^-T D^-1/2;
+//   b. the rest of the 32 rows: U_j,rest = W_jj^T A_j,rest          (DMMA);
+//   c. trailing update A_rest,rest -= U_j,rest^T U_j,rest, upper part (DMMA).
+// Then the off-diagonal blocks of W by increasing distance from the diagonal:
+//   W_ab = -W_aa (sum_{a<m<b} U_am W_mb + U_ab W_bb)                 (DMMA).
+constexpr int kDiagLd = kPanel + 4;      // shared row stride of the block (doubles)
+constexpr int kDiagPb = 32;              // rows per block
+constexpr int kDiagNb = kPanel / kDiagPb;
+constexpr int kDiagTld = kDiagPb + 1;    // row stride of the 32x32 scratch blocks
+constexpr int kDiagWarps = kDiagThreads / 32;
+
+// One 8x8 tile C += X Y with X (8 x K) and Y (K x 8) in shared memory:
+// X(r, k) = xs[r * xr + k * xk], Y(k, c) = ys[k * yk + c * yc].  Lane (g, q):
+// c0 = C(g, 2q), c1 = C(g, 2q + 1).
+RIGW_DEVICE_INLINE void smem_tile_mma(double& c0, double& c1, const double* xs, int xr, int xk, const double* ys,
+                                      int yk, int yc, int K, int lane) {
+  const int g = lane >> 2, q = lane & 3;
+  const double* xp = xs + g * xr + q * xk;
+  const double* yp = ys + q * yk + g * yc;
+#pragma unroll 4
+  for (int k0 = 0; k0 < K; k0 += 4) dmma_8x8x4(c0, c1, xp[k0 * xk], yp[k0 * yk]);
+}
+
+// Step a for the 32x32 block at (j0, j0), one warp, lane l owning column l.
+// Kept out of line: its 32-double column then stays in registers.
+__device__ __noinline__ void diag_block_factor(double* S, double* wdt, int j0, double* piv, double* invd, int* err) {
+  const int lane = threadIdx.x & 31;
+  double col[kDiagPb];
+  double myd = 0.0;
+#pragma unroll
+  for (int i = 0; i < kDiagPb; ++i) col[i] = (i <= lane) ? S[(j0 + i) * kDiagLd + j0 + lane] : 0.0;
+#pragma unroll
+  for (int j = 0; j < kDiagPb; ++j) {
+    const double d = __shfl_sync(0xffffffffu, col[j], j);
+    const double xj = ((lane == j) ? 1.0 : col[j]) * __drcp_rn(d);   // multiplier row j
+#pragma unroll
+    for (int i = j + 1; i < kDiagPb; ++i) {
+      const double aji = __shfl_sync(0xffffffffu, col[j], i);          // A(j,i), held by lane i
+      if (lane >= i || lane <= j) col[i] -= aji * xj;
+    }
+    if (lane == j) myd = d;
+  }
+  const double r = 1.0 / sqrt(myd);
+  piv[j0 + lane] = myd;
+  invd[j0 + lane] = r;
+  if (!(myd > 0.0)) atomicOr(err, kErrNotSPD);
+  // row i <= lane: U(i, lane); row i > lane: W(lane, i) stored transposed;
+  // wdt[i][lane] = W^T(i, lane) densely (zero above the diagonal)
+#pragma unroll
+  for (int i = 0; i < kDiagPb; ++i) {
+    const double v = col[i] * __shfl_sync(0xffffffffu, r, i);
+    S[(j0 + i) * kDiagLd + j0 + lane] = v;
+    wdt[i * kDiagTld + lane] = (i > lane) ? v : (i == lane ? r : 0.0);
+  }
+}
 
 __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* __restrict__ probs,
                                                                  const WorkItem* __restrict__ items, int k) {
@@ -151,56 +205,122 @@ __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* 
   const int w = wi.a;
   const int ld = p.npad;
   double* A = p.eps + size_t(w) * ld * ld + size_t(k) * kPanel * ld + size_t(k) * kPanel;
-  __shared__ double rowbuf[2][kPanel];
-  __shared__ double piv[kPanel];
-  __shared__ double invd[kPanel];
-  const int t = threadIdx.x;
-  const int l = t % kPanel;
-  const int i0 = t / kPanel;
-  double v[kDiagRows];
-#pragma unroll
-  for (int r = 0; r < kDiagRows; ++r) {
-    const int i = i0 + kDiagGroups * r;
-    v[r] = (l >= i) ? A[size_t(i) * ld + l] : 0.0;
+  extern __shared__ double dsm[];
+  double* S = dsm;                                   // [kPanel][kDiagLd]
+  double* WdT = S + kPanel * kDiagLd;                // [kDiagNb][kDiagPb][kDiagTld] dense W_jj^T
+  double* T = WdT + kDiagNb * kDiagPb * kDiagTld;    // [kDiagNb-1][kDiagPb][kDiagTld]
+  double* piv = T + (kDiagNb - 1) * kDiagPb * kDiagTld;   // [kPanel]
+  double* invd = piv + kPanel;                       // [kPanel] 1/U(i,i) = W(i,i)
+  const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+  const int g = lane >> 2, q = lane & 3;
+#pragma unroll 8
+  for (int idx = t; idx < kPanel * kPanel; idx += kDiagThreads) {
+    const int i = idx / kPanel, l = idx % kPanel;
+    S[i * kDiagLd + l] = (l >= i) ? A[size_t(i) * ld + l] : 0.0;
   }
+  __syncthreads();
+
+  for (int jb = 0; jb < kDiagNb; ++jb) {
+    const int j0 = jb * kDiagPb;
+    double* wdt = WdT + jb * kDiagPb * kDiagTld;
+    if (warp == 0) diag_block_factor(S, wdt, j0, piv, invd, p.err);
+    __syncthreads();
+    const int base = j0 + kDiagPb, n = kPanel - base;
+    if (n == 0) break;
+    // b. U_j,rest = W_jj^T A_j,rest: 4 x n/8 tiles, at most 6 per warp; the
+    //    results replace A_j,rest after every warp has read it
+    {
+      constexpr int kMaxTiles = 4 * (kPanel - kDiagPb) / 8 / kDiagWarps;
+      double r0[kMaxTiles], r1[kMaxTiles];
+      const int ntile = 4 * (n / 8);
 #pragma unroll
-  for (int r = 0; r < kDiagRows; ++r) {
-#pragma unroll
-    for (int q = 0; q < kDiagGroups; ++q) {
-      const int j = kDiagGroups * r + q;
-      if (i0 == q) rowbuf[j & 1][l] = v[r];
-      __syncthreads();
-      const double pj = rowbuf[j & 1][j];
-      if (t == 0) piv[j] = pj;
-      // multiplier row: A part (l > j) or the L^-1 part (l < j); the implicit unit diagonal at l == j
-      const double xj = (l == j ? 1.0 : rowbuf[j & 1][l]) / pj;
-#pragma unroll
-      for (int rr = r; rr < kDiagRows; ++rr) {
-        const int i = i0 + kDiagGroups * rr;
-        if (i > j && (l >= i || l <= j)) v[rr] -= rowbuf[j & 1][i] * xj;
+      for (int u = 0; u < kMaxTiles; ++u) {
+        r0[u] = r1[u] = 0.0;
+        const int tile = warp + kDiagWarps * u;
+        if (tile < ntile) {
+          const int rt = tile & 3, ct = tile >> 2;
+          smem_tile_mma(r0[u], r1[u], wdt + 8 * rt * kDiagTld, kDiagTld, 1, S + j0 * kDiagLd + base + 8 * ct,
+                        kDiagLd, 1, kDiagPb, lane);
+        }
       }
+      __syncthreads();
+#pragma unroll
+      for (int u = 0; u < kMaxTiles; ++u) {
+        const int tile = warp + kDiagWarps * u;
+        if (tile < ntile) {
+          const int rt = tile & 3, ct = tile >> 2;
+          double* c = S + (j0 + 8 * rt + g) * kDiagLd + base + 8 * ct + 2 * q;
+          c[0] = r0[u];
+          c[1] = r1[u];
+        }
+      }
+      __syncthreads();
+    }
+    // c. A_rest,rest -= U_j,rest^T U_j,rest on the upper 8x8 tiles
+    {
+      const int nt = n / 8;
+      for (int tile = warp; tile < nt * nt; tile += kDiagWarps) {
+        const int rt = tile / nt, ct = tile % nt;
+        if (rt > ct) continue;
+        double c0 = 0.0, c1 = 0.0;
+        smem_tile_mma(c0, c1, S + j0 * kDiagLd + base + 8 * rt, 1, kDiagLd, S + j0 * kDiagLd + base + 8 * ct,
+                      kDiagLd, 1, kDiagPb, lane);
+        const int row = base + 8 * rt + g, col = base + 8 * ct + 2 * q;
+        if (row <= col) S[row * kDiagLd + col] -= c0;
+        if (row <= col + 1) S[row * kDiagLd + col + 1] -= c1;
+      }
+      __syncthreads();
     }
   }
-  __syncthreads();
-  if (t < kPanel) {
-    const double pv = piv[t];
-    if (!(pv > 0.0)) atomicOr(p.err, kErrNotSPD);
-    invd[t] = 1.0 / sqrt(pv);
+
+  // Off-diagonal blocks of W; W(r, c) (r < c) is kept at S[c][r].
+  for (int lev = 1; lev < kDiagNb; ++lev) {
+    const int ntile = (kDiagNb - lev) * 16;          // 16 tiles of 8x8 per 32x32 block
+    for (int tile = warp; tile < ntile; tile += kDiagWarps) {   // T_a = sum_{a<m<b} U_am W_mb + U_ab W_bb
+      const int a = tile >> 4, rt = (tile >> 2) & 3, ct = tile & 3;
+      const int b = a + lev;
+      double c0 = 0.0, c1 = 0.0;
+      if (lev > 1)
+        smem_tile_mma(c0, c1, S + (a * kDiagPb + 8 * rt) * kDiagLd + (a + 1) * kDiagPb, kDiagLd, 1,
+                      S + (b * kDiagPb + 8 * ct) * kDiagLd + (a + 1) * kDiagPb, 1, kDiagLd, (lev - 1) * kDiagPb, lane);
+      smem_tile_mma(c0, c1, S + (a * kDiagPb + 8 * rt) * kDiagLd + b * kDiagPb, kDiagLd, 1,
+                    WdT + (b * kDiagPb + 8 * ct) * kDiagTld, 1, kDiagTld, kDiagPb, lane);
+      double* tp = T + (a * kDiagPb + 8 * rt + g) * kDiagTld + 8 * ct + 2 * q;
+      tp[0] = c0;
+      tp[1] = c1;
+    }
+    __syncthreads();
+    for (int tile = warp; tile < ntile; tile += kDiagWarps) {   // W_ab = -W_aa T_a
+      const int a = tile >> 4, rt = (tile >> 2) & 3, ct = tile & 3;
+      const int b = a + lev;
+      double c0 = 0.0, c1 = 0.0;
+      smem_tile_mma(c0, c1, WdT + a * kDiagPb * kDiagTld + 8 * rt, 1, kDiagTld, T + a * kDiagPb * kDiagTld + 8 * ct,
+                    kDiagTld, 1, kDiagPb, lane);
+      const int r = a * kDiagPb + 8 * rt + g, c = b * kDiagPb + 8 * ct + 2 * q;
+      S[c * kDiagLd + r] = -c0;
+      S[(c + 1) * kDiagLd + r] = -c1;
+    }
+    __syncthreads();
   }
-  __syncthreads();
+
   double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
-#pragma unroll
-  for (int r = 0; r < kDiagRows; ++r) {
-    const int i = i0 + kDiagGroups * r;
-    if (l >= i) A[size_t(i) * ld + l] = v[r] * invd[i];
-    W[l * kPanel + i] = (l < i) ? v[r] * invd[i] : (l == i ? invd[i] : 0.0);
+#pragma unroll 4
+  for (int idx = t; idx < kPanel * kPanel; idx += kDiagThreads) {
+    const int i = idx / kPanel, l = idx % kPanel;
+    if (l >= i) A[size_t(i) * ld + l] = S[i * kDiagLd + l];
+    // W[i][l] = U^-1(i,l): stored transposed at S[l][i] for i < l
+    W[idx] = (i < l) ? S[l * kDiagLd + i] : (i == l ? invd[i] : 0.0);
   }
   if (t < 32) {
-    double s = 0.0;
-    for (int m = t; m < kPanel; m += 32) s += log(piv[m]);
-    s = warp_sum(s);
-    if (t == 0) p.logdet[size_t(w) * p.npanel + k] = s;
+    double sl = 0.0;
+    for (int m = t; m < kPanel; m += 32) sl += log(piv[m]);
+    sl = warp_sum(sl);
+    if (t == 0) p.logdet[size_t(w) * p.npanel + k] = sl;
   }
+}
+
+size_t chol_diag_smem_bytes() {
+  return (size_t(kPanel) * kDiagLd + size_t(2 * kDiagNb - 1) * kDiagPb * kDiagTld + 2 * kPanel) * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
