@@ -150,6 +150,12 @@ def profile_traffic(name: str):
     return None
 
 
+def compact_tuning(rep: dict) -> dict:
+    """The autotuner's choice and its effect, without the candidate list."""
+    return {k: rep[k] for k in ("chi0_rows", "update_rows", "split_group", "chains", "default_ms", "tuned_ms")} | {
+        "candidates": len(rep["candidates"])}
+
+
 def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
     """The ragged batch (Nocc ~ U{5..60}, Nvirt = round(Nocc*U[8,10]), Naux =
     4(Nocc+Nvirt), 32 frequencies, seeds 4..) in one call, split precision and
@@ -165,7 +171,10 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
         devs.append(dev)
     torch.cuda.synchronize()
     res, outs = {}, {}
+    tuning = {}
     for prec, name in ((RIGW_BF16X3, "bf16x3"), (RIGW_FP64, "fp64")):
+        # the autotuner runs on the first 8 molecules; its choice applies to the whole batch
+        tuning[name] = compact_tuning(eng.autotune(insts[:8], prec, devs[:8], qp_only=True))
         eng.g0w0_batch(insts, prec, devs, qp_only=True)
         dev_ms, wall_ms = [], []
         for _ in range(reps):
@@ -179,7 +188,8 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
         res[name] = {"solves_per_s": count / (np.mean(dev_ms) * 1e-3),
                      "solves_per_s_wall": count / (np.mean(wall_ms) * 1e-3),
                      "ms_per_batch": float(np.mean(dev_ms)), "wall_ms_per_batch": float(np.mean(wall_ms)),
-                     "waves": st["waves"], "chunks": st["chunks"], "kernel_launches": st["kernel_launches"]}
+                     "waves": st["waves"], "chunks": st["chunks"], "kernel_launches": st["kernel_launches"],
+                     "tuning": tuning[name]}
     dqp = max(float(np.abs(a.energy_qp_g - b.energy_qp_g).max()) for a, b in zip(outs["fp64"], outs["bf16x3"]))
     res["qp_max_diff_mev_split_vs_fp64"] = dqp * HA_EV * 1e3
     res["speedup_split_vs_fp64"] = res["bf16x3"]["solves_per_s"] / res["fp64"]["solves_per_s"]
@@ -435,6 +445,8 @@ def main():
         flush.fill_(1.0)
         torch.cuda.synchronize()
 
+    # launch shapes chosen by the library's autotuner on this instance (untimed)
+    tune_main = compact_tuning(eng.autotune([inst], precision, [dev]))
     for _ in range(args.warmup):
         eng.g0w0(inst, precision, device_arrays=dev)
     # ---------------- timed region: device events per solve
@@ -468,6 +480,7 @@ def main():
     other = RIGW_BF16X3 if precision == RIGW_FP64 else RIGW_FP64
     alt = None
     try:
+        tune_alt = compact_tuning(eng.autotune([inst], other, [dev]))
         for _ in range(2):
             eng.g0w0(inst, other, device_arrays=dev)
         alt_ms, alt_chi0, alt_outs = [], [], []
@@ -482,16 +495,10 @@ def main():
                "ms_per_step": float(np.mean(alt_ms)), "chi0_ms": float(np.mean(alt_chi0)),
                "stage_ms": eng.last_stats()["stage_ms"],
                "qp_diff_mev_vs_" + args.precision: float(
-                   np.abs(alt_outs[-1].energy_qp_g - outs[-1].energy_qp_g).max() * HA_EV * 1e3)}
+                   np.abs(alt_outs[-1].energy_qp_g - outs[-1].energy_qp_g).max() * HA_EV * 1e3),
+               "tuning": tune_alt}
     except Exception as exc:    # precision unavailable on this device: reported, not hidden
         alt = {"error": str(exc)}
-
-    batched = None
-    if args.batch_count > 0 and world == 1:
-        try:
-            batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2)
-        except Exception as exc:    # reported, not hidden
-            batched = {"error": str(exc)}
 
     # ---------------- end to end through the host-pointer C-ABI call
     pinned = {k: torch.from_numpy(np.ascontiguousarray(v)).pin_memory().numpy() for k, v in host_arrays.items()}
@@ -518,6 +525,13 @@ def main():
         e2e_total = float(t.item())
     e2e_value = world * args.steps / e2e_total
 
+    batched = None
+    if args.batch_count > 0 and world == 1:
+        try:
+            batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2)
+        except Exception as exc:    # reported, not hidden
+            batched = {"error": str(exc)}
+
     if rank == 0:
         fp64_peak = measured_fp64_peak(torch)
         peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
@@ -540,7 +554,8 @@ def main():
             "config": {"workload": WORKLOAD, "precision": args.precision,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "flushed between solves (512 MiB write)", "sigma_states": "HOMO, LUMO",
-                       "nomega_sigma_calc": inst.nomega_sigma_calc, "nomega_sigma": inst.nomega_sigma},
+                       "nomega_sigma_calc": inst.nomega_sigma_calc, "nomega_sigma": inst.nomega_sigma,
+                       "tuning": tune_main},
             "latency_ms": {"p50": float(np.percentile(dev_ms, 50)), "p99": float(np.percentile(dev_ms, 99))},
             "stage_ms": {"pack": stages[0], "chi0": stages[1], "eps_factor_solve": stages[2],
                          "sigma_qp": stages[3]},

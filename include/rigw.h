@@ -178,6 +178,28 @@ RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* res
 /* Many problems of different sizes in one launch sequence (one CUDA graph). */
 RIGW_API int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_result* results);
 
+/* ---- autotuner ----------------------------------------------------------------
+ * No routine of the reference corresponds to this.  Times launch-shape
+ * candidates on the given batch (which must fit the device in one plan): the
+ * row height of the FP64 chi0 and trailing-update tiles (64 or 128 rows x 128
+ * columns) and the number of frequency chains (the split-precision buffer size
+ * follows the free memory of each batch and is not tuned).  The fastest shapes are kept in the context for every later
+ * batch of the same precision class (FP64, BF16x3, Ozaki, mixed); results of a
+ * solve do not depend on them beyond floating-point summation order. */
+#define RIGW_TUNE_MAX_CANDIDATES 16
+typedef struct rigw_tune_report {
+  int chi0_rows;             /* FP64 chi0 tile rows chosen (64 or 128)                    */
+  int update_rows;           /* trailing-update tile rows chosen (64 or 128)              */
+  int split_group;           /* frequencies per split buffer (0: automatic, not tuned)    */
+  int chains;                /* frequency chains (0: automatic)                           */
+  int precision_class;       /* 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed                    */
+  int ncandidates;
+  int candidate[RIGW_TUNE_MAX_CANDIDATES][4];          /* (chi0_rows, update_rows, split_group, chains) */
+  float candidate_ms[RIGW_TUNE_MAX_CANDIDATES][3];     /* chi0 stage, factorization stage, total      */
+  float default_ms, tuned_ms;  /* device time of one solve before and after tuning        */
+} rigw_tune_report;
+RIGW_API int rigw_autotune(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_tune_report* report);
+
 /* ---- request loop (continuous batching) --------------------------------------
  * No routine of the reference corresponds to this (MOLGW runs one molecule per
  * process); it serves many G0W0 solves on one GPU.  `workers` threads each own a

@@ -123,6 +123,14 @@ int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_re
   return finish(ctx, rigw::solve_batch(ctx->impl, nprob, probs, results));
 }
 
+int rigw_autotune(rigw_ctx* ctx, int nprob, const rigw_problem* probs, rigw_tune_report* report) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (nprob <= 0 || !probs || !report) return finish(ctx, Status::fail(RIGW_ERR_ARG, "empty batch"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::autotune(ctx->impl, nprob, probs, report));
+}
+
 int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result) {
   return rigw_g0w0_batch(ctx, 1, prob, result);
 }

@@ -159,18 +159,30 @@ Plan::~Plan() {
     if (s) cudaStreamDestroy(s);
 }
 
-size_t Plan::measure(const std::vector<Shape>& shapes, PlanMode mode) {
+size_t Plan::measure(const std::vector<Shape>& shapes, PlanMode mode, const Tuning* tune) {
   Plan p;
   size_t bytes = 0;
-  Status s = p.build(nullptr, mode, shapes, {}, &bytes);
+  Status s = p.build(nullptr, mode, shapes, {}, &bytes, tune);
   return s.good() ? bytes : size_t(-1);
 }
 
+int precision_class(const std::vector<Shape>& shapes) {
+  int cls = -1;
+  for (const Shape& sh : shapes) {
+    const int c = sh.precision == RIGW_FP64 ? 0 : (sh.precision == RIGW_BF16X3 ? 1 : 2);
+    cls = (cls < 0 || cls == c) ? c : 3;
+  }
+  return cls < 0 ? 0 : cls;
+}
+
 Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
-                   const std::vector<const ProbDev*>& factors, size_t* measure_only) {
+                   const std::vector<const ProbDev*>& factors, size_t* measure_only, const Tuning* tune) {
   ctx_ = ctx;
   mode_ = mode;
   shapes_ = shapes;
+  tune_ = tune ? *tune : (ctx ? ctx->tuning_for(mode, shapes) : Tuning{});
+  if (tune_.chi0_rows != 128) tune_.chi0_rows = 64;
+  if (tune_.update_rows != 128) tune_.update_rows = 64;
   const int np = int(shapes.size());
   probs_.assign(np, PlanProblem{});
   const bool factor = (mode == kPlanFused || mode == kPlanPolar || mode == kPlanPartial);
@@ -191,6 +203,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     }
   const bool split_whole = split_all <= kSplitWholeBytes;
   auto split_group = [&](const Shape& sh) {
+    if (tune_.split_group > 0) return std::max(1, std::min(sh.nomega, tune_.split_group));
     return split_whole ? std::max(1, sh.nomega) : std::max(1, std::min(sh.nomega, kSplitGroup));
   };
 
@@ -352,8 +365,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   }
 
   // ---- work lists
-  const int BMN = 128;   // column width of every DMMA item
-  const int BM = 64;     // row height of the chi0 and trailing-update items
+  const int BMN = 128;                  // column width of every DMMA item
+  const int BMC = tune_.chi0_rows;      // row height of the FP64 chi0 items
+  const int BM = tune_.update_rows;     // row height of the trailing-update items
   int max_panels = 0, npairs = 0;
   for (int i = 0; i < np; ++i) {
     max_panels = std::max(max_panels, probs_[i].dev.npanel);
@@ -364,7 +378,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // so that one chain's launch tails and diagonal blocks overlap the other's GEMMs.
   // frequency chains: independent factorization sequences on their own streams,
   // at least kChainPairs (problem, frequency) pairs each
-  nchains_ = std::max(1, std::min(kMaxChains, npairs / kChainPairs));
+  nchains_ = tune_.chains > 0 ? std::max(1, std::min({tune_.chains, kMaxChains, npairs}))
+                              : std::max(1, std::min(kMaxChains, npairs / kChainPairs));
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});
@@ -442,7 +457,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
         double* E = p.eps + size_t(w) * npad * npad;
         if (npad > sh.naux) wl_pad_.push_back({i, w, 0, 0});
-        for (int ti = 0; ti < sh.naux; ti += BM)
+        for (int ti = 0; ti < sh.naux; ti += BMC)
           for (int tj = ti / BMN * BMN; tj < sh.naux; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
@@ -451,7 +466,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             g.C = E + size_t(ti) * npad + tj;
             g.ldc = npad;
             g.kscale = p.dscale + size_t(w) * p.nia_pad;
-            g.m = std::min(BM, sh.naux - ti);
+            g.m = std::min(BMC, sh.naux - ti);
             g.n = std::min(BMN, sh.naux - tj);
             g.k = p.nia_pad;
             g.flags = kAddIdentity;
@@ -669,8 +684,14 @@ void Plan::record(cudaStream_t s0, int stage) {
     const GemmItem* gl = reinterpret_cast<const GemmItem*>(lb + L.off);
     switch (L.kind) {
       case 0: pack_m_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
-      case 1: launch_dgemm_64x128(gl, L.count, s); break;
-      case 14: launch_dgemm_64x128(gl, L.count, s); break;
+      case 1:
+        if (tune_.chi0_rows == 128) launch_dgemm_128x128(gl, L.count, s);
+        else launch_dgemm_64x128(gl, L.count, s);
+        break;
+      case 6: case 14:
+        if (tune_.update_rows == 128) launch_dgemm_128x128(gl, L.count, s);
+        else launch_dgemm_64x128(gl, L.count, s);
+        break;
       case 15: trace_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 16: pad_eps_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
@@ -683,7 +704,6 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 4: chol_diag_kernel<<<L.count, kDiagThreads, chol_diag_smem_bytes(), s>>>(probs_dev_, wl, L.arg); break;
       case 5: launch_dgemm_128x128(gl, L.count, s); break;
-      case 6: launch_dgemm_64x128(gl, L.count, s); break;
       case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 8: energy_sum_kernel<<<(L.count + 127) / 128, 128, 0, s>>>(probs_dev_, L.count); break;
       case 9: vchiv_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;

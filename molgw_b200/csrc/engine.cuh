@@ -81,6 +81,18 @@ struct Shape {
   bool operator<(const Shape& o) const;
 };
 
+// Launch shapes of a plan that the autotuner chooses (rigw_autotune); zero
+// fields mean the built-in rule.
+struct Tuning {
+  int chi0_rows = 64;     // FP64 chi0 items: rows per 128-column item (64 or 128)
+  int update_rows = 64;   // trailing-update items: rows per 128-column item (64 or 128)
+  int split_group = 0;    // split precision: frequencies per hi/lo buffer (0: automatic)
+  int chains = 0;         // frequency chains of the factorization stage (0: automatic)
+};
+// Precision class of a batch (tunings are kept per mode and class):
+// 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed.
+int precision_class(const std::vector<Shape>& shapes);
+
 enum PlanMode : int {
   kPlanFused = 0,      // chi0 -> eps -> factor -> [I | M_sigma] solve -> Sigma -> QP
   kPlanPolar = 1,      // chi0 -> eps -> factor -> I solve -> energies (factors stay resident)
@@ -102,10 +114,13 @@ struct PlanProblem {
 // launch sequence of one group of problems.
 class Plan {
  public:
+  // tune: launch shapes (nullptr: the context's tuning for this mode and class)
   Status build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes,
-               const std::vector<const ProbDev*>& factors, size_t* measure_only = nullptr);
+               const std::vector<const ProbDev*>& factors, size_t* measure_only = nullptr,
+               const Tuning* tune = nullptr);
   // Device bytes a plan of these shapes allocates (arena + work lists).
-  static size_t measure(const std::vector<Shape>& shapes, PlanMode mode);
+  static size_t measure(const std::vector<Shape>& shapes, PlanMode mode, const Tuning* tune = nullptr);
+  const Tuning& tuning() const { return tune_; }
   // Copy inputs (host or device pointers) and run; results stay on the device.
   Status stage_inputs(const rigw_problem* probs, cudaStream_t s);
   Status stage_sigma_calc(int i, const double* sigma_calc_host, cudaStream_t s);
@@ -126,6 +141,7 @@ class Plan {
   void record(cudaStream_t s, int stage);
   Context* ctx_ = nullptr;
   PlanMode mode_ = kPlanFused;
+  Tuning tune_;
   std::vector<Shape> shapes_;
   std::vector<PlanProblem> probs_;
   DeviceBuffer arena_;
@@ -185,6 +201,12 @@ class Context {
   std::map<std::pair<int, std::vector<Shape>>, std::unique_ptr<Plan>> plan_cache;
   bool use_graphs = true;
   rigw_stats last_stats{};
+  // autotuned launch shapes by (mode, precision class)
+  std::map<std::pair<int, int>, Tuning> tuned;
+  Tuning tuning_for(int mode, const std::vector<Shape>& shapes) const {
+    auto it = tuned.find({mode, precision_class(shapes)});
+    return it == tuned.end() ? Tuning{} : it->second;
+  }
   Status init(int dev, size_t budget_bytes);
   ~Context();
 };
@@ -205,6 +227,8 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
 bool bf16x3_available();
 Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes);
 Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res);
+Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* rep);
+size_t available_bytes(Context& c);
 Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
 Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows);
 

@@ -17,8 +17,6 @@
 
 namespace rigw {
 
-namespace {
-
 size_t available_bytes(Context& c) {
   size_t free_b = 0, total_b = 0;
   if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
@@ -38,6 +36,8 @@ size_t available_bytes(Context& c) {
   if (c.budget) avail = std::min(avail, c.budget > c.in_use ? c.budget - c.in_use : 0);
   return avail;
 }
+
+namespace {
 
 Status get_plan(Context& c, PlanMode mode, const std::vector<Shape>& shapes, Plan** out) {
   auto key = std::make_pair(int(mode), shapes);
@@ -110,7 +110,8 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
   const size_t usable = avail + cached;
 
   // ---- fits: one fused plan
-  if (Plan::measure(shapes, kPlanFused) <= usable) {
+  const Tuning tune = c.tuning_for(kPlanFused, shapes);
+  if (Plan::measure(shapes, kPlanFused, &tune) <= usable) {
     Plan* plan = nullptr;
     RIGW_TRY(get_plan(c, kPlanFused, shapes, &plan));
     RIGW_TRY(run_plan(c, plan, probs, res, nullptr, true));
@@ -209,6 +210,87 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
   }
   c.last_stats.chunks = int(units.size());
   c.last_stats.waves = waves;
+  return Status::ok();
+}
+
+// ---------------------------------------------------------------------------
+// Autotuner: times launch-shape candidates on the caller's batch (a plan that
+// fits the device) and keeps the fastest per (fused mode, precision class) for
+// every later plan of that class.  Coordinate descent: the chi0-stage shape
+// (FP64 item height) by the chi0 stage time, then the
+// factorization-stage shapes (trailing-update item height, chains) by the
+// factorization stage time; every candidate is launched twice and timed on the
+// second launch (CUDA events between the stage graphs).
+Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* rep) {
+  std::vector<Shape> shapes;
+  RIGW_TRY(validate_batch(n, probs, &shapes));
+  std::memset(rep, 0, sizeof(*rep));
+  c.plan_cache.clear();
+  const size_t avail = available_bytes(c);
+  const int cls = precision_class(shapes);
+  bool any_fp64 = false;
+  for (const Shape& sh : shapes) any_fp64 = any_fp64 || sh.precision == RIGW_FP64;
+  Tuning best = c.tuning_for(kPlanFused, shapes);
+  if (Plan::measure(shapes, kPlanFused, &best) > avail)
+    return Status::fail(RIGW_ERR_NOMEM, "autotune: the batch does not fit the device in one plan");
+
+  auto run = [&](const Tuning& t, float* stage) -> Status {
+    if (Plan::measure(shapes, kPlanFused, &t) > avail) return Status::fail(RIGW_ERR_NOMEM, "candidate too large");
+    Plan p;
+    RIGW_TRY(p.build(&c, kPlanFused, shapes, {}, nullptr, &t));
+    RIGW_TRY(p.stage_inputs(probs, c.stream));
+    for (int rep2 = 0; rep2 < 2; ++rep2) {
+      RIGW_TRY(p.launch(c.stream));
+      RIGW_TRY(p.check_errors(c.stream));
+    }
+    for (int k = 0; k < 4; ++k) stage[k] = p.stage_ms()[k];
+    return Status::ok();
+  };
+  auto record = [&](const Tuning& t, const float* st) {
+    if (rep->ncandidates >= RIGW_TUNE_MAX_CANDIDATES) return;
+    const int k = rep->ncandidates++;
+    rep->candidate[k][0] = t.chi0_rows;
+    rep->candidate[k][1] = t.update_rows;
+    rep->candidate[k][2] = t.split_group;
+    rep->candidate[k][3] = t.chains;
+    rep->candidate_ms[k][0] = st[1];
+    rep->candidate_ms[k][1] = st[2];
+    rep->candidate_ms[k][2] = st[0] + st[1] + st[2] + st[3];
+  };
+  float bst[4];
+  RIGW_TRY(run(best, bst));
+  record(best, bst);
+  rep->default_ms = bst[0] + bst[1] + bst[2] + bst[3];
+  // try one field at a time; keep a candidate when its stage is faster
+  auto try_field = [&](int Tuning::*field, std::initializer_list<int> values, int stage) -> Status {
+    const int cur = best.*field;
+    for (int v : values) {
+      if (v == cur) continue;
+      Tuning t = best;
+      t.*field = v;
+      float st[4];
+      Status s = run(t, st);
+      if (s.code == RIGW_ERR_NOMEM) continue;
+      RIGW_TRY(s);
+      record(t, st);
+      if (st[stage] < bst[stage]) {
+        best = t;
+        std::memcpy(bst, st, sizeof(bst));
+      }
+    }
+    return Status::ok();
+  };
+  if (any_fp64) RIGW_TRY(try_field(&Tuning::chi0_rows, {64, 128}, 1));
+  RIGW_TRY(try_field(&Tuning::update_rows, {64, 128}, 2));
+  RIGW_TRY(try_field(&Tuning::chains, {1, 2}, 2));
+  c.tuned[{int(kPlanFused), cls}] = best;
+  c.plan_cache.clear();
+  rep->chi0_rows = best.chi0_rows;
+  rep->update_rows = best.update_rows;
+  rep->split_group = best.split_group;
+  rep->chains = best.chains;
+  rep->precision_class = cls;
+  rep->tuned_ms = bst[0] + bst[1] + bst[2] + bst[3];
   return Status::ok();
 }
 

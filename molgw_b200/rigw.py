@@ -82,6 +82,19 @@ class Stats(C.Structure):
     ]
 
 
+RIGW_TUNE_MAX_CANDIDATES = 16
+
+
+class TuneReport(C.Structure):
+    _fields_ = [
+        ("chi0_rows", C.c_int), ("update_rows", C.c_int), ("split_group", C.c_int), ("chains", C.c_int),
+        ("precision_class", C.c_int), ("ncandidates", C.c_int),
+        ("candidate", (C.c_int * 4) * RIGW_TUNE_MAX_CANDIDATES),
+        ("candidate_ms", (C.c_float * 3) * RIGW_TUNE_MAX_CANDIDATES),
+        ("default_ms", C.c_float), ("tuned_ms", C.c_float),
+    ]
+
+
 def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     path = Path(path)
     if not path.exists():
@@ -105,6 +118,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
+    lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
     lib.rigw_qp_solve_noalloc.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_int, C.c_int,
                                           C.c_double, C.c_double, C.c_double, C.c_double, _dp, _dp, _dp, _dp,
                                           C.c_void_p, C.c_char_p, C.c_size_t]
@@ -293,6 +307,28 @@ class Engine:
             bufs.append(b)
         self._check(self._lib.rigw_g0w0_batch(self._h, n, probs, ress), "rigw_g0w0_batch")
         return [self._output(ress[i], bufs[i]) for i in range(n)]
+
+    def autotune(self, insts, precision=RIGW_FP64, device_arrays=None, qp_only: bool = False) -> dict:
+        """Time launch-shape candidates on this batch; the context keeps the fastest
+        for later batches of the same precision class.  Returns the report."""
+        n = len(insts)
+        precs = list(precision) if isinstance(precision, (list, tuple)) else [precision] * n
+        probs = (Problem * n)()
+        keep = []
+        for i, inst in enumerate(insts):
+            p, k = self.make_problem(inst, precs[i], device_arrays[i] if device_arrays else None,
+                                     qp_only=qp_only)
+            probs[i] = p
+            keep.append(k)
+        rep = TuneReport()
+        self._check(self._lib.rigw_autotune(self._h, n, probs, C.byref(rep)), "rigw_autotune")
+        cands = [{"chi0_rows": rep.candidate[k][0], "update_rows": rep.candidate[k][1],
+                  "split_group": rep.candidate[k][2], "chains": rep.candidate[k][3],
+                  "chi0_ms": rep.candidate_ms[k][0], "factor_ms": rep.candidate_ms[k][1],
+                  "total_ms": rep.candidate_ms[k][2]} for k in range(rep.ncandidates)]
+        return {"chi0_rows": rep.chi0_rows, "update_rows": rep.update_rows, "split_group": rep.split_group,
+                "chains": rep.chains, "precision_class": rep.precision_class, "default_ms": rep.default_ms,
+                "tuned_ms": rep.tuned_ms, "candidates": cands}
 
     def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False) -> G0W0Output:
         return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None, qp_only)[0]

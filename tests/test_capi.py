@@ -105,3 +105,26 @@ def test_no_cpu_fallback_without_device(lib):
     from molgw_b200.rigw import Engine, RigwError
     with pytest.raises(RigwError):
         Engine(0)
+
+
+def test_tune_report_layout_matches_ctypes(tmp_path):
+    from molgw_b200.rigw import TuneReport
+    fields = [f for f, _ in TuneReport._fields_]
+    body = "".join(f'  printf("T {f} %zu\\n", offsetof(rigw_tune_report, {f}));\n' for f in fields)
+    src = tmp_path / "tune.c"
+    src.write_text(textwrap.dedent(f"""
+        #include <stdio.h>
+        #include <stddef.h>
+        #include "rigw.h"
+        int main(void) {{
+          printf("S %zu\\n", sizeof(rigw_tune_report));
+        {body}  return 0;
+        }}
+    """))
+    exe = tmp_path / "tune"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in
+               subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if line)
+    assert int(out["S"]) == C.sizeof(TuneReport)
+    for f in fields:
+        assert int(out[f"T {f}"]) == getattr(TuneReport, f).offset, f
