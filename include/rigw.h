@@ -47,7 +47,8 @@ enum rigw_status {
   RIGW_ERR_NOT_SPD = 4,    /* eps(iw) not positive definite (a Cholesky pivot <= 0)     */
   RIGW_ERR_NUMERIC = 5,    /* non-finite QP energy or singular Pade recursion           */
   RIGW_ERR_TIMEOUT = 6,    /* a bounded wait expired                                    */
-  RIGW_ERR_UNSUPPORTED = 7 /* precision or option not available in this build           */
+  RIGW_ERR_UNSUPPORTED = 7, /* precision or option not available in this build          */
+  RIGW_ERR_CANCELLED = 8   /* request loop destroyed before the request ran               */
 };
 
 /* Arithmetic of the chi0 = M D M^T contraction (the eps factorization, Sigma and
@@ -204,10 +205,14 @@ RIGW_API int rigw_autotune(rigw_ctx* ctx, int nprob, const rigw_problem* probs, 
  * No routine of the reference corresponds to this (MOLGW runs one molecule per
  * process); it serves many G0W0 solves on one GPU.  `workers` threads each own a
  * context with hbm_budget_bytes/workers of device memory (0: 85% of the free
- * memory); a free worker takes the queued requests in arrival order while their
- * footprints fit its share (at most max_batch) and solves them as one batch, so
- * requests that arrive while others run are admitted as workers and memory free
- * up, and batches of different workers overlap on the GPU.  The caller keeps the
+ * memory).  Requests are admitted by device footprint into a small and a large
+ * lane (footprint above 1/8 of a worker's share); a free worker takes the queued
+ * requests of one lane in arrival order while their footprints fit its share (at
+ * most max_batch) and solves them as one batch, so requests that arrive while
+ * others run are admitted as workers and memory free up, and batches of
+ * different workers overlap on the GPU.  Small requests go first; one large
+ * request runs at a time, started when no small request waits or when the
+ * oldest has waited 5 s.  The caller keeps the
  * arrays of a submitted problem and its result buffers alive until
  * rigw_server_wait returned for its ticket. */
 typedef struct rigw_server rigw_server;
@@ -218,9 +223,30 @@ RIGW_API int rigw_server_submit(rigw_server* srv, const rigw_problem* prob, rigw
 RIGW_API int rigw_server_poll(rigw_server* srv, uint64_t ticket, int* done);
 /* Waits at most timeout_ns; returns the request's status (RIGW_ERR_TIMEOUT if not
  * done yet, the ticket stays valid), releases the ticket otherwise. */
+/* done flag and the steady-clock (CLOCK_MONOTONIC) times of submission and
+ * completion of a ticket that has not been waited for. */
+RIGW_API int rigw_server_info(rigw_server* srv, uint64_t ticket, int* done, int64_t* submit_ns, int64_t* done_ns);
 RIGW_API int rigw_server_wait(rigw_server* srv, uint64_t ticket, int64_t timeout_ns, char* errbuf, size_t errlen);
 RIGW_API int rigw_server_counters(rigw_server* srv, long long* completed, long long* batches, long long* queued);
-/* Finishes the queued requests, then stops the workers. */
+/* Counters of the loop: per lane (0 small, 1 large) batches started, requests
+ * completed and queued, batches put back for lack of memory; failed requests;
+ * time the small lane was held for a large request; device time per lane; busy
+ * (wall) time per worker. */
+#define RIGW_SERVER_MAX_WORKERS 16
+typedef struct rigw_server_stats {
+  long long batches[2], completed[2], queued[2], requeued[2];
+  long long failed;
+  long long hold_ns;
+  double device_ms[2];       /* device time of the lane's batches (CUDA events)          */
+  double build_ms[2];        /* host time building plans for the lane                    */
+  double capture_ms[2];      /* host time capturing and instantiating CUDA graphs          */
+  double alloc_ms[2];        /* host time in device allocations                            */
+  long long busy_ns[RIGW_SERVER_MAX_WORKERS];
+  int workers;
+} rigw_server_stats;
+RIGW_API int rigw_server_stats_get(rigw_server* srv, rigw_server_stats* stats);
+/* Lets the batches already on the GPU finish, cancels the queued requests
+ * (RIGW_ERR_CANCELLED) and stops the workers. */
 RIGW_API int rigw_server_destroy(rigw_server* srv);
 
 /* ---- allocation-free variant -------------------------------------------------

@@ -30,6 +30,10 @@ struct GemmItem {
   int diag;
   int flags;
   double alpha, beta;
+  // The item covers nw frequencies (nw <= 0: one): CTA (item, j) (blockIdx.y =
+  // j < nw) works on the operands advanced by j times these element strides.
+  long long sA, sB, sC, sK, sQ;   // A, B, C and Cin, kscale, colsq
+  int nw;
 };
 
 template <int BM, int BN, int ST = 3>
@@ -54,7 +58,17 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
   constexpr int NT = Cfg::kThreads;
   extern __shared__ __align__(16) double smem[];
 
-  const GemmItem it = items[blockIdx.x];
+  GemmItem it = items[blockIdx.x];
+  const int jw = blockIdx.y;
+  if (jw >= (it.nw > 0 ? it.nw : 1)) return;   // nw <= 0: one frequency
+  if (jw > 0) {
+    it.A += jw * it.sA;
+    it.B += jw * it.sB;
+    it.C += jw * it.sC;
+    if (it.Cin) it.Cin += jw * it.sC;
+    if (it.kscale) it.kscale += jw * it.sK;
+    if (it.colsq) it.colsq += jw * it.sQ;
+  }
   const int tid = threadIdx.x;
   const int lane = tid & 31;
   const int warp = tid >> 5;

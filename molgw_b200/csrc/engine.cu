@@ -1,7 +1,9 @@
 // Host engine of the RI-GW library: plans, device memory, launch sequences.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <tuple>
 
 #include "engine.cuh"
@@ -53,19 +55,35 @@ DeviceBuffer::~DeviceBuffer() { release(); }
 Status DeviceBuffer::allocate(Context* ctx, size_t bytes, const char* name) {
   release();
   if (bytes == 0) return Status::ok();
+  ctx_ = ctx;
+  // the context's spare block (the arena of a released plan) is reused as is
+  if (ctx->spare_ptr && ctx->spare_bytes >= bytes) {
+    ptr_ = ctx->spare_ptr;
+    bytes_ = ctx->spare_bytes;
+    ctx->spare_ptr = nullptr;
+    ctx->spare_bytes = 0;
+    return Status::ok();   // already counted in in_use
+  }
+  if (ctx->budget && ctx->in_use + bytes > ctx->budget) ctx->free_spare();
   if (ctx->budget && ctx->in_use + bytes > ctx->budget)
     return Status::fail(RIGW_ERR_NOMEM, "%s: %zu bytes exceed the HBM budget (%zu in use of %zu)", name, bytes,
                         ctx->in_use, ctx->budget);
   // Stream-ordered allocation from the device pool: memory released by a plan
   // stays mapped in the pool and is handed to the next plan without remapping.
+  const auto t0 = std::chrono::steady_clock::now();
   cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(&ptr_), bytes, ctx->stream);
-  if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+  if (e != cudaSuccess && ctx->spare_ptr) {   // the spare block may be what is missing
+    cudaGetLastError();
+    ctx->free_spare();
+    e = cudaMallocAsync(reinterpret_cast<void**>(&ptr_), bytes, ctx->stream);
+  }
+  if (e == cudaSuccess && !ctx->sync(ctx->stream).good()) e = cudaErrorUnknown;
+  ctx->host_alloc_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (e != cudaSuccess) {
     ptr_ = nullptr;
     cudaGetLastError();
     return Status::fail(RIGW_ERR_NOMEM, "%s: cudaMallocAsync(%zu) failed: %s", name, bytes, cudaGetErrorString(e));
   }
-  ctx_ = ctx;
   bytes_ = bytes;
   ctx->in_use += bytes;
   ctx->peak = std::max(ctx->peak, ctx->in_use);
@@ -74,20 +92,49 @@ Status DeviceBuffer::allocate(Context* ctx, size_t bytes, const char* name) {
 
 void DeviceBuffer::release() {
   if (ptr_) {
-    cudaStreamSynchronize(ctx_->stream);
-    cudaFreeAsync(ptr_, ctx_->stream);
-    ctx_->in_use -= bytes_;
+    ctx_->sync(ctx_->stream);
+    if (bytes_ >= Context::kSpareMin && bytes_ > ctx_->spare_bytes) {
+      // keep the larger block for the next plan of this context
+      ctx_->free_spare();
+      ctx_->spare_ptr = ptr_;
+      ctx_->spare_bytes = bytes_;
+    } else {
+      cudaFreeAsync(ptr_, ctx_->stream);
+      ctx_->in_use -= bytes_;
+    }
   }
   ptr_ = nullptr;
   bytes_ = 0;
 }
 
+Status Context::reserve(size_t bytes) {
+  free_spare();
+  if (bytes < kSpareMin) return Status::ok();
+  DeviceBuffer b;
+  RIGW_TRY(b.allocate(this, bytes, "reserved arena"));
+  b.release();   // a block of at least kSpareMin bytes becomes the spare block
+  return Status::ok();
+}
+
+void Context::free_spare() {
+  if (!spare_ptr) return;
+  cudaFreeAsync(spare_ptr, stream);
+  in_use -= spare_bytes;
+  spare_ptr = nullptr;
+  spare_bytes = 0;
+}
+
 // ---------------------------------------------------------------------------
-Status Context::init(int dev, size_t budget_bytes) {
+Status Context::init(int dev, size_t budget_bytes, int want_priority) {
   device = dev;
   budget = budget_bytes;
   RIGW_CUDA_TRY(cudaSetDevice(dev));
-  RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  int least = 0, greatest = 0;
+  RIGW_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+  priority = want_priority > 0 ? greatest : (want_priority < 0 ? least : 0);
+  RIGW_CUDA_TRY(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, priority));
+  RIGW_CUDA_TRY(cudaEventCreateWithFlags(&sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+  for (auto& e : stage_ev) RIGW_CUDA_TRY(cudaEventCreate(&e));
   cudaMemPool_t pool;
   RIGW_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
   uint64_t keep = ~uint64_t(0);
@@ -100,12 +147,53 @@ Status Context::init(int dev, size_t budget_bytes) {
   return Status::ok();
 }
 
+Status Context::borrow(int nstreams, int nevents, std::vector<cudaStream_t>* streams,
+                       std::vector<cudaEvent_t>* events) {
+  while (int(aux_pool.size()) < nstreams) {
+    cudaStream_t s = nullptr;
+    RIGW_CUDA_TRY(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+    aux_pool.push_back(s);
+  }
+  while (int(order_pool.size()) < nevents) {
+    cudaEvent_t e = nullptr;
+    RIGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    order_pool.push_back(e);
+  }
+  streams->assign(aux_pool.begin(), aux_pool.begin() + nstreams);
+  events->assign(order_pool.begin(), order_pool.begin() + nevents);
+  return Status::ok();
+}
+
+Status Context::sync(cudaStream_t s) {
+  if (!sync_ev) {
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+    return Status::ok();
+  }
+  RIGW_CUDA_TRY(cudaEventRecord(sync_ev, s));
+  RIGW_CUDA_TRY(cudaEventSynchronize(sync_ev));
+  return Status::ok();
+}
+
 Context::~Context() {
   plan_cache.clear();
+  free_spare();
   if (stream) {
     cudaStreamSynchronize(stream);
     cudaStreamDestroy(stream);
   }
+  if (sync_ev) cudaEventDestroy(sync_ev);
+  for (auto& e : stage_ev)
+    if (e) cudaEventDestroy(e);
+  for (auto& e : order_pool) cudaEventDestroy(e);
+  for (auto& x : aux_pool) {
+    cudaStreamSynchronize(x);
+    cudaStreamDestroy(x);
+  }
+  // give the pool's unused memory back to the device (other contexts and
+  // allocators of the process see it again)
+  cudaMemPool_t pool;
+  if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) cudaMemPoolTrimTo(pool, 0);
+  cudaGetLastError();
 }
 
 // ---------------------------------------------------------------------------
@@ -132,6 +220,10 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   return d;
 }
 
+// Transitions per item of the split / slice / row-max kernels: wide items for
+// large problems (fewer items to build), 64 otherwise (enough CTAs to fill the GPU).
+int split_item_t(const Dims& d) { return (size_t(d.nia_pad / 64) * (d.npad / 64) >= 8192) ? kSplitT : 64; }
+
 // Bump allocator over one arena; first pass measures, second pass assigns.
 struct Layout {
   size_t cur = 0;
@@ -151,12 +243,6 @@ Plan::~Plan() {
     if (stage_exec_[st]) cudaGraphExecDestroy(stage_exec_[st]);
     if (stage_graph_[st]) cudaGraphDestroy(stage_graph_[st]);
   }
-  for (auto& e : stage_ev_)
-    if (e) cudaEventDestroy(e);
-  for (auto& e : la_ev_)
-    if (e) cudaEventDestroy(e);
-  for (auto& s : aux_streams_)
-    if (s) cudaStreamDestroy(s);
 }
 
 size_t Plan::measure(const std::vector<Shape>& shapes, PlanMode mode, const Tuning* tune) {
@@ -204,7 +290,12 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   const bool split_whole = split_all <= kSplitWholeBytes;
   auto split_group = [&](const Shape& sh) {
     if (tune_.split_group > 0) return std::max(1, std::min(sh.nomega, tune_.split_group));
-    return split_whole ? std::max(1, sh.nomega) : std::max(1, std::min(sh.nomega, kSplitGroup));
+    if (split_whole) return std::max(1, sh.nomega);
+    // at most kSplitGroup frequencies, and at most kSplitProblemBytes per problem
+    const Dims d = dims_of(sh, mode);
+    const size_t per_w = size_t(d.npad) * d.nia_pad * (is_ozaki(sh.precision) ? ozaki_slices(sh.precision) : 4);
+    const int cap = int(std::max<size_t>(1, kSplitProblemBytes / std::max<size_t>(per_w, 1)));
+    return std::max(1, std::min({sh.nomega, kSplitGroup, cap}));
   };
 
   // ---- memory layout
@@ -278,10 +369,16 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     for (const Shape& sh : shapes) {
       const Dims d = dims_of(sh, mode);
       const size_t t = size_t(d.npanel + 2) * (d.npanel + 2 + (d.ldb + 127) / 128) * 4;
-      lists += size_t(sh.nomega) * t * sizeof(GemmItem) + size_t(d.nia_pad / 8 + d.npad * d.ldb / 1024 + 64) * 16;
-      if (sh.precision != RIGW_FP64)   // split items: one per (group, 64 transitions, 64 aux), + row maxima
-        lists += size_t((sh.nomega + kSplitGroup - 1) / kSplitGroup + 1) * (d.nia_pad / 64) * (d.npad / 64) *
-                     sizeof(WorkItem) + size_t(sh.nomega) * d.npad / 4096 * sizeof(WorkItem) + 64;
+      // GEMM items cover all frequencies of a chain; the WorkItem lists stay per frequency
+      lists += size_t(kMaxChains + 1) * t * sizeof(GemmItem) +
+               size_t(sh.nomega) * (d.npanel + 8) * sizeof(WorkItem) +
+               size_t(d.nia_pad / 8 + d.npad * d.ldb / 1024 + 64) * 16;
+      if (sh.precision != RIGW_FP64) {   // split items: (group, split_t transitions, 64 aux), + row maxima
+        const int g = split_group(sh);
+        lists += size_t((sh.nomega + g - 1) / g + 1) * (d.nia_pad / split_item_t(d) + 1) * (d.npad / 64) *
+                     sizeof(WorkItem) +
+                 size_t(sh.nomega) * d.npad / 4096 * sizeof(WorkItem) + 64;
+      }
     }
     *measure_only = L.cur + lists + (size_t(1) << 20);
     return Status::ok();
@@ -319,11 +416,12 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       p.mp = dp(off[i].mp);
       p.kpad = d.nia_pad;
       p.wgroup = split_group(sh);
+      p.split_t = split_item_t(d);
       if (sh.precision == RIGW_BF16X3) {
         p.xs = base + off[i].xs;
         alignas(64) unsigned char map[128];
         RIGW_TRY(make_split_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * 2 * d.npad));
-        RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
+        RIGW_CUDA_TRY(cudaMemcpyAsync(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice, ctx->stream));
       } else if (is_ozaki(sh.precision)) {
         p.slices = ozaki_slices(sh.precision);
         p.xs = base + off[i].xs;
@@ -331,7 +429,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         p.xexp = reinterpret_cast<int*>(base + off[i].xexp);
         alignas(64) unsigned char map[128];
         RIGW_TRY(make_ozaki_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * p.slices * d.npad));
-        RIGW_CUDA_TRY(cudaMemcpy(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice));
+        RIGW_CUDA_TRY(cudaMemcpyAsync(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice, ctx->stream));
       }
       p.tnorm = dp(off[i].tnorm);
       p.dscale = dp(off[i].dscale);
@@ -399,24 +497,27 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             wl_split_.resize(g + 1);
             tl_syrk_.resize(g + 1);
           }
-          for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+          for (int t0 = 0; t0 < p.nia_pad; t0 += p.split_t)
             for (int p0 = 0; p0 < npad; p0 += 64) wl_split_[g].push_back({i, t0, p0, w0});
         }
-        for (int w = 0; w < sh.nomega; ++w)
+        // one item per (group, tile) covering the group's frequencies
+        for (int w0 = 0; w0 < sh.nomega; w0 += p.wgroup)
           for (int ti = 0; ti < npad; ti += BMN)
             for (int tj = ti; tj < npad; tj += BMN) {
-              const int wl = w % p.wgroup;
               TcItem t{};
               t.tmap = base + off[i].tmap;
-              t.C = p.eps + size_t(w) * npad * npad + size_t(ti) * npad + tj;
+              t.C = p.eps + size_t(w0) * npad * npad + size_t(ti) * npad + tj;
               t.err = err_dev_;
-              t.row_a = wl * 2 * npad + ti;
-              t.row_b = wl * 2 * npad + tj;
+              t.row_a = ti;
+              t.row_b = tj;
               t.lo_off = npad;
               t.ktiles = p.kpad / 64;
               t.ldc = npad;
               t.diag = ti - tj;
-              tl_syrk_[w / p.wgroup].push_back(t);
+              t.nw = std::min(p.wgroup, sh.nomega - w0);
+              t.sC = (long long)npad * npad;
+              t.srow = 2 * npad;
+              tl_syrk_[w0 / p.wgroup].push_back(t);
             }
       }
       // FP64 chi0: upper 128-wide column strips in 64-row items (two CTAs per SM),
@@ -424,48 +525,52 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       if (is_ozaki(sh.precision)) {
         // row maxima of S over every frequency, then per frequency group: slices, chi0
         for (size_t e = 0; e < size_t(sh.nomega) * npad; e += 4096) wl_ozzero_.push_back({i, int(e), 0, 0});
-        for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+        for (int t0 = 0; t0 < p.nia_pad; t0 += p.split_t)
           for (int p0 = 0; p0 < npad; p0 += 64) wl_rowmax_.push_back({i, t0, p0, 0});
         for (int w0 = 0, g = 0; w0 < sh.nomega; w0 += p.wgroup, ++g) {
           if (int(wl_slice_.size()) <= g) {
             wl_slice_.resize(g + 1);
             tl_ozaki_.resize(g + 1);
           }
-          for (int t0 = 0; t0 < p.nia_pad; t0 += 64)
+          for (int t0 = 0; t0 < p.nia_pad; t0 += p.split_t)
             for (int p0 = 0; p0 < npad; p0 += 64) wl_slice_[g].push_back({i, t0, p0, w0});
         }
-        for (int w = 0; w < sh.nomega; ++w)
+        for (int w0 = 0; w0 < sh.nomega; w0 += p.wgroup)
           for (int ti = 0; ti < npad; ti += BMN)
             for (int tj = ti; tj < npad; tj += BMN) {
-              const int wl = w % p.wgroup;
               TcItem t{};
               t.tmap = base + off[i].tmap;
-              t.C = p.eps + size_t(w) * npad * npad + size_t(ti) * npad + tj;
+              t.C = p.eps + size_t(w0) * npad * npad + size_t(ti) * npad + tj;
               t.err = err_dev_;
-              t.row_a = wl * p.slices * npad + ti;
-              t.row_b = wl * p.slices * npad + tj;
+              t.row_a = ti;
+              t.row_b = tj;
               t.lo_off = npad;
               t.ktiles = p.kpad / 128;
               t.ldc = npad;
               t.diag = ti - tj;
-              t.ea = p.xexp + size_t(w) * npad + ti;
-              t.eb = p.xexp + size_t(w) * npad + tj;
+              t.ea = p.xexp + size_t(w0) * npad + ti;
+              t.eb = p.xexp + size_t(w0) * npad + tj;
               t.slices = p.slices;
-              tl_ozaki_[w / p.wgroup].push_back(t);
+              t.nw = std::min(p.wgroup, sh.nomega - w0);
+              t.sC = (long long)npad * npad;
+              t.srow = p.slices * npad;
+              t.se = npad;
+              tl_ozaki_[w0 / p.wgroup].push_back(t);
             }
       }
-      for (int w = 0; w < sh.nomega && sh.precision == RIGW_FP64; ++w) {
-        double* E = p.eps + size_t(w) * npad * npad;
-        if (npad > sh.naux) wl_pad_.push_back({i, w, 0, 0});
+      if (sh.precision == RIGW_FP64) {
+        // one item per tile covering every frequency (blockIdx.y)
+        if (npad > sh.naux)
+          for (int w = 0; w < sh.nomega; ++w) wl_pad_.push_back({i, w, 0, 0});
         for (int ti = 0; ti < sh.naux; ti += BMC)
           for (int tj = ti / BMN * BMN; tj < sh.naux; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
             g.B = p.mp + tj;
             g.lda = g.ldb = npad;
-            g.C = E + size_t(ti) * npad + tj;
+            g.C = p.eps + size_t(ti) * npad + tj;
             g.ldc = npad;
-            g.kscale = p.dscale + size_t(w) * p.nia_pad;
+            g.kscale = p.dscale;
             g.m = std::min(BMC, sh.naux - ti);
             g.n = std::min(BMN, sh.naux - tj);
             g.k = p.nia_pad;
@@ -473,6 +578,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             g.diag = ti - tj;
             g.alpha = 1.0;
             g.beta = 0.0;
+            g.nw = sh.nomega;
+            g.sC = (long long)npad * npad;
+            g.sK = p.nia_pad;
             gl_syrk_.push_back(g);
           }
       }
@@ -486,13 +594,23 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       for (int c0 = 0; c0 < p.ncm; c0 += 8) wl_mnorm_.push_back({i, c0, 0, 0});
     for (int k = 0; k < p.npanel; ++k) {
       const int r0 = (k + 1) * kPanel;
-      for (int w = 0; w < sh.nomega; ++w) {
+      // frequency w belongs to chain (pair + w) % nchains; the items of one chain
+      // cover its frequencies w0, w0 + nchains, ... (blockIdx.y)
+      for (int ch = 0; ch < nchains_; ++ch) {
+        const int w0 = ((ch - pair) % nchains_ + nchains_) % nchains_;
+        if (w0 >= sh.nomega) continue;
+        const int nw = (sh.nomega - w0 + nchains_ - 1) / nchains_;
+        const long long step = nchains_;
+        const int w = w0;
         double* E = p.eps + size_t(w) * npad * npad;
         double* R = p.rhs + size_t(w) * npad * ldb;
         const double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
         double* cs = p.colsq ? p.colsq + (size_t(w) * p.npanel + k) * ldb : nullptr;
-        const int li = ((pair + w) % nchains_) * max_panels + k;   // list of (chain, panel)
-        if (factor) wl_diag_[li].push_back({i, w, 0, 0});
+        const long long sE = step * npad * npad, sR = step * npad * ldb;
+        const long long sW = step * p.npanel * kPanel * kPanel, sQ = step * p.npanel * ldb;
+        const int li = ch * max_panels + k;   // list of (chain, panel)
+        if (factor)
+          for (int wj = w0; wj < sh.nomega; wj += nchains_) wl_diag_[li].push_back({i, wj, 0, 0});
         auto k2 = [&](double* X, int ldx, int c0, int n, double* colsq) {
           GemmItem g{};
           g.A = W;
@@ -506,6 +624,10 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.n = n;
           g.k = kPanel;
           g.alpha = 1.0;
+          g.nw = nw;
+          g.sA = sW;
+          g.sB = g.sC = (X == E) ? sE : sR;
+          g.sQ = sQ;
           gl_k2_[li].push_back(g);
         };
         if (factor)
@@ -531,6 +653,10 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.k = kPanel;
           g.alpha = -1.0;
           g.beta = 1.0;
+          g.nw = nw;
+          g.sA = sE;
+          g.sB = (Bsrc == E) ? sE : sR;
+          g.sC = (Cdst == E) ? sE : sR;
           (next_diag ? gl_k3d_[li] : gl_k3_[li]).push_back(g);
         };
         for (int i0 = r0; i0 < npad; i0 += BM) {
@@ -572,12 +698,19 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     int count;
     int arg;
     int stream, wait_ev, rec_ev;
+    int ny;
   };
   std::vector<Pending> pend;
   auto add = [&](int kind, const void* src, size_t elem, size_t n, int arg, int stream = 0, int wait_ev = -1,
                  int rec_ev = -1) {
     if (n == 0) return false;
-    pend.push_back({kind, src, elem * n, int(n), arg, stream, wait_ev, rec_ev});
+    // grid y of the item lists that cover several frequencies
+    int ny = 1;
+    if (kind == 1 || kind == 5 || kind == 6 || kind == 14)
+      for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const GemmItem*>(src)[j].nw);
+    if (kind == 13 || kind == 20)
+      for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const TcItem*>(src)[j].nw);
+    pend.push_back({kind, src, elem * n, int(n), arg, stream, wait_ev, rec_ev, ny});
     return true;
   };
   add(0, wl_pack_.data(), sizeof(WorkItem), wl_pack_.size(), 0);
@@ -603,7 +736,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // stream 0 is the plan's own stream.  Kind -1 launches nothing (event marker).
   int nev = 0;
   const int fork_ev = nchains_ > 1 ? nev++ : -1;
-  if (fork_ev >= 0) pend.push_back({-1, nullptr, 0, 0, 0, 0, -1, fork_ev});
+  if (fork_ev >= 0) pend.push_back({-1, nullptr, 0, 0, 0, 0, -1, fork_ev, 1});
   std::vector<int> chain_end;
   for (int ch = 0; ch < nchains_; ++ch) {
     const int sm = 2 * ch, sl = 2 * ch + 1;
@@ -626,15 +759,15 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     }
     if (ch > 0) {
       const int ej = nev++;
-      pend.push_back({-1, nullptr, 0, 0, 0, sm, pending, ej});   // joins the lookahead, marks the chain's end
+      pend.push_back({-1, nullptr, 0, 0, 0, sm, pending, ej, 1});   // joins the lookahead, marks the chain's end
       chain_end.push_back(ej);
     } else if (pending >= 0) {
-      pend.push_back({-1, nullptr, 0, 0, 0, 0, pending, -1});
+      pend.push_back({-1, nullptr, 0, 0, 0, 0, pending, -1, 1});
     }
   }
-  for (int ej : chain_end) pend.push_back({-1, nullptr, 0, 0, 0, 0, ej, -1});
+  for (int ej : chain_end) pend.push_back({-1, nullptr, 0, 0, 0, 0, ej, -1, 1});
   add(7, wl_energy_.data(), sizeof(WorkItem), wl_energy_.size(), 0);
-  if (factor) pend.push_back({8, nullptr, 0, np, 0, 0, -1, -1});
+  if (factor) pend.push_back({8, nullptr, 0, np, 0, 0, -1, -1, 1});
   add(9, wl_vchiv_.data(), sizeof(WorkItem), wl_vchiv_.size(), 0);
   add(10, wl_sigma_.data(), sizeof(WorkItem), wl_sigma_.size(), 0);
   add(11, wl_pade_.data(), sizeof(WorkItem), wl_pade_.size(), 0);
@@ -645,14 +778,12 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   for (size_t j = 0; j < pend.size(); ++j) {
     if (pend[j].bytes) std::memcpy(host.data() + offs[j], pend[j].src, pend[j].bytes);
     seq_.push_back({pend[j].kind, offs[j], pend[j].count, pend[j].arg, pend[j].stream, pend[j].wait_ev,
-                    pend[j].rec_ev});
+                    pend[j].rec_ev, pend[j].ny});
   }
-  RIGW_CUDA_TRY(cudaMemcpy(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice));
-  for (auto& e : stage_ev_) RIGW_CUDA_TRY(cudaEventCreate(&e));
-  la_ev_.assign(std::max(nev, 1), nullptr);
-  for (auto& e : la_ev_) RIGW_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-  aux_streams_.assign(2 * nchains_ - 1, nullptr);
-  for (auto& s : aux_streams_) RIGW_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(lists_.data(), host.data(), lbytes, cudaMemcpyHostToDevice, ctx->stream));
+  RIGW_TRY(ctx->sync(ctx->stream));   // the host staging vector goes out of scope
+  RIGW_TRY(ctx->borrow(2 * nchains_ - 1, std::max(nev, 1), &aux_streams_, &la_ev_));
+  for (int k = 0; k < 5; ++k) stage_ev_[k] = ctx->stage_ev[k];
   host_table_.resize(np);
   n_launches_ = int(seq_.size());
   return Status::ok();
@@ -685,25 +816,25 @@ void Plan::record(cudaStream_t s0, int stage) {
     switch (L.kind) {
       case 0: pack_m_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 1:
-        if (tune_.chi0_rows == 128) launch_dgemm_128x128(gl, L.count, s);
-        else launch_dgemm_64x128(gl, L.count, s);
+        if (tune_.chi0_rows == 128) launch_dgemm_128x128(gl, L.count, L.ny, s);
+        else launch_dgemm_64x128(gl, L.count, L.ny, s);
         break;
       case 6: case 14:
-        if (tune_.update_rows == 128) launch_dgemm_128x128(gl, L.count, s);
-        else launch_dgemm_64x128(gl, L.count, s);
+        if (tune_.update_rows == 128) launch_dgemm_128x128(gl, L.count, L.ny, s);
+        else launch_dgemm_64x128(gl, L.count, L.ny, s);
         break;
       case 15: trace_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 16: pad_eps_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
-      case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
+      case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, L.ny, s); break;
       case 17: launch_ozaki_zero(probs_dev_, wl, L.count, s); break;
       case 18: launch_ozaki_rowmax(probs_dev_, wl, L.count, s); break;
       case 19: launch_ozaki_slice(probs_dev_, wl, L.count, s); break;
-      case 20: launch_syrk_ozaki(reinterpret_cast<const TcItem*>(lb + L.off), L.count, s); break;
+      case 20: launch_syrk_ozaki(reinterpret_cast<const TcItem*>(lb + L.off), L.count, L.ny, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 4: chol_diag_kernel<<<L.count, kDiagThreads, chol_diag_smem_bytes(), s>>>(probs_dev_, wl, L.arg); break;
-      case 5: launch_dgemm_128x128(gl, L.count, s); break;
+      case 5: launch_dgemm_128x128(gl, L.count, L.ny, s); break;
       case 7: energy_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 8: energy_sum_kernel<<<(L.count + 127) / 128, 128, 0, s>>>(probs_dev_, L.count); break;
       case 9: vchiv_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
@@ -752,6 +883,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   const bool factor = (mode_ == kPlanFused || mode_ == kPlanPolar || mode_ == kPlanPartial);
   const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma || mode_ == kPlanPartial);
   const bool qp = (mode_ == kPlanFused || mode_ == kPlanQP);
+  std::deque<std::vector<double>> keep;   // host sources of the copies below (stable addresses)
   for (size_t i = 0; i < probs_.size(); ++i) {
     const rigw_problem& q = probs[i];
     PlanProblem& pp = probs_[i];
@@ -782,11 +914,13 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
         p.omega = dp(pp.off_in_omega);
         p.weight = dp(pp.off_in_weight);
       } else {
-        std::vector<double> om(sh.nomega), wt(sh.nomega);
+        keep.emplace_back(sh.nomega);
+        std::vector<double>& om = keep.back();
+        keep.emplace_back(sh.nomega);
+        std::vector<double>& wt = keep.back();
         imag_grid(sh.nomega, om.data(), wt.data());
         RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_omega), om.data(), om.size() * 8, cudaMemcpyHostToDevice, s));
         RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_weight), wt.data(), wt.size() * 8, cudaMemcpyHostToDevice, s));
-        RIGW_CUDA_TRY(cudaStreamSynchronize(s));
         p.omega = dp(pp.off_in_omega);
         p.weight = dp(pp.off_in_weight);
       }
@@ -809,13 +943,13 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
       } else {
         if (sh.technique != RIGW_PADE)
           return Status::fail(RIGW_ERR_ARG, "problem %zu: homolumo technique needs omega_calc", i);
-        std::vector<double> z(2 * sh.nc);
+        keep.emplace_back(2 * sh.nc);
+        std::vector<double>& z = keep.back();
         for (int k = 0; k < sh.nc; ++k) {
           z[2 * k] = q.efermi;
           z[2 * k + 1] = q.step_sigma_calc * k;
         }
         RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_zcalc), z.data(), z.size() * 8, cudaMemcpyHostToDevice, s));
-        RIGW_CUDA_TRY(cudaStreamSynchronize(s));
         p.zcalc = dp(pp.off_in_zcalc);
       }
     }
@@ -834,6 +968,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   }
   RIGW_CUDA_TRY(cudaMemcpyAsync(probs_dev_, host_table_.data(), sizeof(ProbDev) * host_table_.size(),
                                 cudaMemcpyHostToDevice, s));
+  if (!keep.empty()) RIGW_TRY(ctx_->sync(s));
   return Status::ok();
 }
 
@@ -845,7 +980,9 @@ Status Plan::stage_sigma_calc(int i, const double* sc, cudaStream_t s) {
 
 Status Plan::launch(cudaStream_t s) {
   RIGW_CUDA_TRY(cudaMemsetAsync(err_dev_, 0, sizeof(int), s));
-  if (ctx_->use_graphs) {
+  // the first launch of a plan goes straight to the streams; a plan launched
+  // again is captured into CUDA graphs once and replayed from then on
+  if (ctx_->use_graphs && launches_++ > 0) {
     for (int st = 0; st < 4; ++st) {
       if (stage_exec_[st] || stage_empty_[st]) continue;
       bool any = false;
@@ -854,6 +991,7 @@ Status Plan::launch(cudaStream_t s) {
         stage_empty_[st] = true;
         continue;
       }
+      const auto t_cap = std::chrono::steady_clock::now();
       RIGW_CUDA_TRY(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
       record(s, st);
       cudaGraph_t g = nullptr;
@@ -862,6 +1000,8 @@ Status Plan::launch(cudaStream_t s) {
         return Status::fail(RIGW_ERR_CUDA, "graph capture failed: %s", cudaGetErrorString(e));
       stage_graph_[st] = g;
       RIGW_CUDA_TRY(cudaGraphInstantiate(&stage_exec_[st], g, 0));
+      ctx_->host_capture_ms +=
+          std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_cap).count();
     }
     for (int st = 0; st < 4; ++st) {
       RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[st], s));
@@ -884,7 +1024,7 @@ Status Plan::launch(cudaStream_t s) {
 Status Plan::check_errors(cudaStream_t s) {
   int err = 0;
   RIGW_CUDA_TRY(cudaMemcpyAsync(&err, err_dev_, sizeof(int), cudaMemcpyDeviceToHost, s));
-  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  RIGW_TRY(ctx_->sync(s));
   RIGW_CUDA_TRY(cudaEventElapsedTime(&last_ms_, stage_ev_[0], stage_ev_[4]));
   for (int k = 0; k < 4; ++k) RIGW_CUDA_TRY(cudaEventElapsedTime(&stage_ms_[k], stage_ev_[k], stage_ev_[k + 1]));
   if (err & kErrNotSPD) return Status::fail(RIGW_ERR_NOT_SPD, "eps(iw) is not positive definite");
@@ -895,17 +1035,16 @@ Status Plan::check_errors(cudaStream_t s) {
 }
 
 Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStream_t s) {
-  for (size_t i = 0; i < probs_.size(); ++i) {
+  // pass 1: every small output and input of the batch to the host, one wait
+  const size_t np = probs_.size();
+  std::vector<double> en(2 * np, 0.0);
+  std::vector<std::vector<double>> q(np), occ(np);
+  for (size_t i = 0; i < np; ++i) {
     const ProbDev& p = probs_[i].dev;
     rigw_result& r = res[i];
     const int nreal = 2 * p.nsigma_half + 1;
-    if (p.out_energies) {
-      double en[2];
-      RIGW_CUDA_TRY(cudaMemcpyAsync(en, p.out_energies, sizeof(en), cudaMemcpyDeviceToHost, s));
-      RIGW_CUDA_TRY(cudaStreamSynchronize(s));
-      r.erpa = en[0];
-      r.egw = en[1];
-    }
+    if (p.out_energies)
+      RIGW_CUDA_TRY(cudaMemcpyAsync(&en[2 * i], p.out_energies, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
     if (r.sigma_calc && p.sigma_calc && mode_ != kPlanQP)
       RIGW_CUDA_TRY(cudaMemcpyAsync(r.sigma_calc, p.sigma_calc, sizeof(double) * 2 * p.nsig * p.nc,
                                     cudaMemcpyDefault, s));
@@ -913,32 +1052,48 @@ Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStre
       RIGW_CUDA_TRY(
           cudaMemcpyAsync(r.sigma, p.sigma_real, sizeof(double) * 2 * p.nsig * nreal, cudaMemcpyDefault, s));
     if (p.qp) {
-      std::vector<double> q(4 * p.nsig);
-      RIGW_CUDA_TRY(cudaMemcpyAsync(q.data(), p.qp, q.size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      RIGW_CUDA_TRY(cudaStreamSynchronize(s));
-      std::vector<double> occ(p.nsig, 0.0);
+      q[i].assign(4 * p.nsig, 0.0);
+      occ[i].assign(p.nsig, 0.0);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(q[i].data(), p.qp, q[i].size() * sizeof(double), cudaMemcpyDeviceToHost, s));
       if (probs[i].occ_sig)
-        RIGW_CUDA_TRY(cudaMemcpy(occ.data(), probs[i].occ_sig, p.nsig * sizeof(double), cudaMemcpyDefault));
-      std::vector<double> g(p.nsig), z(p.nsig), zz(p.nsig);
+        RIGW_CUDA_TRY(cudaMemcpyAsync(occ[i].data(), probs[i].occ_sig, p.nsig * sizeof(double), cudaMemcpyDefault,
+                                      s));
+    }
+  }
+  RIGW_TRY(ctx_->sync(s));
+  // pass 2: QP energies and output_homolumo on the host, copies to the caller's buffers
+  std::vector<std::vector<double>> g(np), z(np), zz(np);
+  for (size_t i = 0; i < np; ++i) {
+    const ProbDev& p = probs_[i].dev;
+    rigw_result& r = res[i];
+    if (p.out_energies) {
+      r.erpa = en[2 * i];
+      r.egw = en[2 * i + 1];
+    }
+    if (p.qp) {
+      g[i].resize(p.nsig);
+      z[i].resize(p.nsig);
+      zz[i].resize(p.nsig);
       double eh = -HUGE_VAL, el = HUGE_VAL;
       for (int k = 0; k < p.nsig; ++k) {
-        g[k] = q[4 * k];
-        z[k] = q[4 * k + 1];
-        zz[k] = q[4 * k + 2];
+        g[i][k] = q[i][4 * k];
+        z[i][k] = q[i][4 * k + 1];
+        zz[i][k] = q[i][4 * k + 2];
         // output_homolumo, src/m_hamiltonian_tools.f90:564-612 (spin_fact = 2)
-        if (occ[k] / 2.0 > 1.0e-5) eh = std::max(eh, g[k]);
-        if (occ[k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[k]);
+        if (occ[i][k] / 2.0 > 1.0e-5) eh = std::max(eh, g[i][k]);
+        if (occ[i][k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[i][k]);
       }
       r.ehomo = eh;
       r.elumo = el;
-      if (r.energy_qp_g) RIGW_CUDA_TRY(cudaMemcpy(r.energy_qp_g, g.data(), g.size() * 8, cudaMemcpyDefault));
-      if (r.energy_qp_z) RIGW_CUDA_TRY(cudaMemcpy(r.energy_qp_z, z.data(), z.size() * 8, cudaMemcpyDefault));
-      if (r.zz) RIGW_CUDA_TRY(cudaMemcpy(r.zz, zz.data(), zz.size() * 8, cudaMemcpyDefault));
+      if (r.energy_qp_g)
+        RIGW_CUDA_TRY(cudaMemcpyAsync(r.energy_qp_g, g[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
+      if (r.energy_qp_z)
+        RIGW_CUDA_TRY(cudaMemcpyAsync(r.energy_qp_z, z[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
+      if (r.zz) RIGW_CUDA_TRY(cudaMemcpyAsync(r.zz, zz[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
     }
     r.device_ms = last_ms_;
   }
-  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
-  return Status::ok();
+  return ctx_->sync(s);   // the staging vectors go out of scope
 }
 
 }  // namespace rigw

@@ -167,9 +167,10 @@ class Plan {
     int stream;      // 0: the plan's stream, 1: the lookahead stream
     int wait_ev;     // lookahead event to wait for before the launch (-1: none)
     int rec_ev;      // lookahead event to record after the launch (-1: none)
+    int ny;          // grid y: frequencies covered by the items of the list
   };
-  std::vector<cudaEvent_t> la_ev_;
-  std::vector<cudaStream_t> aux_streams_;   // streams 1.. of the launch sequence (0 is the plan's stream)
+  std::vector<cudaEvent_t> la_ev_;           // borrowed from the context
+  std::vector<cudaStream_t> aux_streams_;   // streams 1.. of the launch sequence (0 is the plan's stream); borrowed
   int nchains_ = 1;
   std::vector<Launch> seq_;
   cudaGraph_t stage_graph_[4] = {nullptr, nullptr, nullptr, nullptr};
@@ -179,6 +180,7 @@ class Plan {
   float last_ms_ = 0.0f;
   float stage_ms_[4] = {0, 0, 0, 0};
   bool replayed_ = false;
+  int launches_ = 0;
 
  public:
   const float* stage_ms() const { return stage_ms_; }
@@ -201,13 +203,35 @@ class Context {
   std::map<std::pair<int, std::vector<Shape>>, std::unique_ptr<Plan>> plan_cache;
   bool use_graphs = true;
   rigw_stats last_stats{};
+  double host_build_ms = 0.0, host_capture_ms = 0.0;   // host time in plan builds / graph captures
+  double host_alloc_ms = 0.0;                           // host time in device allocations
+  // one spare device block: the arena of the last released plan, reused by the next
+  static constexpr size_t kSpareMin = size_t(64) << 20;
+  char* spare_ptr = nullptr;
+  size_t spare_bytes = 0;
+  void free_spare();
+  // Streams and events shared by the plans of this context (a context runs one
+  // plan at a time); created once: creating them per plan stalls behind the
+  // work of other contexts.
+  std::vector<cudaStream_t> aux_pool;
+  std::vector<cudaEvent_t> order_pool;   // ordering events (no timing)
+  cudaEvent_t stage_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  Status borrow(int nstreams, int nevents, std::vector<cudaStream_t>* streams, std::vector<cudaEvent_t>* events);
+  // Allocate a block of `bytes` now and keep it as the spare block, so that the
+  // plans of this context take their arena from it instead of growing the pool.
+  Status reserve(size_t bytes);
+  cudaEvent_t sync_ev = nullptr;   // blocking-sync event: host waits sleep instead of spinning
+  // Wait for the work queued on stream s (blocking wait on an event).
+  Status sync(cudaStream_t s);
   // autotuned launch shapes by (mode, precision class)
   std::map<std::pair<int, int>, Tuning> tuned;
   Tuning tuning_for(int mode, const std::vector<Shape>& shapes) const {
     auto it = tuned.find({mode, precision_class(shapes)});
     return it == tuned.end() ? Tuning{} : it->second;
   }
-  Status init(int dev, size_t budget_bytes);
+  int priority = 0;   // CUDA stream priority of every stream of this context (lower = higher)
+  // priority: 0 default; > 0 asks for the highest priority, < 0 for the lowest
+  Status init(int dev, size_t budget_bytes, int want_priority = 0);
   ~Context();
 };
 

@@ -50,19 +50,24 @@ struct TcItem {
   const int* ea;      // row exponents of the A rows (e_p, p = i0 ..)
   const int* eb;      // row exponents of the B rows (e_q, q = j0 ..)
   int slices;
+  // The item covers nw frequencies (nw <= 0: one): CTA (item, j) (blockIdx.y = j < nw) uses
+  // C + j*sC, tensor rows row_a/row_b + j*srow, exponents ea/eb + j*se.
+  long long sC, se;
+  int srow, nw;
 };
 void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
-void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s);
+void launch_syrk_bf16x3(const TcItem* items, int n, int ny, cudaStream_t s);
 void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
-void launch_syrk_ozaki(const TcItem* items, int n, cudaStream_t s);
+void launch_syrk_ozaki(const TcItem* items, int n, int ny, cudaStream_t s);
 cudaError_t prepare_ozaki_kernels();
 cudaError_t prepare_tc_kernels();
 
 // Host-side launchers of the DMMA tile engine (gemm_f64.cu).
-void launch_dgemm_128x128(const GemmItem* items, int n, cudaStream_t s);
-void launch_dgemm_64x128(const GemmItem* items, int n, cudaStream_t s);
+// grid (n items) x (ny frequencies): CTAs with blockIdx.y >= item.nw return at once
+void launch_dgemm_128x128(const GemmItem* items, int n, int ny, cudaStream_t s);
+void launch_dgemm_64x128(const GemmItem* items, int n, int ny, cudaStream_t s);
 cudaError_t prepare_dgemm_kernels();
 
 }  // namespace rigw

@@ -17,8 +17,8 @@ Status run_gemm_items(Context& c, const std::vector<GemmItem>& items, bool wide)
   RIGW_CUDA_TRY(cudaMemcpyAsync(buf.data(), items.data(), items.size() * sizeof(GemmItem), cudaMemcpyHostToDevice,
                                 c.stream));
   const GemmItem* d = reinterpret_cast<const GemmItem*>(buf.data());
-  if (wide) launch_dgemm_128x128(d, int(items.size()), c.stream);
-  else launch_dgemm_64x128(d, int(items.size()), c.stream);
+  if (wide) launch_dgemm_128x128(d, int(items.size()), 1, c.stream);
+  else launch_dgemm_64x128(d, int(items.size()), 1, c.stream);
   RIGW_CUDA_TRY(cudaGetLastError());
   RIGW_CUDA_TRY(cudaStreamSynchronize(c.stream));
   return Status::ok();

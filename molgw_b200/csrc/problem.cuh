@@ -50,6 +50,7 @@ struct ProbDev {
   int kpad;                  // transitions padded to the tensor-core K tile (== nia_pad)
   int wgroup;                // frequencies per split group (one buffer, reused group by group)
   int slices;                // Ozaki slices (0: not Ozaki)
+  int split_t;               // transitions per item of the split / slice / row-max kernels
   unsigned long long* rmax;  // Ozaki: [nomega][npad] max_t |S_pt| as double bits (atomicMax)
   int* xexp;                 // Ozaki: [nomega][npad] row exponents e_p
   double* tnorm;

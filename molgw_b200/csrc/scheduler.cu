@@ -10,6 +10,7 @@
 // (src/m_gw_selfenergy_grid.f90:118-191, 290-321), which is also what makes the
 // poorman frequency split of the reference (:626,658) exact.
 #include <algorithm>
+#include <chrono>
 #include <cstring>
 #include <vector>
 
@@ -32,8 +33,10 @@ size_t available_bytes(Context& c) {
   }
   cudaGetLastError();
   free_b += size_t(reserved > used ? reserved - used : 0);
-  size_t avail = size_t(double(free_b) * 0.9);
-  if (c.budget) avail = std::min(avail, c.budget > c.in_use ? c.budget - c.in_use : 0);
+  // the context's spare block is allocated but free for its next plan
+  size_t avail = size_t(double(free_b) * 0.9) + c.spare_bytes;
+  const size_t held = c.in_use - c.spare_bytes;
+  if (c.budget) avail = std::min(avail, c.budget > held ? c.budget - held : 0);
   return avail;
 }
 
@@ -47,6 +50,7 @@ Status get_plan(Context& c, PlanMode mode, const std::vector<Shape>& shapes, Pla
     return Status::ok();
   }
   if (c.plan_cache.size() >= 8) c.plan_cache.clear();
+  const auto t0 = std::chrono::steady_clock::now();
   std::unique_ptr<Plan> p(new Plan());
   Status s = p->build(&c, mode, shapes, {});
   if (s.code == RIGW_ERR_NOMEM && !c.plan_cache.empty()) {   // cached plans hold memory: drop them, retry once
@@ -55,6 +59,7 @@ Status get_plan(Context& c, PlanMode mode, const std::vector<Shape>& shapes, Pla
     s = p->build(&c, mode, shapes, {});
   }
   RIGW_TRY(s);
+  c.host_build_ms += std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
   *out = p.get();
   c.plan_cache.emplace(key, std::move(p));
   return Status::ok();
@@ -142,8 +147,9 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
     om[i].resize(sh.nomega);
     wt[i].resize(sh.nomega);
     if (probs[i].omega && probs[i].weight) {
-      RIGW_CUDA_TRY(cudaMemcpy(om[i].data(), probs[i].omega, sh.nomega * 8, cudaMemcpyDefault));
-      RIGW_CUDA_TRY(cudaMemcpy(wt[i].data(), probs[i].weight, sh.nomega * 8, cudaMemcpyDefault));
+      RIGW_CUDA_TRY(cudaMemcpyAsync(om[i].data(), probs[i].omega, sh.nomega * 8, cudaMemcpyDefault, c.stream));
+      RIGW_CUDA_TRY(cudaMemcpyAsync(wt[i].data(), probs[i].weight, sh.nomega * 8, cudaMemcpyDefault, c.stream));
+      RIGW_TRY(c.sync(c.stream));
     } else {
       imag_grid(sh.nomega, om[i].data(), wt[i].data());
     }
@@ -205,7 +211,9 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
     res[i].erpa = acc_en[2 * i];
     res[i].egw = acc_en[2 * i + 1];
     if (res[i].sigma_calc)
-      RIGW_CUDA_TRY(cudaMemcpy(res[i].sigma_calc, acc_sig[i].data(), acc_sig[i].size() * 8, cudaMemcpyDefault));
+      RIGW_CUDA_TRY(cudaMemcpyAsync(res[i].sigma_calc, acc_sig[i].data(), acc_sig[i].size() * 8, cudaMemcpyDefault,
+                                    c.stream));
+      RIGW_TRY(c.sync(c.stream));
     res[i].device_ms = c.last_stats.total_ms;
   }
   c.last_stats.chunks = int(units.size());

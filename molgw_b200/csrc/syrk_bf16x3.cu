@@ -26,38 +26,43 @@ constexpr int kTcTileBytes = 128 * 64 * 2;
 constexpr int kTcStageBytes = 4 * kTcTileBytes;
 constexpr size_t kTcSmemBytes = size_t(kTcStages) * kTcStageBytes + 1024 + 256;
 
-// item: (prob, t0, p0); 256 threads.
+// item: (prob, t0, p0, w0): split_t transitions from t0 x 64 rows from p0, the
+// frequencies w0 .. w0+wgroup-1; 256 threads.
 __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __restrict__ probs,
                                                            const WorkItem* __restrict__ items) {
   const WorkItem wi = items[blockIdx.x];
   const ProbDev& p = probs[wi.prob];
-  const int t0 = wi.a, p0 = wi.b;
+  const int p0 = wi.b;
   __shared__ double tile[64][65];   // [P][t]
   __shared__ double sc[64];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int idx = tid; idx < 64 * 64; idx += 256) {
-    const int tt = idx >> 6, pp = idx & 63;
-    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
-  }
   __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(p.xs);
   const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);   // this item's frequency group
-  for (int w = w0; w < w1; ++w) {
-    const int wl = w - w0;
+  const int tend = min(p.nia_pad, wi.a + p.split_t);
+  for (int t0 = wi.a; t0 < tend; t0 += 64) {               // 64-transition sub-tiles of the item
     __syncthreads();
-    if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
-    __syncthreads();
-    const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
+    for (int idx = tid; idx < 64 * 64; idx += 256) {
+      const int tt = idx >> 6, pp = idx & 63;
+      tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
+    }
+    for (int w = w0; w < w1; ++w) {
+      const int wl = w - w0;
+      __syncthreads();
+      if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+      __syncthreads();
+      const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
 #pragma unroll
-    for (int pr = 0; pr < 8; ++pr) {
-      const int pp = warp * 8 + pr;
-      const double v0 = tile[pp][2 * lane] * s0, v1 = tile[pp][2 * lane + 1] * s1;
-      const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
-      const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
-      const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
-      const size_t hi_row = (size_t(2 * wl) * p.npad + p0 + pp) * p.kpad + t0;
-      const size_t lo_row = (size_t(2 * wl + 1) * p.npad + p0 + pp) * p.kpad + t0;
-      reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
-      reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
+      for (int pr = 0; pr < 8; ++pr) {
+        const int pp = warp * 8 + pr;
+        const double v0 = tile[pp][2 * lane] * s0, v1 = tile[pp][2 * lane + 1] * s1;
+        const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
+        const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
+        const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
+        const size_t hi_row = (size_t(2 * wl) * p.npad + p0 + pp) * p.kpad + t0;
+        const size_t lo_row = (size_t(2 * wl + 1) * p.npad + p0 + pp) * p.kpad + t0;
+        reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
+        reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
+      }
     }
   }
 }
@@ -71,7 +76,16 @@ constexpr int kTcChunk = 8;
 constexpr int kTcThreads = 320;    // warp 0 TMA, warp 1 MMA, warps 2..9 epilogue
 
 __global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem* __restrict__ items) {
-  const TcItem it = items[blockIdx.x];
+  TcItem it = items[blockIdx.x];
+  const int jw = blockIdx.y;
+  if (jw >= (it.nw > 0 ? it.nw : 1)) return;   // the whole CTA, before any barrier or TMEM use
+  it.C += jw * it.sC;
+  it.row_a += jw * it.srow;
+  it.row_b += jw * it.srow;
+  if (it.ea) {
+    it.ea += jw * it.se;
+    it.eb += jw * it.se;
+  }
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kTcStages * kTcStageBytes);
@@ -245,8 +259,8 @@ void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cud
   if (n > 0) split_bf16x3_kernel<<<n, 256, 0, s>>>(probs, items);
 }
 
-void launch_syrk_bf16x3(const TcItem* items, int n, cudaStream_t s) {
-  if (n > 0) syrk_bf16x3_kernel<<<n, kTcThreads, kTcSmemBytes, s>>>(items);
+void launch_syrk_bf16x3(const TcItem* items, int n, int ny, cudaStream_t s) {
+  if (n > 0 && ny > 0) syrk_bf16x3_kernel<<<dim3(n, ny), kTcThreads, kTcSmemBytes, s>>>(items);
 }
 
 cudaError_t prepare_tc_kernels() {

@@ -40,21 +40,25 @@ __global__ void __launch_bounds__(256) ozaki_zero_kernel(const ProbDev* __restri
   }
 }
 
-// item: (prob, t0, p0): a 64 (transitions) x 64 (rows) tile, every frequency.
+// item: (prob, t0, p0): split_t transitions from t0 x 64 rows from p0, every
+// frequency, in 64-transition sub-tiles.
 __global__ void __launch_bounds__(256) ozaki_rowmax_kernel(const ProbDev* __restrict__ probs,
                                                            const WorkItem* __restrict__ items) {
   const WorkItem wi = items[blockIdx.x];
   const ProbDev& p = probs[wi.prob];
-  const int t0 = wi.a, p0 = wi.b;
+  const int p0 = wi.b;
   __shared__ double tile[64][65];   // [row p][transition t]
   __shared__ double sc[64];
   __shared__ double part[4][64];
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < 64 * 64; idx += 256) {
-    const int tt = idx >> 6, pp = idx & 63;
-    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
-  }
   const int pp = tid & 63, tq = tid >> 6;
+  const int tend = min(p.nia_pad, wi.a + p.split_t);
+  for (int t0 = wi.a; t0 < tend; t0 += 64) {
+  __syncthreads();
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int tt = idx >> 6, pq = idx & 63;
+    tile[pq][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pq];
+  }
   for (int w = 0; w < p.nomega; ++w) {
     __syncthreads();
     if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
@@ -69,25 +73,29 @@ __global__ void __launch_bounds__(256) ozaki_rowmax_kernel(const ProbDev* __rest
       if (m > 0.0) atomicMax(p.rmax + size_t(w) * p.npad + p0 + tid, (unsigned long long)__double_as_longlong(m));
     }
   }
+  }
 }
 
-// item: (prob, t0, p0, w0): the same tile for the frequencies w0 .. w0+wgroup-1.
+// item: (prob, t0, p0, w0): the same tiles for the frequencies w0 .. w0+wgroup-1.
 __global__ void __launch_bounds__(256) ozaki_slice_kernel(const ProbDev* __restrict__ probs,
                                                           const WorkItem* __restrict__ items) {
   const WorkItem wi = items[blockIdx.x];
   const ProbDev& p = probs[wi.prob];
-  const int t0 = wi.a, p0 = wi.b;
+  const int p0 = wi.b;
   __shared__ double tile[64][65];   // [row p][transition t]
   __shared__ double sc[64];         // sqrt(D_w(t0 + t))
   __shared__ double rs[64];         // 2^-e_p
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  int8_t* xq = reinterpret_cast<int8_t*>(p.xs);
+  const int ns = p.slices;
+  const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);
+  const int tend = min(p.nia_pad, wi.a + p.split_t);
+  for (int t0 = wi.a; t0 < tend; t0 += 64) {
+  __syncthreads();
   for (int idx = tid; idx < 64 * 64; idx += 256) {
     const int tt = idx >> 6, pp = idx & 63;
     tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
   }
-  int8_t* xq = reinterpret_cast<int8_t*>(p.xs);
-  const int ns = p.slices;
-  const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);
   for (int w = w0; w < w1; ++w) {
     const int wl = w - w0;
     __syncthreads();
@@ -118,6 +126,7 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const ProbDev* __restr
       }
     }
   }
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -130,7 +139,16 @@ constexpr int kOzAcc = 4;                               // TMEM accumulators of 
 constexpr int kOzThreads = 320;                         // warp 0 TMA, warp 1 MMA, warps 2..9 drain
 
 __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem* __restrict__ items) {
-  const TcItem it = items[blockIdx.x];
+  TcItem it = items[blockIdx.x];
+  const int jw = blockIdx.y;
+  if (jw >= (it.nw > 0 ? it.nw : 1)) return;   // the whole CTA, before any barrier or TMEM use
+  it.C += jw * it.sC;
+  it.row_a += jw * it.srow;
+  it.row_b += jw * it.srow;
+  if (it.ea) {
+    it.ea += jw * it.se;
+    it.eb += jw * it.se;
+  }
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOzStages * kOzStageBytes);
@@ -284,8 +302,8 @@ void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cud
 void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
   if (n > 0) ozaki_slice_kernel<<<n, 256, 0, s>>>(probs, items);
 }
-void launch_syrk_ozaki(const TcItem* items, int n, cudaStream_t s) {
-  if (n > 0) syrk_ozaki_kernel<<<n, kOzThreads, kOzSmemBytes, s>>>(items);
+void launch_syrk_ozaki(const TcItem* items, int n, int ny, cudaStream_t s) {
+  if (n > 0 && ny > 0) syrk_ozaki_kernel<<<dim3(n, ny), kOzThreads, kOzSmemBytes, s>>>(items);
 }
 
 cudaError_t prepare_ozaki_kernels() {

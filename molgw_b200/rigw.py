@@ -83,6 +83,17 @@ class Stats(C.Structure):
 
 
 RIGW_TUNE_MAX_CANDIDATES = 16
+RIGW_SERVER_MAX_WORKERS = 16
+
+
+class ServerStats(C.Structure):
+    _fields_ = [
+        ("batches", C.c_longlong * 2), ("completed", C.c_longlong * 2), ("queued", C.c_longlong * 2),
+        ("requeued", C.c_longlong * 2), ("failed", C.c_longlong), ("hold_ns", C.c_longlong),
+        ("device_ms", C.c_double * 2), ("build_ms", C.c_double * 2), ("capture_ms", C.c_double * 2),
+        ("alloc_ms", C.c_double * 2),
+        ("busy_ns", C.c_longlong * RIGW_SERVER_MAX_WORKERS), ("workers", C.c_int),
+    ]
 
 
 class TuneReport(C.Structure):
@@ -416,6 +427,9 @@ class Server:
         L.rigw_server_wait.argtypes = [C.c_void_p, C.c_uint64, C.c_int64, C.c_char_p, C.c_size_t]
         L.rigw_server_counters.argtypes = [C.c_void_p] + [C.POINTER(C.c_longlong)] * 3
         L.rigw_server_destroy.argtypes = [C.c_void_p]
+        L.rigw_server_info.argtypes = [C.c_void_p, C.c_uint64, C.POINTER(C.c_int), C.POINTER(C.c_int64),
+                                       C.POINTER(C.c_int64)]
+        L.rigw_server_stats_get.argtypes = [C.c_void_p, C.POINTER(ServerStats)]
         h = C.c_void_p()
         rc = L.rigw_server_create(C.byref(h), device, hbm_budget_bytes, workers, max_batch)
         if rc:
@@ -441,6 +455,14 @@ class Server:
         self._lib.rigw_server_poll(self._h, ticket, C.byref(d))
         return bool(d.value)
 
+    def info(self, ticket: int) -> tuple[bool, int, int]:
+        """(done, submit time, completion time); times in ns of time.monotonic_ns's clock."""
+        d, a, b = C.c_int(), C.c_int64(), C.c_int64()
+        rc = self._lib.rigw_server_info(self._h, ticket, C.byref(d), C.byref(a), C.byref(b))
+        if rc:
+            raise RigwError(rc, "rigw_server_info")
+        return bool(d.value), a.value, b.value
+
     def wait(self, ticket: int, timeout_s: float = 600.0) -> G0W0Output:
         buf = C.create_string_buffer(512)
         rc = self._lib.rigw_server_wait(self._h, ticket, int(timeout_s * 1e9), buf, 512)
@@ -450,6 +472,17 @@ class Server:
         if rc:
             raise RigwError(rc, buf.value.decode())
         return Engine._output(r, bufs)
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        self._lib.rigw_server_stats_get(self._h, C.byref(st))
+        return {"batches": list(st.batches), "completed": list(st.completed), "queued": list(st.queued),
+                "requeued": list(st.requeued), "failed": st.failed, "hold_s": st.hold_ns * 1e-9,
+                "device_s": [st.device_ms[0] * 1e-3, st.device_ms[1] * 1e-3],
+                "build_s": [st.build_ms[0] * 1e-3, st.build_ms[1] * 1e-3],
+                "capture_s": [st.capture_ms[0] * 1e-3, st.capture_ms[1] * 1e-3],
+                "alloc_s": [st.alloc_ms[0] * 1e-3, st.alloc_ms[1] * 1e-3],
+                "busy_s": [st.busy_ns[k] * 1e-9 for k in range(st.workers)]}
 
     def counters(self) -> dict:
         a, b, c = C.c_longlong(), C.c_longlong(), C.c_longlong()

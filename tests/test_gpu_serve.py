@@ -68,3 +68,23 @@ def test_concurrent_submitters_and_small_budget(engine):
     for r, o in zip(refs, outs):
         _close(r, o, tight=False)
         assert abs(r.erpa - o.erpa) <= 1e-12 * max(1.0, abs(r.erpa))
+
+
+def test_completion_stamps_and_cancel_on_close():
+    """The loop stamps submission and completion on the monotonic clock; closing
+    it with requests still queued cancels them instead of running them all."""
+    import time
+    insts = _mix()
+    srv = Server(0, workers=1, max_batch=1)
+    t_before = time.monotonic_ns()
+    tickets = [srv.submit(inst) for inst in insts * 4]        # 24 requests, one per batch
+    while not srv.info(tickets[0])[0]:
+        time.sleep(0.001)
+    done, sub, fin = srv.info(tickets[0])
+    assert done and t_before <= sub <= fin <= time.monotonic_ns()
+    queued = srv.counters()["queued"]
+    th = threading.Thread(target=srv.close)
+    th.start()
+    th.join(timeout=120)
+    assert not th.is_alive()
+    assert queued > 0
