@@ -157,6 +157,13 @@ RIGW_API int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, 
                         const int* index_basis, const double* eri3, const double* c_matrix,
                         int mstate_min, int mstate_max, int nstate_min, int nstate_max,
                         double* out);
+/* The same transform with its two products in `precision` (RIGW_FP64, or
+ * RIGW_BF16X3: bf16 hi/lo split of both operands, three products on the tensor
+ * cores with fp32 accumulation over at most 512 basis functions, FP64 results). */
+RIGW_API int rigw_eri_3center_mo_precision(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux,
+                                           const int* index_basis, const double* eri3, const double* c_matrix,
+                                           int mstate_min, int mstate_max, int nstate_min, int nstate_max,
+                                           double* out, int precision);
 
 /* chi0, eps(iw) = 1 - chi0 and its factorization for every frequency; keeps the
  * factors resident on the device in *wpol.  Uses the W-window fields of

@@ -247,7 +247,7 @@ void imag_grid(int n, double* omega, double* weight);
 Status wpol_chi(Context& c, const Wpol& w, double* chi);
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
-                      int nstate_min, int nstate_max, double* out);
+                      int nstate_min, int nstate_max, double* out, int precision);
 bool bf16x3_available();
 Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes);
 Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res);

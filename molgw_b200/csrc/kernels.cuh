@@ -54,8 +54,24 @@ struct TcItem {
   // C + j*sC, tensor rows row_a/row_b + j*srow, exponents ea/eb + j*se.
   long long sC, se;
   int srow, nw;
+  // General products (syrk_bf16x3_kernel only): B from its own tensor map (nullptr:
+  // the A map) whose lo rows are lo_off_b below the hi rows; only the first mrows
+  // x ncols of the tile are stored (0: all 128).
+  const void* tmap_b;
+  int lo_off_b, mrows, ncols;
 };
 void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
+// Split of a general FP64 operand into K-major bf16 hi/lo for the tensor-core
+// kernel: element (r, k) of batch z is src[z*zs_src + r*rs + k*ks]; dst holds
+// [2][Rpad][Kpad] per batch (hi rows, then lo rows), zero padded.
+struct SplitOp {
+  const double* src;
+  long long rs, ks, zs_src;
+  int R, K, Rpad, Kpad, nz;
+  void* dst;
+  long long zs_dst;   // elements between batches of dst
+};
+void launch_split_kmajor(const SplitOp& op, cudaStream_t s);
 void launch_syrk_bf16x3(const TcItem* items, int n, int ny, cudaStream_t s);
 void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);

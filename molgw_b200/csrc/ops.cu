@@ -61,11 +61,43 @@ Status wpol_chi(Context& c, const Wpol& w, double* chi) {
 }
 
 // out[n][m][P] = sum_{mu,nu} C[m][mu] C[n][nu] B(mu nu, P)  (src/m_eri_ao_mo.f90:416-582).
+namespace {
+// One split operand of a tensor-core product: K-major bf16 hi/lo in `buf`, its
+// tensor map (rows = nz * 2 * Rpad, columns = Kpad) at `map_dev`.
+Status split_operand(Context& c, const SplitOp& shape, DeviceBuffer* buf, void* map_dev) {
+  SplitOp op = shape;
+  RIGW_TRY(buf->allocate(&c, size_t(op.nz) * 2 * op.Rpad * op.Kpad * 2, "split operand"));
+  op.dst = buf->data();
+  op.zs_dst = (long long)2 * op.Rpad * op.Kpad;
+  launch_split_kmajor(op, c.stream);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  alignas(64) unsigned char map[128];
+  RIGW_TRY(make_split_tmap(map, op.dst, op.Kpad, (long long)op.nz * 2 * op.Rpad));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(map_dev, map, sizeof(map), cudaMemcpyHostToDevice, c.stream));
+  return Status::ok();
+}
+
+Status run_tc_items(Context& c, const std::vector<TcItem>& items) {
+  if (items.empty()) return Status::ok();
+  DeviceBuffer buf;
+  RIGW_TRY(buf.allocate(&c, items.size() * sizeof(TcItem), "tensor-core items"));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(buf.data(), items.data(), items.size() * sizeof(TcItem), cudaMemcpyHostToDevice,
+                                c.stream));
+  launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(buf.data()), int(items.size()), 1, c.stream);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  return c.sync(c.stream);
+}
+}  // namespace
+
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
-                      int nstate_min, int nstate_max, double* out) {
+                      int nstate_min, int nstate_max, double* out, int precision) {
   if (nbf <= 0 || nstate <= 0 || npair <= 0 || naux <= 0 || !index_basis || !eri3 || !c_matrix || !out)
     return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: invalid arguments");
+  if (precision != RIGW_FP64 && precision != RIGW_BF16X3)
+    return Status::fail(RIGW_ERR_UNSUPPORTED, "eri_3center_mo: precision %d (FP64 or BF16X3)", precision);
+  const bool split = precision == RIGW_BF16X3;
+  if (split && !bf16x3_available()) return Status::fail(RIGW_ERR_UNSUPPORTED, "tensor maps unavailable");
   if (mstate_min < 1 || mstate_max > nstate || mstate_min > mstate_max || nstate_min < 1 ||
       nstate_max > nstate || nstate_min > nstate_max)
     return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: state ranges outside [1, %d]", nstate);
@@ -103,6 +135,23 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   double* dfull = reinterpret_cast<double*>(b_full.data());
   double* dt = reinterpret_cast<double*>(b_t.data());
   double* dout = reinterpret_cast<double*>(b_out.data());
+  // split precision: C^T blocks split once; the unpacked tensor and the half
+  // transform are split per auxiliary chunk (BF16x3 products, FP64 results)
+  const int Kp = round_up(nbf, 64);
+  const int Rp1 = round_up(ncp, 128), Rp2 = round_up(mcp, 128), Rpw = round_up(nbf * pcp, 128);
+  const int Rpp = round_up(pcp, 128);
+  DeviceBuffer s_a1, s_a2, s_b1, s_b2, s_maps, s_err;
+  char* maps = nullptr;
+  int* errp = nullptr;
+  if (split) {
+    RIGW_TRY(s_maps.allocate(&c, 4 * 128, "split tensor maps"));
+    RIGW_TRY(s_err.allocate(&c, sizeof(int), "split error flag"));
+    maps = s_maps.data();
+    errp = reinterpret_cast<int*>(s_err.data());
+    RIGW_CUDA_TRY(cudaMemsetAsync(errp, 0, sizeof(int), s));
+    RIGW_TRY(split_operand(c, SplitOp{dctn, 1, ncp, 0, ncp, nbf, Rp1, Kp, 1, nullptr, 0}, &s_a1, maps));
+    RIGW_TRY(split_operand(c, SplitOp{dctm, 1, mcp, 0, mcp, nbf, Rp2, Kp, 1, nullptr, 0}, &s_a2, maps + 256));
+  }
   for (int p0 = 0; p0 < naux; p0 += pc) {
     const int cnt = std::min(pc, naux - p0);
     RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), eri3 + size_t(p0) * npair, size_t(cnt) * npair * 8,
@@ -114,9 +163,60 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     dim3 grid((npair + 31) / 32, (cnt + 31) / 32);
     aomo_unpack_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const AomoUnpackItem*>(b_item.data()));
     RIGW_CUDA_TRY(cudaGetLastError());
+    const int wide = nbf * pcp;
+    if (split) {
+      // step 1: T[n][j] = sum_nu ctn^T[n][nu] B^T[j][nu],  j = (mu, P)
+      RIGW_TRY(split_operand(c, SplitOp{dfull, 1, wide, 0, wide, nbf, Rpw, Kp, 1, nullptr, 0}, &s_b1, maps + 128));
+      std::vector<TcItem> t1;
+      for (int i0 = 0; i0 < ncp; i0 += 128)
+        for (int j0 = 0; j0 < wide; j0 += 128) {
+          TcItem t{};
+          t.tmap = maps;
+          t.row_a = i0;
+          t.lo_off = Rp1;
+          t.tmap_b = maps + 128;
+          t.row_b = j0;
+          t.lo_off_b = Rpw;
+          t.ktiles = Kp / 64;
+          t.C = dt + size_t(i0) * wide + j0;
+          t.ldc = wide;
+          t.mrows = std::min(128, ncp - i0);
+          t.ncols = std::min(128, wide - j0);
+          t.err = errp;
+          t.nw = 1;
+          t1.push_back(t);
+        }
+      RIGW_TRY(run_tc_items(c, t1));
+      // step 2: O[n][m][P] = sum_mu ctm^T[m][mu] T[n]^T[P][mu], every n in one launch
+      RIGW_TRY(split_operand(c, SplitOp{dt, 1, pcp, wide, pcp, nbf, Rpp, Kp, nc, nullptr, 0}, &s_b2, maps + 384));
+      std::vector<TcItem> t2;
+      for (int n = 0; n < nc; ++n)
+        for (int i0 = 0; i0 < mcp; i0 += 128)
+          for (int j0 = 0; j0 < pcp; j0 += 128) {
+            TcItem t{};
+            t.tmap = maps + 256;
+            t.row_a = i0;
+            t.lo_off = Rp2;
+            t.tmap_b = maps + 384;
+            t.row_b = n * 2 * Rpp + j0;
+            t.lo_off_b = Rpp;
+            t.ktiles = Kp / 64;
+            t.C = dout + (size_t(n) * mcp + i0) * pcp + j0;
+            t.ldc = pcp;
+            t.mrows = std::min(128, mcp - i0);
+            t.ncols = std::min(128, pcp - j0);
+            t.err = errp;
+            t.nw = 1;
+            t2.push_back(t);
+          }
+      RIGW_TRY(run_tc_items(c, t2));
+      int herr = 0;
+      RIGW_CUDA_TRY(cudaMemcpyAsync(&herr, errp, sizeof(int), cudaMemcpyDeviceToHost, s));
+      RIGW_TRY(c.sync(s));
+      if (herr) return Status::fail(RIGW_ERR_TIMEOUT, "eri_3center_mo: a bounded device wait expired");
+    } else {
     // step 1: T[n][(mu,P)] = sum_nu ctn[nu][n] B[nu][(mu,P)]
     std::vector<GemmItem> g1;
-    const int wide = nbf * pcp;
     for (int i0 = 0; i0 < ncp; i0 += 128)
       for (int j0 = 0; j0 < wide; j0 += 128) {
         GemmItem g{};
@@ -152,6 +252,7 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
           g2.push_back(g);
         }
     RIGW_TRY(run_gemm_items(c, g2, true));
+    }
     // out[n][m][p0 : p0+cnt]
     for (int n = 0; n < nc; ++n)
       RIGW_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t(n) * mc) * naux + p0, size_t(naux) * 8,

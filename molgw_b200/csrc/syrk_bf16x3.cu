@@ -67,6 +67,32 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
   }
 }
 
+// General operand split: 64 (rows) x 64 (K) tiles through shared memory, read
+// along the source's contiguous index and written K-contiguous.
+__global__ void __launch_bounds__(256) split_kmajor_kernel(const SplitOp op) {
+  __shared__ double tile[64][65];   // [row][k]
+  const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 64, z = blockIdx.z;
+  const double* src = op.src + size_t(z) * op.zs_src;
+  __nv_bfloat16* dst = reinterpret_cast<__nv_bfloat16*>(op.dst) + size_t(z) * op.zs_dst;
+  const bool rfast = op.rs == 1;
+  for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
+    const int a = idx >> 6, b = idx & 63;
+    const int rr = rfast ? b : a, kk = rfast ? a : b;
+    const int r = r0 + rr, k = k0 + kk;
+    tile[rr][kk] = (r < op.R && k < op.K) ? src[r * op.rs + k * op.ks] : 0.0;
+  }
+  __syncthreads();
+  for (int idx = threadIdx.x; idx < 64 * 64; idx += 256) {
+    const int rr = idx >> 6, kk = idx & 63;
+    const double v = tile[rr][kk];
+    const __nv_bfloat16 h = __double2bfloat16(v);
+    const __nv_bfloat16 l = __double2bfloat16(v - double(__bfloat162float(h)));
+    const size_t o = size_t(r0 + rr) * op.Kpad + k0 + kk;
+    dst[o] = h;
+    dst[o + size_t(op.Rpad) * op.Kpad] = l;
+  }
+}
+
 // K is consumed in chunks of kTcChunk k-tiles (512 transitions).  Each chunk
 // accumulates in fp32 in one of two TMEM accumulators (128 columns each); eight
 // epilogue warps drain a finished chunk into FP64 registers while the MMA warp
@@ -116,7 +142,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem
 
   if (tid == 0) {
     // ---- TMA producer
+    const void* tmb = it.tmap_b ? it.tmap_b : it.tmap;
+    const int lob = it.tmap_b ? it.lo_off_b : it.lo_off;
     tc::tmap_acquire(it.tmap);
+    if (it.tmap_b) tc::tmap_acquire(it.tmap_b);
     int issued[kTcStages] = {0, 0, 0};
     bool ok = true;
     for (int kt = 0; kt < nk && ok; ++kt) {
@@ -129,8 +158,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem
       const int k0 = kt * 64;
       tc::tma_load_2d(tile(s, 0), it.tmap, &full[s], k0, it.row_a);
       tc::tma_load_2d(tile(s, 1), it.tmap, &full[s], k0, it.row_a + it.lo_off);
-      tc::tma_load_2d(tile(s, 2), it.tmap, &full[s], k0, it.row_b);
-      tc::tma_load_2d(tile(s, 3), it.tmap, &full[s], k0, it.row_b + it.lo_off);
+      tc::tma_load_2d(tile(s, 2), tmb, &full[s], k0, it.row_b);
+      tc::tma_load_2d(tile(s, 3), tmb, &full[s], k0, it.row_b + lob);
       ++issued[s];
     }
     if (!ok) atomicOr(it.err, kErrTimeout);
@@ -193,7 +222,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem
       __syncwarp();
       if (lane == 0) tc::mbar_arrive(&acce[b]);
     }
-    if (ok) {
+    if (ok && it.mrows == 0) {
       double* dst = it.C + size_t(row) * it.ldc + half * 64;
 #pragma unroll
       for (int j = 0; j < 64; j += 2) {
@@ -202,6 +231,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) syrk_bf16x3_kernel(const TcItem
         if (col - row == it.diag) v0 += 1.0;
         if (col + 1 - row == it.diag) v1 += 1.0;
         *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
+      }
+    } else if (ok) {
+      // edge tile of a general product: rows < mrows, columns < ncols, no identity
+      if (row < it.mrows) {
+        double* dst = it.C + size_t(row) * it.ldc;
+#pragma unroll
+        for (int j = 0; j < 64; ++j)
+          if (half * 64 + j < it.ncols) dst[half * 64 + j] = acc[j];
       }
     } else if (lane == 0) {
       atomicOr(it.err, kErrTimeout);
@@ -257,6 +294,11 @@ Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows)
 
 void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
   if (n > 0) split_bf16x3_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+
+void launch_split_kmajor(const SplitOp& op, cudaStream_t s) {
+  if (op.Rpad > 0 && op.Kpad > 0 && op.nz > 0)
+    split_kmajor_kernel<<<dim3(op.Kpad / 64, op.Rpad / 64, op.nz), 256, 0, s>>>(op);
 }
 
 void launch_syrk_bf16x3(const TcItem* items, int n, int ny, cudaStream_t s) {

@@ -122,6 +122,9 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_imag_grid.argtypes = [C.c_int, _dp, _dp]
     lib.rigw_eri_3center_mo.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                         _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+    lib.rigw_eri_3center_mo_precision.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                                  C.POINTER(C.c_int), _dp, _dp, C.c_int, C.c_int, C.c_int,
+                                                  C.c_int, _dp, C.c_int]
     lib.rigw_polarizability_imag.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, _dp, C.POINTER(C.c_void_p)]
     lib.rigw_wpol_chi.argtypes = [C.c_void_p, C.c_void_p, _dp]
     lib.rigw_gw_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
@@ -376,15 +379,16 @@ class Engine:
         return out
 
     def calculate_eri_3center_mo(self, eri3: np.ndarray, index_basis: np.ndarray, c_matrix: np.ndarray,
-                                 m_min: int, m_max: int, n_min: int, n_max: int) -> np.ndarray:
+                                 m_min: int, m_max: int, n_min: int, n_max: int,
+                                 precision: int = RIGW_FP64) -> np.ndarray:
         naux, npair = eri3.shape
         nstate, nbf = c_matrix.shape
         idx = np.ascontiguousarray(index_basis, dtype=np.int32)
         out = np.zeros((n_max - n_min + 1, m_max - m_min + 1, naux))
-        self._check(self._lib.rigw_eri_3center_mo(
+        self._check(self._lib.rigw_eri_3center_mo_precision(
             self._h, nbf, nstate, npair, naux, idx.ctypes.data_as(C.POINTER(C.c_int)),
             _ptr(np.ascontiguousarray(eri3)), _ptr(np.ascontiguousarray(c_matrix)), m_min, m_max, n_min, n_max,
-            _ptr(out)), "rigw_eri_3center_mo")
+            _ptr(out), precision), "rigw_eri_3center_mo_precision")
         return out
 
 

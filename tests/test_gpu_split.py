@@ -54,3 +54,24 @@ def test_split_precision_ragged_batch(engine):
     for inst, o in zip(insts, outs):
         ref = engine.g0w0(inst, RIGW_FP64)
         assert np.abs(o.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3 <= 1.0
+
+
+@pytest.mark.parametrize("nbf,naux,ranges", [(37, 61, [(6, 37, 1, 5), (3, 3, 2, 9)]),
+                                              (300, 700, [(41, 300, 1, 40), (1, 300, 39, 42)])])
+def test_split_precision_aomo_matches_fp64(engine, nbf, naux, ranges):
+    """AO->MO with both products split (bf16 hi/lo on tcgen05, FP64 results):
+    within 2e-5 of the largest entry of the FP64 transform, and not identical to it."""
+    from oracle import rigw_oracle as o
+    rng = np.random.default_rng(nbf)
+    pairs = np.array([(k, l) for l in range(1, nbf + 1) for k in range(1, l + 1)])
+    pairs = pairs[rng.random(len(pairs)) > 0.1]
+    eri3 = rng.standard_normal((naux, len(pairs)))
+    c = np.linalg.qr(rng.standard_normal((nbf, nbf)))[0].T.copy()
+    for (m0, m1, n0, n1) in ranges:
+        f64 = engine.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1)
+        spl = engine.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1, precision=RIGW_BF16X3)
+        err = np.abs(spl - f64).max() / np.abs(f64).max()
+        assert 0.0 < err <= 2e-5, err
+        if nbf < 100:
+            ref = o.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1)
+            assert np.abs(spl - ref).max() <= 2e-5 * np.abs(ref).max()
