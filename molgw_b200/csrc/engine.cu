@@ -477,7 +477,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // frequency chains: independent factorization sequences on their own streams,
   // at least kChainPairs (problem, frequency) pairs each
   nchains_ = tune_.chains > 0 ? std::max(1, std::min({tune_.chains, kMaxChains, npairs}))
-                              : std::max(1, std::min(kMaxChains, npairs / kChainPairs));
+                              : std::max(1, std::min(kAutoChains, npairs / kChainPairs));
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});
@@ -883,7 +883,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   const bool factor = (mode_ == kPlanFused || mode_ == kPlanPolar || mode_ == kPlanPartial);
   const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma || mode_ == kPlanPartial);
   const bool qp = (mode_ == kPlanFused || mode_ == kPlanQP);
-  std::deque<std::vector<double>> keep;   // host sources of the copies below (stable addresses)
+  std::deque<std::vector<double>> keep;   // host sources of the copies below
   for (size_t i = 0; i < probs_.size(); ++i) {
     const rigw_problem& q = probs[i];
     PlanProblem& pp = probs_[i];
@@ -968,7 +968,8 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   }
   RIGW_CUDA_TRY(cudaMemcpyAsync(probs_dev_, host_table_.data(), sizeof(ProbDev) * host_table_.size(),
                                 cudaMemcpyHostToDevice, s));
-  if (!keep.empty()) RIGW_TRY(ctx_->sync(s));
+  // copies from pageable host memory are staged before cudaMemcpyAsync returns:
+  // the host vectors in `keep` may go out of scope without a wait
   return Status::ok();
 }
 
