@@ -42,7 +42,7 @@ WORKLOAD = "single synthetic RI-GW instance Nocc=21 Nvirt=207 Naux=840, 32 imagi
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
@@ -85,7 +85,7 @@ def oracle_solve(inst):
 
 class ClockSampler:
     """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
-    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
@@ -104,6 +104,10 @@ class ClockSampler:
         except Exception:
             self.proc = None
 
+    def mark(self, which: str):
+        """Wall-clock bounds of the timed region (samples outside it are not used)."""
+        setattr(self, which, time.time())
+
     def stop(self) -> dict:
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
@@ -111,12 +115,24 @@ class ClockSampler:
         self.proc.wait(timeout=10)
         self.f.close()
         rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.strip()]
-        sm = [float(r[1]) for r in rows if len(r) >= 9 and r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if len(r) >= 9 and r[2].replace(".", "").isdigit()]
+        rows = [r[1:] for r in rows if len(r) >= 10 and self._in_region(r[0])]
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows if len(r) >= 9 for k in range(4) if r[5 + k].strip() == "Active"})
+        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows)}
+                "reasons": reasons, "samples": len(rows), "window": "samples taken inside the timed region"}
+
+    def _in_region(self, stamp: str) -> bool:
+        t0, t1 = getattr(self, "begin", None), getattr(self, "end", None)
+        if t0 is None or t1 is None:
+            return True
+        try:
+            import datetime
+            t = datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
+        except ValueError:
+            return True
+        return t0 - 0.25 <= t <= t1 + 0.25
 
 
 def measured_fp64_peak(torch) -> float:
@@ -458,14 +474,15 @@ def main():
 
     # launch shapes chosen by the library's autotuner on this instance (untimed)
     tune_main = compact_tuning(eng.autotune([inst], precision, [dev]))
+    clocks = ClockSampler(local)     # started before the warm-up: sampling runs when timing starts
+    clocks.start()
     for _ in range(args.warmup):
         eng.g0w0(inst, precision, device_arrays=dev)
     # ---------------- timed region: device events per solve
-    clocks = ClockSampler(local)
-    clocks.start()
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
+    clocks.mark("begin")
     dev_ms, chi0_ms, launches, outs = [], [], 0, []
     for _ in range(args.steps):
         flush_l2()
@@ -476,6 +493,7 @@ def main():
         launches += st["kernel_launches"]
         outs.append(out)
     torch.cuda.synchronize()
+    clocks.mark("end")
     if world > 1:
         dist.barrier()
     clk = clocks.stop()

@@ -3,7 +3,7 @@
 //   eps(iw) = 1 + S S^T,  S = M diag(sqrt(D_w))
 //   row p of S is scaled by 2^-e_p, e_p the exponent of max_t |S_pt| (so |x| < 1):
 //     x_pt = S_pt 2^-e_p = sum_{k=1..s} q_k(p,t) 2^-7k + r,  q_k integers in [-127, 127],
-//   each q_k the truncated integer part of the residual times 128 (exact in FP64).
+//   the base-128 digits of trunc(x 2^7s) (an exact 64-bit integer), with the sign of x.
 //   (S S^T)_pq ~= 2^(e_p+e_q) sum_{d=2..s+1} 2^-7d L_d(p,q),   L_d = sum_{i+j=d} Q_i Q_j^T
 //   (the products of level i+j > s+1 are dropped, as in the Ozaki scheme).
 //
@@ -54,26 +54,36 @@ __global__ void __launch_bounds__(256) ozaki_rowmax_kernel(const ProbDev* __rest
   const int pp = tid & 63, tq = tid >> 6;
   const int tend = min(p.nia_pad, wi.a + p.split_t);
   for (int t0 = wi.a; t0 < tend; t0 += 64) {
-  __syncthreads();
-  for (int idx = tid; idx < 64 * 64; idx += 256) {
-    const int tt = idx >> 6, pq = idx & 63;
-    tile[pq][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pq];
-  }
-  for (int w = 0; w < p.nomega; ++w) {
     __syncthreads();
-    if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
-    __syncthreads();
-    double m = 0.0;
+    for (int idx = tid; idx < 64 * 64; idx += 256) {
+      const int tt = idx >> 6, pq = idx & 63;
+      tile[pq][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pq];
+    }
+    for (int w = 0; w < p.nomega; ++w) {
+      __syncthreads();
+      if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+      __syncthreads();
+      double m = 0.0;
 #pragma unroll
-    for (int t = tq * 16; t < tq * 16 + 16; ++t) m = fmax(m, fabs(tile[pp][t] * sc[t]));
-    part[tq][pp] = m;
-    __syncthreads();
-    if (tid < 64) {
-      m = fmax(fmax(part[0][tid], part[1][tid]), fmax(part[2][tid], part[3][tid]));
-      if (m > 0.0) atomicMax(p.rmax + size_t(w) * p.npad + p0 + tid, (unsigned long long)__double_as_longlong(m));
+      for (int t = tq * 16; t < tq * 16 + 16; ++t) m = fmax(m, fabs(tile[pp][t] * sc[t]));
+      part[tq][pp] = m;
+      __syncthreads();
+      if (tid < 64) {
+        m = fmax(fmax(part[0][tid], part[1][tid]), fmax(part[2][tid], part[3][tid]));
+        if (m > 0.0) atomicMax(p.rmax + size_t(w) * p.npad + p0 + tid, (unsigned long long)__double_as_longlong(m));
+      }
     }
   }
-  }
+}
+
+// Base-128 digits of x (|x| < 1) truncated after s digits: X = trunc(x 2^(7s)) is
+// exact in 64-bit integers (7s <= 49 bits), and digit k (k = 1..s) of |X|, with
+// the sign of x, equals the k-th integer part taken by repeated x <- 128x - trunc(128x).
+RIGW_DEVICE_INLINE long long ozaki_fixed(double x, int s) { return (long long)ldexp(x, 7 * s); }
+RIGW_DEVICE_INLINE int ozaki_digit(long long X, int s, int k) {
+  const long long a = X < 0 ? -X : X;
+  const int d = int((a >> (7 * (s - k))) & 127);
+  return X < 0 ? -d : d;
 }
 
 // item: (prob, t0, p0, w0): the same tiles for the frequencies w0 .. w0+wgroup-1.
@@ -91,41 +101,38 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const ProbDev* __restr
   const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);
   const int tend = min(p.nia_pad, wi.a + p.split_t);
   for (int t0 = wi.a; t0 < tend; t0 += 64) {
-  __syncthreads();
-  for (int idx = tid; idx < 64 * 64; idx += 256) {
-    const int tt = idx >> 6, pp = idx & 63;
-    tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
-  }
-  for (int w = w0; w < w1; ++w) {
-    const int wl = w - w0;
     __syncthreads();
-    if (tid < 64) {
-      sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
-    } else if (tid < 128) {
-      const int pp = tid - 64;
-      const double m = __longlong_as_double((long long)p.rmax[size_t(w) * p.npad + p0 + pp]);
-      int e = 0;
-      if (m > 0.0) frexp(m, &e);    // m = f 2^e, f in [0.5, 1): every |S_pt| of the row is < 2^e
-      rs[pp] = ldexp(1.0, -e);
-      if (t0 == 0) p.xexp[size_t(w) * p.npad + p0 + pp] = e;
+    for (int idx = tid; idx < 64 * 64; idx += 256) {
+      const int tt = idx >> 6, pp = idx & 63;
+      tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
     }
-    __syncthreads();
-    const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
+    for (int w = w0; w < w1; ++w) {
+      const int wl = w - w0;
+      __syncthreads();
+      if (tid < 64) {
+        sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+      } else if (tid < 128) {
+        const int pp = tid - 64;
+        const double m = __longlong_as_double((long long)p.rmax[size_t(w) * p.npad + p0 + pp]);
+        int e = 0;
+        if (m > 0.0) frexp(m, &e);    // m = f 2^e, f in [0.5, 1): every |S_pt| of the row is < 2^e
+        rs[pp] = ldexp(1.0, -e);
+        if (t0 == 0) p.xexp[size_t(w) * p.npad + p0 + pp] = e;
+      }
+      __syncthreads();
+      const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
 #pragma unroll 1
-    for (int pr = 0; pr < 8; ++pr) {
-      const int pp = warp * 8 + pr;
-      double x0 = tile[pp][2 * lane] * s0 * rs[pp];
-      double x1 = tile[pp][2 * lane + 1] * s1 * rs[pp];
-      for (int k = 0; k < ns; ++k) {
-        const double v0 = x0 * 128.0, v1 = x1 * 128.0;
-        const double q0 = trunc(v0), q1 = trunc(v1);
-        x0 = v0 - q0;
-        x1 = v1 - q1;
-        const size_t row = (size_t(wl * ns + k) * p.npad + p0 + pp) * p.kpad + t0;
-        reinterpret_cast<char2*>(xq + row)[lane] = make_char2(char(int(q0)), char(int(q1)));
+      for (int pr = 0; pr < 8; ++pr) {
+        const int pp = warp * 8 + pr;
+        const long long X0 = ozaki_fixed(tile[pp][2 * lane] * s0 * rs[pp], ns);
+        const long long X1 = ozaki_fixed(tile[pp][2 * lane + 1] * s1 * rs[pp], ns);
+        for (int k = 1; k <= ns; ++k) {
+          const size_t row = (size_t(wl * ns + k - 1) * p.npad + p0 + pp) * p.kpad + t0;
+          reinterpret_cast<char2*>(xq + row)[lane] =
+              make_char2(char(ozaki_digit(X0, ns, k)), char(ozaki_digit(X1, ns, k)));
+        }
       }
     }
-  }
   }
 }
 
