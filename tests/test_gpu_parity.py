@@ -186,3 +186,19 @@ def test_aomo_matches_oracle(engine):
         out = engine.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1)
         ref = o.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1)
         assert np.abs(out - ref).max() < 1e-12 * np.abs(ref).max()
+
+
+@pytest.mark.parametrize("nocc,nvirt,naux,nomega", [(1, 3, 1, 1), (1, 1, 7, 2), (2, 5, 130, 1), (3, 40, 64, 3)])
+def test_tiny_shapes_all_precisions(engine, nocc, nvirt, naux, nomega):
+    """One transition, one auxiliary function, one frequency: everything is padded
+    (64- or 128-wide transition tiles, 128-wide auxiliary panels).  FP64 against
+    the oracle; the tensor-core chi0 paths against FP64."""
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_OZAKI
+    inst = synth.make_instance(nocc, nvirt, naux, nomega, seed=100 + naux)
+    out, ref = engine.g0w0(inst), oracle_outputs(inst)
+    assert abs(out.erpa - ref["erpa"]) < 1e-10 * max(1.0, abs(ref["erpa"]))
+    assert np.abs(out.sigma_calc - ref["sigma_calc"]).max() < 1e-9 * np.abs(ref["sigma_calc"]).max()
+    for prec in (RIGW_BF16X3, RIGW_OZAKI(4)):
+        sp = engine.g0w0(inst, prec)
+        assert abs(sp.erpa - out.erpa) <= 1e-4 * max(1e-12, abs(out.erpa)) + 1e-14
+        assert np.abs(sp.sigma_calc - out.sigma_calc).max() <= 1e-4 * np.abs(out.sigma_calc).max()
