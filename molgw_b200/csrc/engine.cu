@@ -125,7 +125,7 @@ void Context::free_spare() {
 }
 
 // ---------------------------------------------------------------------------
-Status Context::init(int dev, size_t budget_bytes, int want_priority) {
+Status Context::init(int dev, size_t budget_bytes, int want_priority, bool blocking_waits) {
   device = dev;
   budget = budget_bytes;
   RIGW_CUDA_TRY(cudaSetDevice(dev));
@@ -133,7 +133,8 @@ Status Context::init(int dev, size_t budget_bytes, int want_priority) {
   RIGW_CUDA_TRY(cudaDeviceGetStreamPriorityRange(&least, &greatest));
   priority = want_priority > 0 ? greatest : (want_priority < 0 ? least : 0);
   RIGW_CUDA_TRY(cudaStreamCreateWithPriority(&stream, cudaStreamNonBlocking, priority));
-  RIGW_CUDA_TRY(cudaEventCreateWithFlags(&sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
+  if (blocking_waits)
+    RIGW_CUDA_TRY(cudaEventCreateWithFlags(&sync_ev, cudaEventBlockingSync | cudaEventDisableTiming));
   for (auto& e : stage_ev) RIGW_CUDA_TRY(cudaEventCreate(&e));
   cudaMemPool_t pool;
   RIGW_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, dev));
@@ -164,6 +165,20 @@ Status Context::borrow(int nstreams, int nevents, std::vector<cudaStream_t>* str
   return Status::ok();
 }
 
+char* Context::stage_take(size_t bytes) {
+  if (!host_stage) {
+    if (cudaHostAlloc(reinterpret_cast<void**>(&host_stage), kHostStage, cudaHostAllocPortable) != cudaSuccess) {
+      cudaGetLastError();
+      host_stage = nullptr;
+      return nullptr;
+    }
+  }
+  const size_t o = align_up(host_stage_used, kAlign);
+  if (o + bytes > kHostStage) return nullptr;
+  host_stage_used = o + bytes;
+  return host_stage + o;
+}
+
 Status Context::sync(cudaStream_t s) {
   if (!sync_ev) {
     RIGW_CUDA_TRY(cudaStreamSynchronize(s));
@@ -182,6 +197,7 @@ Context::~Context() {
     cudaStreamDestroy(stream);
   }
   if (sync_ev) cudaEventDestroy(sync_ev);
+  if (host_stage) cudaFreeHost(host_stage);
   for (auto& e : stage_ev)
     if (e) cudaEventDestroy(e);
   for (auto& e : order_pool) cudaEventDestroy(e);
@@ -884,6 +900,22 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
   const bool sigma = (mode_ == kPlanFused || mode_ == kPlanSigma || mode_ == kPlanPartial);
   const bool qp = (mode_ == kPlanFused || mode_ == kPlanQP);
   std::deque<std::vector<double>> keep;   // host sources of the copies below
+  ctx_->stage_reset();
+  // host -> device copy of `bytes`; small host sources go through the pinned staging area
+  auto h2d = [&](void* dst, const void* src, size_t bytes) -> Status {
+    cudaPointerAttributes a{};
+    const bool dev_src = cudaPointerGetAttributes(&a, src) == cudaSuccess &&
+                         (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    char* st = (!dev_src && bytes <= (size_t(1) << 20)) ? ctx_->stage_take(bytes) : nullptr;
+    if (st) {
+      std::memcpy(st, src, bytes);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(dst, st, bytes, cudaMemcpyHostToDevice, s));
+    } else {
+      RIGW_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDefault, s));
+    }
+    return Status::ok();
+  };
   for (size_t i = 0; i < probs_.size(); ++i) {
     const rigw_problem& q = probs[i];
     PlanProblem& pp = probs_[i];
@@ -899,7 +931,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
       if (on_dev) {
         *slot = user;
       } else {
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(off), user, n * sizeof(double), cudaMemcpyHostToDevice, s));
+        RIGW_TRY(h2d(dp(off), user, n * sizeof(double)));
         *slot = dp(off);
       }
       return Status::ok();
@@ -909,8 +941,8 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
       if (q.omega && q.weight) {
         // small arrays: always copied (host or device source), so that a frequency
         // chunk may pass host subsets of the grid beside device-resident tensors
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_omega), q.omega, sh.nomega * 8, cudaMemcpyDefault, s));
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_weight), q.weight, sh.nomega * 8, cudaMemcpyDefault, s));
+        RIGW_TRY(h2d(dp(pp.off_in_omega), q.omega, sh.nomega * 8));
+        RIGW_TRY(h2d(dp(pp.off_in_weight), q.weight, sh.nomega * 8));
         p.omega = dp(pp.off_in_omega);
         p.weight = dp(pp.off_in_weight);
       } else {
@@ -919,8 +951,8 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
         keep.emplace_back(sh.nomega);
         std::vector<double>& wt = keep.back();
         imag_grid(sh.nomega, om.data(), wt.data());
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_omega), om.data(), om.size() * 8, cudaMemcpyHostToDevice, s));
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_weight), wt.data(), wt.size() * 8, cudaMemcpyHostToDevice, s));
+        RIGW_TRY(h2d(dp(pp.off_in_omega), om.data(), om.size() * 8));
+        RIGW_TRY(h2d(dp(pp.off_in_weight), wt.data(), wt.size() * 8));
         p.omega = dp(pp.off_in_omega);
         p.weight = dp(pp.off_in_weight);
       }
@@ -949,7 +981,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
           z[2 * k] = q.efermi;
           z[2 * k + 1] = q.step_sigma_calc * k;
         }
-        RIGW_CUDA_TRY(cudaMemcpyAsync(dp(pp.off_in_zcalc), z.data(), z.size() * 8, cudaMemcpyHostToDevice, s));
+        RIGW_TRY(h2d(dp(pp.off_in_zcalc), z.data(), z.size() * 8));
         p.zcalc = dp(pp.off_in_zcalc);
       }
     }
@@ -966,8 +998,7 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
     }
     host_table_[i] = p;
   }
-  RIGW_CUDA_TRY(cudaMemcpyAsync(probs_dev_, host_table_.data(), sizeof(ProbDev) * host_table_.size(),
-                                cudaMemcpyHostToDevice, s));
+  RIGW_TRY(h2d(probs_dev_, host_table_.data(), sizeof(ProbDev) * host_table_.size()));
   // copies from pageable host memory are staged before cudaMemcpyAsync returns:
   // the host vectors in `keep` may go out of scope without a wait
   return Status::ok();
@@ -1036,65 +1067,113 @@ Status Plan::check_errors(cudaStream_t s) {
 }
 
 Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStream_t s) {
-  // pass 1: every small output and input of the batch to the host, one wait
+  // pass 1: every small output and input of the batch to pinned host memory, one wait
   const size_t np = probs_.size();
-  std::vector<double> en(2 * np, 0.0);
-  std::vector<std::vector<double>> q(np), occ(np);
+  ctx_->stage_reset();
+  auto is_dev = [](const void* ptr) {
+    cudaPointerAttributes a{};
+    const bool d = cudaPointerGetAttributes(&a, ptr) == cudaSuccess &&
+                   (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    return d;
+  };
+  struct Host {
+    double* en = nullptr;      // [2]
+    double* q = nullptr;       // [4 nsig]
+    double* occ = nullptr;     // [nsig]
+    double* sc = nullptr;      // sigma_calc staged for a host destination
+    double* sr = nullptr;      // sigma (real grid) staged for a host destination
+  };
+  std::vector<Host> h(np);
+  std::vector<std::vector<double>> own;   // fallback when the staging area is full
+  auto take = [&](size_t n) -> double* {
+    char* st = ctx_->stage_take(n * sizeof(double));
+    if (st) return reinterpret_cast<double*>(st);
+    own.emplace_back(n);
+    return own.back().data();
+  };
   for (size_t i = 0; i < np; ++i) {
     const ProbDev& p = probs_[i].dev;
     rigw_result& r = res[i];
     const int nreal = 2 * p.nsigma_half + 1;
-    if (p.out_energies)
-      RIGW_CUDA_TRY(cudaMemcpyAsync(&en[2 * i], p.out_energies, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
-    if (r.sigma_calc && p.sigma_calc && mode_ != kPlanQP)
-      RIGW_CUDA_TRY(cudaMemcpyAsync(r.sigma_calc, p.sigma_calc, sizeof(double) * 2 * p.nsig * p.nc,
-                                    cudaMemcpyDefault, s));
-    if (r.sigma && p.sigma_real)
-      RIGW_CUDA_TRY(
-          cudaMemcpyAsync(r.sigma, p.sigma_real, sizeof(double) * 2 * p.nsig * nreal, cudaMemcpyDefault, s));
+    const size_t nsc = size_t(2) * p.nsig * p.nc, nsr = size_t(2) * p.nsig * nreal;
+    if (p.out_energies) {
+      h[i].en = take(2);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].en, p.out_energies, 2 * sizeof(double), cudaMemcpyDeviceToHost, s));
+    }
+    if (r.sigma_calc && p.sigma_calc && mode_ != kPlanQP) {
+      if (is_dev(r.sigma_calc)) {
+        RIGW_CUDA_TRY(cudaMemcpyAsync(r.sigma_calc, p.sigma_calc, nsc * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      } else {
+        h[i].sc = take(nsc);
+        RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].sc, p.sigma_calc, nsc * sizeof(double), cudaMemcpyDeviceToHost, s));
+      }
+    }
+    if (r.sigma && p.sigma_real) {
+      if (is_dev(r.sigma)) {
+        RIGW_CUDA_TRY(cudaMemcpyAsync(r.sigma, p.sigma_real, nsr * sizeof(double), cudaMemcpyDeviceToDevice, s));
+      } else {
+        h[i].sr = take(nsr);
+        RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].sr, p.sigma_real, nsr * sizeof(double), cudaMemcpyDeviceToHost, s));
+      }
+    }
     if (p.qp) {
-      q[i].assign(4 * p.nsig, 0.0);
-      occ[i].assign(p.nsig, 0.0);
-      RIGW_CUDA_TRY(cudaMemcpyAsync(q[i].data(), p.qp, q[i].size() * sizeof(double), cudaMemcpyDeviceToHost, s));
-      if (probs[i].occ_sig)
-        RIGW_CUDA_TRY(cudaMemcpyAsync(occ[i].data(), probs[i].occ_sig, p.nsig * sizeof(double), cudaMemcpyDefault,
-                                      s));
+      h[i].q = take(4 * size_t(p.nsig));
+      h[i].occ = take(p.nsig);
+      std::fill(h[i].occ, h[i].occ + p.nsig, 0.0);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].q, p.qp, 4 * p.nsig * sizeof(double), cudaMemcpyDeviceToHost, s));
+      if (probs[i].occ_sig) {
+        if (is_dev(probs[i].occ_sig))
+          RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].occ, probs[i].occ_sig, p.nsig * sizeof(double), cudaMemcpyDeviceToHost,
+                                        s));
+        else
+          std::memcpy(h[i].occ, probs[i].occ_sig, p.nsig * sizeof(double));
+      }
     }
   }
   RIGW_TRY(ctx_->sync(s));
   // pass 2: QP energies and output_homolumo on the host, copies to the caller's buffers
-  std::vector<std::vector<double>> g(np), z(np), zz(np);
+  std::deque<std::vector<double>> out_dev;   // host sources of copies to device destinations
+  auto put = [&](double* dst, const double* src, size_t n) -> Status {
+    if (is_dev(dst)) {
+      out_dev.emplace_back(src, src + n);
+      RIGW_CUDA_TRY(cudaMemcpyAsync(dst, out_dev.back().data(), n * sizeof(double), cudaMemcpyHostToDevice, s));
+    } else {
+      std::memcpy(dst, src, n * sizeof(double));
+    }
+    return Status::ok();
+  };
   for (size_t i = 0; i < np; ++i) {
     const ProbDev& p = probs_[i].dev;
     rigw_result& r = res[i];
-    if (p.out_energies) {
-      r.erpa = en[2 * i];
-      r.egw = en[2 * i + 1];
+    const int nreal = 2 * p.nsigma_half + 1;
+    if (h[i].en) {
+      r.erpa = h[i].en[0];
+      r.egw = h[i].en[1];
     }
-    if (p.qp) {
-      g[i].resize(p.nsig);
-      z[i].resize(p.nsig);
-      zz[i].resize(p.nsig);
+    if (h[i].sc) std::memcpy(r.sigma_calc, h[i].sc, size_t(2) * p.nsig * p.nc * sizeof(double));
+    if (h[i].sr) std::memcpy(r.sigma, h[i].sr, size_t(2) * p.nsig * nreal * sizeof(double));
+    if (h[i].q) {
+      std::vector<double> g(p.nsig), z(p.nsig), zz(p.nsig);
       double eh = -HUGE_VAL, el = HUGE_VAL;
       for (int k = 0; k < p.nsig; ++k) {
-        g[i][k] = q[i][4 * k];
-        z[i][k] = q[i][4 * k + 1];
-        zz[i][k] = q[i][4 * k + 2];
+        g[k] = h[i].q[4 * k];
+        z[k] = h[i].q[4 * k + 1];
+        zz[k] = h[i].q[4 * k + 2];
         // output_homolumo, src/m_hamiltonian_tools.f90:564-612 (spin_fact = 2)
-        if (occ[i][k] / 2.0 > 1.0e-5) eh = std::max(eh, g[i][k]);
-        if (occ[i][k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[i][k]);
+        if (h[i].occ[k] / 2.0 > 1.0e-5) eh = std::max(eh, g[k]);
+        if (h[i].occ[k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[k]);
       }
       r.ehomo = eh;
       r.elumo = el;
-      if (r.energy_qp_g)
-        RIGW_CUDA_TRY(cudaMemcpyAsync(r.energy_qp_g, g[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
-      if (r.energy_qp_z)
-        RIGW_CUDA_TRY(cudaMemcpyAsync(r.energy_qp_z, z[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
-      if (r.zz) RIGW_CUDA_TRY(cudaMemcpyAsync(r.zz, zz[i].data(), p.nsig * 8, cudaMemcpyDefault, s));
+      if (r.energy_qp_g) RIGW_TRY(put(r.energy_qp_g, g.data(), p.nsig));
+      if (r.energy_qp_z) RIGW_TRY(put(r.energy_qp_z, z.data(), p.nsig));
+      if (r.zz) RIGW_TRY(put(r.zz, zz.data(), p.nsig));
     }
     r.device_ms = last_ms_;
   }
-  return ctx_->sync(s);   // the staging vectors go out of scope
+  if (!out_dev.empty()) RIGW_TRY(ctx_->sync(s));   // the staged sources go out of scope
+  return Status::ok();
 }
 
 }  // namespace rigw

@@ -217,6 +217,13 @@ class Context {
   std::vector<cudaEvent_t> order_pool;   // ordering events (no timing)
   cudaEvent_t stage_ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   Status borrow(int nstreams, int nevents, std::vector<cudaStream_t>* streams, std::vector<cudaEvent_t>* events);
+  // Pinned host staging for the small inputs and outputs of one call: copies from
+  // it are asynchronous (pageable sources make every copy wait for the stream).
+  static constexpr size_t kHostStage = size_t(16) << 20;
+  char* host_stage = nullptr;
+  size_t host_stage_used = 0;
+  char* stage_take(size_t bytes);   // nullptr when the area is full or unavailable
+  void stage_reset() { host_stage_used = 0; }
   // Allocate a block of `bytes` now and keep it as the spare block, so that the
   // plans of this context take their arena from it instead of growing the pool.
   Status reserve(size_t bytes);
@@ -231,7 +238,9 @@ class Context {
   }
   int priority = 0;   // CUDA stream priority of every stream of this context (lower = higher)
   // priority: 0 default; > 0 asks for the highest priority, < 0 for the lowest
-  Status init(int dev, size_t budget_bytes, int want_priority = 0);
+  // blocking_waits: host waits sleep on an event (request-loop workers, many
+  // threads) instead of spinning (one caller: lowest latency)
+  Status init(int dev, size_t budget_bytes, int want_priority = 0, bool blocking_waits = false);
   ~Context();
 };
 

@@ -200,7 +200,7 @@ RIGW_API int rigw_server_create(rigw_server** srv, int device, size_t hbm_budget
   S.share = budget / size_t(workers);
   for (int w = 0; w < workers; ++w) {
     S.ctx.emplace_back(new rigw::Context());
-    rigw::Status st = S.ctx.back()->init(device, S.share);
+    rigw::Status st = S.ctx.back()->init(device, S.share, 0, /*blocking_waits=*/true);
     // the worker's device memory is reserved once: batch plans take their arena
     // from it, so no batch waits for the memory pool to grow
     if (st.good() && S.share > (size_t(2) << 30)) st = S.ctx.back()->reserve(S.share - (size_t(1) << 30));
