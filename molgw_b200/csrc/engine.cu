@@ -700,6 +700,17 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     pair += sh.nomega;
   }
 
+  // chi0 items longest first: the block scheduler hands out CTAs in index order,
+  // so a ragged batch ends on short tiles (results do not depend on the order)
+  std::stable_sort(gl_syrk_.begin(), gl_syrk_.end(), [](const GemmItem& a, const GemmItem& b) {
+    return double(a.k) * a.m * a.n * std::max(a.nw, 1) > double(b.k) * b.m * b.n * std::max(b.nw, 1);
+  });
+  auto by_cost = [](const TcItem& a, const TcItem& b) {
+    return double(a.ktiles) * std::max(a.nw, 1) > double(b.ktiles) * std::max(b.nw, 1);
+  };
+  for (auto& l : tl_syrk_) std::stable_sort(l.begin(), l.end(), by_cost);
+  for (auto& l : tl_ozaki_) std::stable_sort(l.begin(), l.end(), by_cost);
+
   // ---- upload the lists and the launch sequence
   size_t lbytes = 0;
   auto reserve = [&](size_t n) {
