@@ -499,6 +499,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   gl_k2_.assign(nlists, {});
   gl_k3_.assign(nlists, {});
   gl_k3d_.assign(nlists, {});
+  gl_k3a_.assign(nlists, {});
   int pair = 0;
   for (int i = 0; i < np; ++i) {
     const Shape& sh = shapes[i];
@@ -651,39 +652,49 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         if (p.want_identity)
           for (int c0 = 0; c0 < r0; c0 += BMN) k2(R, ldb, c0, std::min(BMN, r0 - c0), cs + c0);
         for (int c0 = p.moff; c0 < ldb; c0 += BMN) k2(R, ldb, c0, std::min(BMN, ldb - c0), cs + c0);
-        // trailing update of panel k, in 64-row items; the items of the next
-        // diagonal block go to their own list so that its factorization can start
-        // while the rest of the update runs (lookahead)
+        // Trailing update, panels in pairs (k even, k + 1): after panel k only the
+        // rows of panel k + 1 are updated (K = 128, the U rows of panel k); after
+        // panel k + 1 every row below it is updated once with the U rows of both
+        // panels (K = 256), so each trailing tile is read and written once per
+        // pair.  Items of the next diagonal block go to their own list so that its
+        // factorization can start while the rest of the update runs (lookahead).
+        const bool first_of_pair = (k % 2) == 0;
+        const int kp = first_of_pair ? k : k - 1;               // first panel of the U rows used
+        const int kdim = first_of_pair ? kPanel : 2 * kPanel;
+        const int iend = first_of_pair ? std::min(npad, r0 + kPanel) : npad;
         auto k3 = [&](const double* Bsrc, int ldbs, double* Cdst, int ldc, int i0, int c0, int m, int n,
-                      bool next_diag) {
+                      std::vector<GemmItem>& dst) {
           GemmItem g{};
-          g.A = E + size_t(k) * kPanel * npad + i0;
+          g.A = E + size_t(kp) * kPanel * npad + i0;
           g.lda = npad;
-          g.B = Bsrc + size_t(k) * kPanel * ldbs + c0;
+          g.B = Bsrc + size_t(kp) * kPanel * ldbs + c0;
           g.ldb = ldbs;
           g.C = Cdst + size_t(i0) * ldc + c0;
           g.Cin = g.C;
           g.ldc = ldc;
           g.m = m;
           g.n = n;
-          g.k = kPanel;
+          g.k = kdim;
           g.alpha = -1.0;
           g.beta = 1.0;
           g.nw = nw;
           g.sA = sE;
           g.sB = (Bsrc == E) ? sE : sR;
           g.sC = (Cdst == E) ? sE : sR;
-          (next_diag ? gl_k3d_[li] : gl_k3_[li]).push_back(g);
+          dst.push_back(g);
         };
-        for (int i0 = r0; i0 < npad; i0 += BM) {
-          const int m = std::min(BM, npad - i0);
+        std::vector<GemmItem>& rest = first_of_pair ? gl_k3a_[li] : gl_k3_[li];
+        for (int i0 = r0; i0 < iend; i0 += BM) {
+          const int m = std::min(BM, iend - i0);
           if (factor)
-            for (int j0 = i0 / BMN * BMN; j0 < npad; j0 += BMN)
-              k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0), i0 < r0 + kPanel && j0 == r0);
+            for (int j0 = i0 / BMN * BMN; j0 < npad; j0 += BMN) {
+              const bool next_diag = !first_of_pair && i0 < r0 + kPanel && j0 == r0;
+              k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0), next_diag ? gl_k3d_[li] : rest);
+            }
+          // I block: columns below r0 only (the U rows of panel kp have zeros beyond it there)
           if (p.want_identity)
-            for (int c0 = 0; c0 < r0; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, r0 - c0), false);
-          for (int c0 = p.moff; c0 < ldb; c0 += BMN)
-            k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, ldb - c0), false);
+            for (int c0 = 0; c0 < r0; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, r0 - c0), rest);
+          for (int c0 = p.moff; c0 < ldb; c0 += BMN) k3(R, ldb, R, ldb, i0, c0, m, std::min(BMN, ldb - c0), rest);
         }
       }
     }
@@ -774,6 +785,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         pending = -1;
       if (add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm, pending)) pending = -1;
       const bool next = k + 1 < max_panels && !wl_diag_[L(k + 1)].empty();
+      if (k % 2 == 0) {
+        // first panel of a pair: the rows of panel k + 1, then its diagonal block
+        if (add(6, gl_k3a_[L(k)].data(), sizeof(GemmItem), gl_k3a_[L(k)].size(), k, sm, pending)) pending = -1;
+        if (next && add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sm,
+                        pending))
+          pending = -1;
+        continue;
+      }
       const int ea = next ? nev++ : -1, eb = next ? nev++ : -1;
       if (next && !gl_k3d_[L(k)].empty()) {
         add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm, -1, ea);
