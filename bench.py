@@ -192,7 +192,7 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
         # the autotuner runs on the first 8 molecules; its choice applies to the whole batch
         tuning[name] = compact_tuning(eng.autotune(insts[:8], prec, devs[:8], qp_only=True))
         eng.g0w0_batch(insts, prec, devs, qp_only=True)
-        dev_ms, wall_ms = [], []
+        dev_ms, wall_ms, stage_ms = [], [], []
         for _ in range(reps):
             flush_l2()
             t0 = time.perf_counter()
@@ -200,10 +200,13 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
             wall_ms.append((time.perf_counter() - t0) * 1e3)
             st = eng.last_stats()
             dev_ms.append(st["total_ms"])
+            stage_ms.append(st["stage_ms"])
         outs[name] = o
         res[name] = {"solves_per_s": count / (np.mean(dev_ms) * 1e-3),
                      "solves_per_s_wall": count / (np.mean(wall_ms) * 1e-3),
                      "ms_per_batch": float(np.mean(dev_ms)), "wall_ms_per_batch": float(np.mean(wall_ms)),
+                     "stage_ms": dict(zip(("pack", "chi0", "eps_factor_solve", "sigma_qp"),
+                                          np.mean(np.array(stage_ms), axis=0).round(3).tolist())),
                      "waves": st["waves"], "chunks": st["chunks"], "kernel_launches": st["kernel_launches"],
                      "tuning": tuning[name]}
     dqp = max(float(np.abs(a.energy_qp_g - b.energy_qp_g).max()) for a, b in zip(outs["fp64"], outs["bf16x3"]))

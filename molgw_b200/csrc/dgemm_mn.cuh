@@ -134,6 +134,9 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
 
   const int q = lane >> 2;   // fragment row (A) / column (B) within the 8-wide tile
   const int r = lane & 3;    // fragment k index
+  // 8-column fragments of this warp inside the item (warp-uniform); edge tiles
+  // skip the MMAs of columns beyond n, whose values are never stored
+  const int nfrag = min(4, max(0, (it.n - wn0 + 7) >> 3));
   for (int kt = 0; kt < ktiles; ++kt) {
     cp_async_wait<ST - 2>();
     __syncthreads();
@@ -164,10 +167,18 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
       }
 #pragma unroll
       for (int j = 0; j < 4; ++j) b[j] = bs[kk * Cfg::kLdbS + 8 * j];
+      if (nfrag == 4) {
 #pragma unroll
-      for (int i = 0; i < 8; ++i)
+        for (int i = 0; i < 8; ++i)
 #pragma unroll
-        for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+          for (int j = 0; j < 4; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+          if (j < nfrag)
+#pragma unroll
+            for (int i = 0; i < 8; ++i) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
+      }
     }
   }
   cp_async_wait<0>();

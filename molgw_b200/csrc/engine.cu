@@ -576,11 +576,13 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
             }
       }
       if (sh.precision == RIGW_FP64) {
-        // one item per tile covering every frequency (blockIdx.y)
+        // one item per tile covering every frequency (blockIdx.y); the tiles of a
+        // row block start at its diagonal, so only the lower half of the
+        // diagonal BMC x BMC block lies below it, and end at naux
         if (npad > sh.naux)
           for (int w = 0; w < sh.nomega; ++w) wl_pad_.push_back({i, w, 0, 0});
         for (int ti = 0; ti < sh.naux; ti += BMC)
-          for (int tj = ti / BMN * BMN; tj < sh.naux; tj += BMN) {
+          for (int tj = ti; tj < sh.naux; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
             g.B = p.mp + tj;
