@@ -157,9 +157,12 @@ RIGW_API int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, 
                         const int* index_basis, const double* eri3, const double* c_matrix,
                         int mstate_min, int mstate_max, int nstate_min, int nstate_max,
                         double* out);
-/* The same transform with its two products in `precision` (RIGW_FP64, or
- * RIGW_BF16X3: bf16 hi/lo split of both operands, three products on the tensor
- * cores with fp32 accumulation over at most 512 basis functions, FP64 results). */
+/* The same transform with its two products in `precision`: RIGW_FP64;
+ * RIGW_BF16X3 (bf16 hi/lo split of both operands, three products on the tensor
+ * cores with fp32 accumulation over at most 512 basis functions, FP64 results);
+ * or RIGW_OZAKI(s), 3 <= s <= 7 (each operand row scaled by a power of two to its
+ * largest entry and cut into s int8 base-128 digits, exact INT32 products of the
+ * digit levels i + j <= s + 1, FP64 recombination). */
 RIGW_API int rigw_eri_3center_mo_precision(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux,
                                            const int* index_basis, const double* eri3, const double* c_matrix,
                                            int mstate_min, int mstate_max, int nstate_min, int nstate_max,

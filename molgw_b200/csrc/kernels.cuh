@@ -54,9 +54,9 @@ struct TcItem {
   // C + j*sC, tensor rows row_a/row_b + j*srow, exponents ea/eb + j*se.
   long long sC, se;
   int srow, nw;
-  // General products (syrk_bf16x3_kernel only): B from its own tensor map (nullptr:
-  // the A map) whose lo rows are lo_off_b below the hi rows; only the first mrows
-  // x ncols of the tile are stored (0: all 128).
+  // General products: B from its own tensor map (nullptr: the A map) whose lo
+  // rows (Ozaki: next slice) are lo_off_b below the hi rows (first slice); only
+  // the first mrows x ncols of the tile are stored, without identity (0: all 128).
   const void* tmap_b;
   int lo_off_b, mrows, ncols;
 };
@@ -72,6 +72,20 @@ struct SplitOp {
   long long zs_dst;   // elements between batches of dst
 };
 void launch_split_kmajor(const SplitOp& op, cudaStream_t s);
+// Ozaki slicing of a general FP64 operand: element (r, k) of batch z is
+// src[z*zs_src + r*rs + k*ks]; row r is scaled by 2^-e_r (e_r the exponent of
+// max_k |x_rk|, to exps[z*Rpad + r]) and cut into `slices` int8 base-128 digits,
+// stored K-contiguous as [nz][slices][Rpad][Kpad] (Kpad a multiple of 128, zero
+// padded).  rmax is [nz][Rpad] scratch.
+struct SliceOp {
+  const double* src;
+  long long rs, ks, zs_src;
+  int R, K, Rpad, Kpad, nz, slices;
+  void* dst;
+  unsigned long long* rmax;
+  int* exps;
+};
+void launch_slice_kmajor(const SliceOp& op, cudaStream_t s);
 void launch_syrk_bf16x3(const TcItem* items, int n, int ny, cudaStream_t s);
 void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);

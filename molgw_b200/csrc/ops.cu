@@ -77,13 +77,41 @@ Status split_operand(Context& c, const SplitOp& shape, DeviceBuffer* buf, void* 
   return Status::ok();
 }
 
-Status run_tc_items(Context& c, const std::vector<TcItem>& items) {
+// One Ozaki operand: `slices` int8 digit planes K-major in `buf`, row exponents
+// in `exps` ([nz][Rpad]), its tensor map (rows = nz * slices * Rpad, columns =
+// Kpad bytes) at `map_dev`.
+Status slice_operand(Context& c, const SplitOp& shape, int slices, DeviceBuffer* buf, DeviceBuffer* exps,
+                     void* map_dev) {
+  SliceOp op{shape.src, shape.rs, shape.ks, shape.zs_src, shape.R, shape.K, shape.Rpad, shape.Kpad, shape.nz,
+             slices, nullptr, nullptr, nullptr};
+  const size_t rows = size_t(op.nz) * slices * op.Rpad;
+  RIGW_TRY(buf->allocate(&c, rows * op.Kpad, "sliced operand"));
+  RIGW_TRY(exps->allocate(&c, size_t(op.nz) * op.Rpad * (sizeof(int) + sizeof(unsigned long long)),
+                          "row exponents"));
+  op.dst = buf->data();
+  op.rmax = reinterpret_cast<unsigned long long*>(exps->data());
+  op.exps = reinterpret_cast<int*>(exps->data() + size_t(op.nz) * op.Rpad * sizeof(unsigned long long));
+  launch_slice_kmajor(op, c.stream);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  alignas(64) unsigned char map[128];
+  RIGW_TRY(make_ozaki_tmap(map, op.dst, op.Kpad, (long long)rows));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(map_dev, map, sizeof(map), cudaMemcpyHostToDevice, c.stream));
+  return Status::ok();
+}
+const int* exps_of(const DeviceBuffer& e, int nz, int Rpad) {
+  return reinterpret_cast<const int*>(e.data() + size_t(nz) * Rpad * sizeof(unsigned long long));
+}
+
+Status run_tc_items(Context& c, const std::vector<TcItem>& items, bool ozaki = false) {
   if (items.empty()) return Status::ok();
   DeviceBuffer buf;
   RIGW_TRY(buf.allocate(&c, items.size() * sizeof(TcItem), "tensor-core items"));
   RIGW_CUDA_TRY(cudaMemcpyAsync(buf.data(), items.data(), items.size() * sizeof(TcItem), cudaMemcpyHostToDevice,
                                 c.stream));
-  launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(buf.data()), int(items.size()), 1, c.stream);
+  if (ozaki)
+    launch_syrk_ozaki(reinterpret_cast<const TcItem*>(buf.data()), int(items.size()), 1, c.stream);
+  else
+    launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(buf.data()), int(items.size()), 1, c.stream);
   RIGW_CUDA_TRY(cudaGetLastError());
   return c.sync(c.stream);
 }
@@ -94,9 +122,11 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
                       int nstate_min, int nstate_max, double* out, int precision) {
   if (nbf <= 0 || nstate <= 0 || npair <= 0 || naux <= 0 || !index_basis || !eri3 || !c_matrix || !out)
     return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: invalid arguments");
-  if (precision != RIGW_FP64 && precision != RIGW_BF16X3)
-    return Status::fail(RIGW_ERR_UNSUPPORTED, "eri_3center_mo: precision %d (FP64 or BF16X3)", precision);
-  const bool split = precision == RIGW_BF16X3;
+  if (precision != RIGW_FP64 && precision != RIGW_BF16X3 && !is_ozaki(precision))
+    return Status::fail(RIGW_ERR_UNSUPPORTED, "eri_3center_mo: precision %d (FP64, BF16X3 or OZAKI(3..7))",
+                        precision);
+  const int ns = ozaki_slices(precision);
+  const bool split = precision == RIGW_BF16X3 || ns > 0;
   if (split && !bf16x3_available()) return Status::fail(RIGW_ERR_UNSUPPORTED, "tensor maps unavailable");
   if (mstate_min < 1 || mstate_max > nstate || mstate_min > mstate_max || nstate_min < 1 ||
       nstate_max > nstate || nstate_min > nstate_max)
@@ -137,10 +167,11 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   double* dout = reinterpret_cast<double*>(b_out.data());
   // split precision: C^T blocks split once; the unpacked tensor and the half
   // transform are split per auxiliary chunk (BF16x3 products, FP64 results)
-  const int Kp = round_up(nbf, 64);
+  const int Kp = round_up(nbf, ns > 0 ? 128 : 64);   // 64 bf16 or 128 int8 per k-tile
   const int Rp1 = round_up(ncp, 128), Rp2 = round_up(mcp, 128), Rpw = round_up(nbf * pcp, 128);
   const int Rpp = round_up(pcp, 128);
   DeviceBuffer s_a1, s_a2, s_b1, s_b2, s_maps, s_err;
+  DeviceBuffer e_a1, e_a2, e_b1, e_b2;   // Ozaki row exponents
   char* maps = nullptr;
   int* errp = nullptr;
   if (split) {
@@ -149,9 +180,19 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     maps = s_maps.data();
     errp = reinterpret_cast<int*>(s_err.data());
     RIGW_CUDA_TRY(cudaMemsetAsync(errp, 0, sizeof(int), s));
-    RIGW_TRY(split_operand(c, SplitOp{dctn, 1, ncp, 0, ncp, nbf, Rp1, Kp, 1, nullptr, 0}, &s_a1, maps));
-    RIGW_TRY(split_operand(c, SplitOp{dctm, 1, mcp, 0, mcp, nbf, Rp2, Kp, 1, nullptr, 0}, &s_a2, maps + 256));
+    const SplitOp a1{dctn, 1, ncp, 0, ncp, nbf, Rp1, Kp, 1, nullptr, 0};
+    const SplitOp a2{dctm, 1, mcp, 0, mcp, nbf, Rp2, Kp, 1, nullptr, 0};
+    if (ns > 0) {
+      RIGW_TRY(slice_operand(c, a1, ns, &s_a1, &e_a1, maps));
+      RIGW_TRY(slice_operand(c, a2, ns, &s_a2, &e_a2, maps + 256));
+    } else {
+      RIGW_TRY(split_operand(c, a1, &s_a1, maps));
+      RIGW_TRY(split_operand(c, a2, &s_a2, maps + 256));
+    }
   }
+  // rows between the first planes of two operand blocks (hi/lo, or the slices)
+  const int planes = ns > 0 ? ns : 2;
+  const int ktiles = ns > 0 ? Kp / 128 : Kp / 64;
   for (int p0 = 0; p0 < naux; p0 += pc) {
     const int cnt = std::min(pc, naux - p0);
     RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), eri3 + size_t(p0) * npair, size_t(cnt) * npair * 8,
@@ -166,7 +207,11 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     const int wide = nbf * pcp;
     if (split) {
       // step 1: T[n][j] = sum_nu ctn^T[n][nu] B^T[j][nu],  j = (mu, P)
-      RIGW_TRY(split_operand(c, SplitOp{dfull, 1, wide, 0, wide, nbf, Rpw, Kp, 1, nullptr, 0}, &s_b1, maps + 128));
+      const SplitOp b1{dfull, 1, wide, 0, wide, nbf, Rpw, Kp, 1, nullptr, 0};
+      if (ns > 0)
+        RIGW_TRY(slice_operand(c, b1, ns, &s_b1, &e_b1, maps + 128));
+      else
+        RIGW_TRY(split_operand(c, b1, &s_b1, maps + 128));
       std::vector<TcItem> t1;
       for (int i0 = 0; i0 < ncp; i0 += 128)
         for (int j0 = 0; j0 < wide; j0 += 128) {
@@ -177,18 +222,27 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
           t.tmap_b = maps + 128;
           t.row_b = j0;
           t.lo_off_b = Rpw;
-          t.ktiles = Kp / 64;
+          t.ktiles = ktiles;
           t.C = dt + size_t(i0) * wide + j0;
           t.ldc = wide;
           t.mrows = std::min(128, ncp - i0);
           t.ncols = std::min(128, wide - j0);
           t.err = errp;
           t.nw = 1;
+          if (ns > 0) {
+            t.slices = ns;
+            t.ea = exps_of(e_a1, 1, Rp1) + i0;
+            t.eb = exps_of(e_b1, 1, Rpw) + j0;
+          }
           t1.push_back(t);
         }
-      RIGW_TRY(run_tc_items(c, t1));
+      RIGW_TRY(run_tc_items(c, t1, ns > 0));
       // step 2: O[n][m][P] = sum_mu ctm^T[m][mu] T[n]^T[P][mu], every n in one launch
-      RIGW_TRY(split_operand(c, SplitOp{dt, 1, pcp, wide, pcp, nbf, Rpp, Kp, nc, nullptr, 0}, &s_b2, maps + 384));
+      const SplitOp b2{dt, 1, pcp, wide, pcp, nbf, Rpp, Kp, nc, nullptr, 0};
+      if (ns > 0)
+        RIGW_TRY(slice_operand(c, b2, ns, &s_b2, &e_b2, maps + 384));
+      else
+        RIGW_TRY(split_operand(c, b2, &s_b2, maps + 384));
       std::vector<TcItem> t2;
       for (int n = 0; n < nc; ++n)
         for (int i0 = 0; i0 < mcp; i0 += 128)
@@ -198,18 +252,23 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
             t.row_a = i0;
             t.lo_off = Rp2;
             t.tmap_b = maps + 384;
-            t.row_b = n * 2 * Rpp + j0;
+            t.row_b = n * planes * Rpp + j0;
             t.lo_off_b = Rpp;
-            t.ktiles = Kp / 64;
+            t.ktiles = ktiles;
             t.C = dout + (size_t(n) * mcp + i0) * pcp + j0;
             t.ldc = pcp;
             t.mrows = std::min(128, mcp - i0);
             t.ncols = std::min(128, pcp - j0);
             t.err = errp;
             t.nw = 1;
+            if (ns > 0) {
+              t.slices = ns;
+              t.ea = exps_of(e_a2, 1, Rp2) + i0;
+              t.eb = exps_of(e_b2, nc, Rpp) + size_t(n) * Rpp + j0;
+            }
             t2.push_back(t);
           }
-      RIGW_TRY(run_tc_items(c, t2));
+      RIGW_TRY(run_tc_items(c, t2, ns > 0));
       int herr = 0;
       RIGW_CUDA_TRY(cudaMemcpyAsync(&herr, errp, sizeof(int), cudaMemcpyDeviceToHost, s));
       RIGW_TRY(c.sync(s));

@@ -18,7 +18,11 @@
 //                      bit pattern of a non-negative double: order independent).
 // ozaki_slice_kernel:  row exponents and the s int8 slices of one frequency group,
 //                      K-major (transition-contiguous) for TMA.
-// syrk_ozaki_kernel:   one 128x128 upper tile of eps(iw) per CTA; warp 0 issues
+// slice_rowmax_kernel, slice_kmajor_kernel: the same slicing for the general
+//                      operands of the AO->MO products (row exponents from the
+//                      row maxima over K).
+// syrk_ozaki_kernel:   one 128x128 upper tile of eps(iw), or one tile of a general
+//                      product A B^T, per CTA; warp 0 issues
 //                      TMA loads (one A and one B slice tile of 128 rows x 128
 //                      transitions per stage, 128-byte swizzle, 6 stages), warp 1
 //                      issues the MMAs, warps 2..9 drain.  All waits are bounded.
@@ -137,6 +141,71 @@ __global__ void __launch_bounds__(256) ozaki_slice_kernel(const ProbDev* __restr
 }
 
 // ---------------------------------------------------------------------------
+// General operands (the AO->MO products): 64 x 64 tiles through shared memory,
+// read along the source's contiguous index.  Pass 1 takes the row maxima, pass 2
+// the row exponents and the digits, written K-contiguous.
+__global__ void __launch_bounds__(256) slice_rowmax_kernel(const SliceOp op) {
+  __shared__ double tile[64][65];   // [row][k]
+  __shared__ double part[4][64];
+  const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 64, z = blockIdx.z;
+  const double* src = op.src + size_t(z) * op.zs_src;
+  const bool rfast = op.rs == 1;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int a = idx >> 6, b = idx & 63;
+    const int rr = rfast ? b : a, kk = rfast ? a : b;
+    const int r = r0 + rr, k = k0 + kk;
+    tile[rr][kk] = (r < op.R && k < op.K) ? fabs(src[r * op.rs + k * op.ks]) : 0.0;
+  }
+  __syncthreads();
+  const int rr = tid & 63, kq = tid >> 6;
+  double m = 0.0;
+#pragma unroll
+  for (int kk = kq * 16; kk < kq * 16 + 16; ++kk) m = fmax(m, tile[rr][kk]);
+  part[kq][rr] = m;
+  __syncthreads();
+  if (tid < 64) {
+    m = fmax(fmax(part[0][tid], part[1][tid]), fmax(part[2][tid], part[3][tid]));
+    if (m > 0.0) atomicMax(op.rmax + size_t(z) * op.Rpad + r0 + tid, (unsigned long long)__double_as_longlong(m));
+  }
+}
+
+__global__ void __launch_bounds__(256) slice_kmajor_kernel(const SliceOp op) {
+  __shared__ double tile[64][65];   // [row][k]
+  __shared__ double rs[64];         // 2^-e_r
+  const int k0 = blockIdx.x * 64, r0 = blockIdx.y * 64, z = blockIdx.z;
+  const double* src = op.src + size_t(z) * op.zs_src;
+  const bool rfast = op.rs == 1;
+  const int tid = threadIdx.x, ns = op.slices;
+  for (int idx = tid; idx < 64 * 64; idx += 256) {
+    const int a = idx >> 6, b = idx & 63;
+    const int rr = rfast ? b : a, kk = rfast ? a : b;
+    const int r = r0 + rr, k = k0 + kk;
+    tile[rr][kk] = (r < op.R && k < op.K) ? src[r * op.rs + k * op.ks] : 0.0;
+  }
+  if (tid < 64) {
+    const size_t e_at = size_t(z) * op.Rpad + r0 + tid;
+    const double m = __longlong_as_double((long long)op.rmax[e_at]);
+    int e = 0;
+    if (m > 0.0) frexp(m, &e);      // every |x| of the row is < 2^e
+    rs[tid] = ldexp(1.0, -e);
+    if (blockIdx.x == 0) op.exps[e_at] = e;
+  }
+  __syncthreads();
+  int8_t* dst = reinterpret_cast<int8_t*>(op.dst);
+  for (int idx = tid; idx < 64 * 32; idx += 256) {
+    const int rr = idx >> 5, kp = (idx & 31) * 2;
+    const long long X0 = ozaki_fixed(tile[rr][kp] * rs[rr], ns);
+    const long long X1 = ozaki_fixed(tile[rr][kp + 1] * rs[rr], ns);
+    for (int k = 1; k <= ns; ++k) {
+      const size_t row = (size_t(z) * ns + k - 1) * op.Rpad + r0 + rr;
+      *reinterpret_cast<char2*>(dst + row * op.Kpad + k0 + kp) =
+          make_char2(char(ozaki_digit(X0, ns, k)), char(ozaki_digit(X1, ns, k)));
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
 constexpr int kOzStages = 6;
 constexpr int kOzTileBytes = 128 * 128;                 // 128 rows x 128 int8 transitions
 constexpr int kOzStageBytes = 2 * kOzTileBytes;
@@ -189,7 +258,10 @@ __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem*
 
   if (tid == 0) {
     // ---- TMA producer
+    const void* tmb = it.tmap_b ? it.tmap_b : it.tmap;
+    const int lob = it.tmap_b ? it.lo_off_b : it.lo_off;
     tc::tmap_acquire(it.tmap);
+    if (it.tmap_b) tc::tmap_acquire(it.tmap_b);
     int issued[kOzStages] = {0, 0, 0, 0, 0, 0};
     bool ok = true;
     int step = 0;
@@ -205,7 +277,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem*
             }
             tc::mbar_arrive_expect_tx(&full[s], kOzStageBytes);
             tc::tma_load_2d(tile(s, 0), it.tmap, &full[s], kt * 128, it.row_a + (i - 1) * it.lo_off);
-            tc::tma_load_2d(tile(s, 1), it.tmap, &full[s], kt * 128, it.row_b + (d - i - 1) * it.lo_off);
+            tc::tma_load_2d(tile(s, 1), tmb, &full[s], kt * 128, it.row_b + (d - i - 1) * lob);
             ++issued[s];
           }
     }
@@ -278,7 +350,7 @@ __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem*
         __syncwarp();
         if (lane == 0) tc::mbar_arrive(&acce[b]);
       }
-    if (ok) {
+    if (ok && it.mrows == 0) {
       const int er = it.ea[row];
       double* dst = it.C + size_t(row) * it.ldc + half * 64;
 #pragma unroll
@@ -288,6 +360,17 @@ __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem*
         if (col - row == it.diag) v0 += 1.0;
         if (col + 1 - row == it.diag) v1 += 1.0;
         *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
+      }
+    } else if (ok) {
+      // edge tile of a general product: rows < mrows, columns < ncols, no identity
+      if (row < it.mrows) {
+        const int er = it.ea[row];
+        double* dst = it.C + size_t(row) * it.ldc;
+#pragma unroll
+        for (int j = 0; j < 64; ++j) {
+          const int col = half * 64 + j;
+          if (col < it.ncols) dst[col] = ldexp(acc[j], er + it.eb[col]);
+        }
       }
     } else if (lane == 0) {
       atomicOr(it.err, kErrTimeout);
@@ -308,6 +391,13 @@ void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cud
 }
 void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
   if (n > 0) ozaki_slice_kernel<<<n, 256, 0, s>>>(probs, items);
+}
+void launch_slice_kmajor(const SliceOp& op, cudaStream_t s) {
+  if (op.Rpad <= 0 || op.Kpad <= 0 || op.nz <= 0) return;
+  cudaMemsetAsync(op.rmax, 0, size_t(op.nz) * op.Rpad * sizeof(unsigned long long), s);
+  const dim3 grid(op.Kpad / 64, op.Rpad / 64, op.nz);
+  slice_rowmax_kernel<<<grid, 256, 0, s>>>(op);
+  slice_kmajor_kernel<<<grid, 256, 0, s>>>(op);
 }
 void launch_syrk_ozaki(const TcItem* items, int n, int ny, cudaStream_t s) {
   if (n > 0 && ny > 0) syrk_ozaki_kernel<<<dim3(n, ny), kOzThreads, kOzSmemBytes, s>>>(items);

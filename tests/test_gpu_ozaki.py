@@ -100,3 +100,27 @@ def test_ozaki_rejects_bad_slice_counts():
         RIGW_OZAKI(2)
     with pytest.raises(ValueError):
         RIGW_OZAKI(8)
+
+
+@pytest.mark.parametrize("nbf,naux,ranges", [(37, 61, [(6, 37, 1, 5), (3, 3, 2, 9)]),
+                                              (300, 700, [(41, 300, 1, 40), (1, 300, 39, 42)])])
+def test_ozaki_aomo_matches_fp64(engine, nbf, naux, ranges):
+    """AO->MO with both products Ozaki-sliced (rows of each operand scaled to their
+    own maximum, s int8 digits, exact INT32 products, FP64 recombination).  The
+    truncation error of one product is about sqrt(nbf) 2^-7s of its largest entry;
+    the bound allows 64 times that, floored at 1e-13, and the error must fall with s."""
+    rng = np.random.default_rng(nbf + 1)
+    pairs = np.array([(k, l) for l in range(1, nbf + 1) for k in range(1, l + 1)])
+    pairs = pairs[rng.random(len(pairs)) > 0.1]
+    eri3 = rng.standard_normal((naux, len(pairs)))
+    c = np.linalg.qr(rng.standard_normal((nbf, nbf)))[0].T.copy()
+    for (m0, m1, n0, n1) in ranges:
+        f64 = engine.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1)
+        scale = np.abs(f64).max()
+        errs = []
+        for s in (3, 5, 7):
+            oz = engine.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1, precision=RIGW_OZAKI(s))
+            err = np.abs(oz - f64).max() / scale
+            assert err <= max(64.0 * np.sqrt(nbf) * 2.0 ** (-7 * s), 1e-13), (s, err)
+            errs.append(err)
+        assert 0.0 < errs[0] and errs[1] < errs[0] and errs[2] <= errs[1]
