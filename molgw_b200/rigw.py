@@ -18,7 +18,7 @@ without the built library, or calling it without a CUDA device, raises.
 from __future__ import annotations
 
 import ctypes as C
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 from pathlib import Path
 
 import numpy as np
@@ -243,12 +243,15 @@ class Engine:
         arrays (all W/Sigma inputs must then be device tensors)."""
         nocc, nvirt = inst.nocc, inst.nvirt
         e = np.ascontiguousarray(inst.energy, dtype=np.float64)
+        # G is built from energy_g (the Sigma sum over p and se_init's efermi); W and
+        # the energy0 of the QP equation from the mean-field energies
+        eg = e if getattr(inst, "energy_g", None) is None else np.ascontiguousarray(inst.energy_g, dtype=np.float64)
         occ = np.ascontiguousarray(inst.occupation, dtype=np.float64)
         nsemin, nsemax = inst.nsemin, inst.nsemax
         host = {
             "e_occ": e[:nocc].copy(), "e_virt": e[nocc:nocc + nvirt].copy(),
             "occ_occ": occ[:nocc].copy(), "occ_virt": occ[nocc:nocc + nvirt].copy(),
-            "e_p": e.copy(), "e_sig": e[nsemin - 1:nsemax].copy(),
+            "e_p": eg.copy(), "e_sig": e[nsemin - 1:nsemax].copy(),
         }
         if inst.m_ia is not None:
             host["m_ia"] = np.ascontiguousarray(inst.m_ia)
@@ -260,7 +263,7 @@ class Engine:
             arrs.update(device_arrays)
             flags = RIGW_PROBLEM_DEVICE_POINTERS
             occ_sig = device_arrays.get("occ_sig", occ_sig)
-        efermi = 0.5 * (e[nocc - 1] + e[nocc])
+        efermi = 0.5 * (eg[nocc - 1] + eg[nocc])
         p = Problem()
         p.naux = inst.naux
         p.nocc, p.nvirt = nocc, nvirt
@@ -357,8 +360,12 @@ class Engine:
                                                        C.byref(w)), "rigw_polarizability_imag")
         return erpa.value, egw.value, WPol(self, w, inst.naux, inst.nomega)
 
-    def gw_selfenergy_imag_scalapack(self, wpol: "WPol", inst) -> np.ndarray:
+    def gw_selfenergy_imag_scalapack(self, wpol: "WPol", inst, omega_calc=None) -> np.ndarray:
         p, keep = self.make_problem(inst)
+        if omega_calc is not None:
+            oc = np.ascontiguousarray(np.stack([omega_calc.real, omega_calc.imag], -1))
+            p.omega_calc = _ptr(oc)
+            keep.append(oc)
         r, bufs = self._alloc_result(p)
         self._check(self._lib.rigw_gw_selfenergy_imag(self._h, wpol.handle, C.byref(p), C.byref(r)),
                     "rigw_gw_selfenergy_imag")
@@ -377,6 +384,49 @@ class Engine:
         out = self._output(r, bufs)
         out.sigma_calc = sigma_calc
         return out
+
+    def gw_imag_force_energy_qp(self, inst, nstep: int = 1, precision: int = RIGW_FP64, workdir=None,
+                                technique: int = RIGW_PADE) -> list[G0W0Output]:
+        """``nstep`` successive imaginary-axis GW runs under force_energy_qp: run k
+        takes the QP energies of run k-1 as the energies in G (the first run: the
+        ENERGY_QP file of ``workdir`` when it reads with status 0, else the mean-field
+        energies), keeps the mean-field energies for W and for the energy0 of the QP
+        equation, and hands on the mean-field energies with the Sigma range replaced
+        by its graphical QP energies (src/m_selfenergy_evaluation.f90:164-181,
+        241-245, 587-611; src/m_selfenergy_tools.f90:358-359).  With ``workdir``
+        every run reads and writes ``workdir/ENERGY_QP`` as the reference does.
+
+        W does not depend on energy_g, so it is factored once and stays resident;
+        each run evaluates Sigma from the resident factors and solves the QP
+        equation.  Each output carries the run's E_RPA and E_GW."""
+        from .energy_qp import read_energy_qp, write_energy_qp
+        ns = inst.nsemin - 1
+        energy = np.asarray(inst.energy, dtype=np.float64)
+        eq = None
+        if workdir is not None:
+            e_read, status = read_energy_qp(workdir, energy.size)
+            eq = e_read[:, 0] if status == 0 else None
+        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        outs = []
+        try:
+            for _ in range(nstep):
+                g = replace(inst, energy_g=energy if eq is None else eq)
+                zc = None
+                if technique == RIGW_HOMOLUMO:   # se_init: real points inside the gap of energy_g
+                    nc = inst.nomega_sigma_calc
+                    eh, el = g.energy_g[inst.nocc - 1], g.energy_g[inst.nocc]
+                    zc = (eh + 0.01 + np.arange(nc) / (nc - 1.0) * (el - eh - 0.02)).astype(np.complex128)
+                sc = self.gw_selfenergy_imag_scalapack(wpol, g, zc)
+                out = self.qp_solve(g, sc, technique, zc)
+                out.erpa, out.egw = erpa, egw
+                outs.append(out)
+                eq = energy.copy()
+                eq[ns:ns + out.energy_qp_g.size] = out.energy_qp_g
+                if workdir is not None:
+                    write_energy_qp(workdir, eq)
+        finally:
+            wpol.release()
+        return outs
 
     def calculate_eri_3center_mo(self, eri3: np.ndarray, index_basis: np.ndarray, c_matrix: np.ndarray,
                                  m_min: int, m_max: int, n_min: int, n_max: int,

@@ -48,6 +48,9 @@ class GWInstance:
     step_sigma: float = 0.025
     eta: float = 0.01
     seed: int = 0
+    # Energies of the states in G (energy_g of selfenergy_evaluation); None: ``energy``.
+    # W and the QP equation keep ``energy`` (src/m_selfenergy_evaluation.f90:164-181).
+    energy_g: np.ndarray | None = None
 
     @property
     def nstate(self) -> int:

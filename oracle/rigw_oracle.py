@@ -531,13 +531,19 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
               step_sigma: float = 0.01, nomega_sigma_calc: int = 50,
               step_sigma_calc: float = 0.075, eta: float = 0.01,
               exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
-              ncore_w: int = 0) -> G0W0Result:
+              ncore_w: int = 0, energy_g: np.ndarray | None = None) -> G0W0Result:
     """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
     (src/m_selfenergy_evaluation.f90:214-246, 587-611).
 
     ``m_ia`` is the W-window tensor ``[nocc_w, nvirt_w, naux]``; ``m_sigma`` is
     ``[nsig, prange, naux]`` with p = ncore_G+1.. nvirtual_G-1.
+
+    ``energy_g`` (default ``energy``) are the energies in G, as read from
+    ENERGY_QP under force_energy_qp (:164-181): se%init and the Sigma sum take
+    them, W (energy_w = energy for GW) and the energy0 of the QP equation
+    (find_qp_energy_*(se, ..., energy, ...), :587-590) keep ``energy``.
     """
+    eg = energy if energy_g is None else energy_g
     occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
     e_occ = energy[ncore_w:ncore_w + m_ia.shape[0]]
     nlumo = ncore_w + m_ia.shape[0]
@@ -545,9 +551,9 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     occ_v = occupation[nlumo:nlumo + m_ia.shape[1]]
     omega, weight = imaginary_quad_grid(nomega_chi_imag)
     sf = polarizability_grid(m_ia, e_occ, e_virt, occ_w, occ_v, omega, weight)
-    se = se_init_imaginary_axis(energy, rng, technique, nomega_sigma, step_sigma,
+    se = se_init_imaginary_axis(eg, rng, technique, nomega_sigma, step_sigma,
                                 nomega_sigma_calc, step_sigma_calc)
-    se.sigma_calc[:] = gw_selfenergy_imag(energy, m_sigma, sf, se.omega_calc, rng.ncore_g + 1)
+    se.sigma_calc[:] = gw_selfenergy_imag(eg, m_sigma, sf, se.omega_calc, rng.ncore_g + 1)
     if technique == "pade":
         se_pade_fit(se, eta)
     else:
