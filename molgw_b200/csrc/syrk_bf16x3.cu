@@ -33,8 +33,9 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
   const WorkItem wi = items[blockIdx.x];
   const ProbDev& p = probs[wi.prob];
   const int p0 = wi.b;
+  constexpr int kWb = 16;            // frequencies per block of scale factors
   __shared__ double tile[64][65];   // [P][t]
-  __shared__ double sc[64];
+  __shared__ double sc[kWb][64];    // sqrt(D_w(t0 + t)) for kWb frequencies
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   __nv_bfloat16* xs = reinterpret_cast<__nv_bfloat16*>(p.xs);
   const int w0 = wi.c, w1 = min(p.nomega, w0 + p.wgroup);   // this item's frequency group
@@ -45,23 +46,28 @@ __global__ void __launch_bounds__(256) split_bf16x3_kernel(const ProbDev* __rest
       const int tt = idx >> 6, pp = idx & 63;
       tile[pp][tt] = p.mp[size_t(t0 + tt) * p.npad + p0 + pp];
     }
-    for (int w = w0; w < w1; ++w) {
-      const int wl = w - w0;
+    // the scale factors of a block of frequencies, then its conversions without barriers
+    for (int wb = w0; wb < w1; wb += kWb) {
+      const int nwb = min(kWb, w1 - wb);
       __syncthreads();
-      if (tid < 64) sc[tid] = sqrt(p.dscale[size_t(w) * p.nia_pad + t0 + tid]);
+      for (int idx = tid; idx < nwb * 64; idx += 256)
+        sc[idx >> 6][idx & 63] = sqrt(p.dscale[size_t(wb + (idx >> 6)) * p.nia_pad + t0 + (idx & 63)]);
       __syncthreads();
-      const double s0 = sc[2 * lane], s1 = sc[2 * lane + 1];
+      for (int w = wb; w < wb + nwb; ++w) {
+        const int wl = w - w0;
+        const double s0 = sc[w - wb][2 * lane], s1 = sc[w - wb][2 * lane + 1];
 #pragma unroll
-      for (int pr = 0; pr < 8; ++pr) {
-        const int pp = warp * 8 + pr;
-        const double v0 = tile[pp][2 * lane] * s0, v1 = tile[pp][2 * lane + 1] * s1;
-        const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
-        const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
-        const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
-        const size_t hi_row = (size_t(2 * wl) * p.npad + p0 + pp) * p.kpad + t0;
-        const size_t lo_row = (size_t(2 * wl + 1) * p.npad + p0 + pp) * p.kpad + t0;
-        reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
-        reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
+        for (int pr = 0; pr < 8; ++pr) {
+          const int pp = warp * 8 + pr;
+          const double v0 = tile[pp][2 * lane] * s0, v1 = tile[pp][2 * lane + 1] * s1;
+          const __nv_bfloat16 h0 = __double2bfloat16(v0), h1 = __double2bfloat16(v1);
+          const __nv_bfloat16 l0 = __double2bfloat16(v0 - double(__bfloat162float(h0)));
+          const __nv_bfloat16 l1 = __double2bfloat16(v1 - double(__bfloat162float(h1)));
+          const size_t hi_row = (size_t(2 * wl) * p.npad + p0 + pp) * p.kpad + t0;
+          const size_t lo_row = (size_t(2 * wl + 1) * p.npad + p0 + pp) * p.kpad + t0;
+          reinterpret_cast<__nv_bfloat162*>(xs + hi_row)[lane] = __halves2bfloat162(h0, h1);
+          reinterpret_cast<__nv_bfloat162*>(xs + lo_row)[lane] = __halves2bfloat162(l0, l1);
+        }
       }
     }
   }
