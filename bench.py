@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=32,
                     help="molecules of the ragged batch measured beside the single instance (0: skip)")
     ap.add_argument("--batch-reps", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep"])
+    ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep", "aomo"])
     ap.add_argument("--sweep-reps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-duration", type=float, default=60.0)
@@ -392,6 +392,72 @@ def run_sweep_line(args):
     print(json.dumps(line), flush=True)
 
 
+def run_aomo_line(args):
+    """`--workload aomo`: the RI AO->MO transform (calculate_eri_3center_mo) through
+    the host-pointer C ABI, FP64, BF16x3 and Ozaki INT8 (4 slices), for the two
+    calls of a G0W0 run: the W window (m = virtual, n = occupied) and the Sigma
+    states (m = all, n = HOMO, LUMO).  Sizes: nbf = Nocc + Nvirt with the 840
+    instance's Nocc=21/Nvirt=207/Naux=840, and nbf=600/Naux=2000 with 50
+    occupied states; B(mu nu, P) ~ N(0,1) over all pairs, C orthonormal.  The
+    device times come from the library's CUDA events: upload + unpack of the AO
+    tensor, the two products (with the operand splits), download.  TFLOP/s use
+    F = Naux (4 npair n + 2 n m nbf), the algorithmic count of the two products.
+    One JSON line."""
+    import torch
+    from molgw_b200 import build
+    build.build()
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64, RIGW_OZAKI, Engine
+    peaks = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    fp64_peak = measured_fp64_peak(torch)
+    eng = Engine(0)
+    cases = []
+    for (nbf, naux, nocc) in ((228, 840, 21), (600, 2000, 50)):
+        rng = np.random.default_rng(nbf)
+        pairs = np.array([(k, l) for l in range(1, nbf + 1) for k in range(1, l + 1)], dtype=np.int32)
+        eri3 = rng.standard_normal((naux, len(pairs)))
+        c = np.linalg.qr(rng.standard_normal((nbf, nbf)))[0].T.copy()
+        for call, (m0, m1, n0, n1) in (("W window", (nocc + 1, nbf, 1, nocc)),
+                                       ("Sigma states", (1, nbf, nocc, nocc + 1))):
+            mc, nc = m1 - m0 + 1, n1 - n0 + 1
+            flops = float(naux) * (4.0 * len(pairs) * nc + 2.0 * nc * mc * nbf)
+            res, ref = {}, None
+            for name, prec, products, peak in (("fp64", RIGW_FP64, 1, fp64_peak),
+                                               ("bf16x3", RIGW_BF16X3, 3, bf16_peak),
+                                               ("ozaki4", RIGW_OZAKI(4), 10, 2.0 * bf16_peak)):
+                eng.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1, precision=prec)
+                walls, stats = [], []
+                for _ in range(3):
+                    t0 = time.perf_counter()
+                    o = eng.calculate_eri_3center_mo(eri3, pairs, c, m0, m1, n0, n1, precision=prec)
+                    walls.append((time.perf_counter() - t0) * 1e3)
+                    stats.append(eng.last_stats())
+                if ref is None:
+                    ref = o
+                best = int(np.argmin([st["stage_ms"][1] for st in stats]))
+                st = stats[best]
+                prod_ms = st["stage_ms"][1]
+                tf = flops / (prod_ms * 1e-3) / 1e12
+                res[name] = {"wall_ms": float(min(walls)), "device_ms": st["total_ms"],
+                             "upload_unpack_ms": st["stage_ms"][0], "products_ms": prod_ms,
+                             "download_ms": st["stage_ms"][2], "products_tflops_algorithmic": tf,
+                             "frac_of_peak": tf * products / peak, "tensor_products": products,
+                             "rel_err_vs_fp64": float(np.abs(o - ref).max() / np.abs(ref).max())}
+            cases.append({"nbf": nbf, "naux": naux, "npair": len(pairs), "call": call, "m": [m0, m1], "n": [n0, n1],
+                          "flops_algorithmic": flops, "precisions": res})
+    eng.close()
+    w = cases[0]["precisions"]["fp64"]
+    line = {"metric": "AO->MO transforms/s", "value": 1e3 / w["wall_ms"], "unit": "transforms/s", "n_gpus": 1,
+            "steps": 3, "warmup": 1, "ms_per_step": w["wall_ms"], "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded PCG64; B ~ N(0,1) over all basis pairs, C orthonormal)",
+            "config": {"workload": "RI AO->MO transform through the host-pointer C ABI (host arrays in and out); "
+                                   "value = the W-window call of the nbf=228/Naux=840 case in FP64",
+                       "fp64_peak_tflops": fp64_peak, "bf16_peak_tflops": bf16_peak},
+            "cases": cases}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the MOLGW path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -441,6 +507,9 @@ def main():
         return
     if args.workload == "serve":
         run_serve_line(args)
+        return
+    if args.workload == "aomo":
+        run_aomo_line(args)
         return
 
     import torch

@@ -92,8 +92,8 @@ typedef struct rigw_problem {
   int nstate_p;              /* p = ncore_G+1 .. nvirtual_G-1                              */
   int nsig;                  /* Sigma states nsemin..nsemax                               */
   const double* m_pm;        /* [nsig][nstate_p][naux] = eri_3center_mo(naux, p, m)        */
-  const double* e_p;         /* [nstate_p] energy(p)                                      */
-  const double* e_sig;       /* [nsig] energy0 of the Sigma states                        */
+  const double* e_p;         /* [nstate_p] energy(p) in G (energy_g under force_energy_qp)  */
+  const double* e_sig;       /* [nsig] energy0 of the QP equation (mean-field energies)   */
   const double* occ_sig;     /* [nsig] occupation of the Sigma states (HOMO/LUMO output)   */
   const double* exchange_m_vxc; /* [nsig] Sigma_x - V_xc; NULL: zero (G0W0@HF)             */
   int technique;             /* rigw_technique                                            */
@@ -103,7 +103,7 @@ typedef struct rigw_problem {
   int nomega_sigma;          /* real grid has 2*(nomega_sigma/2)+1 points                 */
   double step_sigma;
   double eta;
-  double efermi;             /* se_init efermi (mid-gap or mu_origin)                      */
+  double efermi;             /* se_init efermi (mid-gap of the G energies, or mu_origin)   */
   int precision;             /* rigw_precision                                            */
   int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS                               */
 } rigw_problem;
@@ -122,7 +122,10 @@ typedef struct rigw_result {
 } rigw_result;
 
 /* Per-call statistics of the last solve on a context (the device-side analogue of
- * MOLGW's stage timers timer_rpa_dynamic / timer_gw_self, src/m_timing.f90:268-284). */
+ * MOLGW's stage timers timer_rpa_dynamic / timer_gw_self, src/m_timing.f90:268-284).
+ * After rigw_eri_3center_mo*: stage_ms = upload + unpack of the AO tensor, the two
+ * products with their operand splits, download of the result; chunks = auxiliary
+ * chunks (timer_aomo_gw). */
 typedef struct rigw_stats {
   double stage_ms[4];        /* CUDA-event times: input packing, chi0 contraction,
                                 eps factorization + triangular solves, energies + Sigma + QP */

@@ -157,6 +157,24 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   RIGW_TRY(b_out.allocate(&c, size_t(ncp) * mcp * pcp * 8, "aomo out chunk"));
   RIGW_TRY(b_item.allocate(&c, sizeof(AomoUnpackItem), "aomo item"));
   cudaStream_t s = c.stream;
+  // stage times (CUDA events on the stream): AO tensor upload + unpack, the two
+  // products with their operand splits, result download
+  struct Events {
+    cudaEvent_t e[6] = {};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  for (cudaEvent_t& x : ev.e) RIGW_CUDA_TRY(cudaEventCreate(&x));
+  double stage[3] = {0.0, 0.0, 0.0};
+  int launches = 0;
+  auto elapsed = [&](int a, int b) {
+    float ms = 0.0f;
+    cudaEventElapsedTime(&ms, ev.e[a], ev.e[b]);
+    return double(ms);
+  };
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[4], s));
   RIGW_CUDA_TRY(cudaMemcpyAsync(b_ctm.data(), ctm.data(), ctm.size() * 8, cudaMemcpyHostToDevice, s));
   RIGW_CUDA_TRY(cudaMemcpyAsync(b_ctn.data(), ctn.data(), ctn.size() * 8, cudaMemcpyHostToDevice, s));
   RIGW_CUDA_TRY(cudaMemcpyAsync(b_idx.data(), index_basis, size_t(2) * npair * sizeof(int), cudaMemcpyHostToDevice, s));
@@ -189,12 +207,15 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
       RIGW_TRY(split_operand(c, a1, &s_a1, maps));
       RIGW_TRY(split_operand(c, a2, &s_a2, maps + 256));
     }
+    launches += ns > 0 ? 4 : 2;
   }
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[5], s));
   // rows between the first planes of two operand blocks (hi/lo, or the slices)
   const int planes = ns > 0 ? ns : 2;
   const int ktiles = ns > 0 ? Kp / 128 : Kp / 64;
   for (int p0 = 0; p0 < naux; p0 += pc) {
     const int cnt = std::min(pc, naux - p0);
+    RIGW_CUDA_TRY(cudaEventRecord(ev.e[0], s));
     RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), eri3 + size_t(p0) * npair, size_t(cnt) * npair * 8,
                                   cudaMemcpyHostToDevice, s));
     RIGW_CUDA_TRY(cudaMemsetAsync(dfull, 0, size_t(nbf) * nbf * pcp * 8, s));
@@ -204,6 +225,8 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     dim3 grid((npair + 31) / 32, (cnt + 31) / 32);
     aomo_unpack_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const AomoUnpackItem*>(b_item.data()));
     RIGW_CUDA_TRY(cudaGetLastError());
+    RIGW_CUDA_TRY(cudaEventRecord(ev.e[1], s));
+    launches += 1 + (split ? (ns > 0 ? 6 : 4) : 2);
     const int wide = nbf * pcp;
     if (split) {
       // step 1: T[n][j] = sum_nu ctn^T[n][nu] B^T[j][nu],  j = (mu, P)
@@ -313,12 +336,27 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     RIGW_TRY(run_gemm_items(c, g2, true));
     }
     // out[n][m][p0 : p0+cnt]
+    RIGW_CUDA_TRY(cudaEventRecord(ev.e[2], s));
     for (int n = 0; n < nc; ++n)
       RIGW_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t(n) * mc) * naux + p0, size_t(naux) * 8,
                                       dout + size_t(n) * mcp * pcp, size_t(pcp) * 8, size_t(cnt) * 8, mc,
                                       cudaMemcpyDeviceToHost, s));
+    RIGW_CUDA_TRY(cudaEventRecord(ev.e[3], s));
     RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+    stage[0] += elapsed(0, 1);
+    stage[1] += elapsed(1, 2);
+    stage[2] += elapsed(2, 3);
   }
+  stage[1] += elapsed(4, 5);   // C uploads and the splits of the C operands
+  rigw_stats st{};
+  st.stage_ms[0] = stage[0];
+  st.stage_ms[1] = stage[1];
+  st.stage_ms[2] = stage[2];
+  st.total_ms = elapsed(4, 3);
+  st.kernel_launches = launches;
+  st.chunks = (naux + pc - 1) / pc;
+  st.waves = 1;
+  c.last_stats = st;
   return Status::ok();
 }
 
