@@ -73,6 +73,9 @@ enum rigw_technique {
 /* Compute only what the QP energies need: skips the tr eps^-1 solve behind
  * 'GW  correlation energy' (egw is returned as NaN); E_RPA is still computed. */
 #define RIGW_PROBLEM_QP_ONLY 2
+/* Occupations are per spin channel (nspin = 2): output_homolumo then uses
+ * spin_fact = 1 instead of 2.  Implied when the second channel is present. */
+#define RIGW_PROBLEM_SPIN_CHANNEL 4
 
 typedef struct rigw_ctx rigw_ctx;
 typedef struct rigw_wpol rigw_wpol;
@@ -106,6 +109,18 @@ typedef struct rigw_problem {
   double efermi;             /* se_init efermi (mid-gap of the G energies, or mu_origin)   */
   int precision;             /* rigw_precision                                            */
   int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS                               */
+  /* Second spin channel of the W window (nspin = 2; nocc_2 = 0 for a closed shell):
+   * its transitions join those of the first channel in one chi0, as the spin index
+   * of MOLGW's transition table does (src/m_gw_selfenergy_grid.f90:118-149), with
+   * per-spin occupations (1 or 0).  Sigma and the QP equation then run per spin
+   * (rigw_gw_selfenergy_imag + rigw_qp_solve with the resident factors); the fused
+   * rigw_g0w0* calls take the first channel's Sigma states. */
+  int nocc_2, nvirt_2;
+  const double* m_ia_2;      /* [nocc_2][nvirt_2][naux] = eri_3center_mo(naux, a, i, 2)     */
+  const double* e_occ_2;     /* [nocc_2]  energy(i, 2)                                     */
+  const double* e_virt_2;    /* [nvirt_2] energy(a, 2)                                     */
+  const double* occ_occ_2;   /* [nocc_2]  occupation(i, 2)                                 */
+  const double* occ_virt_2;  /* [nvirt_2] occupation(a, 2)                                 */
 } rigw_problem;
 
 /* Outputs of one problem; every array is caller-owned host memory (or device

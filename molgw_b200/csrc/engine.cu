@@ -18,15 +18,17 @@ inline int round_up(int v, int a) { return (v + a - 1) / a * a; }
 
 // ---------------------------------------------------------------------------
 bool Shape::operator<(const Shape& o) const {
-  return std::tie(naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision, qp_only) <
-         std::tie(o.naux, o.nocc, o.nvirt, o.nomega, o.nstate_p, o.nsig, o.nc, o.nsigma_half, o.technique,
-                  o.precision, o.qp_only);
+  return std::tie(naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision, qp_only, nocc2,
+                  nvirt2) < std::tie(o.naux, o.nocc, o.nvirt, o.nomega, o.nstate_p, o.nsig, o.nc, o.nsigma_half,
+                                     o.technique, o.precision, o.qp_only, o.nocc2, o.nvirt2);
 }
 
 Status make_shape(const rigw_problem& p, Shape* sh) {
   if (p.naux <= 0 || p.nocc < 0 || p.nvirt < 0 || p.nomega <= 0)
     return Status::fail(RIGW_ERR_ARG, "invalid W-window sizes naux=%d nocc=%d nvirt=%d nomega=%d", p.naux,
                         p.nocc, p.nvirt, p.nomega);
+  if (p.nocc_2 < 0 || p.nvirt_2 < 0)
+    return Status::fail(RIGW_ERR_ARG, "invalid second spin channel nocc_2=%d nvirt_2=%d", p.nocc_2, p.nvirt_2);
   if (p.nsig < 0 || p.nstate_p < 0)
     return Status::fail(RIGW_ERR_ARG, "invalid Sigma sizes nsig=%d nstate_p=%d", p.nsig, p.nstate_p);
   if (p.nomega_sigma_calc < 0 || p.nomega_sigma_calc > 128)
@@ -38,6 +40,8 @@ Status make_shape(const rigw_problem& p, Shape* sh) {
   sh->naux = p.naux;
   sh->nocc = p.nocc;
   sh->nvirt = p.nvirt;
+  sh->nocc2 = p.nocc_2;
+  sh->nvirt2 = p.nvirt_2;
   sh->nomega = p.nomega;
   sh->nstate_p = p.nstate_p;
   sh->nsig = p.nsig;
@@ -223,7 +227,7 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   Dims d;
   d.npad = round_up(sh.naux, kPanel);
   d.npanel = d.npad / kPanel;
-  d.nia = sh.nocc * sh.nvirt;
+  d.nia = sh.nocc * sh.nvirt + sh.nocc2 * sh.nvirt2;
   // the int8 tensor-core K tile is 128 transitions (128 bytes), the bf16 one 64
   d.nia_pad = round_up(std::max(d.nia, 1), is_ozaki(sh.precision) ? 128 : 64);
   d.want_identity =
@@ -326,11 +330,17 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     PlanProblem& pp = probs_[i];
     pp.sh = sh;
     if (factor) {
-      pp.off_in_m = L.take(size_t(d.nia) * sh.naux * D);
+      pp.off_in_m = L.take(size_t(sh.nocc) * sh.nvirt * sh.naux * D);
       pp.off_in_eocc = L.take(size_t(sh.nocc) * D);
       pp.off_in_evirt = L.take(size_t(sh.nvirt) * D);
       pp.off_in_oocc = L.take(size_t(sh.nocc) * D);
       pp.off_in_ovirt = L.take(size_t(sh.nvirt) * D);
+      const size_t nia2 = size_t(sh.nocc2) * sh.nvirt2;
+      pp.off_in_m2 = L.take(nia2 * sh.naux * D);
+      pp.off_in_eocc2 = L.take(size_t(sh.nocc2) * D);
+      pp.off_in_evirt2 = L.take(size_t(sh.nvirt2) * D);
+      pp.off_in_oocc2 = L.take(size_t(sh.nocc2) * D);
+      pp.off_in_ovirt2 = L.take(size_t(sh.nvirt2) * D);
       pp.off_in_omega = L.take(size_t(sh.nomega) * D);
       pp.off_in_weight = L.take(size_t(sh.nomega) * D);
       off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
@@ -415,6 +425,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     p.npad = d.npad;
     p.nocc = sh.nocc;
     p.nvirt = sh.nvirt;
+    p.nocc2 = sh.nocc2;
+    p.nvirt2 = sh.nvirt2;
+    p.nia1 = sh.nocc * sh.nvirt;
     p.nia = d.nia;
     p.nia_pad = d.nia_pad;
     p.nomega = sh.nomega;
@@ -996,6 +1009,12 @@ Status Plan::stage_inputs(const rigw_problem* probs, cudaStream_t s) {
       RIGW_TRY(bind(q.e_virt, pp.off_in_evirt, sh.nvirt, "e_virt", &p.e_virt));
       RIGW_TRY(bind(q.occ_occ, pp.off_in_oocc, sh.nocc, "occ_occ", &p.occ_occ));
       RIGW_TRY(bind(q.occ_virt, pp.off_in_ovirt, sh.nvirt, "occ_virt", &p.occ_virt));
+      const size_t nia2 = size_t(sh.nocc2) * sh.nvirt2;
+      RIGW_TRY(bind(q.m_ia_2, pp.off_in_m2, nia2 * sh.naux, "m_ia_2", &p.m_in2));
+      RIGW_TRY(bind(q.e_occ_2, pp.off_in_eocc2, sh.nocc2, "e_occ_2", &p.e_occ2));
+      RIGW_TRY(bind(q.e_virt_2, pp.off_in_evirt2, sh.nvirt2, "e_virt_2", &p.e_virt2));
+      RIGW_TRY(bind(q.occ_occ_2, pp.off_in_oocc2, sh.nocc2, "occ_occ_2", &p.occ_occ2));
+      RIGW_TRY(bind(q.occ_virt_2, pp.off_in_ovirt2, sh.nvirt2, "occ_virt_2", &p.occ_virt2));
     }
     if (sigma) {
       RIGW_TRY(bind(q.m_pm, pp.off_in_msig, size_t(sh.nsig) * sh.nstate_p * sh.naux, "m_pm", &p.msig_in));
@@ -1113,6 +1132,7 @@ Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStre
     double* en = nullptr;      // [2]
     double* q = nullptr;       // [4 nsig]
     double* occ = nullptr;     // [nsig]
+    double spin_fact = 2.0;    // occupation of a full state
     double* sc = nullptr;      // sigma_calc staged for a host destination
     double* sr = nullptr;      // sigma (real grid) staged for a host destination
   };
@@ -1153,6 +1173,7 @@ Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStre
       h[i].q = take(4 * size_t(p.nsig));
       h[i].occ = take(p.nsig);
       std::fill(h[i].occ, h[i].occ + p.nsig, 0.0);
+      h[i].spin_fact = ((probs[i].flags & RIGW_PROBLEM_SPIN_CHANNEL) || probs[i].nocc_2 > 0) ? 1.0 : 2.0;
       RIGW_CUDA_TRY(cudaMemcpyAsync(h[i].q, p.qp, 4 * p.nsig * sizeof(double), cudaMemcpyDeviceToHost, s));
       if (probs[i].occ_sig) {
         if (is_dev(probs[i].occ_sig))
@@ -1192,9 +1213,9 @@ Status Plan::fetch_results(const rigw_problem* probs, rigw_result* res, cudaStre
         g[k] = h[i].q[4 * k];
         z[k] = h[i].q[4 * k + 1];
         zz[k] = h[i].q[4 * k + 2];
-        // output_homolumo, src/m_hamiltonian_tools.f90:564-612 (spin_fact = 2)
-        if (h[i].occ[k] / 2.0 > 1.0e-5) eh = std::max(eh, g[k]);
-        if (h[i].occ[k] / 2.0 < 1.0 - 1.0e-5) el = std::min(el, g[k]);
+        // output_homolumo, src/m_hamiltonian_tools.f90:564-612 (spin_fact 2, or 1 per spin channel)
+        if (h[i].occ[k] / h[i].spin_fact > 1.0e-5) eh = std::max(eh, g[k]);
+        if (h[i].occ[k] / h[i].spin_fact < 1.0 - 1.0e-5) el = std::min(el, g[k]);
       }
       r.ehomo = eh;
       r.elumo = el;

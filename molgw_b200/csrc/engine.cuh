@@ -78,6 +78,7 @@ inline int ozaki_slices(int precision) { return is_ozaki(precision) ? precision 
 struct Shape {
   int naux, nocc, nvirt, nomega, nstate_p, nsig, nc, nsigma_half, technique, precision;
   int qp_only;
+  int nocc2 = 0, nvirt2 = 0;   // second spin channel of the W window
   bool operator<(const Shape& o) const;
 };
 
@@ -106,6 +107,7 @@ struct PlanProblem {
   Shape sh;
   ProbDev dev;                 // device descriptor (input pointers patched per call)
   size_t off_in_m = 0, off_in_eocc = 0, off_in_evirt = 0, off_in_oocc = 0, off_in_ovirt = 0;
+  size_t off_in_m2 = 0, off_in_eocc2 = 0, off_in_evirt2 = 0, off_in_oocc2 = 0, off_in_ovirt2 = 0;
   size_t off_in_omega = 0, off_in_weight = 0, off_in_msig = 0, off_in_ep = 0, off_in_esig = 0;
   size_t off_in_xc = 0, off_in_zcalc = 0, off_out = 0, off_sigma_in = 0;
 };

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(256) pack_m_kernel(const ProbDev* __restrict__
   if (t >= p.nia_pad) return;
   double sq = 0.0;
   if (t < p.nia) {
-    const double* src = p.m_in + size_t(t) * p.naux;
+    const double* src = t < p.nia1 ? p.m_in + size_t(t) * p.naux : p.m_in2 + size_t(t - p.nia1) * p.naux;
     double* dst = p.mp + size_t(t) * p.npad;
     for (int q = lane; q < p.npad; q += 32) {
       const double v = q < p.naux ? src[q] : 0.0;
@@ -72,10 +72,14 @@ __global__ void __launch_bounds__(256) pack_m_kernel(const ProbDev* __restrict__
   sq = warp_sum(sq);
   if (lane == 0) p.tnorm[t] = sq;
   double dcoef = 0.0, de = 0.0;
-  if (t < p.nia) {
+  if (t < p.nia1) {
     const int i = t / p.nvirt, a = t % p.nvirt;
     de = p.e_virt[a] - p.e_occ[i];
     dcoef = 2.0 * (p.occ_occ[i] - p.occ_virt[a]) * de;
+  } else if (t < p.nia) {          // second spin channel
+    const int i = (t - p.nia1) / p.nvirt2, a = (t - p.nia1) % p.nvirt2;
+    de = p.e_virt2[a] - p.e_occ2[i];
+    dcoef = 2.0 * (p.occ_occ2[i] - p.occ_virt2[a]) * de;
   }
   for (int w = lane; w < p.nomega; w += 32) {
     const double om = p.omega[w];

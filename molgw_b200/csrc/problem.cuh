@@ -36,6 +36,13 @@ struct ProbDev {
   const double* e_virt;      // [nvirt]
   const double* occ_occ;     // [nocc]
   const double* occ_virt;    // [nvirt]
+  // second spin channel: transitions nia1 .. nia-1 (nocc2 x nvirt2, a fastest)
+  int nocc2, nvirt2, nia1;
+  const double* m_in2;       // [nocc2*nvirt2][naux]
+  const double* e_occ2;      // [nocc2]
+  const double* e_virt2;     // [nvirt2]
+  const double* occ_occ2;    // [nocc2]
+  const double* occ_virt2;   // [nvirt2]
   const double* omega;       // [nomega] imaginary parts
   const double* weight;      // [nomega]
   const double* msig_in;     // [nsig*nstate_p][naux]

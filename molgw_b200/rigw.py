@@ -41,6 +41,7 @@ RIGW_PADE = 0
 RIGW_HOMOLUMO = 1
 RIGW_PROBLEM_DEVICE_POINTERS = 1
 RIGW_PROBLEM_QP_ONLY = 2
+RIGW_PROBLEM_SPIN_CHANNEL = 4
 STATUS_NAMES = {0: "OK", 1: "ERR_ARG", 2: "ERR_CUDA", 3: "ERR_NOMEM", 4: "ERR_NOT_SPD", 5: "ERR_NUMERIC",
                 6: "ERR_TIMEOUT", 7: "ERR_UNSUPPORTED"}
 
@@ -63,7 +64,21 @@ class Problem(C.Structure):
         ("technique", C.c_int), ("nomega_sigma_calc", C.c_int), ("step_sigma_calc", C.c_double),
         ("omega_calc", _dp), ("nomega_sigma", C.c_int), ("step_sigma", C.c_double), ("eta", C.c_double),
         ("efermi", C.c_double), ("precision", C.c_int), ("flags", C.c_int),
+        ("nocc_2", C.c_int), ("nvirt_2", C.c_int), ("m_ia_2", _dp), ("e_occ_2", _dp), ("e_virt_2", _dp),
+        ("occ_occ_2", _dp), ("occ_virt_2", _dp),
     ]
+
+
+def efermi_of(inst) -> float:
+    """se_init's efermi from the energies in G: half-way between the highest
+    energy of state nhomo_G and the lowest of state nhomo_G + 1 over the spin
+    channels, nhomo_G the highest state occupied in any channel
+    (src/m_selfenergy_tools.f90:584-585)."""
+    chans = [inst] + ([inst.spin2] if getattr(inst, "spin2", None) is not None else [])
+    eg = [np.asarray(c.energy if getattr(c, "energy_g", None) is None else c.energy_g, dtype=np.float64)
+          for c in chans]
+    nhomo = max(c.nocc for c in chans)
+    return 0.5 * (max(e[nhomo - 1] for e in eg) + min(e[nhomo] for e in eg))
 
 
 class Result(C.Structure):
@@ -236,7 +251,8 @@ class Engine:
 
     # ---------------------------------------------------------------- problems
     def make_problem(self, inst, precision: int = RIGW_FP64, device_arrays: dict | None = None,
-                     technique: int = RIGW_PADE, qp_only: bool = False) -> tuple[Problem, list]:
+                     technique: int = RIGW_PADE, qp_only: bool = False,
+                     efermi: float | None = None) -> tuple[Problem, list]:
         """Problem descriptor for a ``molgw_b200.synth.GWInstance``-like object.
 
         ``device_arrays`` maps field names to CUDA tensors that replace the host
@@ -263,7 +279,8 @@ class Engine:
             arrs.update(device_arrays)
             flags = RIGW_PROBLEM_DEVICE_POINTERS
             occ_sig = device_arrays.get("occ_sig", occ_sig)
-        efermi = 0.5 * (eg[nocc - 1] + eg[nocc])
+        if efermi is None:
+            efermi = efermi_of(inst)
         p = Problem()
         p.naux = inst.naux
         p.nocc, p.nvirt = nocc, nvirt
@@ -282,7 +299,23 @@ class Engine:
         p.efermi = efermi
         p.precision = precision
         p.flags = flags | (RIGW_PROBLEM_QP_ONLY if qp_only else 0)
+        if getattr(inst, "spin_channel", False) or getattr(inst, "spin2", None) is not None:
+            p.flags |= RIGW_PROBLEM_SPIN_CHANNEL
         keep = [arrs, occ_sig]
+        s2 = getattr(inst, "spin2", None)
+        if s2 is not None:
+            # second spin channel of the W window (its own energies and occupations)
+            e2 = np.ascontiguousarray(s2.energy, dtype=np.float64)
+            o2 = np.ascontiguousarray(s2.occupation, dtype=np.float64)
+            w2 = {"m_ia_2": np.ascontiguousarray(s2.m_ia), "e_occ_2": e2[:s2.nocc].copy(),
+                  "e_virt_2": e2[s2.nocc:s2.nocc + s2.nvirt].copy(), "occ_occ_2": o2[:s2.nocc].copy(),
+                  "occ_virt_2": o2[s2.nocc:s2.nocc + s2.nvirt].copy()}
+            if device_arrays:
+                w2.update({k: v for k, v in device_arrays.items() if k.endswith("_2")})
+            p.nocc_2, p.nvirt_2 = s2.nocc, s2.nvirt
+            for k, v in w2.items():
+                setattr(p, k, _ptr(v))
+            keep.append(w2)
         return p, keep
 
     def _alloc_result(self, p: Problem):
@@ -360,8 +393,8 @@ class Engine:
                                                        C.byref(w)), "rigw_polarizability_imag")
         return erpa.value, egw.value, WPol(self, w, inst.naux, inst.nomega)
 
-    def gw_selfenergy_imag_scalapack(self, wpol: "WPol", inst, omega_calc=None) -> np.ndarray:
-        p, keep = self.make_problem(inst)
+    def gw_selfenergy_imag_scalapack(self, wpol: "WPol", inst, omega_calc=None, efermi=None) -> np.ndarray:
+        p, keep = self.make_problem(inst, efermi=efermi)
         if omega_calc is not None:
             oc = np.ascontiguousarray(np.stack([omega_calc.real, omega_calc.imag], -1))
             p.omega_calc = _ptr(oc)
@@ -372,8 +405,9 @@ class Engine:
         sc = bufs["sigma_calc"]
         return sc[..., 0] + 1j * sc[..., 1]
 
-    def qp_solve(self, inst, sigma_calc: np.ndarray, technique: int = RIGW_PADE, omega_calc=None) -> G0W0Output:
-        p, keep = self.make_problem(inst, technique=technique)
+    def qp_solve(self, inst, sigma_calc: np.ndarray, technique: int = RIGW_PADE, omega_calc=None,
+                 efermi=None) -> G0W0Output:
+        p, keep = self.make_problem(inst, technique=technique, efermi=efermi)
         if omega_calc is not None:
             oc = np.ascontiguousarray(np.stack([omega_calc.real, omega_calc.imag], -1))
             p.omega_calc = _ptr(oc)
@@ -384,6 +418,35 @@ class Engine:
         out = self._output(r, bufs)
         out.sigma_calc = sigma_calc
         return out
+
+    def g0w0_spin(self, inst, precision: int = RIGW_FP64, technique: int = RIGW_PADE) -> list[G0W0Output]:
+        """Open-shell (nspin = 2) G0W0 on the imaginary axis: one W from the
+        transitions of both spin channels (``inst`` and ``inst.spin2``), then Sigma
+        and the QP equation per channel with the factors resident, on the
+        evaluation points of the common efermi (src/m_gw_selfenergy_grid.f90:118-149,
+        279-319; src/m_selfenergy_tools.f90:584-585).  Returns one output per
+        channel, each carrying E_RPA and E_GW of the whole W."""
+        if getattr(inst, "spin2", None) is None:
+            raise ValueError("g0w0_spin needs inst.spin2 (the second spin channel)")
+        ef = efermi_of(inst)
+        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        outs = []
+        try:
+            for ch in (replace(inst, spin2=None, spin_channel=True), replace(inst.spin2, spin_channel=True)):
+                zc = None
+                if technique == RIGW_HOMOLUMO:   # se_init: real points inside the gap, over both channels
+                    nc = ch.nomega_sigma_calc
+                    nh = max(inst.nocc, inst.spin2.nocc)
+                    eh = max(inst.energy[nh - 1], inst.spin2.energy[nh - 1])
+                    el = min(inst.energy[nh], inst.spin2.energy[nh])
+                    zc = (eh + 0.01 + np.arange(nc) / (nc - 1.0) * (el - eh - 0.02)).astype(np.complex128)
+                sc = self.gw_selfenergy_imag_scalapack(wpol, ch, zc, efermi=ef)
+                out = self.qp_solve(ch, sc, technique, zc, efermi=ef)
+                out.erpa, out.egw = erpa, egw
+                outs.append(out)
+        finally:
+            wpol.release()
+        return outs
 
     def gw_imag_force_energy_qp(self, inst, nstep: int = 1, precision: int = RIGW_FP64, workdir=None,
                                 technique: int = RIGW_PADE) -> list[G0W0Output]:

@@ -51,6 +51,10 @@ class GWInstance:
     # Energies of the states in G (energy_g of selfenergy_evaluation); None: ``energy``.
     # W and the QP equation keep ``energy`` (src/m_selfenergy_evaluation.f90:164-181).
     energy_g: np.ndarray | None = None
+    # Second spin channel (nspin = 2): its own window, energies, occupations (1 or 0)
+    # and M tensors over the same states and auxiliary basis; None: closed shell.
+    spin2: "GWInstance | None" = None
+    spin_channel: bool = False        # occupations per spin channel (1 or 0), not 2 or 0
 
     @property
     def nstate(self) -> int:

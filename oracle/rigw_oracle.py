@@ -186,7 +186,7 @@ class SpectralFunction:
 def polarizability_grid(m_ia: np.ndarray, e_occ: np.ndarray, e_virt: np.ndarray,
                         occ_occ: np.ndarray, occ_virt: np.ndarray,
                         omega: np.ndarray, weight: np.ndarray, keep_chi: bool = True,
-                        keep_eigval: bool = False) -> SpectralFunction:
+                        keep_eigval: bool = False, spin2: tuple | None = None) -> SpectralFunction:
     """RPA polarizability on the imaginary grid, src/m_gw_selfenergy_grid.f90:33-209.
 
     ``m_ia`` is ``[nocc, nvirt, naux]`` (transition t = (i, a), a fastest, as the
@@ -195,11 +195,20 @@ def polarizability_grid(m_ia: np.ndarray, e_occ: np.ndarray, e_virt: np.ndarray,
     symmetrize lower->upper (src/m_scalapack.f90:2461-2551 serial branch), 1-chi0,
     DSYEV('N') eigenvalues -> E_RPA, E_GW (:171-173), DGETRF/DGETRI inverse
     (src/m_linear_algebra.f90:179-205), DGEMM chi = (1-chi0)^-1 chi0 (:179-188).
+
+    ``spin2`` = (m_ia, e_occ, e_virt, occ_occ, occ_virt) of the second spin channel:
+    its transitions follow those of the first, as the spin index of the transition
+    table orders them (src/m_spectral_function.f90:239-266), in the same DSYRK.
     """
     nocc, nvirt, naux = m_ia.shape
     docc = (occ_occ[:, None] - occ_virt[None, :]).reshape(-1)
     de = (e_virt[None, :] - e_occ[:, None]).reshape(-1)
     m_t = np.ascontiguousarray(m_ia.reshape(nocc * nvirt, naux).T)   # eri3(naux, t), Fortran order
+    if spin2 is not None:
+        m2, eo2, ev2, oo2, ov2 = spin2
+        docc = np.concatenate([docc, (oo2[:, None] - ov2[None, :]).reshape(-1)])
+        de = np.concatenate([de, (ev2[None, :] - eo2[:, None]).reshape(-1)])
+        m_t = np.ascontiguousarray(np.concatenate([m_t, m2.reshape(-1, naux).T], axis=1))
     sf = SpectralFunction(omega=omega.copy(), weight_quad=weight.copy())
     if keep_chi:
         sf.chi = np.zeros((len(omega), naux, naux))
@@ -315,9 +324,11 @@ def fermi_level(energy0: np.ndarray, nhomo_g: int, mu_origin: float = -100.0) ->
 def se_init_imaginary_axis(energy0: np.ndarray, rng: StateRange, technique: str = "pade",
                            nomega_sigma: int = 51, step_sigma: float = 0.01,
                            nomega_sigma_calc: int = 1, step_sigma_calc: float = 0.03,
-                           mu_origin: float = -100.0) -> SelfEnergyGrid:
-    """se_init for imaginary_axis_pade / imaginary_axis_homolumo, :557-699."""
-    efermi = fermi_level(energy0, rng.nhomo_g, mu_origin)
+                           mu_origin: float = -100.0, efermi: float | None = None) -> SelfEnergyGrid:
+    """se_init for imaginary_axis_pade / imaginary_axis_homolumo, :557-699.
+    ``efermi``: the value over both spin channels (nspin = 2), else from energy0."""
+    if efermi is None:
+        efermi = fermi_level(energy0, rng.nhomo_g, mu_origin)
     nom = nomega_sigma // 2
     omega = efermi + step_sigma * np.arange(-nom, nom + 1, dtype=np.float64)
     if technique == "pade":
@@ -567,3 +578,56 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     ehomo, elumo = output_homolumo(occupation, full, rng.nsemin, rng.nsemax)
     return G0W0Result(sf.erpa, sf.egw, se.sigma_calc.copy(), se.sigma.copy(), eqp_g, eqp_z, zz_g,
                       ehomo, elumo, rng.nsemin, rng.nsemax)
+
+
+def fermi_level_spin(energy0_spins: list, nhomo_g: int) -> float:
+    """efermi of se_init over spin channels, src/m_selfenergy_tools.f90:584-585:
+    0.5 (max over spins of energy0(nhomo_G) + min over spins of energy0(nhomo_G+1))."""
+    return 0.5 * (max(e[nhomo_g - 1] for e in energy0_spins) + min(e[nhomo_g] for e in energy0_spins))
+
+
+def g0w0_imag_spin(channels: list, nomega_chi_imag: int, nomega_sigma: int = 51, step_sigma: float = 0.01,
+                   nomega_sigma_calc: int = 50, step_sigma_calc: float = 0.075, eta: float = 0.01,
+                   technique: str = "pade") -> list:
+    """Open-shell (nspin = 2) selfenergy_evaluation for imaginary_axis_pade /
+    _homolumo: one W from the transitions of both channels
+    (src/m_gw_selfenergy_grid.f90:118-149), Sigma per spin (:279-319), the QP
+    equation per spin, se_init's efermi over both spins.
+
+    ``channels``: two dicts with energy, occupation (1 or 0), m_ia [nocc, nvirt,
+    naux], m_sigma [nsig, nstate, naux], nsemin, nsemax (1-based).  Returns one
+    G0W0Result per channel (E_RPA and E_GW of the whole W in each)."""
+    c1, c2 = channels
+    no1, no2 = c1["m_ia"].shape[0], c2["m_ia"].shape[0]
+    omega, weight = imaginary_quad_grid(nomega_chi_imag)
+    blk = lambda c, no: (c["m_ia"], c["energy"][:no], c["energy"][no:no + c["m_ia"].shape[1]],
+                         c["occupation"][:no], c["occupation"][no:no + c["m_ia"].shape[1]])
+    sf = polarizability_grid(*blk(c1, no1), omega, weight, spin2=blk(c2, no2))
+    nhomo = max(no1, no2)
+    efermi = fermi_level_spin([c1["energy"], c2["energy"]], nhomo)
+    out = []
+    for c in channels:
+        nstate = c["energy"].size
+        rng = StateRange(0, nstate + 1, nhomo, nhomo + 1, c["nsemin"], c["nsemax"])
+        se = se_init_imaginary_axis(c["energy"], rng, technique, nomega_sigma, step_sigma, nomega_sigma_calc,
+                                    step_sigma_calc, efermi=efermi)
+        if technique == "homolumo":
+            eh = max(ch["energy"][nhomo - 1] for ch in channels)
+            el = min(ch["energy"][nhomo] for ch in channels)
+            se.omega_calc = (eh + 0.01 + np.arange(nomega_sigma_calc) / (nomega_sigma_calc - 1.0)
+                             * (el - eh - 0.02)).astype(np.complex128)
+        se.sigma_calc[:] = gw_selfenergy_imag(c["energy"], c["m_sigma"], sf, se.omega_calc, 1)
+        if technique == "pade":
+            se_pade_fit(se, eta)
+        else:
+            self_energy_polynomial(se)
+        e0 = c["energy"][c["nsemin"] - 1: c["nsemax"]]
+        xc = np.zeros_like(e0)
+        eqp_z, zz = find_qp_energy_linearization(se, xc, e0)
+        eqp_g, zz_g, _, _ = find_qp_energy_graphical(se, xc, e0)
+        full = c["energy"].copy()
+        full[c["nsemin"] - 1: c["nsemax"]] = eqp_g
+        ehomo, elumo = output_homolumo(c["occupation"], full, c["nsemin"], c["nsemax"], spin_fact=1.0)
+        out.append(G0W0Result(sf.erpa, sf.egw, se.sigma_calc.copy(), se.sigma.copy(), eqp_g, eqp_z, zz_g,
+                              ehomo, elumo, c["nsemin"], c["nsemax"]))
+    return out

@@ -1,0 +1,35 @@
+"""Open-shell (nspin = 2) restatement in the oracle: one chi0 over the transitions
+of both spin channels (src/m_gw_selfenergy_grid.f90:118-149), Sigma and the QP
+equation per channel (:279-319), se_init's efermi over both channels
+(src/m_selfenergy_tools.f90:584-585)."""
+import numpy as np
+
+from molgw_b200 import synth
+from oracle import rigw_oracle as o
+from tests.spin_cases import as_two_channels, open_shell_instance, oracle_channels
+
+
+def test_two_identical_channels_reproduce_the_closed_shell():
+    # 16 frequencies: an 8-frequency Pade fit amplifies 1e-14 changes of Sigma to 1e-3 meV
+    inst = synth.make_instance(9, 80, 200, 16, seed=42)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    kw = dict(nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma, nomega_sigma_calc=inst.nomega_sigma_calc,
+              step_sigma_calc=inst.step_sigma_calc, eta=inst.eta)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng, **kw)
+    for r in o.g0w0_imag_spin(oracle_channels(as_two_channels(inst)), inst.nomega, **kw):
+        assert abs(r.erpa - ref.erpa) <= 1e-12 * abs(ref.erpa)
+        assert abs(r.egw - ref.egw) <= 1e-12 * abs(ref.egw)
+        assert np.abs(r.sigma_calc - ref.sigma_calc).max() <= 1e-12 * np.abs(ref.sigma_calc).max()
+        assert np.abs(r.energy_qp_g - ref.energy_qp_g).max() <= 1e-9
+        assert abs(r.ehomo - ref.ehomo) <= 1e-9 and abs(r.elumo - ref.elumo) <= 1e-9
+
+
+def test_spin_polarized_instance_runs():
+    inst = open_shell_instance()
+    out = o.g0w0_imag_spin(oracle_channels(inst), inst.nomega, nomega_sigma=inst.nomega_sigma,
+                           step_sigma=inst.step_sigma, nomega_sigma_calc=inst.nomega_sigma_calc,
+                           step_sigma_calc=inst.step_sigma_calc, eta=inst.eta)
+    assert len(out) == 2 and out[0].erpa == out[1].erpa and out[0].erpa < 0.0
+    for r in out:
+        assert np.all(np.isfinite(r.energy_qp_g)) and r.ehomo < r.elumo
