@@ -77,7 +77,7 @@ def efermi_of(inst) -> float:
     chans = [inst] + ([inst.spin2] if getattr(inst, "spin2", None) is not None else [])
     eg = [np.asarray(c.energy if getattr(c, "energy_g", None) is None else c.energy_g, dtype=np.float64)
           for c in chans]
-    nhomo = max(c.nocc for c in chans)
+    nhomo = max(getattr(c, "ncore_w", 0) + c.nocc for c in chans)
     return 0.5 * (max(e[nhomo - 1] for e in eg) + min(e[nhomo] for e in eg))
 
 
@@ -264,10 +264,11 @@ class Engine:
         eg = e if getattr(inst, "energy_g", None) is None else np.ascontiguousarray(inst.energy_g, dtype=np.float64)
         occ = np.ascontiguousarray(inst.occupation, dtype=np.float64)
         nsemin, nsemax = inst.nsemin, inst.nsemax
+        cw, cg = getattr(inst, "ncore_w", 0), getattr(inst, "ncore_g", 0)   # frozen core of W and of G
         host = {
-            "e_occ": e[:nocc].copy(), "e_virt": e[nocc:nocc + nvirt].copy(),
-            "occ_occ": occ[:nocc].copy(), "occ_virt": occ[nocc:nocc + nvirt].copy(),
-            "e_p": eg.copy(), "e_sig": e[nsemin - 1:nsemax].copy(),
+            "e_occ": e[cw:cw + nocc].copy(), "e_virt": e[cw + nocc:cw + nocc + nvirt].copy(),
+            "occ_occ": occ[cw:cw + nocc].copy(), "occ_virt": occ[cw + nocc:cw + nocc + nvirt].copy(),
+            "e_p": eg[cg:].copy(), "e_sig": e[nsemin - 1:nsemax].copy(),
         }
         if inst.m_ia is not None:
             host["m_ia"] = np.ascontiguousarray(inst.m_ia)
@@ -288,7 +289,7 @@ class Engine:
         for k in ("m_ia", "e_occ", "e_virt", "occ_occ", "occ_virt", "m_pm", "e_p", "e_sig"):
             setattr(p, k, _ptr(arrs[k]))
         p.occ_sig = _ptr(occ_sig)
-        p.nstate_p = e.shape[0]
+        p.nstate_p = e.shape[0] - cg
         p.nsig = nsemax - nsemin + 1
         p.technique = technique
         p.nomega_sigma_calc = inst.nomega_sigma_calc
@@ -307,9 +308,11 @@ class Engine:
             # second spin channel of the W window (its own energies and occupations)
             e2 = np.ascontiguousarray(s2.energy, dtype=np.float64)
             o2 = np.ascontiguousarray(s2.occupation, dtype=np.float64)
-            w2 = {"m_ia_2": np.ascontiguousarray(s2.m_ia), "e_occ_2": e2[:s2.nocc].copy(),
-                  "e_virt_2": e2[s2.nocc:s2.nocc + s2.nvirt].copy(), "occ_occ_2": o2[:s2.nocc].copy(),
-                  "occ_virt_2": o2[s2.nocc:s2.nocc + s2.nvirt].copy()}
+            c2 = s2.ncore_w
+            w2 = {"m_ia_2": np.ascontiguousarray(s2.m_ia), "e_occ_2": e2[c2:c2 + s2.nocc].copy(),
+                  "e_virt_2": e2[c2 + s2.nocc:c2 + s2.nocc + s2.nvirt].copy(),
+                  "occ_occ_2": o2[c2:c2 + s2.nocc].copy(),
+                  "occ_virt_2": o2[c2 + s2.nocc:c2 + s2.nocc + s2.nvirt].copy()}
             if device_arrays:
                 w2.update({k: v for k, v in device_arrays.items() if k.endswith("_2")})
             p.nocc_2, p.nvirt_2 = s2.nocc, s2.nvirt
@@ -436,7 +439,7 @@ class Engine:
                 zc = None
                 if technique == RIGW_HOMOLUMO:   # se_init: real points inside the gap, over both channels
                     nc = ch.nomega_sigma_calc
-                    nh = max(inst.nocc, inst.spin2.nocc)
+                    nh = max(inst.ncore_w + inst.nocc, inst.spin2.ncore_w + inst.spin2.nocc)
                     eh = max(inst.energy[nh - 1], inst.spin2.energy[nh - 1])
                     el = min(inst.energy[nh], inst.spin2.energy[nh])
                     zc = (eh + 0.01 + np.arange(nc) / (nc - 1.0) * (el - eh - 0.02)).astype(np.complex128)
@@ -477,7 +480,8 @@ class Engine:
                 zc = None
                 if technique == RIGW_HOMOLUMO:   # se_init: real points inside the gap of energy_g
                     nc = inst.nomega_sigma_calc
-                    eh, el = g.energy_g[inst.nocc - 1], g.energy_g[inst.nocc]
+                    nh = inst.ncore_w + inst.nocc
+                    eh, el = g.energy_g[nh - 1], g.energy_g[nh]
                     zc = (eh + 0.01 + np.arange(nc) / (nc - 1.0) * (el - eh - 0.02)).astype(np.complex128)
                 sc = self.gw_selfenergy_imag_scalapack(wpol, g, zc)
                 out = self.qp_solve(g, sc, technique, zc)

@@ -55,6 +55,11 @@ class GWInstance:
     # and M tensors over the same states and auxiliary basis; None: closed shell.
     spin2: "GWInstance | None" = None
     spin_channel: bool = False        # occupations per spin channel (1 or 0), not 2 or 0
+    # Frozen core (MOLGW's ncorew / ncoreg): the W window starts at state ncore_w + 1
+    # (m_ia covers occupied states ncore_w+1 .. ncore_w+nocc), the states p of Sigma
+    # at ncore_g + 1 (m_sigma is [nsig, nstate - ncore_g, naux]).
+    ncore_w: int = 0
+    ncore_g: int = 0
 
     @property
     def nstate(self) -> int:

@@ -1,0 +1,34 @@
+"""Frozen core (MOLGW's ncorew / ncoreg): the W window and the states p of Sigma
+start above the core, src/m_selfenergy_tools.f90:67-122 and
+src/m_gw_selfenergy_grid.f90:92-93, 270-290.  The engine takes the windows as the
+Fortran passes them; checked against the oracle with the same windows."""
+from dataclasses import replace
+
+import numpy as np
+import pytest
+
+from molgw_b200 import synth
+from molgw_b200.rigw import RIGW_FP64
+from oracle import rigw_oracle as o
+from tests.conftest import HA_EV
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("ncore", [1, 3])
+def test_frozen_core_matches_oracle(engine, ncore):
+    full = synth.make_instance(9, 80, 200, 16, seed=42)
+    inst = replace(full, nocc=full.nocc - ncore, m_ia=np.ascontiguousarray(full.m_ia[ncore:]),
+                   m_sigma=np.ascontiguousarray(full.m_sigma[:, ncore:]), ncore_w=ncore, ncore_g=ncore)
+    out = engine.g0w0(inst, RIGW_FP64)
+    rng = o.selfenergy_set_state_range(full.nstate, full.occupation, ncoreg=ncore, selfenergy_state_min=full.nsemin,
+                                       selfenergy_state_max=full.nsemax)
+    ref = o.g0w0_imag(full.energy, full.occupation, inst.m_ia, inst.m_sigma, full.nomega, rng,
+                      nomega_sigma=full.nomega_sigma, step_sigma=full.step_sigma,
+                      nomega_sigma_calc=full.nomega_sigma_calc, step_sigma_calc=full.step_sigma_calc, eta=full.eta,
+                      ncore_w=ncore)
+    assert abs(out.erpa - ref.erpa) <= 1e-10 * abs(ref.erpa)
+    assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
+    assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
+    # freezing changes the answer (the core transitions and core states in G are gone)
+    assert abs(out.erpa - engine.g0w0(full, RIGW_FP64).erpa) > 1e-8
