@@ -274,6 +274,8 @@ class Engine:
             host["m_ia"] = np.ascontiguousarray(inst.m_ia)
             host["m_pm"] = np.ascontiguousarray(inst.m_sigma)
         occ_sig = occ[nsemin - 1:nsemax].copy()
+        if getattr(inst, "exchange_m_vxc", None) is not None:
+            host["exchange_m_vxc"] = np.ascontiguousarray(inst.exchange_m_vxc, dtype=np.float64)
         arrs = dict(host)
         flags = 0
         if device_arrays:
@@ -289,6 +291,8 @@ class Engine:
         for k in ("m_ia", "e_occ", "e_virt", "occ_occ", "occ_virt", "m_pm", "e_p", "e_sig"):
             setattr(p, k, _ptr(arrs[k]))
         p.occ_sig = _ptr(occ_sig)
+        if "exchange_m_vxc" in arrs:
+            p.exchange_m_vxc = _ptr(arrs["exchange_m_vxc"])
         p.nstate_p = e.shape[0] - cg
         p.nsig = nsemax - nsemin + 1
         p.technique = technique

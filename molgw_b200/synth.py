@@ -60,6 +60,9 @@ class GWInstance:
     # at ncore_g + 1 (m_sigma is [nsig, nstate - ncore_g, naux]).
     ncore_w: int = 0
     ncore_g: int = 0
+    # Sigma_x - V_xc of the Sigma states (setup_exchange_m_vxc diagonal, [nsig] Ha);
+    # None: zero (G0W0@HF)
+    exchange_m_vxc: np.ndarray | None = None
 
     @property
     def nstate(self) -> int:

@@ -1,7 +1,7 @@
-"""Frozen core (MOLGW's ncorew / ncoreg): the W window and the states p of Sigma
-start above the core, src/m_selfenergy_tools.f90:67-122 and
-src/m_gw_selfenergy_grid.f90:92-93, 270-290.  The engine takes the windows as the
-Fortran passes them; checked against the oracle with the same windows."""
+"""Frozen core (MOLGW's ncorew / ncoreg) and Sigma_x - V_xc on the GPU against the
+oracle.  Frozen core: the W window and the states p of Sigma start above the core
+(src/m_selfenergy_tools.f90:67-122, src/m_gw_selfenergy_grid.f90:92-93, 270-290);
+the engine takes the windows as the Fortran passes them."""
 from dataclasses import replace
 
 import numpy as np
@@ -32,3 +32,20 @@ def test_frozen_core_matches_oracle(engine, ncore):
     assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
     # freezing changes the answer (the core transitions and core states in G are gone)
     assert abs(out.erpa - engine.g0w0(full, RIGW_FP64).erpa) > 1e-8
+
+
+def test_exchange_minus_vxc_matches_oracle(engine):
+    """Sigma_x - V_xc of the Sigma states (a DFT starting point): enters the QP
+    equation only (src/m_selfenergy_tools.f90:202-363)."""
+    inst = synth.make_instance(9, 80, 200, 16, seed=42)
+    xc = np.array([-0.085, 0.043])
+    out = engine.g0w0(replace(inst, exchange_m_vxc=xc), RIGW_FP64)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng,
+                      nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma,
+                      nomega_sigma_calc=inst.nomega_sigma_calc, step_sigma_calc=inst.step_sigma_calc, eta=inst.eta,
+                      exchange_m_vxc=xc)
+    assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
+    assert np.abs(out.energy_qp_z - ref.energy_qp_z).max() * HA_EV <= 1e-6
+    assert np.abs(out.energy_qp_g - engine.g0w0(inst, RIGW_FP64).energy_qp_g).max() > 1e-3
