@@ -180,12 +180,15 @@ __device__ __noinline__ void diag_block_factor(double* S, double* wdt, int j0, d
 #pragma unroll
   for (int j = 0; j < kDiagPb; ++j) {
     const double d = __shfl_sync(0xffffffffu, col[j], j);
+    // row j of the block, A(j,i) held by lane i: every shuffle is issued before the
+    // updates, so that their latencies overlap instead of pairing with each update
+    double aj[kDiagPb];
+#pragma unroll
+    for (int i = j + 1; i < kDiagPb; ++i) aj[i] = __shfl_sync(0xffffffffu, col[j], i);
     const double xj = ((lane == j) ? 1.0 : col[j]) * __drcp_rn(d);   // multiplier row j
 #pragma unroll
-    for (int i = j + 1; i < kDiagPb; ++i) {
-      const double aji = __shfl_sync(0xffffffffu, col[j], i);          // A(j,i), held by lane i
-      if (lane >= i || lane <= j) col[i] -= aji * xj;
-    }
+    for (int i = j + 1; i < kDiagPb; ++i)
+      if (lane >= i || lane <= j) col[i] -= aj[i] * xj;
     if (lane == j) myd = d;
   }
   const double r = 1.0 / sqrt(myd);
