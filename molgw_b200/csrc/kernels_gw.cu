@@ -220,10 +220,18 @@ __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* 
   double* invd = piv + kPanel;                       // [kPanel] 1/U(i,i) = W(i,i)
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int g = lane >> 2, q = lane & 3;
-#pragma unroll 8
+  // the block: asynchronous 16-byte copies of whole rows (all in flight at once),
+  // then zeros below the diagonal
+  for (int c = t; c < kPanel * kPanel / 2; c += kDiagThreads) {
+    const int i = c / (kPanel / 2), l = (c % (kPanel / 2)) * 2;
+    cp_async16(S + i * kDiagLd + l, A + size_t(i) * ld + l, 16);
+  }
+  cp_async_commit();
+  cp_async_wait<0>();
+  __syncthreads();
   for (int idx = t; idx < kPanel * kPanel; idx += kDiagThreads) {
     const int i = idx / kPanel, l = idx % kPanel;
-    S[i * kDiagLd + l] = (l >= i) ? A[size_t(i) * ld + l] : 0.0;
+    if (l < i) S[i * kDiagLd + l] = 0.0;
   }
   __syncthreads();
 
