@@ -1061,6 +1061,12 @@ Status Plan::stage_sigma_calc(int i, const double* sc, cudaStream_t s) {
   return Status::ok();
 }
 
+// NVTX labels of the four stages (the reference's timer names)
+static const char* const kStageRange[4] = {"Response function chi on grid: packing",
+                                           "Response function chi on grid: chi0",
+                                           "Response function chi on grid: eps factorization and solves",
+                                           "GW self-energy"};
+
 Status Plan::launch(cudaStream_t s) {
   RIGW_CUDA_TRY(cudaMemsetAsync(err_dev_, 0, sizeof(int), s));
   // the first launch of a plan goes straight to the streams; a plan launched
@@ -1087,6 +1093,7 @@ Status Plan::launch(cudaStream_t s) {
           std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_cap).count();
     }
     for (int st = 0; st < 4; ++st) {
+      NvtxRange range(kStageRange[st]);
       RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[st], s));
       if (stage_exec_[st]) RIGW_CUDA_TRY(cudaGraphLaunch(stage_exec_[st], s));
     }
@@ -1095,6 +1102,7 @@ Status Plan::launch(cudaStream_t s) {
   } else {
     replayed_ = false;
     for (int st = 0; st < 4; ++st) {
+      NvtxRange range(kStageRange[st]);
       RIGW_CUDA_TRY(cudaEventRecord(stage_ev_[st], s));
       record(s, st);
       RIGW_CUDA_TRY(cudaGetLastError());

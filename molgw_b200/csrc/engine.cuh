@@ -12,9 +12,20 @@
 #include <vector>
 
 #include "../../include/rigw.h"
+#include <nvtx3/nvToolsExt.h>
 #include "kernels.cuh"
 
 namespace rigw {
+
+// NVTX range named like the reference's stage timers (src/m_timing.f90:268-284);
+// a no-op unless a profiler is attached.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
+
 
 struct Status {
   int code = RIGW_OK;

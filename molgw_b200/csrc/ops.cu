@@ -122,6 +122,7 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
                       int nstate_min, int nstate_max, double* out, int precision) {
   if (nbf <= 0 || nstate <= 0 || npair <= 0 || naux <= 0 || !index_basis || !eri3 || !c_matrix || !out)
     return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: invalid arguments");
+  NvtxRange range("3-center AO to MO transform");
   if (precision != RIGW_FP64 && precision != RIGW_BF16X3 && !is_ozaki(precision))
     return Status::fail(RIGW_ERR_UNSUPPORTED, "eri_3center_mo: precision %d (FP64, BF16X3 or OZAKI(3..7))",
                         precision);
