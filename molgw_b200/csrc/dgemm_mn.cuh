@@ -16,6 +16,9 @@ namespace rigw {
 enum GemmFlags : int {
   kAddIdentity = 1,   // C += 1 where (col - row) == diag
   kSubIdentity = 2,   // C -= 1 where (col - row) == diag
+  kUpperA = 4,        // A[k][m] = 0 for k > m, with m counted from the item's first row (the
+                      // triangular inverse of the panel solves): the warps of rows
+                      // m < wm0 + 64 skip the MMAs of k >= wm0 + 64, which add exact zeros
 };
 
 struct GemmItem {
@@ -78,6 +81,7 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
   const int wn0 = wn * 32;
   const int ktiles = (it.k + BK - 1) / BK;
   const bool has_scale = it.kscale != nullptr;
+  const int klim = (it.flags & kUpperA) ? min(it.k, wm0 + 64) : it.k;   // warp-uniform
 
   auto stage_a = [&](int s) { return smem + s * Cfg::kStageDoubles; };
   auto stage_b = [&](int s) { return smem + s * Cfg::kStageDoubles + BK * Cfg::kLdaS; };
@@ -146,6 +150,7 @@ dgemm_mn_kernel(const GemmItem* __restrict__ items) {
       cp_async_commit();
     }
     const int s = kt % ST;
+    if (kt * BK >= klim) continue;   // this warp's rows see only zeros of A from here on
     const double* as = stage_a(s) + wm0 + 8 * q;
     const double* bs = stage_b(s) + wn0 + q;
     const double* ks = stage_k(s);

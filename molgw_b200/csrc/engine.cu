@@ -656,6 +656,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.n = n;
           g.k = kPanel;
           g.alpha = 1.0;
+          g.flags = kUpperA;   // W = U^-1 of the diagonal block is upper triangular
           g.nw = nw;
           g.sA = sW;
           g.sB = g.sC = (X == E) ? sE : sR;
