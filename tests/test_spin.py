@@ -33,3 +33,21 @@ def test_spin_polarized_instance_runs():
     assert len(out) == 2 and out[0].erpa == out[1].erpa and out[0].erpa < 0.0
     for r in out:
         assert np.all(np.isfinite(r.energy_qp_g)) and r.ehomo < r.elumo
+
+
+def test_host_efermi_rule():
+    """molgw_b200.rigw.efermi_of follows se_init (src/m_selfenergy_tools.f90:584-585):
+    half-way between the highest energy of state nhomo_G and the lowest of state
+    nhomo_G + 1 over the spin channels, from the energies in G."""
+    from dataclasses import replace
+    from molgw_b200.rigw import efermi_of
+    inst = synth.make_instance(4, 30, 70, 8, seed=41)
+    e = inst.energy
+    assert efermi_of(inst) == 0.5 * (e[3] + e[4])
+    fc = replace(inst, nocc=3, m_ia=inst.m_ia[1:], ncore_w=1, ncore_g=1)     # frozen core keeps nhomo_G
+    assert efermi_of(fc) == efermi_of(inst)
+    eg = e + 0.01
+    assert efermi_of(replace(inst, energy_g=eg)) == 0.5 * (eg[3] + eg[4])
+    two = open_shell_instance()
+    e1, e2 = two.energy, two.spin2.energy
+    assert efermi_of(two) == 0.5 * (max(e1[4], e2[4]) + min(e1[5], e2[5]))
