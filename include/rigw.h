@@ -80,7 +80,8 @@ enum rigw_technique {
 typedef struct rigw_ctx rigw_ctx;
 typedef struct rigw_wpol rigw_wpol;
 
-/* One closed-shell (nspin = 1) G0W0 problem on the imaginary axis. */
+/* One G0W0 problem on the imaginary axis: closed shell (nspin = 1), or the W
+ * window of an open-shell system with its second spin channel below (nspin = 2). */
 typedef struct rigw_problem {
   int naux;                  /* auxiliary functions kept (nauxil_global)                  */
   int nocc, nvirt;           /* W window: occupied ncore_W+1..nhomo_W, virtual nlumo_W..nvirtual_W-1 */

@@ -1,7 +1,8 @@
 """Seeded synthetic RI-GW instances with the shapes and value distributions of the
 benchmark workloads (no public dataset exists for this path).
 
-One instance is a closed-shell (nspin=1) G0W0@HF problem on the imaginary axis:
+One instance is a closed-shell (nspin=1) G0W0@HF problem on the imaginary axis (an
+open-shell one carries its second spin channel in ``spin2``):
 
 * occupied energies ~ U[-30, -8] eV, virtual energies ~ U[0.5, 40] eV, sorted,
   stored in Hartree (eV / 27.21138505, src/m_definitions.f90:43);

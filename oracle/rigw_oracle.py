@@ -509,7 +509,8 @@ def find_qp_energy_graphical(se: SelfEnergyGrid, exchange_m_vxc: np.ndarray, ene
 
 def output_homolumo(occupation: np.ndarray, energy: np.ndarray, istate_min: int, istate_max: int,
                     spin_fact: float = 2.0):
-    """HOMO/LUMO over a state range, src/m_hamiltonian_tools.f90:564-612 (nspin=1)."""
+    """HOMO/LUMO over a state range for one spin channel, src/m_hamiltonian_tools.f90:564-612
+    (spin_fact 2 for nspin = 1, 1 for a channel of nspin = 2)."""
     ehomo, elumo = -np.inf, np.inf
     for s in range(istate_min, istate_max + 1):
         if occupation[s - 1] / spin_fact > COMPLETELY_EMPTY:
