@@ -457,7 +457,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         p.rmax = reinterpret_cast<unsigned long long*>(base + off[i].rmax);
         p.xexp = reinterpret_cast<int*>(base + off[i].xexp);
         alignas(64) unsigned char map[128];
-        RIGW_TRY(make_ozaki_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * p.slices * d.npad));
+        RIGW_TRY(make_ozaki_tmap(map, p.xs, d.nia_pad, (long long)p.wgroup * p.slices * d.npad,
+                                 p.slices <= kOzaFusedMaxSlices ? 64 : 128));
         RIGW_CUDA_TRY(cudaMemcpyAsync(base + off[i].tmap, map, sizeof(map), cudaMemcpyHostToDevice, ctx->stream));
       }
       p.tnorm = dp(off[i].tnorm);
@@ -561,6 +562,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           if (int(wl_slice_.size()) <= g) {
             wl_slice_.resize(g + 1);
             tl_ozaki_.resize(g + 1);
+            tl_ozaki4_.resize(g + 1);
           }
           for (int t0 = 0; t0 < p.nia_pad; t0 += p.split_t)
             for (int p0 = 0; p0 < npad; p0 += 64) wl_slice_[g].push_back({i, t0, p0, w0});
@@ -575,7 +577,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
               t.row_a = ti;
               t.row_b = tj;
               t.lo_off = npad;
-              t.ktiles = p.kpad / 128;
+              const bool fused = p.slices <= kOzaFusedMaxSlices;
+              t.ktiles = p.kpad / (fused ? 64 : 128);
               t.ldc = npad;
               t.diag = ti - tj;
               t.ea = p.xexp + size_t(w0) * npad + ti;
@@ -585,7 +588,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
               t.sC = (long long)npad * npad;
               t.srow = p.slices * npad;
               t.se = npad;
-              tl_ozaki_[w0 / p.wgroup].push_back(t);
+              (fused ? tl_ozaki4_ : tl_ozaki_)[w0 / p.wgroup].push_back(t);
             }
       }
       if (sh.precision == RIGW_FP64) {
@@ -737,6 +740,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   };
   for (auto& l : tl_syrk_) std::stable_sort(l.begin(), l.end(), by_cost);
   for (auto& l : tl_ozaki_) std::stable_sort(l.begin(), l.end(), by_cost);
+  for (auto& l : tl_ozaki4_) std::stable_sort(l.begin(), l.end(), by_cost);
 
   // ---- upload the lists and the launch sequence
   size_t lbytes = 0;
@@ -762,7 +766,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     int ny = 1;
     if (kind == 1 || kind == 5 || kind == 6 || kind == 14)
       for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const GemmItem*>(src)[j].nw);
-    if (kind == 13 || kind == 20)
+    if (kind == 13 || kind == 20 || kind == 21)
       for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const TcItem*>(src)[j].nw);
     pend.push_back({kind, src, elem * n, int(n), arg, stream, wait_ev, rec_ev, ny});
     return true;
@@ -780,6 +784,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   for (size_t g = 0; g < wl_slice_.size(); ++g) {
     add(19, wl_slice_[g].data(), sizeof(WorkItem), wl_slice_[g].size(), 0);
     add(20, tl_ozaki_[g].data(), sizeof(TcItem), tl_ozaki_[g].size(), 0);
+    add(21, tl_ozaki4_[g].data(), sizeof(TcItem), tl_ozaki4_[g].size(), 0);
   }
   add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
@@ -857,7 +862,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: case 12: case 13: case 15: case 16: case 17: case 18: case 19: case 20: return 1;
+    case 1: case 12: case 13: case 15: case 16: case 17: case 18: case 19: case 20: case 21: return 1;
     case -1: case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
@@ -893,6 +898,7 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 18: launch_ozaki_rowmax(probs_dev_, wl, L.count, s); break;
       case 19: launch_ozaki_slice(probs_dev_, wl, L.count, s); break;
       case 20: launch_syrk_ozaki(reinterpret_cast<const TcItem*>(lb + L.off), L.count, L.ny, s); break;
+      case 21: launch_syrk_ozaki_fused(reinterpret_cast<const TcItem*>(lb + L.off), L.count, L.ny, s); break;
       case 2: init_rhs_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 3: mnorm_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 4: chol_diag_kernel<<<L.count, kDiagThreads, chol_diag_smem_bytes(), s>>>(probs_dev_, wl, L.arg); break;

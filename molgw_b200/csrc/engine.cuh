@@ -169,7 +169,7 @@ class Plan {
   std::vector<std::vector<TcItem>> tl_syrk_;
   std::vector<WorkItem> wl_ozzero_, wl_rowmax_;    // Ozaki: row maxima over every frequency
   std::vector<std::vector<WorkItem>> wl_slice_;   // Ozaki: per frequency group
-  std::vector<std::vector<TcItem>> tl_ozaki_;
+  std::vector<std::vector<TcItem>> tl_ozaki_, tl_ozaki4_;   // s >= 5 / s <= 4 (fused slice pairs)
   std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_, gl_k3a_;
   std::vector<WorkItem> wl_trace_, wl_pad_;
   struct Launch {
@@ -276,6 +276,7 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
 Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* rep);
 size_t available_bytes(Context& c);
 Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
-Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows);
+// box_bytes 128: 128-byte swizzle (syrk_ozaki_kernel); 64: 64-byte swizzle (syrk_ozaki_fused_kernel)
+Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows, int box_bytes = 128);
 
 }  // namespace rigw

@@ -91,6 +91,9 @@ void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaS
 void launch_ozaki_rowmax(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_ozaki_slice(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s);
 void launch_syrk_ozaki(const TcItem* items, int n, int ny, cudaStream_t s);
+// s <= 4: every slice pair of a k-tile from one stage (64-byte swizzled tensor map)
+void launch_syrk_ozaki_fused(const TcItem* items, int n, int ny, cudaStream_t s);
+constexpr int kOzaFusedMaxSlices = 4;
 cudaError_t prepare_ozaki_kernels();
 cudaError_t prepare_tc_kernels();
 

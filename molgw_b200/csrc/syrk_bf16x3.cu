@@ -274,17 +274,19 @@ bool bf16x3_available() {
   return true;
 }
 
-// Row-major [rows][kpad] tensor read in boxes of 128 rows x 128 bytes, 128-byte swizzle.
+// Row-major [rows][kpad] tensor read in boxes of 128 rows x box_bytes (128: 128-byte
+// swizzle; 64: 64-byte swizzle).
 static Status make_kmajor_tmap(void* host_map, CUtensorMapDataType type, int esize, const void* base, int kpad,
-                               long long rows) {
+                               long long rows, int box_bytes = 128) {
   if (!bf16x3_available()) return Status::fail(RIGW_ERR_UNSUPPORTED, "cuTensorMapEncodeTiled unavailable");
   CUtensorMap* m = reinterpret_cast<CUtensorMap*>(host_map);
   cuuint64_t dims[2] = {cuuint64_t(kpad), cuuint64_t(rows)};
   cuuint64_t strides[1] = {cuuint64_t(kpad) * esize};
-  cuuint32_t box[2] = {cuuint32_t(128 / esize), 128};
+  cuuint32_t box[2] = {cuuint32_t(box_bytes / esize), 128};
   cuuint32_t estr[2] = {1, 1};
   CUresult r = g_encode(m, type, 2, const_cast<void*>(base), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
-                        CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        box_bytes == 64 ? CU_TENSOR_MAP_SWIZZLE_64B : CU_TENSOR_MAP_SWIZZLE_128B,
+                        CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
   if (r != CUDA_SUCCESS) return Status::fail(RIGW_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", int(r));
   return Status::ok();
@@ -294,8 +296,8 @@ Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows)
   return make_kmajor_tmap(host_map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, xs, kpad, rows);
 }
 
-Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows) {
-  return make_kmajor_tmap(host_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, xq, kpad, rows);
+Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows, int box_bytes) {
+  return make_kmajor_tmap(host_map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 1, xq, kpad, rows, box_bytes);
 }
 
 void launch_split_bf16x3(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {

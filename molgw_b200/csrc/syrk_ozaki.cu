@@ -382,6 +382,171 @@ __global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_kernel(const TcItem*
 }
 
 // ---------------------------------------------------------------------------
+// Ozaki chi0 for s <= 4 slices: every slice pair of a k-tile from one stage.
+//
+// A stage holds the s A-slice and s B-slice tiles of one k-tile of 64 transitions
+// (128 rows x 64 int8 each, 64-byte swizzle, 8 KB), so each tile loaded feeds all
+// the pair products it appears in: for s = 4, 20 MMAs (M=128 N=128 K=32) per 64 KB
+// staged, against 4 MMAs per 32 KB when one pair is staged at a time.  Level d =
+// i+j accumulates in its own TMEM accumulator (d-2: columns 128(d-2)..), exact in
+// INT32 over chunks of kOzfChunk k-tiles (4096 transitions: |L_d| <= 4 * 4096 *
+// 127^2 < 2^31); after a chunk the eight drain warps add the s levels into FP64
+// with weight 2^-7d, and the MMA warp waits for that before the next chunk (the s
+// accumulators fill TMEM, so there is no second set).
+constexpr int kOzfMaxSlices = 4;
+constexpr int kOzfTileBytes = 128 * 64;                            // 128 rows x 64 int8
+constexpr int kOzfStageBytes = 2 * kOzfMaxSlices * kOzfTileBytes;  // 64 KB
+constexpr int kOzfStages = 3;
+constexpr size_t kOzfSmemBytes = size_t(kOzfStages) * kOzfStageBytes + 1024 + 256;
+constexpr int kOzfChunk = 64;                                      // k-tiles per exact INT32 accumulation
+
+__global__ void __launch_bounds__(kOzThreads, 1) syrk_ozaki_fused_kernel(const TcItem* __restrict__ items) {
+  TcItem it = items[blockIdx.x];
+  const int jw = blockIdx.y;
+  if (jw >= (it.nw > 0 ? it.nw : 1)) return;   // the whole CTA, before any barrier or TMEM use
+  it.C += jw * it.sC;
+  it.row_a += jw * it.srow;
+  it.row_b += jw * it.srow;
+  if (it.ea) {
+    it.ea += jw * it.se;
+    it.eb += jw * it.se;
+  }
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  uint64_t* full = reinterpret_cast<uint64_t*>(smem + kOzfStages * kOzfStageBytes);
+  uint64_t* empty = full + kOzfStages;
+  uint64_t* accf = empty + kOzfStages;    // chunk accumulated (all levels)
+  uint64_t* acce = accf + 1;              // chunk drained
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(acce + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int ns = it.slices;               // 3 or 4
+  // tile (s, 0, i) = A slice i + 1, tile (s, 1, j) = B slice j + 1
+  auto tile = [&](int st, int which, int sl) {
+    return smem + st * kOzfStageBytes + (which * kOzfMaxSlices + sl) * kOzfTileBytes;
+  };
+
+  if (tid == 0) {
+    for (int st = 0; st < kOzfStages; ++st) {
+      tc::mbar_init(&full[st], 1);
+      tc::mbar_init(&empty[st], 1);
+    }
+    tc::mbar_init(accf, 1);
+    tc::mbar_init(acce, 8);
+    tc::fence_mbar_init();
+  }
+  if (warp == 0) tc::tmem_alloc(tslot, 128 * kOzAcc);
+  __syncthreads();
+  tc::tc_fence_after();
+  const uint32_t tmem = *tslot;
+  const int nk = it.ktiles;
+  const int nchunks = (nk + kOzfChunk - 1) / kOzfChunk;
+
+  if (tid == 0) {
+    // ---- TMA producer: the 2 ns slice tiles of each k-tile
+    tc::tmap_acquire(it.tmap);
+    int issued[kOzfStages] = {0, 0, 0};
+    bool ok = true;
+    const uint32_t bytes = uint32_t(2 * ns * kOzfTileBytes);
+    for (int kt = 0; kt < nk && ok; ++kt) {
+      const int st = kt % kOzfStages;
+      if (kt >= kOzfStages && !tc::mbar_wait(&empty[st], ((kt / kOzfStages) - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      tc::mbar_arrive_expect_tx(&full[st], bytes);
+      for (int sl = 0; sl < ns; ++sl) {
+        tc::tma_load_2d(tile(st, 0, sl), it.tmap, &full[st], kt * 64, it.row_a + sl * it.lo_off);
+        tc::tma_load_2d(tile(st, 1, sl), it.tmap, &full[st], kt * 64, it.row_b + sl * it.lo_off);
+      }
+      ++issued[st];
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+    for (int st = 0; st < kOzfStages; ++st)
+      if (issued[st] > 0 && !tc::mbar_wait(&full[st], (issued[st] - 1) & 1)) atomicOr(it.err, kErrTimeout);
+  } else if (tid == 32) {
+    // ---- MMA issuer: per k-tile every pair (i, j) with i + j <= ns + 1 into level i + j
+    constexpr uint32_t idesc = tc::idesc_s8_s32(128, 128);
+    bool ok = true;
+    for (int kt = 0; kt < nk && ok; ++kt) {
+      const int c = kt / kOzfChunk;
+      const bool chunk_first = (kt % kOzfChunk) == 0;
+      if (chunk_first && c >= 1 && !tc::mbar_wait(acce, (c - 1) & 1)) {
+        ok = false;
+        break;
+      }
+      const int st = kt % kOzfStages;
+      if (!tc::mbar_wait(&full[st], (kt / kOzfStages) & 1)) {
+        ok = false;
+        break;
+      }
+      tc::tc_fence_after();
+      for (int d = 2; d <= ns + 1; ++d) {
+        const uint32_t dt = tmem + uint32_t((d - 2) * 128);
+        bool first = chunk_first;
+        for (int i = max(1, d - ns); i <= min(ns, d - 1); ++i) {
+          const uint64_t ad = tc::desc_kmajor_sw64(tile(st, 0, i - 1));
+          const uint64_t bd = tc::desc_kmajor_sw64(tile(st, 1, d - i - 1));
+#pragma unroll
+          for (int sub = 0; sub < 2; ++sub) {
+            const uint64_t o = uint64_t(sub * 2);   // 32 int8 = 32 bytes along K
+            tc::mma_s8(dt, ad + o, bd + o, idesc, (first && sub == 0) ? 0u : 1u);
+          }
+          first = false;
+        }
+      }
+      tc::mma_commit(&empty[st]);
+      if ((kt % kOzfChunk) == kOzfChunk - 1 || kt == nk - 1) tc::mma_commit(accf);
+    }
+    if (!ok) atomicOr(it.err, kErrTimeout);
+  } else if (warp >= 2) {
+    // ---- drain: after each chunk, every level into FP64 with weight 2^-7d
+    const int quad = warp & 3;                 // TMEM lanes 32*quad .. 32*quad+31 (rows)
+    const int half = (warp - 2) >> 2;          // columns 64*half .. 64*half+63
+    const int row = quad * 32 + lane;
+    double acc[64];
+#pragma unroll
+    for (int j = 0; j < 64; ++j) acc[j] = 0.0;
+    bool ok = true;
+    for (int c = 0; c < nchunks && ok; ++c) {
+      ok = __all_sync(0xffffffffu, tc::mbar_wait(accf, c & 1));
+      if (!ok) break;
+      tc::tc_fence_after();
+      for (int d = 2; d <= ns + 1; ++d) {
+        const double wd = ldexp(1.0, -7 * d);
+        const uint32_t base = tmem + uint32_t((d - 2) * 128 + half * 64) + (uint32_t(quad * 32) << 16);
+        uint32_t r[32];
+        tc::tmem_ld_32x32(base, r);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[j] += double(int(r[j])) * wd;
+        tc::tmem_ld_32x32(base + 32, r);
+#pragma unroll
+        for (int j = 0; j < 32; ++j) acc[32 + j] += double(int(r[j])) * wd;
+      }
+      tc::tc_fence_before();
+      __syncwarp();
+      if (lane == 0) tc::mbar_arrive(acce);
+    }
+    if (ok) {
+      const int er = it.ea[row];
+      double* dst = it.C + size_t(row) * it.ldc + half * 64;
+#pragma unroll
+      for (int j = 0; j < 64; j += 2) {
+        const int col = half * 64 + j;
+        double v0 = ldexp(acc[j], er + it.eb[col]), v1 = ldexp(acc[j + 1], er + it.eb[col + 1]);
+        if (col - row == it.diag) v0 += 1.0;
+        if (col + 1 - row == it.diag) v1 += 1.0;
+        *reinterpret_cast<double2*>(dst + j) = make_double2(v0, v1);
+      }
+    } else if (lane == 0) {
+      atomicOr(it.err, kErrTimeout);
+    }
+  }
+  tc::tc_fence_before();
+  __syncthreads();
+  if (warp == 0) tc::tmem_dealloc(tmem, 128 * kOzAcc);
+}
+
+// ---------------------------------------------------------------------------
 // Host side
 void launch_ozaki_zero(const ProbDev* probs, const WorkItem* items, int n, cudaStream_t s) {
   if (n > 0) ozaki_zero_kernel<<<n, 256, 0, s>>>(probs, items);
@@ -399,12 +564,19 @@ void launch_slice_kmajor(const SliceOp& op, cudaStream_t s) {
   slice_rowmax_kernel<<<grid, 256, 0, s>>>(op);
   slice_kmajor_kernel<<<grid, 256, 0, s>>>(op);
 }
+void launch_syrk_ozaki_fused(const TcItem* items, int n, int ny, cudaStream_t s) {
+  if (n > 0 && ny > 0) syrk_ozaki_fused_kernel<<<dim3(n, ny), kOzThreads, kOzfSmemBytes, s>>>(items);
+}
 void launch_syrk_ozaki(const TcItem* items, int n, int ny, cudaStream_t s) {
   if (n > 0 && ny > 0) syrk_ozaki_kernel<<<dim3(n, ny), kOzThreads, kOzSmemBytes, s>>>(items);
 }
 
 cudaError_t prepare_ozaki_kernels() {
-  return cudaFuncSetAttribute(syrk_ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kOzSmemBytes));
+  cudaError_t e =
+      cudaFuncSetAttribute(syrk_ozaki_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kOzSmemBytes));
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(syrk_ozaki_fused_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              int(kOzfSmemBytes));
 }
 
 }  // namespace rigw

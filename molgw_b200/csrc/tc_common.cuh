@@ -127,6 +127,19 @@ RIGW_DEVICE_INLINE uint64_t desc_kmajor_sw128(const void* smem) {
   return d;
 }
 
+// The same for rows of 64 bytes written with 64-byte swizzling (8-row atoms of
+// 512 bytes).
+RIGW_DEVICE_INLINE uint64_t desc_kmajor_sw64(const void* smem) {
+  const uint64_t addr = smem_u32(smem);
+  uint64_t d = 0;
+  d |= (addr >> 4) & 0x3FFFull;            // start address
+  d |= uint64_t(1) << 16;                  // leading byte offset (unused for swizzled K-major)
+  d |= uint64_t(512 >> 4) << 32;           // stride byte offset: 8 rows x 64 B
+  d |= uint64_t(1) << 46;                  // descriptor version (sm_100)
+  d |= uint64_t(4) << 61;                  // SWIZZLE_64B
+  return d;
+}
+
 // Instruction descriptor, kind::i8: signed 8-bit A/B (K-major), s32 D, shape M x N.
 constexpr uint32_t idesc_s8_s32(int M, int N) {
   return (2u << 4) | (1u << 7) | (1u << 10) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
