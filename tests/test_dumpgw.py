@@ -67,3 +67,22 @@ def test_dumped_problem_on_the_gpu_matches_the_oracle(tmp_path, engine):
     assert abs(out.erpa - ref.erpa) < 1e-10 * max(1.0, abs(ref.erpa))
     assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() < 1e-9 * np.abs(ref.sigma_calc).max()
     assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV < 1e-6
+
+
+def test_open_shell_dump_round_trip(tmp_path):
+    """nspin = 2: v.bin holds both spins, energies.dat spin 1; the second channel's
+    occupied count and energies come from the caller."""
+    n, naux = 21, 27
+    v = np.stack([_vertex(n, naux, 5), _vertex(n, naux, 6)])
+    e1 = _energies(n, 5)
+    e2 = np.sort(e1 + np.random.default_rng(7).normal(0.0, 0.01, n))
+    dumpgw.write_dump_gw(tmp_path, e1, v)
+    inst = dumpgw.read_dump_gw(tmp_path, 5, nomega=8, nocc_2=4, energy_2=e2)
+    assert inst.spin2 is not None and inst.spin_channel and inst.spin2.spin_channel
+    assert np.array_equal(inst.m_ia, v[0, :5, 5:]) and np.array_equal(inst.spin2.m_ia, v[1, :4, 4:])
+    assert np.array_equal(inst.occupation[:5], np.ones(5)) and inst.occupation[5] == 0.0
+    assert np.array_equal(inst.spin2.energy, e2) and inst.spin2.nocc == 4
+    assert np.array_equal(inst.spin2.m_sigma, v[1, 4:6])
+    out = o.g0w0_imag_spin([dict(energy=c.energy, occupation=c.occupation, m_ia=c.m_ia, m_sigma=c.m_sigma,
+                                 nsemin=c.nsemin, nsemax=c.nsemax) for c in (inst, inst.spin2)], inst.nomega)
+    assert all(np.all(np.isfinite(r.energy_qp_g)) for r in out)
