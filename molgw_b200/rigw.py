@@ -252,7 +252,7 @@ class Engine:
     # ---------------------------------------------------------------- problems
     def make_problem(self, inst, precision: int = RIGW_FP64, device_arrays: dict | None = None,
                      technique: int = RIGW_PADE, qp_only: bool = False,
-                     efermi: float | None = None) -> tuple[Problem, list]:
+                     efermi: float | None = None, freq: tuple | None = None) -> tuple[Problem, list]:
         """Problem descriptor for a ``molgw_b200.synth.GWInstance``-like object.
 
         ``device_arrays`` maps field names to CUDA tensors that replace the host
@@ -288,6 +288,12 @@ class Engine:
         p.naux = inst.naux
         p.nocc, p.nvirt = nocc, nvirt
         p.nomega = inst.nomega
+        if freq is not None:
+            # a subset of the imaginary grid (omega, weight): the frequencies of one rank
+            om, wt = (np.ascontiguousarray(a, dtype=np.float64) for a in freq)
+            p.nomega = om.size
+            p.omega, p.weight = _ptr(om), _ptr(wt)
+            arrs["omega"], arrs["weight"] = om, wt
         for k in ("m_ia", "e_occ", "e_virt", "occ_occ", "occ_virt", "m_pm", "e_p", "e_sig"):
             setattr(p, k, _ptr(arrs[k]))
         p.occ_sig = _ptr(occ_sig)
@@ -425,6 +431,32 @@ class Engine:
         out = self._output(r, bufs)
         out.sigma_calc = sigma_calc
         return out
+
+    def frequency_partials(self, inst, freq_index, precision: int = RIGW_FP64):
+        """The share of one rank in MOLGW's frequency split ("poorman",
+        src/m_gw_selfenergy_grid.f90:626,658): W and Sigma_c(z_k) on the imaginary
+        frequencies ``freq_index`` (0-based, of the inst.nomega Gauss-Legendre grid).
+        Returns (sigma_calc [nsig, nc] complex, [erpa, egw]) partial sums; summed
+        over ranks (``parallel.allreduce_partials``) they are the full quantities,
+        and ``qp_solve`` on the sum finishes the run."""
+        idx = np.asarray(freq_index, dtype=np.int64)
+        om, wt = imag_grid(inst.nomega)
+        freq = (om[idx], wt[idx])
+        p, keep = self.make_problem(inst, precision, freq=freq)
+        erpa, egw = C.c_double(), C.c_double()
+        w = C.c_void_p()
+        self._check(self._lib.rigw_polarizability_imag(self._h, C.byref(p), C.byref(erpa), C.byref(egw),
+                                                       C.byref(w)), "rigw_polarizability_imag")
+        wpol = WPol(self, w, inst.naux, idx.size)
+        try:
+            r, bufs = self._alloc_result(p)
+            self._check(self._lib.rigw_gw_selfenergy_imag(self._h, wpol.handle, C.byref(p), C.byref(r)),
+                        "rigw_gw_selfenergy_imag")
+            sc = bufs["sigma_calc"]
+            sigma = sc[..., 0] + 1j * sc[..., 1]
+        finally:
+            wpol.release()
+        return sigma, np.array([erpa.value, egw.value])
 
     def g0w0_spin(self, inst, precision: int = RIGW_FP64, technique: int = RIGW_PADE) -> list[G0W0Output]:
         """Open-shell (nspin = 2) G0W0 on the imaginary axis: one W from the

@@ -1,5 +1,5 @@
-"""Frozen core (MOLGW's ncorew / ncoreg) and Sigma_x - V_xc on the GPU against the
-oracle.  Frozen core: the W window and the states p of Sigma start above the core
+"""Frozen core (MOLGW's ncorew / ncoreg), Sigma_x - V_xc and the frequency split on
+the GPU against the oracle or the one-GPU solve.  Frozen core: the W window and the states p of Sigma start above the core
 (src/m_selfenergy_tools.f90:67-122, src/m_gw_selfenergy_grid.f90:92-93, 270-290);
 the engine takes the windows as the Fortran passes them."""
 from dataclasses import replace
@@ -49,3 +49,19 @@ def test_exchange_minus_vxc_matches_oracle(engine):
     assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
     assert np.abs(out.energy_qp_z - ref.energy_qp_z).max() * HA_EV <= 1e-6
     assert np.abs(out.energy_qp_g - engine.g0w0(inst, RIGW_FP64).energy_qp_g).max() > 1e-3
+
+
+def test_frequency_split_partials_sum_to_the_full_solve(engine):
+    """MOLGW's frequency split on one GPU: two ranks' partial Sigma_c and energies
+    (W on each rank's frequencies) summed, then the QP equation on the sum, equal
+    the one-GPU solve (src/m_gw_selfenergy_grid.f90:325, 626, 658)."""
+    from molgw_b200 import parallel
+    inst = synth.make_instance(9, 80, 200, 16, seed=42)
+    full = engine.g0w0(inst, RIGW_FP64)
+    parts = [engine.frequency_partials(inst, parallel.frequency_shard(inst.nomega, r, 2)) for r in range(2)]
+    sig = sum(p[0] for p in parts)
+    en = sum(p[1] for p in parts)
+    assert abs(en[0] - full.erpa) <= 1e-12 * abs(full.erpa) and abs(en[1] - full.egw) <= 1e-12 * abs(full.egw)
+    assert np.abs(sig - full.sigma_calc).max() <= 1e-12 * np.abs(full.sigma_calc).max()
+    qp = engine.qp_solve(inst, sig)
+    assert np.abs(qp.energy_qp_g - full.energy_qp_g).max() * HA_EV <= 1e-6
