@@ -92,7 +92,10 @@ class ClockSampler:
     def __init__(self, gpu_index: int):
         self.gpu = gpu_index
         self.proc = None
-        self.path = ROOT / "gpurun_out" / f"clocks_rank{gpu_index}.csv"
+        # the raw samples go to $RIGW_CLOCKS_CSV (a directory) or the system temp directory
+        import tempfile
+        base = Path(os.environ.get("RIGW_CLOCKS_CSV", tempfile.gettempdir()))
+        self.path = base / f"clocks_rank{gpu_index}.csv"
 
     def start(self):
         try:
