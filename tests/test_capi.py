@@ -74,6 +74,24 @@ def test_struct_layout_matches_ctypes(tmp_path):
         assert vals[("R", f)] == getattr(Result, f).offset, f
 
 
+def test_constants_match_the_header(tmp_path):
+    """Precision codes, techniques, problem flags and status codes of the Python
+    mirror are the header's values."""
+    from molgw_b200 import rigw
+    names = ["RIGW_FP64", "RIGW_BF16X3", "RIGW_OZAKI_INT8", "RIGW_PADE", "RIGW_HOMOLUMO",
+             "RIGW_PROBLEM_DEVICE_POINTERS", "RIGW_PROBLEM_QP_ONLY", "RIGW_PROBLEM_SPIN_CHANNEL"]
+    src = tmp_path / "consts.c"
+    body = "".join(f'  printf("{n} %d\\n", (int){n});\n' for n in names)
+    src.write_text("#include <stdio.h>\n#include \"rigw.h\"\nint main(void) {\n" + body + "  return 0;\n}\n")
+    exe = tmp_path / "consts"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    vals = dict(zip(out[0::2], map(int, out[1::2])))
+    for n in names:
+        assert vals[n] == getattr(rigw, n), n
+    assert rigw.RIGW_OZAKI(5) == vals["RIGW_OZAKI_INT8"] + 5
+
+
 def test_imag_grid_matches_oracle(lib):
     from molgw_b200 import rigw
     for n in (1, 16, 32, 48, 64):
