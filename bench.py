@@ -171,7 +171,8 @@ def profile_traffic(name: str):
 
 def compact_tuning(rep: dict) -> dict:
     """The autotuner's choice and its effect, without the candidate list."""
-    return {k: rep[k] for k in ("chi0_rows", "update_rows", "split_group", "chains", "default_ms", "tuned_ms")} | {
+    return {k: rep[k] for k in ("chi0_rows", "update_rows", "split_group", "chains", "panel_group", "default_ms",
+                                "tuned_ms")} | {
         "candidates": len(rep["candidates"])}
 
 

@@ -222,9 +222,11 @@ typedef struct rigw_tune_report {
   int update_rows;           /* trailing-update tile rows chosen (64 or 128)              */
   int split_group;           /* frequencies per split buffer (0: automatic, not tuned)    */
   int chains;                /* frequency chains (0: automatic)                           */
+  int panel_group;           /* panels per trailing update of the factorization (2..4)    */
   int precision_class;       /* 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed                    */
   int ncandidates;
-  int candidate[RIGW_TUNE_MAX_CANDIDATES][4];          /* (chi0_rows, update_rows, split_group, chains) */
+  int candidate[RIGW_TUNE_MAX_CANDIDATES][5];          /* (chi0_rows, update_rows, split_group, chains,
+                                                          panel_group) */
   float candidate_ms[RIGW_TUNE_MAX_CANDIDATES][3];     /* chi0 stage, factorization stage, total      */
   float default_ms, tuned_ms;  /* device time of one solve before and after tuning        */
 } rigw_tune_report;

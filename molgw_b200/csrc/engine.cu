@@ -508,6 +508,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   // at least kChainPairs (problem, frequency) pairs each
   nchains_ = tune_.chains > 0 ? std::max(1, std::min({tune_.chains, kMaxChains, npairs}))
                               : std::max(1, std::min(kAutoChains, npairs / kChainPairs));
+  // panels per trailing update: longer updates pay off when many problems keep
+  // the GPU busy; one or few problems keep pairs, whose factorization chain is shorter
+  group_ = tune_.panel_group > 0 ? std::max(1, std::min(tune_.panel_group, 4)) : (np >= 4 ? 4 : 2);
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});
@@ -671,15 +674,17 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         if (p.want_identity)
           for (int c0 = 0; c0 < r0; c0 += BMN) k2(R, ldb, c0, std::min(BMN, r0 - c0), cs + c0);
         for (int c0 = p.moff; c0 < ldb; c0 += BMN) k2(R, ldb, c0, std::min(BMN, ldb - c0), cs + c0);
-        // Trailing update, panels in pairs (k even, k + 1): after panel k only the
-        // rows of panel k + 1 are updated (K = 128, the U rows of panel k); after
-        // panel k + 1 every row below it is updated once with the U rows of both
-        // panels (K = 256), so each trailing tile is read and written once per
-        // pair.  Items of the next diagonal block go to their own list so that its
+        // Trailing update, panels in groups of G = group_: after panel k at position
+        // j of its group (first panel kp = k - j) only the rows of panel k + 1 are
+        // updated, with the U rows of panels kp .. k (K = (j+1) 128); after the last
+        // panel of the group every row below it is updated once with the U rows of
+        // the whole group, so each trailing tile is read and written once per group.
+        // Items of the next diagonal block go to their own list so that its
         // factorization can start while the rest of the update runs (lookahead).
-        const bool first_of_pair = (k % 2) == 0;
-        const int kp = first_of_pair ? k : k - 1;               // first panel of the U rows used
-        const int kdim = first_of_pair ? kPanel : 2 * kPanel;
+        const int jg = k % group_;
+        const bool first_of_pair = jg != group_ - 1;           // not the group's last panel
+        const int kp = k - jg;                                  // first panel of the U rows used
+        const int kdim = (jg + 1) * kPanel;
         const int iend = first_of_pair ? std::min(npad, r0 + kPanel) : npad;
         auto k3 = [&](const double* Bsrc, int ldbs, double* Cdst, int ldc, int i0, int c0, int m, int n,
                       std::vector<GemmItem>& dst) {
@@ -806,8 +811,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         pending = -1;
       if (add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm, pending)) pending = -1;
       const bool next = k + 1 < max_panels && !wl_diag_[L(k + 1)].empty();
-      if (k % 2 == 0) {
-        // first panel of a pair: the rows of panel k + 1, then its diagonal block
+      if (k % group_ != group_ - 1) {
+        // not the last panel of its group: the rows of panel k + 1, then its diagonal block
         if (add(6, gl_k3a_[L(k)].data(), sizeof(GemmItem), gl_k3a_[L(k)].size(), k, sm, pending)) pending = -1;
         if (next && add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sm,
                         pending))

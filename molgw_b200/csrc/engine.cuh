@@ -100,6 +100,7 @@ struct Tuning {
   int update_rows = 64;   // trailing-update items: rows per 128-column item (64 or 128)
   int split_group = 0;    // split precision: frequencies per hi/lo buffer (0: automatic)
   int chains = 0;         // frequency chains of the factorization stage (0: automatic)
+  int panel_group = 0;    // panels per trailing update (0: automatic, 4 for batches of >= 4 problems, else 2)
 };
 // Precision class of a batch (tunings are kept per mode and class):
 // 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed.
@@ -185,6 +186,7 @@ class Plan {
   std::vector<cudaEvent_t> la_ev_;           // borrowed from the context
   std::vector<cudaStream_t> aux_streams_;   // streams 1.. of the launch sequence (0 is the plan's stream); borrowed
   int nchains_ = 1;
+  int group_ = 2;          // panels per trailing update
   std::vector<Launch> seq_;
   cudaGraph_t stage_graph_[4] = {nullptr, nullptr, nullptr, nullptr};
   cudaGraphExec_t stage_exec_[4] = {nullptr, nullptr, nullptr, nullptr};

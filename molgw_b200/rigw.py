@@ -114,8 +114,8 @@ class ServerStats(C.Structure):
 class TuneReport(C.Structure):
     _fields_ = [
         ("chi0_rows", C.c_int), ("update_rows", C.c_int), ("split_group", C.c_int), ("chains", C.c_int),
-        ("precision_class", C.c_int), ("ncandidates", C.c_int),
-        ("candidate", (C.c_int * 4) * RIGW_TUNE_MAX_CANDIDATES),
+        ("panel_group", C.c_int), ("precision_class", C.c_int), ("ncandidates", C.c_int),
+        ("candidate", (C.c_int * 5) * RIGW_TUNE_MAX_CANDIDATES),
         ("candidate_ms", (C.c_float * 3) * RIGW_TUNE_MAX_CANDIDATES),
         ("default_ms", C.c_float), ("tuned_ms", C.c_float),
     ]
@@ -387,10 +387,12 @@ class Engine:
         self._check(self._lib.rigw_autotune(self._h, n, probs, C.byref(rep)), "rigw_autotune")
         cands = [{"chi0_rows": rep.candidate[k][0], "update_rows": rep.candidate[k][1],
                   "split_group": rep.candidate[k][2], "chains": rep.candidate[k][3],
+                  "panel_group": rep.candidate[k][4],
                   "chi0_ms": rep.candidate_ms[k][0], "factor_ms": rep.candidate_ms[k][1],
                   "total_ms": rep.candidate_ms[k][2]} for k in range(rep.ncandidates)]
         return {"chi0_rows": rep.chi0_rows, "update_rows": rep.update_rows, "split_group": rep.split_group,
-                "chains": rep.chains, "precision_class": rep.precision_class, "default_ms": rep.default_ms,
+                "chains": rep.chains, "panel_group": rep.panel_group, "precision_class": rep.precision_class,
+                "default_ms": rep.default_ms,
                 "tuned_ms": rep.tuned_ms, "candidates": cands}
 
     def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False) -> G0W0Output:
