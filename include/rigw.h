@@ -222,7 +222,7 @@ typedef struct rigw_tune_report {
   int update_rows;           /* trailing-update tile rows chosen (64 or 128)              */
   int split_group;           /* frequencies per split buffer (0: automatic, not tuned)    */
   int chains;                /* frequency chains (0: automatic)                           */
-  int panel_group;           /* panels per trailing update of the factorization (2..8)    */
+  int panel_group;           /* panels per trailing update of the factorization (2..32)   */
   int precision_class;       /* 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed                    */
   int ncandidates;
   int candidate[RIGW_TUNE_MAX_CANDIDATES][5];          /* (chi0_rows, update_rows, split_group, chains,

@@ -510,7 +510,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
                               : std::max(1, std::min(kAutoChains, npairs / kChainPairs));
   // panels per trailing update: longer updates pay off when many problems keep
   // the GPU busy; one or few problems keep pairs, whose factorization chain is shorter
-  group_ = tune_.panel_group > 0 ? std::max(1, std::min(tune_.panel_group, 8)) : (np >= 4 ? 8 : 2);
+  group_ = tune_.panel_group > 0 ? std::max(1, std::min(tune_.panel_group, 32)) : (np >= 4 ? 16 : 2);
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});

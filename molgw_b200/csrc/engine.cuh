@@ -100,7 +100,7 @@ struct Tuning {
   int update_rows = 64;   // trailing-update items: rows per 128-column item (64 or 128)
   int split_group = 0;    // split precision: frequencies per hi/lo buffer (0: automatic)
   int chains = 0;         // frequency chains of the factorization stage (0: automatic)
-  int panel_group = 0;    // panels per trailing update (0: automatic, 8 for batches of >= 4 problems, else 2)
+  int panel_group = 0;    // panels per trailing update (0: automatic, 16 for batches of >= 4 problems, else 2)
 };
 // Precision class of a batch (tunings are kept per mode and class):
 // 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed.

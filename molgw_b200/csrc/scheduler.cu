@@ -273,7 +273,7 @@ Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* 
     rep->candidate[k][1] = t.update_rows;
     rep->candidate[k][2] = t.split_group;
     rep->candidate[k][3] = t.chains;
-    rep->candidate[k][4] = t.panel_group > 0 ? t.panel_group : (n >= 4 ? 8 : 2);
+    rep->candidate[k][4] = t.panel_group > 0 ? t.panel_group : (n >= 4 ? 16 : 2);
     rep->candidate_ms[k][0] = st[1];
     rep->candidate_ms[k][1] = st[2];
     rep->candidate_ms[k][2] = st[0] + st[1] + st[2] + st[3];
@@ -304,14 +304,14 @@ Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* 
   if (any_fp64) RIGW_TRY(try_field(&Tuning::chi0_rows, {64, 128}, 1));
   RIGW_TRY(try_field(&Tuning::update_rows, {64, 128}, 2));
   RIGW_TRY(try_field(&Tuning::chains, {1, 2, 4}, 2));
-  RIGW_TRY(try_field(&Tuning::panel_group, {2, 4, 8}, 2));
+  RIGW_TRY(try_field(&Tuning::panel_group, {2, 8, 16}, 2));
   c.tuned[{int(kPlanFused), cls}] = best;
   c.plan_cache.clear();
   rep->chi0_rows = best.chi0_rows;
   rep->update_rows = best.update_rows;
   rep->split_group = best.split_group;
   rep->chains = best.chains;
-  rep->panel_group = best.panel_group > 0 ? best.panel_group : (n >= 4 ? 8 : 2);
+  rep->panel_group = best.panel_group > 0 ? best.panel_group : (n >= 4 ? 16 : 2);
   rep->precision_class = cls;
   rep->tuned_ms = bst[0] + bst[1] + bst[2] + bst[3];
   return Status::ok();
