@@ -50,7 +50,7 @@ def parse():
     ap.add_argument("--batch-count", type=int, default=32,
                     help="molecules of the ragged batch measured beside the single instance (0: skip)")
     ap.add_argument("--batch-reps", type=int, default=2)
-    ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep", "aomo"])
+    ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep", "aomo", "sox"])
     ap.add_argument("--sweep-reps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0)
     ap.add_argument("--serve-duration", type=float, default=60.0)
@@ -462,6 +462,75 @@ def run_aomo_line(args):
     print(json.dumps(line), flush=True)
 
 
+def run_sox_line(args):
+    """`--workload sox`: GW+SOX on the imaginary axis (postscf 'GW+SOX_PADE').
+    Sigma^SOX (sox_selfenergy_imag_grid) through the host-pointer C ABI on the
+    Nocc=21/Nvirt=207/Naux=840 instance and on Nocc=50/Nvirt=500/Naux=2000 (50
+    evaluation points each): the (p q|j c) product on the DMMA tile engine,
+    F = 2 nsig (Nocc+Nvirt) Nocc Nvirt Naux, and the frequency sums in
+    (element x point)/s over Nocc^2 Nvirt + Nocc Nvirt (Nvirt+1)/2 elements per
+    state; the oracle's Sigma^SOX timed on the host cores beside it.  value = the
+    whole GW+SOX solve (W, Sigma_c, Sigma^SOX, Pade, QP) per second on the 840
+    instance through the host-pointer calls.  One JSON line."""
+    import torch
+    from threadpoolctl import threadpool_limits
+    from molgw_b200 import build, synth
+    build.build()
+    from molgw_b200.rigw import Engine, efermi_of
+    from oracle import rigw_oracle as o
+    fp64_peak = measured_fp64_peak(torch)
+    eng = Engine(0)
+    cases = []
+    for name, inst in (("840", synth.single_instance_840()), ("2000", synth.make_instance(50, 500, 2000, 32, seed=1))):
+        z = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
+        for _ in range(2):
+            out = eng.sox_selfenergy_imag_grid(inst, z)
+        walls, stats = [], []
+        for _ in range(max(3, args.steps)):
+            t0 = time.perf_counter()
+            out = eng.sox_selfenergy_imag_grid(inst, z)
+            walls.append((time.perf_counter() - t0) * 1e3)
+            stats.append(eng.last_stats())
+        st = min(stats, key=lambda s: s["total_ms"])
+        no, nv = inst.m_ia.shape[0], inst.m_ia.shape[1]
+        nsig, ng = inst.m_sigma.shape[0], inst.m_sigma.shape[1]
+        flops = 2.0 * nsig * ng * no * nv * inst.naux
+        elems = nsig * (no * no * nv + no * nv * (nv + 1) / 2)
+        window = inst.energy[:ng]
+        with threadpool_limits(limits=os.cpu_count() or 1):
+            t0 = time.perf_counter()
+            ref = o.sox_selfenergy_imag(window, inst.m_sigma, inst.m_ia, z)
+            cpu_ms = (time.perf_counter() - t0) * 1e3
+        tf = flops / (st["stage_ms"][1] * 1e-3) / 1e12
+        cases.append({"instance": name, "nocc": no, "nvirt": nv, "naux": inst.naux, "nsig": nsig, "points": int(z.size),
+                      "wall_ms": float(min(walls)), "device_ms": st["total_ms"],
+                      "upload_transpose_ms": st["stage_ms"][0], "product_ms": st["stage_ms"][1],
+                      "product_tflops": tf, "product_frac_of_measured_fp64": tf / fp64_peak,
+                      "sums_ms": st["stage_ms"][3],
+                      "sums_gelem_points_per_s": elems * z.size / (st["stage_ms"][3] * 1e-3) / 1e9,
+                      "max_abs_diff_vs_oracle_rel": float(np.abs(out - ref).max() / np.abs(ref).max()),
+                      "oracle_ms": cpu_ms})
+    inst = synth.single_instance_840()
+    eng.gw_sox_imag(inst)
+    walls = []
+    for _ in range(max(3, args.steps)):
+        t0 = time.perf_counter()
+        res = eng.gw_sox_imag(inst)
+        walls.append((time.perf_counter() - t0) * 1e3)
+    gw = eng.g0w0(inst)
+    shift = float(np.abs(res.energy_qp_g - gw.energy_qp_g).max() * HA_EV)
+    eng.close()
+    ms = float(np.median(walls))
+    line = {"metric": "GW+SOX solves/s", "value": 1e3 / ms, "unit": "solves/s", "n_gpus": 1,
+            "steps": max(3, args.steps), "warmup": 1, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded instances of molgw_b200.synth)",
+            "config": {"workload": "GW+SOX on the imaginary axis through the host-pointer calls, Nocc=21 Nvirt=207 "
+                                   "Naux=840, 32 imaginary frequencies, 50 evaluation points",
+                       "fp64_peak_tflops": fp64_peak},
+            "sox_qp_shift_ev": shift, "cases": cases}
+    print(json.dumps(line), flush=True)
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the MOLGW path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -514,6 +583,9 @@ def main():
         return
     if args.workload == "aomo":
         run_aomo_line(args)
+        return
+    if args.workload == "sox":
+        run_sox_line(args)
         return
 
     import torch

@@ -20,6 +20,9 @@
  *                               find_qp_energy_graphical      src/m_selfenergy_tools.f90:253-420
  *   rigw_g0w0, rigw_g0w0_batch  the sequence of selfenergy_evaluation for
  *                               imaginary_axis_pade / _homolumo, src/m_selfenergy_evaluation.f90:214-246,587-611
+ *   rigw_sox_selfenergy_imag    sox_selfenergy_imag_grid      src/m_g3w2_selfenergy.f90:2482-2591
+ *                               (GW+SOX_PADE: added to sigma_calc before the Pade fit,
+ *                               src/m_selfenergy_evaluation.f90:494-503)
  */
 #ifndef RIGW_H
 #define RIGW_H
@@ -141,7 +144,9 @@ typedef struct rigw_result {
  * MOLGW's stage timers timer_rpa_dynamic / timer_gw_self, src/m_timing.f90:268-284).
  * After rigw_eri_3center_mo*: stage_ms = upload + unpack of the AO tensor, the two
  * products with their operand splits, download of the result; chunks = auxiliary
- * chunks (timer_aomo_gw). */
+ * chunks (timer_aomo_gw).  After rigw_sox_selfenergy_imag: stage_ms[0] = uploads,
+ * operand transposes and download, [1] = the (p q|j c) products, [3] = the
+ * frequency sums; chunks = Sigma-state chunks (timer_vertex_selfenergy). */
 typedef struct rigw_stats {
   double stage_ms[4];        /* CUDA-event times: input packing, chi0 contraction,
                                 eps factorization + triangular solves, energies + Sigma + QP */
@@ -202,6 +207,27 @@ RIGW_API int rigw_wpol_release(rigw_ctx* ctx, rigw_wpol* wpol);
 /* Continuation + QP equation from sigma_calc (host arrays of ``result``). */
 RIGW_API int rigw_qp_solve(rigw_ctx* ctx, const rigw_problem* prob, const double* sigma_calc,
                   rigw_result* result);
+
+/* Second-order screened exchange on the evaluation points, one spin channel
+ * (sox_selfenergy_imag_grid).  With C_p[q][(j,c)] = (p q|j c) over the G window,
+ *   Sigma^SOX_p(z) = - sum_{i,k occ; b empty} C_p[i][(k,b)] C_p[k][(i,b)] / (z - e_i - e_k + e_b)
+ *                    - sum_{a,c empty; j occ} C_p[a][(j,c)] C_p[c][(j,a)] / (z - e_a - e_c + e_j).
+ * GW+SOX adds it to sigma_calc of rigw_gw_selfenergy_imag / rigw_g0w0 and then
+ * calls rigw_qp_solve. */
+typedef struct rigw_sox_problem {
+  int naux;
+  int nocc, nvirt;           /* G window: occupied ncore_G+1..nhomo_G, empty nhomo_G+1..nvirtual_G-1 */
+  const double* m_ov;        /* [nocc][nvirt][naux] = eri_3center_mo(naux, b, k) over the G window */
+  int nsig;                  /* Sigma states nsemin..nsemax                                */
+  const double* m_pq;        /* [nsig][nocc+nvirt][naux] = eri_3center_mo(naux, q, p)       */
+  const double* energy;      /* [nocc+nvirt] energy_g over the G window (Ha)               */
+  int nomega_calc;           /* evaluation points (se%omega_calc)                          */
+  const double* omega_calc;  /* [nomega_calc][2] complex points                            */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS                               */
+} rigw_sox_problem;
+/* sigma_sox: [nsig][nomega_calc][2], overwritten (host memory, or device memory
+ * under RIGW_PROBLEM_DEVICE_POINTERS). */
+RIGW_API int rigw_sox_selfenergy_imag(rigw_ctx* ctx, const rigw_sox_problem* prob, double* sigma_sox);
 
 /* ---- fused solves ----------------------------------------------------------- */
 RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result);

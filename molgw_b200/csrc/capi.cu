@@ -200,6 +200,14 @@ int rigw_qp_solve(rigw_ctx* ctx, const rigw_problem* prob, const double* sigma_c
   return finish(ctx, run_batch(ctx->impl, rigw::kPlanQP, 1, prob, result, &tmp, {}, sc));
 }
 
+int rigw_sox_selfenergy_imag(rigw_ctx* ctx, const rigw_sox_problem* prob, double* sigma_sox) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!prob || !sigma_sox) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::sox_selfenergy_imag(ctx->impl, *prob, sigma_sox));
+}
+
 int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux, const int* index_basis,
                         const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                         int nstate_min, int nstate_max, double* out) {

@@ -69,6 +69,13 @@ class Problem(C.Structure):
     ]
 
 
+class SoxProblem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nocc", C.c_int), ("nvirt", C.c_int), ("m_ov", _dp), ("nsig", C.c_int),
+        ("m_pq", _dp), ("energy", _dp), ("nomega_calc", C.c_int), ("omega_calc", _dp), ("flags", C.c_int),
+    ]
+
+
 def efermi_of(inst) -> float:
     """se_init's efermi from the energies in G: half-way between the highest
     energy of state nhomo_G and the lowest of state nhomo_G + 1 over the spin
@@ -145,6 +152,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_gw_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_wpol_release.argtypes = [C.c_void_p, C.c_void_p]
     lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
+    lib.rigw_sox_selfenergy_imag.argtypes = [C.c_void_p, C.POINTER(SoxProblem), _dp]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -432,6 +440,51 @@ class Engine:
         self._check(self._lib.rigw_qp_solve(self._h, C.byref(p), _ptr(sc), C.byref(r)), "rigw_qp_solve")
         out = self._output(r, bufs)
         out.sigma_calc = sigma_calc
+        return out
+
+    def sox_selfenergy_imag_grid(self, inst, omega_calc, m_ov=None) -> np.ndarray:
+        """Sigma^SOX on the evaluation points ``omega_calc`` for the Sigma states
+        of ``inst`` (sox_selfenergy_imag_grid, src/m_g3w2_selfenergy.f90:2482-2591),
+        [nsig, nomega_calc] complex, from energy_g over the G window.  ``m_ov`` is
+        the occupied x empty block [nocc_G, nvirt_G, naux] of the G window; the
+        default ``inst.m_ia`` is that block when the W and G windows coincide."""
+        cg = getattr(inst, "ncore_g", 0)
+        if m_ov is None:
+            if getattr(inst, "ncore_w", 0) != cg:
+                raise ValueError("sox_selfenergy_imag_grid: pass m_ov when the W and G windows differ")
+            m_ov = inst.m_ia
+        m_ov = np.ascontiguousarray(m_ov, dtype=np.float64)
+        mpq = np.ascontiguousarray(inst.m_sigma, dtype=np.float64)
+        e = inst.energy if getattr(inst, "energy_g", None) is None else inst.energy_g
+        ew = np.ascontiguousarray(np.asarray(e, dtype=np.float64)[cg:cg + mpq.shape[1]])
+        oc = np.ascontiguousarray(np.stack([np.real(omega_calc), np.imag(omega_calc)], -1), dtype=np.float64)
+        sp = SoxProblem()
+        sp.naux = inst.naux
+        sp.nocc, sp.nvirt = m_ov.shape[0], m_ov.shape[1]
+        if sp.nocc + sp.nvirt != mpq.shape[1]:
+            raise ValueError("sox_selfenergy_imag_grid: m_ov does not span the window of m_sigma")
+        sp.m_ov, sp.m_pq, sp.energy, sp.omega_calc = _ptr(m_ov), _ptr(mpq), _ptr(ew), _ptr(oc)
+        sp.nsig = mpq.shape[0]
+        sp.nomega_calc = oc.shape[0]
+        out = np.zeros((sp.nsig, sp.nomega_calc, 2))
+        self._check(self._lib.rigw_sox_selfenergy_imag(self._h, C.byref(sp), _ptr(out)),
+                    "rigw_sox_selfenergy_imag")
+        return out[..., 0] + 1j * out[..., 1]
+
+    def gw_sox_imag(self, inst, precision: int = RIGW_FP64, m_ov=None) -> G0W0Output:
+        """GW+SOX on the imaginary axis (postscf 'GW+SOX_PADE'): W and Sigma_c on
+        the evaluation points, Sigma^SOX added to sigma_calc, then the
+        Pade continuation and the QP equation (src/m_selfenergy_evaluation.f90:494-503,
+        587-611; the imaginary-axis vertex path exists for imaginary_axis_pade only)."""
+        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        try:
+            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst)
+        finally:
+            wpol.release()
+        oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
+        sigma = sigma + self.sox_selfenergy_imag_grid(inst, oc, m_ov)
+        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc)
+        out.erpa, out.egw = erpa, egw
         return out
 
     def frequency_partials(self, inst, freq_index, precision: int = RIGW_FP64):

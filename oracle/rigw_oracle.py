@@ -24,6 +24,9 @@ the same BLAS/LAPACK call sequence (through SciPy's bundled OpenBLAS):
 * ``find_qp_energy_linearization`` src/m_selfenergy_tools.f90:202-249
 * ``find_qp_energy_graphical`` / ``find_fixed_point`` src/m_selfenergy_tools.f90:253-420
 * ``output_homolumo``         src/m_hamiltonian_tools.f90:564-612
+* ``sox_selfenergy_imag``     src/m_g3w2_selfenergy.f90:2482-2591 (GW+SOX on the
+                              imaginary axis, added before the Pade fit,
+                              src/m_selfenergy_evaluation.f90:494-503)
 
 Pinning: the reference's own known answer that needs no Gaussian integrals is
 the analytic RPA correlation energy of bulk LiH from the shipped CC4S tensor
@@ -543,7 +546,8 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
               step_sigma: float = 0.01, nomega_sigma_calc: int = 50,
               step_sigma_calc: float = 0.075, eta: float = 0.01,
               exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
-              ncore_w: int = 0, energy_g: np.ndarray | None = None) -> G0W0Result:
+              ncore_w: int = 0, energy_g: np.ndarray | None = None, sox: bool = False,
+              m_ov_g: np.ndarray | None = None) -> G0W0Result:
     """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
     (src/m_selfenergy_evaluation.f90:214-246, 587-611).
 
@@ -554,6 +558,10 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     ENERGY_QP under force_energy_qp (:164-181): se%init and the Sigma sum take
     them, W (energy_w = energy for GW) and the energy0 of the QP equation
     (find_qp_energy_*(se, ..., energy, ...), :587-590) keep ``energy``.
+
+    ``sox``: GW+SOX_PADE, Sigma^SOX from energy_g added to sigma_calc before the
+    fit (:494-503); ``m_ov_g`` is the occupied x empty block of the G window
+    (default ``m_ia``, the W window, when both windows start at the same state).
     """
     eg = energy if energy_g is None else energy_g
     occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
@@ -566,6 +574,12 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     se = se_init_imaginary_axis(eg, rng, technique, nomega_sigma, step_sigma,
                                 nomega_sigma_calc, step_sigma_calc)
     se.sigma_calc[:] = gw_selfenergy_imag(eg, m_sigma, sf, se.omega_calc, rng.ncore_g + 1)
+    if sox:
+        mov = m_ia if m_ov_g is None else m_ov_g
+        if m_ov_g is None and ncore_w != rng.ncore_g:
+            raise ValueError("sox: pass m_ov_g when the W and G windows differ")
+        window = eg[rng.ncore_g: rng.ncore_g + m_sigma.shape[1]]
+        se.sigma_calc += sox_selfenergy_imag(window, m_sigma, mov, se.omega_calc).T
     if technique == "pade":
         se_pade_fit(se, eta)
     else:
@@ -631,4 +645,74 @@ def g0w0_imag_spin(channels: list, nomega_chi_imag: int, nomega_sigma: int = 51,
         ehomo, elumo = output_homolumo(c["occupation"], full, c["nsemin"], c["nsemax"], spin_fact=1.0)
         out.append(G0W0Result(sf.erpa, sf.egw, se.sigma_calc.copy(), se.sigma.copy(), eqp_g, eqp_z, zz_g,
                               ehomo, elumo, c["nsemin"], c["nsemax"]))
+    return out
+
+
+def sox_selfenergy_imag(energy_g: np.ndarray, m_sigma: np.ndarray, m_ov: np.ndarray,
+                        omega_calc: np.ndarray, chunk: int = 1 << 17) -> np.ndarray:
+    """Second-order screened exchange on the evaluation points of the imaginary
+    axis, sox_selfenergy_imag_grid (src/m_g3w2_selfenergy.f90:2482-2591), one spin.
+
+    ``energy_g`` are the G energies over the window ncore_G+1 .. nvirtual_G-1
+    (occupied first: ``nocc = m_ov.shape[0]`` of them), ``m_sigma`` is
+    ``[nsig, nocc + nvirt, naux]`` = eri_3center_mo(:, q, p) for the Sigma states
+    p, ``m_ov`` is ``[nocc, nvirt, naux]`` = eri_3center_mo(:, b, k) over the
+    same window.  With C_p[q][(j, c)] = (p q | j c) the two sums of :2534-2577 are
+
+      - sum_{b,i,k} C_p[i][(k,b)] C_p[k][(i,b)] / (z - e_i - e_k + e_b)
+      - sum_{c,j,a} C_p[a][(j,c)] C_p[c][(j,a)] / (z - e_a - e_c + e_j)
+
+    (vcoul1 = (p i|b k), vcoul2 = (i b|k p); vcoul1 = (p a|j c), vcoul2 =
+    (a j|c p)).  Returns Sigma^SOX [nsig, nomega_calc] complex; the reference adds
+    it to sigma_calc (:2584-2585) before the Pade fit."""
+    no, nv, naux = m_ov.shape
+    e_o, e_v = energy_g[:no], energy_g[no:no + nv]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    mov = m_ov.reshape(no * nv, naux)
+    d1 = (e_o[:, None, None] + e_o[None, :, None] - e_v[None, None, :]).ravel()
+    d2 = (e_v[:, None, None] + e_v[None, None, :] - e_o[None, :, None]).ravel()
+    out = np.zeros((m_sigma.shape[0], z.size), dtype=np.complex128)
+
+    def contract(prod, delta):
+        s = np.zeros(z.size, dtype=np.complex128)
+        for a in range(0, prod.size, chunk):
+            s += (1.0 / (z[:, None] - delta[None, a:a + chunk])) @ prod[a:a + chunk]
+        return s
+
+    for p in range(m_sigma.shape[0]):
+        cp = (m_sigma[p, :no + nv] @ mov.T).reshape(no + nv, no, nv)
+        occ = cp[:no]                                   # [i][k][b] = (p i|b k)
+        prod1 = (occ * occ.transpose(1, 0, 2)).ravel()  # (p i|b k) (i b|k p)
+        vir = cp[no:]                                   # [a][j][c] = (p a|j c)
+        prod2 = (vir * vir.transpose(2, 1, 0)).ravel()  # (p a|j c) (a j|c p)
+        out[p] = -contract(prod1, d1) - contract(prod2, d2)
+    return out
+
+
+def sox_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, nocc: int, sig_states,
+                              omega_calc: np.ndarray) -> np.ndarray:
+    """Loop-for-loop restatement of sox_selfenergy_imag_grid
+    (src/m_g3w2_selfenergy.f90:2532-2578) for small cases: evaluate_eri_mo(p, q,
+    r, s) = sum_P M(p,q)_P M(r,s)_P over the full window tensor ``m_full``
+    [nstate, nstate, naux] (symmetric in its first two indices), occupied states
+    0 .. nocc-1, empty ones nocc .. nstate-1; ``sig_states`` are 0-based window
+    indices of the Sigma states."""
+    nstate = m_full.shape[0]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    eri = lambda p, q, r, s: float(m_full[p, q] @ m_full[r, s])
+    out = np.zeros((len(sig_states), z.size), dtype=np.complex128)
+    for b in range(nocc, nstate):
+        for i in range(nocc):
+            for k in range(nocc):
+                for ip, p in enumerate(sig_states):
+                    v1 = eri(p, i, b, k)
+                    v2 = eri(i, b, k, p)
+                    out[ip] -= v1 * v2 / (z - energy_g[i] - energy_g[k] + energy_g[b])
+    for c in range(nocc, nstate):
+        for j in range(nocc):
+            for a in range(nocc, nstate):
+                for ip, p in enumerate(sig_states):
+                    v1 = eri(p, a, j, c)
+                    v2 = eri(a, j, c, p)
+                    out[ip] -= v1 * v2 / (z - energy_g[a] - energy_g[c] + energy_g[j])
     return out

@@ -146,3 +146,26 @@ def test_tune_report_layout_matches_ctypes(tmp_path):
     assert int(out["S"]) == C.sizeof(TuneReport)
     for f in fields:
         assert int(out[f"T {f}"]) == getattr(TuneReport, f).offset, f
+
+
+def test_sox_problem_layout_matches_ctypes(tmp_path):
+    from molgw_b200.rigw import SoxProblem
+    fields = [f for f, _ in SoxProblem._fields_]
+    body = "".join(f'  printf("X {f} %zu\\n", offsetof(rigw_sox_problem, {f}));\n' for f in fields)
+    src = tmp_path / "sox.c"
+    src.write_text(textwrap.dedent(f"""
+        #include <stdio.h>
+        #include <stddef.h>
+        #include "rigw.h"
+        int main(void) {{
+          printf("S %zu\\n", sizeof(rigw_sox_problem));
+        {body}  return 0;
+        }}
+    """))
+    exe = tmp_path / "sox"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in
+               subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if line)
+    assert int(out["S"]) == C.sizeof(SoxProblem)
+    for f in fields:
+        assert int(out[f"X {f}"]) == getattr(SoxProblem, f).offset, f
