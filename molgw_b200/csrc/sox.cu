@@ -278,8 +278,10 @@ Status sox_selfenergy_imag(Context& c, const rigw_sox_problem& pr, double* sigma
     const int pcn = std::min(pc, nsig - p0);
     const long long mrows = (long long)pcn * ngp;
     items.clear();
-    for (long long i0 = 0; i0 < mrows; i0 += 128)
-      for (long long j0 = 0; j0 < novp; j0 += 128) {
+    // column blocks outer: the CTAs in flight share a few 128-column tiles of
+    // M_ov^T while all of M_pq^T stays in L2, so M_ov^T comes from HBM about once
+    for (long long j0 = 0; j0 < novp; j0 += 128)
+      for (long long i0 = 0; i0 < mrows; i0 += 128) {
         GemmItem g{};
         g.A = at + (long long)p0 * ngp + i0;
         g.lda = int(lda);

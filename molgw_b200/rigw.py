@@ -442,13 +442,33 @@ class Engine:
         out.sigma_calc = sigma_calc
         return out
 
-    def sox_selfenergy_imag_grid(self, inst, omega_calc, m_ov=None) -> np.ndarray:
+    def sox_selfenergy_imag_grid(self, inst, omega_calc, m_ov=None, device_arrays: dict | None = None) -> np.ndarray:
         """Sigma^SOX on the evaluation points ``omega_calc`` for the Sigma states
         of ``inst`` (sox_selfenergy_imag_grid, src/m_g3w2_selfenergy.f90:2482-2591),
         [nsig, nomega_calc] complex, from energy_g over the G window.  ``m_ov`` is
         the occupied x empty block [nocc_G, nvirt_G, naux] of the G window; the
-        default ``inst.m_ia`` is that block when the W and G windows coincide."""
+        default ``inst.m_ia`` is that block when the W and G windows coincide.
+        ``device_arrays`` {"m_ov", "m_pq"}: CUDA tensors used in place
+        (RIGW_PROBLEM_DEVICE_POINTERS; the result is then written on the device)."""
         cg = getattr(inst, "ncore_g", 0)
+        if device_arrays:
+            import torch
+            dov, dpq = device_arrays["m_ov"], device_arrays["m_pq"]
+            e = inst.energy if getattr(inst, "energy_g", None) is None else inst.energy_g
+            ew = np.ascontiguousarray(np.asarray(e, dtype=np.float64)[cg:cg + dpq.shape[1]])
+            oc = np.ascontiguousarray(np.stack([np.real(omega_calc), np.imag(omega_calc)], -1), dtype=np.float64)
+            sp = SoxProblem()
+            sp.naux = inst.naux
+            sp.nocc, sp.nvirt = dov.shape[0], dov.shape[1]
+            sp.m_ov, sp.m_pq = C.cast(dov.data_ptr(), _dp), C.cast(dpq.data_ptr(), _dp)
+            sp.energy, sp.omega_calc = _ptr(ew), _ptr(oc)
+            sp.nsig, sp.nomega_calc = dpq.shape[0], oc.shape[0]
+            sp.flags = RIGW_PROBLEM_DEVICE_POINTERS
+            out = torch.empty((sp.nsig, sp.nomega_calc, 2), dtype=torch.float64, device=dov.device)
+            self._check(self._lib.rigw_sox_selfenergy_imag(self._h, C.byref(sp), C.cast(out.data_ptr(), _dp)),
+                        "rigw_sox_selfenergy_imag")
+            o = out.cpu().numpy()
+            return o[..., 0] + 1j * o[..., 1]
         if m_ov is None:
             if getattr(inst, "ncore_w", 0) != cg:
                 raise ValueError("sox_selfenergy_imag_grid: pass m_ov when the W and G windows differ")
@@ -513,15 +533,20 @@ class Engine:
             wpol.release()
         return sigma, np.array([erpa.value, egw.value])
 
-    def g0w0_spin(self, inst, precision: int = RIGW_FP64, technique: int = RIGW_PADE) -> list[G0W0Output]:
+    def g0w0_spin(self, inst, precision: int = RIGW_FP64, technique: int = RIGW_PADE,
+                  sox: bool = False) -> list[G0W0Output]:
         """Open-shell (nspin = 2) G0W0 on the imaginary axis: one W from the
         transitions of both spin channels (``inst`` and ``inst.spin2``), then Sigma
         and the QP equation per channel with the factors resident, on the
         evaluation points of the common efermi (src/m_gw_selfenergy_grid.f90:118-149,
         279-319; src/m_selfenergy_tools.f90:584-585).  Returns one output per
-        channel, each carrying E_RPA and E_GW of the whole W."""
+        channel, each carrying E_RPA and E_GW of the whole W.  ``sox``: GW+SOX_PADE,
+        Sigma^SOX of each channel (its own integrals and energies,
+        src/m_g3w2_selfenergy.f90:2532-2580) added to its sigma_calc before the fit."""
         if getattr(inst, "spin2", None) is None:
             raise ValueError("g0w0_spin needs inst.spin2 (the second spin channel)")
+        if sox and technique != RIGW_PADE:
+            raise ValueError("g0w0_spin: SOX runs with the Pade continuation (imaginary_axis_pade) only")
         ef = efermi_of(inst)
         erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
         outs = []
@@ -534,7 +559,11 @@ class Engine:
                     eh = max(inst.energy[nh - 1], inst.spin2.energy[nh - 1])
                     el = min(inst.energy[nh], inst.spin2.energy[nh])
                     zc = (eh + 0.01 + np.arange(nc) / (nc - 1.0) * (el - eh - 0.02)).astype(np.complex128)
+                if sox:
+                    zc = ef + 1j * ch.step_sigma_calc * np.arange(ch.nomega_sigma_calc)
                 sc = self.gw_selfenergy_imag_scalapack(wpol, ch, zc, efermi=ef)
+                if sox:
+                    sc = sc + self.sox_selfenergy_imag_grid(ch, zc)
                 out = self.qp_solve(ch, sc, technique, zc, efermi=ef)
                 out.erpa, out.egw = erpa, egw
                 outs.append(out)

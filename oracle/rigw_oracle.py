@@ -603,7 +603,7 @@ def fermi_level_spin(energy0_spins: list, nhomo_g: int) -> float:
 
 def g0w0_imag_spin(channels: list, nomega_chi_imag: int, nomega_sigma: int = 51, step_sigma: float = 0.01,
                    nomega_sigma_calc: int = 50, step_sigma_calc: float = 0.075, eta: float = 0.01,
-                   technique: str = "pade") -> list:
+                   technique: str = "pade", sox: bool = False) -> list:
     """Open-shell (nspin = 2) selfenergy_evaluation for imaginary_axis_pade /
     _homolumo: one W from the transitions of both channels
     (src/m_gw_selfenergy_grid.f90:118-149), Sigma per spin (:279-319), the QP
@@ -632,6 +632,9 @@ def g0w0_imag_spin(channels: list, nomega_chi_imag: int, nomega_sigma: int = 51,
             se.omega_calc = (eh + 0.01 + np.arange(nomega_sigma_calc) / (nomega_sigma_calc - 1.0)
                              * (el - eh - 0.02)).astype(np.complex128)
         se.sigma_calc[:] = gw_selfenergy_imag(c["energy"], c["m_sigma"], sf, se.omega_calc, 1)
+        if sox:   # per spin, the channel's own integrals and energies (src/m_g3w2_selfenergy.f90:2530-2580)
+            se.sigma_calc += sox_selfenergy_imag(c["energy"][:c["m_sigma"].shape[1]], c["m_sigma"], c["m_ia"],
+                                                 se.omega_calc).T
         if technique == "pade":
             se_pade_fit(se, eta)
         else:

@@ -105,6 +105,7 @@ def test_bad_arguments_return_status_not_abort(lib):
     assert lib.rigw_imag_grid(0, None, None) == 1
     assert lib.rigw_create(None, 0, 0) == 1
     assert lib.rigw_g0w0(None, None, None) == 1
+    assert lib.rigw_sox_selfenergy_imag(None, None, None) == 1
     assert lib.rigw_version() == 1
 
 

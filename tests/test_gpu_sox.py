@@ -70,3 +70,14 @@ def test_gw_plus_sox_qp_matches_oracle(engine):
                       eta=inst.eta, sox=True)
     assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
     assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
+
+
+def test_sox_device_pointers_match_host_pointers(engine):
+    import torch
+    inst = synth.make_instance(5, 37, 51, 8, seed=2)
+    z = _points(inst)
+    host = engine.sox_selfenergy_imag_grid(inst, z)
+    dev = engine.sox_selfenergy_imag_grid(inst, z, device_arrays={
+        "m_ov": torch.from_numpy(np.ascontiguousarray(inst.m_ia)).cuda(),
+        "m_pq": torch.from_numpy(np.ascontiguousarray(inst.m_sigma)).cuda()})
+    assert np.array_equal(host, dev)

@@ -45,3 +45,14 @@ def test_open_shell_split_precision(engine):
     f64, spl = engine.g0w0_spin(inst, RIGW_FP64), engine.g0w0_spin(inst, RIGW_BF16X3)
     for a, b in zip(f64, spl):
         assert np.abs(a.energy_qp_g - b.energy_qp_g).max() * HA_EV * 1e3 <= 1.0
+
+
+def test_open_shell_gw_plus_sox_matches_oracle(engine):
+    inst = open_shell_instance()
+    outs = engine.g0w0_spin(inst, RIGW_FP64, sox=True)
+    refs = o.g0w0_imag_spin(oracle_channels(inst), inst.nomega, nomega_sigma=inst.nomega_sigma,
+                            step_sigma=inst.step_sigma, nomega_sigma_calc=inst.nomega_sigma_calc,
+                            step_sigma_calc=inst.step_sigma_calc, eta=inst.eta, sox=True)
+    for out, ref in zip(outs, refs):
+        assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
+        assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6

@@ -51,3 +51,21 @@ def test_host_efermi_rule():
     two = open_shell_instance()
     e1, e2 = two.energy, two.spin2.energy
     assert efermi_of(two) == 0.5 * (max(e1[4], e2[4]) + min(e1[5], e2[5]))
+
+
+def test_gw_plus_sox_two_identical_channels_reproduce_the_closed_shell():
+    """Sigma^SOX runs per spin with no spin factor (src/m_g3w2_selfenergy.f90:2530-2580),
+    and W from two identical half-occupied channels is the closed-shell W, so GW+SOX
+    per channel equals the closed-shell GW+SOX."""
+    from tests.spin_cases import as_two_channels, oracle_channels
+    # 16 frequencies: an 8-frequency Pade fit amplifies the 1e-16 differences of the
+    # two chi0 summation orders to 1e-5 Ha in the QP energies, without SOX as well
+    inst = synth.make_instance(9, 80, 200, 16, seed=42)
+    kw = dict(nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma,
+              nomega_sigma_calc=inst.nomega_sigma_calc, step_sigma_calc=inst.step_sigma_calc, eta=inst.eta)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng, sox=True, **kw)
+    for out in o.g0w0_imag_spin(oracle_channels(as_two_channels(inst)), inst.nomega, sox=True, **kw):
+        assert np.abs(out.sigma_calc - ref.sigma_calc).max() <= 1e-14 * np.abs(ref.sigma_calc).max()
+        assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() <= 1e-10
