@@ -23,6 +23,8 @@
  *   rigw_sox_selfenergy_imag    sox_selfenergy_imag_grid      src/m_g3w2_selfenergy.f90:2482-2591
  *                               (GW+SOX_PADE: added to sigma_calc before the Pade fit,
  *                               src/m_selfenergy_evaluation.f90:494-503)
+ *   rigw_sosex_selfenergy_imag  sosex_selfenergy_imag_grid    src/m_g3w2_selfenergy.f90:2200-2478
+ *                               (GW+SOSEX_PADE: added after SOX, src/m_selfenergy_evaluation.f90:498-500)
  */
 #ifndef RIGW_H
 #define RIGW_H
@@ -228,6 +230,29 @@ typedef struct rigw_sox_problem {
 /* sigma_sox: [nsig][nomega_calc][2], overwritten (host memory, or device memory
  * under RIGW_PROBLEM_DEVICE_POINTERS). */
 RIGW_API int rigw_sox_selfenergy_imag(rigw_ctx* ctx, const rigw_sox_problem* prob, double* sigma_sox);
+
+/* SOSEX without its SOX part on the evaluation points, one spin channel
+ * (sosex_selfenergy_imag_grid), with W - v = v^1/2 chi v^1/2 from the resident
+ * factors of ``wpol`` (its frequency grid and weights are wpol_imag's).  With
+ * T_k(r; i,a) = (r m|W(i w_k) - v|i a), B1 = (r a|i m), B2 = (r i|a m), D = e_a - e_i:
+ *   Sigma_m(z) = f/(2 pi) sum_k w_k sum_{s=+-1} sum_{r,i,a}
+ *                T_k / (z + s i w_k - e_r) [B1 / (s i w_k - D) - B2 / (s i w_k + D)].
+ * The wpol must hold the identity part of the solve (not RIGW_PROBLEM_QP_ONLY). */
+typedef struct rigw_sosex_problem {
+  int naux;
+  int nocc, nvirt;           /* G window: occupied ncore_G+1..nhomo_G, empty nhomo_G+1..nvirtual_G-1 */
+  const double* m_full;      /* [nocc+nvirt][nocc+nvirt][naux] = eri_3center_mo(naux, q, r) over the window */
+  int nsig;                  /* Sigma states nsemin..nsemax                                */
+  int sig_first;             /* window index (0-based) of nsemin: nsemin - ncore_G - 1     */
+  const double* energy;      /* [nocc+nvirt] energy_g over the window (Ha)                 */
+  int nomega_calc;
+  const double* omega_calc;  /* [nomega_calc][2] complex points                            */
+  double factor_sosex;       /* factor_sosex: 1, or 2 for the 2SOSEX variants              */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS (m_full, sigma_sosex on the device) */
+} rigw_sosex_problem;
+/* sigma_sosex: [nsig][nomega_calc][2], overwritten. */
+RIGW_API int rigw_sosex_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_sosex_problem* prob,
+                                        double* sigma_sosex);
 
 /* ---- fused solves ----------------------------------------------------------- */
 RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result);

@@ -1,5 +1,6 @@
-// GW+SOX on the imaginary axis: the second-order screened exchange on the
-// evaluation points, sox_selfenergy_imag_grid (src/m_g3w2_selfenergy.f90:2482-2591).
+// Vertex corrections on the imaginary axis.  GW+SOX: the second-order screened
+// exchange on the evaluation points, sox_selfenergy_imag_grid
+// (src/m_g3w2_selfenergy.f90:2482-2591); GW+SOSEX further below.
 //
 //   C_p[q][(j,c)] = (p q|j c) = sum_P M_pq[P] M_jc[P]               FP64 DMMA product
 //   Sigma_p(z) = - sum_{i,k occ; b empty} C_p[i][(k,b)] C_p[k][(i,b)] / (z - e_i - e_k + e_b)
@@ -27,10 +28,17 @@ constexpr int kSoxBlockB = kSoxThreads;   // empty states b per unit of the firs
 
 inline long long round_up_ll(long long v, long long a) { return (v + a - 1) / a * a; }
 
-// dst[P][(r / group) * group_pad + r % group] = src[r][P]: rows of naux values
-// become columns, each group of rows padded to an even width (zeros stay in the pad).
-__global__ void sox_transpose_kernel(const double* __restrict__ src, long long nrows, int naux, long long group,
-                                     long long group_pad, double* __restrict__ dst, long long ld_dst) {
+// Column of row r = o * group + q in a transposed operand: groups of rows padded
+// to group_pad, the rows of a group at or after `split` moved by `shift`, and the
+// groups at or after `osplit` moved by `oshift` (even widths for the 16-byte
+// operand loads of the DMMA tile engine; zeros stay in the gaps).
+struct TransposeMap {
+  long long group, group_pad, split, shift, osplit, oshift;
+};
+
+// dst[P][column(r)] = src[r][P]: rows of naux values become columns.
+__global__ void sox_transpose_kernel(const double* __restrict__ src, long long nrows, int naux, TransposeMap map,
+                                     double* __restrict__ dst, long long ld_dst) {
   __shared__ double t[32][33];
   const long long r0 = (long long)blockIdx.x * 32;
   const int p0 = blockIdx.y * 32;
@@ -43,7 +51,11 @@ __global__ void sox_transpose_kernel(const double* __restrict__ src, long long n
   for (int y = threadIdx.y; y < 32; y += 8) {
     const int p = p0 + y;
     const long long r = r0 + threadIdx.x;
-    if (p < naux && r < nrows) dst[p * ld_dst + (r / group) * group_pad + r % group] = t[threadIdx.x][y];
+    if (p < naux && r < nrows) {
+      const long long o = r / map.group, q = r % map.group;
+      const long long col = (o + (o >= map.osplit ? map.oshift : 0)) * map.group_pad + q + (q >= map.split ? map.shift : 0);
+      dst[p * ld_dst + col] = t[threadIdx.x][y];
+    }
   }
 }
 
@@ -227,10 +239,11 @@ Status sox_selfenergy_imag(Context& c, const rigw_sox_problem& pr, double* sigma
   if (ngp != ng) RIGW_CUDA_TRY(cudaMemsetAsync(at, 0, size_t(naux) * lda * 8, s));
   {
     const dim3 blk(32, 8);
+    const long long never = 1LL << 62;
     sox_transpose_kernel<<<dim3(unsigned((nov + 31) / 32), unsigned((naux + 31) / 32)), blk, 0, s>>>(
-        mov, nov, naux, nov, novp, bt, novp);
+        mov, nov, naux, TransposeMap{nov, novp, never, 0, never, 0}, bt, novp);
     sox_transpose_kernel<<<dim3(unsigned(((long long)nsig * ng + 31) / 32), unsigned((naux + 31) / 32)), blk, 0,
-                           s>>>(mpq, (long long)nsig * ng, naux, ng, ngp, at, lda);
+                           s>>>(mpq, (long long)nsig * ng, naux, TransposeMap{ng, ngp, never, 0, never, 0}, at, lda);
     RIGW_CUDA_TRY(cudaGetLastError());
     launches += 2;
   }
@@ -328,6 +341,339 @@ Status sox_selfenergy_imag(Context& c, const rigw_sox_problem& pr, double* sigma
   st.stage_ms[1] = ms_gemm;
   st.stage_ms[3] = ms_sum;
   st.total_ms = total;
+  st.kernel_launches = launches;
+  st.chunks = (nsig + pc - 1) / pc;
+  st.waves = 1;
+  st.device_bytes_in_use = c.in_use;
+  st.device_bytes_peak = c.peak;
+  c.last_stats = st;
+  return Status::ok();
+}
+
+
+// ---- SOSEX on the imaginary axis (sosex_selfenergy_imag_grid) -----------------
+//
+// Sigma_m(z) = f/(2 pi) sum_k w_k sum_r [K_k(m, r) / (z + i w_k - e_r) + conj(K_k(m, r)) / (z - i w_k - e_r)]
+// K_k(m, r)  = sum_{i,a} T_k(r; i,a) [B1(r; i,a) / (i w_k - D) - B2(r; i,a) / (i w_k + D)],  D = e_a - e_i
+// T_k(r; i,a) = (r m|W - v|i a) = sum_Q R_k[Q][r] M[Q](i,a),  R_k = W~_k M(., m),  W~_k = Y_k^T Y_k - 1
+// B1 = (r a|i m), B2 = (r i|a m)  (bare, frequency independent)
+//
+// The reference recomputes its bra-kets for every evaluation point and sign
+// (:2262-2466); K_k does not depend on z, and the s = -1 sum is the conjugate of
+// the s = +1 one, so the products run once per (Sigma state, frequency).  The
+// window tensor is held once, transposed: Mft[P][pos(r) * wq + pos(q)], with the
+// occupied and empty blocks each padded to an even width (pos).
+namespace {
+
+constexpr int kSosexThreads = 256;
+
+struct SosexKArgs {
+  const double* T;     // [pc][wq][niap], rows at window positions, columns i * nvp + a
+  const double* B1;
+  const double* B2;
+  const double* epos;  // [wq] energy_g at window positions (0 in the gaps)
+  int no, nv, nop, nvp, wq;
+  long long niap;
+  double om;           // w_k
+  double* K;           // [nsig][nwp][wq][2]
+  int k, nwp, p0;
+};
+
+// Sum of (a, b) over the block in a fixed order; thread 0 holds the result.
+__device__ __forceinline__ void block_sum2(double& a, double& b, double (*red)[2]) {
+  for (int o = 16; o > 0; o >>= 1) {
+    a += __shfl_xor_sync(0xffffffffu, a, o);
+    b += __shfl_xor_sync(0xffffffffu, b, o);
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  if (lane == 0) {
+    red[warp][0] = a;
+    red[warp][1] = b;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = 0.0;
+    for (int wp = 0; wp < kSosexThreads / 32; ++wp) {
+      a += red[wp][0];
+      b += red[wp][1];
+    }
+  }
+}
+
+// One block per (window row r, Sigma state of the chunk): K_k(m, r).
+__global__ void __launch_bounds__(kSosexThreads) sosex_k_kernel(SosexKArgs a) {
+  __shared__ double red[kSosexThreads / 32][2];
+  const int r = blockIdx.x, ml = blockIdx.y;
+  const long long base = ((long long)ml * a.wq + r) * a.niap;
+  const double om2 = a.om * a.om;
+  double sr = 0.0, si = 0.0;
+  for (long long ia = threadIdx.x; ia < a.niap; ia += kSosexThreads) {
+    const int i = int(ia / a.nvp), av = int(ia % a.nvp);
+    if (i >= a.no || av >= a.nv) continue;
+    const double d = a.epos[a.nop + av] - a.epos[i];
+    const double t = a.T[base + ia], b1 = a.B1[base + ia], b2 = a.B2[base + ia];
+    const double inv = __drcp_rn(fma(d, d, om2));
+    // B1 / (i w - D) - B2 / (i w + D) = [-D (B1 + B2) - i w (B1 - B2)] / (D^2 + w^2)
+    sr = fma(-t * d * (b1 + b2), inv, sr);
+    si = fma(-t * (b1 - b2), inv, si);
+  }
+  block_sum2(sr, si, red);
+  if (threadIdx.x == 0) {
+    double* out = a.K + (((long long)(a.p0 + ml) * a.nwp + a.k) * a.wq + r) * 2;
+    out[0] = sr;
+    out[1] = a.om * si;
+  }
+}
+
+// One block per (Sigma state, evaluation point): the sum over (k, r).
+__global__ void __launch_bounds__(kSosexThreads)
+sosex_sigma_kernel(const double* __restrict__ K, const double* __restrict__ omega, const double* __restrict__ weight,
+                   const double* __restrict__ epos, const double* __restrict__ z, int nwp, int wq, int nw,
+                   double scale, double* __restrict__ out) {
+  __shared__ double red[kSosexThreads / 32][2];
+  const int m = blockIdx.x, iz = blockIdx.y;
+  const double zr = z[2 * iz], zi = z[2 * iz + 1];
+  double sr = 0.0, si = 0.0;
+  const int n = nwp * wq;
+  for (int t = threadIdx.x; t < n; t += kSosexThreads) {
+    const int k = t / wq, r = t % wq;
+    const double* kk = K + (((long long)m * nwp + k) * wq + r) * 2;
+    const double kr = kk[0], ki = kk[1], wk = weight[k], om = omega[k];
+    const double x = zr - epos[r];
+    // K / (x + i (zi + w)) + conj(K) / (x + i (zi - w))
+    const double y1 = zi + om, y2 = zi - om;
+    const double i1 = __drcp_rn(fma(x, x, y1 * y1)), i2 = __drcp_rn(fma(x, x, y2 * y2));
+    sr += wk * ((kr * x + ki * y1) * i1 + (kr * x - ki * y2) * i2);
+    si += wk * ((ki * x - kr * y1) * i1 + (-ki * x - kr * y2) * i2);
+  }
+  block_sum2(sr, si, red);
+  if (threadIdx.x == 0) {
+    out[((long long)m * nw + iz) * 2] = scale * sr;
+    out[((long long)m * nw + iz) * 2 + 1] = scale * si;
+  }
+}
+
+Status upload_items(Context& c, DeviceBuffer* buf, const std::vector<GemmItem>& items, const char* what) {
+  if (items.empty()) return Status::ok();
+  RIGW_TRY(buf->allocate(&c, items.size() * sizeof(GemmItem), what));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(buf->data(), items.data(), items.size() * sizeof(GemmItem), cudaMemcpyHostToDevice,
+                                c.stream));
+  return Status::ok();
+}
+
+}  // namespace
+
+Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem& pr, double* sigma) {
+  const int no = pr.nocc, nv = pr.nvirt, naux = pr.naux, nsig = pr.nsig, nw = pr.nomega_calc;
+  const int ng = no + nv;
+  if (no <= 0 || nv <= 0 || naux <= 0 || nsig <= 0 || nw <= 0 || nw > 65535 || !pr.m_full || !pr.energy ||
+      !pr.omega_calc || !sigma || pr.sig_first < 0 || pr.sig_first + nsig > ng)
+    return Status::fail(RIGW_ERR_ARG, "sosex_selfenergy_imag: invalid arguments");
+  const ProbDev& pd = w.plan->problems()[0].dev;
+  if (naux != pd.naux) return Status::fail(RIGW_ERR_ARG, "sosex_selfenergy_imag: naux differs from the polarizability");
+  if (!pd.want_identity)
+    return Status::fail(RIGW_ERR_UNSUPPORTED, "sosex_selfenergy_imag: the polarizability was solved without W (QP-only)");
+  NvtxRange range("SOSEX self-energy");
+  const bool on_dev = (pr.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
+  const int nop = no + (no & 1), nvp = nv + (nv & 1), wq = nop + nvp;
+  const long long niap = (long long)nop * nvp, ldm = (long long)wq * wq;
+  const int naux_e = naux + (naux & 1), npad = pd.npad, nwp = pd.nomega;
+  if (ldm >= (1LL << 31) || niap >= (1LL << 31))
+    return Status::fail(RIGW_ERR_ARG, "sosex_selfenergy_imag: window beyond 2^31 operand columns");
+  auto pos = [&](int q) { return q < no ? q : q + (nop - no); };
+  cudaStream_t s = c.stream;
+  struct Events {
+    cudaEvent_t e[4] = {};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  for (cudaEvent_t& x : ev.e) RIGW_CUDA_TRY(cudaEventCreate(&x));
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[0], s));
+
+  // window tensor, transposed once: Mft[P][pos(r) * wq + pos(q)]
+  DeviceBuffer b_in, b_mft, b_e, b_z;
+  const double* min = pr.m_full;
+  if (!on_dev) {
+    RIGW_TRY(b_in.allocate(&c, size_t(ng) * ng * naux * 8, "sosex window tensor"));
+    RIGW_CUDA_TRY(cudaMemcpyAsync(b_in.data(), pr.m_full, size_t(ng) * ng * naux * 8, cudaMemcpyHostToDevice, s));
+    min = reinterpret_cast<const double*>(b_in.data());
+  }
+  RIGW_TRY(b_mft.allocate(&c, size_t(naux) * ldm * 8, "sosex window tensor^T"));
+  double* mft = reinterpret_cast<double*>(b_mft.data());
+  RIGW_CUDA_TRY(cudaMemsetAsync(mft, 0, size_t(naux) * ldm * 8, s));
+  sox_transpose_kernel<<<dim3(unsigned(((long long)ng * ng + 31) / 32), unsigned((naux + 31) / 32)), dim3(32, 8), 0,
+                         s>>>(min, (long long)ng * ng, naux, TransposeMap{ng, wq, no, nop - no, no, nop - no}, mft, ldm);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  int launches = 1;
+  std::vector<double> epos(wq, 0.0);
+  {
+    std::vector<double> e(ng);
+    RIGW_CUDA_TRY(cudaMemcpy(e.data(), pr.energy, size_t(ng) * 8, cudaMemcpyDefault));
+    for (int q = 0; q < ng; ++q) epos[pos(q)] = e[q];
+  }
+  std::vector<double> om(nwp);
+  RIGW_CUDA_TRY(cudaMemcpy(om.data(), pd.omega, size_t(nwp) * 8, cudaMemcpyDeviceToHost));
+  RIGW_TRY(b_e.allocate(&c, size_t(wq) * 8, "sosex energies"));
+  RIGW_TRY(b_z.allocate(&c, size_t(nw) * 16, "sosex omega_calc"));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_e.data(), epos.data(), size_t(wq) * 8, cudaMemcpyHostToDevice, s));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_z.data(), pr.omega_calc, size_t(nw) * 16, cudaMemcpyDefault, s));
+  const double* de = reinterpret_cast<const double*>(b_e.data());
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[1], s));
+
+  // Sigma states per pass: T, B1, B2 and R of a chunk below ~2 GB and below half
+  // of what the HBM budget has left
+  const size_t per_m = (size_t(3) * wq * niap + size_t(naux_e) * wq) * 8;
+  size_t cap = size_t(2) << 30;
+  if (c.budget > 0) cap = std::min(cap, c.budget > c.in_use ? (c.budget - c.in_use) / 2 : size_t(0));
+  const int pc = int(std::max<size_t>(1, std::min<size_t>(size_t(nsig), cap / per_m)));
+  DeviceBuffer b_t, b_b1, b_b2, b_r, b_wt, b_k, b_out, b_iw;
+  RIGW_TRY(b_t.allocate(&c, size_t(pc) * wq * niap * 8, "sosex T"));
+  RIGW_TRY(b_b1.allocate(&c, size_t(pc) * wq * niap * 8, "sosex B1"));
+  RIGW_TRY(b_b2.allocate(&c, size_t(pc) * wq * niap * 8, "sosex B2"));
+  RIGW_TRY(b_r.allocate(&c, size_t(pc) * naux_e * wq * 8, "sosex R"));
+  RIGW_TRY(b_wt.allocate(&c, size_t(npad) * npad * 8, "sosex W~"));
+  RIGW_TRY(b_k.allocate(&c, size_t(nsig) * nwp * wq * 16, "sosex K"));
+  double* dt = reinterpret_cast<double*>(b_t.data());
+  double* db1 = reinterpret_cast<double*>(b_b1.data());
+  double* db2 = reinterpret_cast<double*>(b_b2.data());
+  double* dr = reinterpret_cast<double*>(b_r.data());
+  double* wt = reinterpret_cast<double*>(b_wt.data());
+  double* dk = reinterpret_cast<double*>(b_k.data());
+  // rows at the gaps of the window positions stay zero in B1 and B2 (no item writes them)
+  RIGW_CUDA_TRY(cudaMemsetAsync(db1, 0, size_t(pc) * wq * niap * 8, s));
+  RIGW_CUDA_TRY(cudaMemsetAsync(db2, 0, size_t(pc) * wq * niap * 8, s));
+  double* out = sigma;
+  if (!on_dev) {
+    RIGW_TRY(b_out.allocate(&c, size_t(nsig) * nw * 16, "sosex sigma"));
+    out = reinterpret_cast<double*>(b_out.data());
+  }
+  // W~_k = Y_k^T Y_k - 1 for every frequency (Y_k = U_k^-T, the identity part of the resident solve)
+  std::vector<GemmItem> iw;
+  for (int k = 0; k < nwp; ++k) {
+    const double* y = pd.rhs + size_t(k) * npad * pd.ldb;
+    for (int i0 = 0; i0 < npad; i0 += 128)
+      for (int j0 = 0; j0 < npad; j0 += 128) {
+        GemmItem g{};
+        g.A = y + i0;
+        g.lda = pd.ldb;
+        g.B = y + j0;
+        g.ldb = pd.ldb;
+        g.C = wt + size_t(i0) * npad + j0;
+        g.ldc = npad;
+        g.m = std::min(128, npad - i0);
+        g.n = std::min(128, npad - j0);
+        g.k = npad;
+        g.flags = kSubIdentity;
+        g.diag = i0 - j0;
+        g.alpha = 1.0;
+        iw.push_back(g);
+      }
+  }
+  const int nwt = int(iw.size()) / nwp;
+  RIGW_TRY(upload_items(c, &b_iw, iw, "sosex W~ items"));
+  const GemmItem* d_iw = reinterpret_cast<const GemmItem*>(b_iw.data());
+  for (int p0 = 0; p0 < nsig; p0 += pc) {
+    const int pcn = std::min(pc, nsig - p0);
+    std::vector<GemmItem> ib, ir, it;
+    for (int ml = 0; ml < pcn; ++ml) {
+      const long long colm = (long long)pos(pr.sig_first + p0 + ml) * wq;   // columns of M(., m) in Mft
+      for (int q = 0; q < ng; ++q) {
+        const int r = pos(q);
+        for (int i0 = 0; i0 < nop; i0 += 64)   // 64-row items of the 64 x 128 tile engine
+          for (int a0 = 0; a0 < nvp; a0 += 128) {
+            GemmItem g{};
+            g.ldc = nvp;
+            g.m = std::min(64, nop - i0);
+            g.n = std::min(128, nvp - a0);
+            g.k = naux;
+            g.alpha = 1.0;
+            g.lda = g.ldb = int(ldm);
+            // B1[r][i][a] = sum_P M[P](i, m) M[P](r, a)
+            g.A = mft + colm + i0;
+            g.B = mft + (long long)r * wq + nop + a0;
+            g.C = db1 + ((long long)ml * wq + r) * niap + (long long)i0 * nvp + a0;
+            ib.push_back(g);
+            // B2[r][i][a] = sum_P M[P](r, i) M[P](a, m)
+            g.A = mft + (long long)r * wq + i0;
+            g.B = mft + colm + nop + a0;
+            g.C = db2 + ((long long)ml * wq + r) * niap + (long long)i0 * nvp + a0;
+            ib.push_back(g);
+          }
+      }
+      // R[Q][r] = sum_P W~[P][Q] M[P](r, m)
+      for (int q0 = 0; q0 < naux_e; q0 += 128)
+        for (int r0 = 0; r0 < wq; r0 += 128) {
+          GemmItem g{};
+          g.A = wt + q0;
+          g.lda = npad;
+          g.B = mft + colm + r0;
+          g.ldb = int(ldm);
+          g.C = dr + (size_t(ml) * naux_e + q0) * wq + r0;
+          g.ldc = wq;
+          g.m = std::min(128, naux_e - q0);
+          g.n = std::min(128, wq - r0);
+          g.k = naux;
+          g.alpha = 1.0;
+          ir.push_back(g);
+        }
+      // T[r][i][a] = sum_Q R[Q][r] M[Q](i, a)
+      for (int r0 = 0; r0 < wq; r0 += 128)
+        for (int i = 0; i < no; ++i)
+          for (int a0 = 0; a0 < nvp; a0 += 128) {
+            GemmItem g{};
+            g.A = dr + size_t(ml) * naux_e * wq + r0;
+            g.lda = wq;
+            g.B = mft + (long long)i * wq + nop + a0;
+            g.ldb = int(ldm);
+            g.C = dt + ((long long)ml * wq + r0) * niap + (long long)i * nvp + a0;
+            g.ldc = int(niap);
+            g.m = std::min(128, wq - r0);
+            g.n = std::min(128, nvp - a0);
+            g.k = naux;
+            g.alpha = 1.0;
+            it.push_back(g);
+          }
+    }
+    DeviceBuffer b_ib, b_ir, b_it;
+    RIGW_TRY(upload_items(c, &b_ib, ib, "sosex B items"));
+    RIGW_TRY(upload_items(c, &b_ir, ir, "sosex R items"));
+    RIGW_TRY(upload_items(c, &b_it, it, "sosex T items"));
+    launch_dgemm_64x128(reinterpret_cast<const GemmItem*>(b_ib.data()), int(ib.size()), 1, s);
+    RIGW_CUDA_TRY(cudaGetLastError());
+    ++launches;
+    for (int k = 0; k < nwp; ++k) {
+      launch_dgemm_128x128(d_iw + size_t(k) * nwt, nwt, 1, s);
+      launch_dgemm_128x128(reinterpret_cast<const GemmItem*>(b_ir.data()), int(ir.size()), 1, s);
+      launch_dgemm_128x128(reinterpret_cast<const GemmItem*>(b_it.data()), int(it.size()), 1, s);
+      RIGW_CUDA_TRY(cudaGetLastError());
+      SosexKArgs a{dt, db1, db2, de, no, nv, nop, nvp, wq, niap, om[k], dk, k, nwp, p0};
+      sosex_k_kernel<<<dim3(wq, pcn), kSosexThreads, 0, s>>>(a);
+      RIGW_CUDA_TRY(cudaGetLastError());
+      launches += 4;
+    }
+    // the item buffers of this chunk are released at the end of the iteration
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  }
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[2], s));
+  sosex_sigma_kernel<<<dim3(nsig, nw), kSosexThreads, 0, s>>>(dk, pd.omega, pd.weight, de,
+                                                              reinterpret_cast<const double*>(b_z.data()), nwp, wq,
+                                                              nw, pr.factor_sosex / (2.0 * M_PI), out);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  ++launches;
+  if (!on_dev) RIGW_CUDA_TRY(cudaMemcpyAsync(sigma, out, size_t(nsig) * nw * 16, cudaMemcpyDeviceToHost, s));
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[3], s));
+  RIGW_CUDA_TRY(cudaEventSynchronize(ev.e[3]));
+  float t01 = 0.0f, t12 = 0.0f, t23 = 0.0f;
+  cudaEventElapsedTime(&t01, ev.e[0], ev.e[1]);
+  cudaEventElapsedTime(&t12, ev.e[1], ev.e[2]);
+  cudaEventElapsedTime(&t23, ev.e[2], ev.e[3]);
+  rigw_stats st{};
+  st.stage_ms[0] = t01;   // upload and transpose of the window tensor
+  st.stage_ms[1] = t12;   // products (B1, B2, W~, R, T) and the K reductions
+  st.stage_ms[3] = t23;   // sums over (frequency, r) and the download
+  st.total_ms = double(t01) + t12 + t23;
   st.kernel_launches = launches;
   st.chunks = (nsig + pc - 1) / pc;
   st.waves = 1;

@@ -76,6 +76,14 @@ class SoxProblem(C.Structure):
     ]
 
 
+class SosexProblem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nocc", C.c_int), ("nvirt", C.c_int), ("m_full", _dp), ("nsig", C.c_int),
+        ("sig_first", C.c_int), ("energy", _dp), ("nomega_calc", C.c_int), ("omega_calc", _dp),
+        ("factor_sosex", C.c_double), ("flags", C.c_int),
+    ]
+
+
 def efermi_of(inst) -> float:
     """se_init's efermi from the energies in G: half-way between the highest
     energy of state nhomo_G and the lowest of state nhomo_G + 1 over the spin
@@ -153,6 +161,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_wpol_release.argtypes = [C.c_void_p, C.c_void_p]
     lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
     lib.rigw_sox_selfenergy_imag.argtypes = [C.c_void_p, C.POINTER(SoxProblem), _dp]
+    lib.rigw_sosex_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SosexProblem), _dp]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -503,6 +512,52 @@ class Engine:
             wpol.release()
         oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
         sigma = sigma + self.sox_selfenergy_imag_grid(inst, oc, m_ov)
+        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc)
+        out.erpa, out.egw = erpa, egw
+        return out
+
+    def sosex_selfenergy_imag_grid(self, wpol: "WPol", inst, m_full, omega_calc,
+                                   factor_sosex: float = 1.0) -> np.ndarray:
+        """SOSEX (without its SOX part) on the evaluation points ``omega_calc`` for
+        the Sigma states of ``inst`` (sosex_selfenergy_imag_grid,
+        src/m_g3w2_selfenergy.f90:2200-2478), [nsig, nomega_calc] complex, with
+        W from the resident factors of ``wpol``.  ``m_full`` is the window tensor
+        [nstate_G, nstate_G, naux] (``synth.with_window``)."""
+        cg = getattr(inst, "ncore_g", 0)
+        mf = np.ascontiguousarray(m_full, dtype=np.float64)
+        ng = mf.shape[0]
+        e = inst.energy if getattr(inst, "energy_g", None) is None else inst.energy_g
+        ew = np.ascontiguousarray(np.asarray(e, dtype=np.float64)[cg:cg + ng])
+        oc = np.ascontiguousarray(np.stack([np.real(omega_calc), np.imag(omega_calc)], -1), dtype=np.float64)
+        sp = SosexProblem()
+        sp.naux = inst.naux
+        sp.nocc = getattr(inst, "ncore_w", 0) + inst.nocc - cg
+        sp.nvirt = ng - sp.nocc
+        sp.m_full, sp.energy, sp.omega_calc = _ptr(mf), _ptr(ew), _ptr(oc)
+        sp.nsig = inst.nsemax - inst.nsemin + 1
+        sp.sig_first = inst.nsemin - 1 - cg
+        sp.nomega_calc = oc.shape[0]
+        sp.factor_sosex = factor_sosex
+        out = np.zeros((sp.nsig, sp.nomega_calc, 2))
+        self._check(self._lib.rigw_sosex_selfenergy_imag(self._h, wpol.handle, C.byref(sp), _ptr(out)),
+                    "rigw_sosex_selfenergy_imag")
+        return out[..., 0] + 1j * out[..., 1]
+
+    def gw_sosex_imag(self, inst, m_full, precision: int = RIGW_FP64, factor_sosex: float = 1.0) -> G0W0Output:
+        """GW+SOSEX on the imaginary axis (postscf 'GW+SOSEX_PADE'; factor_sosex = 2
+        for 'GW+2SOSEX_PADE'): W, then Sigma_c + Sigma^SOX + factor_sosex Sigma^SOSEX
+        on the evaluation points, then the Pade continuation and the QP equation
+        (src/m_selfenergy_evaluation.f90:494-503)."""
+        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
+        cg = getattr(inst, "ncore_g", 0)
+        no = getattr(inst, "ncore_w", 0) + inst.nocc - cg
+        try:
+            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst)
+            sigma = sigma + self.sosex_selfenergy_imag_grid(wpol, inst, m_full, oc, factor_sosex)
+        finally:
+            wpol.release()
+        sigma = sigma + self.sox_selfenergy_imag_grid(inst, oc, m_full[:no, no:])
         out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc)
         out.erpa, out.egw = erpa, egw
         return out

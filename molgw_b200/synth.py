@@ -23,7 +23,7 @@ LUMO = nocc+1; the Sigma range is nsemin..nsemax = HOMO..LUMO.
 """
 from __future__ import annotations
 
-from dataclasses import dataclass
+from dataclasses import dataclass, replace
 
 import numpy as np
 
@@ -130,6 +130,27 @@ def make_instance(nocc: int, nvirt: int, naux: int, nomega: int, seed: int,
     return GWInstance(nocc=nocc, nvirt=nvirt, naux=naux, nomega=nomega, energy=energy,
                       occupation=occupation, m_ia=m_ia, m_sigma=m_sigma,
                       nsemin=homo, nsemax=lumo, seed=seed)
+
+
+def with_window(inst: GWInstance, seed: int = 0) -> tuple[GWInstance, np.ndarray]:
+    """The full 3-center tensor of the window, [nstate, nstate, naux] symmetric
+    in its first two indices (eri_3center_mo(:, q, r) over ncore_G+1 ..
+    nvirtual_G-1), for the vertex corrections that need the occupied-occupied
+    and empty-empty blocks.  The occupied-empty block is ``inst.m_ia``; the
+    other blocks are seeded N(0, 1) scaled like it; ``m_ia`` and ``m_sigma`` of
+    the returned instance are re-read from the tensor so that every input agrees."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    no, nv, naux = inst.m_ia.shape
+    s = float(inst.m_ia.std())
+    m = np.empty((no + nv, no + nv, naux))
+    oo = rng.standard_normal((no, no, naux)) * s
+    vv = rng.standard_normal((nv, nv, naux)) * s
+    m[:no, :no] = 0.5 * (oo + oo.transpose(1, 0, 2))
+    m[no:, no:] = 0.5 * (vv + vv.transpose(1, 0, 2))
+    m[:no, no:] = inst.m_ia
+    m[no:, :no] = inst.m_ia.transpose(1, 0, 2)
+    sig = np.arange(inst.nsemin - 1, inst.nsemax)
+    return replace(inst, m_ia=np.ascontiguousarray(m[:no, no:]), m_sigma=np.ascontiguousarray(m[sig])), m
 
 
 # Workloads of the benchmark table --------------------------------------------

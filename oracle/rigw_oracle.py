@@ -27,6 +27,8 @@ the same BLAS/LAPACK call sequence (through SciPy's bundled OpenBLAS):
 * ``sox_selfenergy_imag``     src/m_g3w2_selfenergy.f90:2482-2591 (GW+SOX on the
                               imaginary axis, added before the Pade fit,
                               src/m_selfenergy_evaluation.f90:494-503)
+* ``sosex_selfenergy_imag``   src/m_g3w2_selfenergy.f90:2200-2478 (GW+SOSEX on the
+                              imaginary axis, after SOX, :498-500)
 
 Pinning: the reference's own known answer that needs no Gaussian integrals is
 the analytic RPA correlation energy of bulk LiH from the shipped CC4S tensor
@@ -547,7 +549,8 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
               step_sigma_calc: float = 0.075, eta: float = 0.01,
               exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
               ncore_w: int = 0, energy_g: np.ndarray | None = None, sox: bool = False,
-              m_ov_g: np.ndarray | None = None) -> G0W0Result:
+              m_ov_g: np.ndarray | None = None, factor_sosex: float | None = None,
+              m_full: np.ndarray | None = None) -> G0W0Result:
     """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
     (src/m_selfenergy_evaluation.f90:214-246, 587-611).
 
@@ -562,6 +565,9 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     ``sox``: GW+SOX_PADE, Sigma^SOX from energy_g added to sigma_calc before the
     fit (:494-503); ``m_ov_g`` is the occupied x empty block of the G window
     (default ``m_ia``, the W window, when both windows start at the same state).
+    ``factor_sosex``: GW+SOSEX_PADE (GW+2SOSEX_PADE with 2), SOX and then
+    factor_sosex x SOSEX added (:496-500); ``m_full`` is the G-window tensor
+    [nstate_G, nstate_G, naux].
     """
     eg = energy if energy_g is None else energy_g
     occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
@@ -580,6 +586,11 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
             raise ValueError("sox: pass m_ov_g when the W and G windows differ")
         window = eg[rng.ncore_g: rng.ncore_g + m_sigma.shape[1]]
         se.sigma_calc += sox_selfenergy_imag(window, m_sigma, mov, se.omega_calc).T
+    if factor_sosex is not None:
+        window = eg[rng.ncore_g: rng.ncore_g + m_sigma.shape[1]]
+        sig = list(range(rng.nsemin - 1 - rng.ncore_g, rng.nsemax - rng.ncore_g))
+        se.sigma_calc += sosex_selfenergy_imag(window, m_full, rng.nhomo_g - rng.ncore_g, sig, sf.chi, sf.omega,
+                                               sf.weight_quad, se.omega_calc, factor_sosex).T
     if technique == "pade":
         se_pade_fit(se, eta)
     else:
@@ -719,3 +730,90 @@ def sox_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, nocc: in
                     v2 = eri(a, j, c, p)
                     out[ip] -= v1 * v2 / (z - energy_g[a] - energy_g[c] + energy_g[j])
     return out
+
+
+def sosex_selfenergy_imag(energy_g: np.ndarray, m_full: np.ndarray, nocc: int, sig_states,
+                          chi: np.ndarray, omega_p: np.ndarray, weight_p: np.ndarray,
+                          omega_calc: np.ndarray, factor_sosex: float = 1.0) -> np.ndarray:
+    """SOSEX without its SOX part on the evaluation points of the imaginary axis,
+    sosex_selfenergy_imag_grid (src/m_g3w2_selfenergy.f90:2200-2478), one spin,
+    with W - v = v^1/2 chi v^1/2 = ``chi`` [nomega', naux, naux] on the grid
+    (omega'_k, w_k) of wpol_imag.
+
+    ``m_full`` [nstate, nstate, naux] is eri_3center_mo over the G window
+    (occupied states 0 .. nocc-1 first), ``sig_states`` the 0-based window indices
+    of the Sigma states.  With T(r; i, a) = (r m|W-v|i a), B1 = (r a|i m),
+    B2 = (r i|a m) and D = e_a - e_i, the sums of :2316-2453 are
+
+      Sigma_m(z) = f/(2 pi) sum_k w_k sum_{s=+-1} sum_{r,i,a}
+                   T / (z + s i w_k - e_r) [B1 / (s i w_k - D) - B2 / (s i w_k + D)]
+
+    (the bra-ket of W(i w +- i w') is the bare v, chi_wwp = 1 at :2283-2286).
+    The z-independent inner sums K_k(r) are formed once per frequency; the
+    s = -1 term is the complex conjugate of the s = +1 one for real integrals."""
+    no = nocc
+    nv = m_full.shape[0] - no
+    e_o, e_v = energy_g[:no], energy_g[no:no + nv]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    dlt = e_v[None, :] - e_o[:, None]                                  # [i, a]
+    m_ov = m_full[:no, no:]                                            # [i, a, P]
+    out = np.zeros((len(sig_states), z.size), dtype=np.complex128)
+    nst = no + nv
+    m_ov2 = m_ov.reshape(no * nv, -1)
+    for ip, m in enumerate(sig_states):
+        b1 = (m_full[:, no:] @ m_full[:no, m].T).transpose(0, 2, 1)   # (r a|i m) as [r, i, a]
+        b2 = m_full[:, :no] @ m_full[no:, m].T                          # (r i|a m) as [r, i, a]
+        for k, (wk, om) in enumerate(zip(weight_p, omega_p)):
+            t = ((m_full[:, m] @ chi[k]) @ m_ov2.T).reshape(nst, no, nv)   # (r m|W-v|i a)
+            g = b1 / (1j * om - dlt)[None] - b2 / (1j * om + dlt)[None]
+            kr = (t * g).sum(axis=(1, 2))                             # K_k(r), s = +1
+            den_p = z[:, None] + 1j * om - energy_g[None, :no + nv]
+            den_m = z[:, None] - 1j * om - energy_g[None, :no + nv]
+            out[ip] += wk * ((kr[None] / den_p).sum(axis=1) + (kr.conj()[None] / den_m).sum(axis=1))
+    return factor_sosex * out / (2.0 * PI)
+
+
+def sosex_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, nocc: int, sig_states,
+                                chi: np.ndarray, omega_p: np.ndarray, weight_p: np.ndarray,
+                                omega_calc: np.ndarray, factor_sosex: float = 1.0) -> np.ndarray:
+    """Loop-for-loop restatement of sosex_selfenergy_imag_grid
+    (src/m_g3w2_selfenergy.f90:2262-2466) for small cases: for every omega',
+    sign and evaluation point, the bra-kets of :2316-2336 and :2385-2408 as
+    matrix products for each empty (resp. occupied) state, then the double loops
+    over (r, i) and (a, r)."""
+    no = nocc
+    nst = m_full.shape[0]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    out = np.zeros((len(sig_states), z.size), dtype=np.complex128)
+    for ip, m in enumerate(sig_states):
+        for k in range(len(omega_p)):
+            chi_wp = chi[k]
+            for isignp in (1, -1):
+                for iz in range(z.size):
+                    s = 0.0 + 0.0j
+                    eri3_r_m = m_full[:, m].T                              # (naux, r)
+                    eri3_i_m = m_full[:no, m].T                            # (naux, i)
+                    for a in range(no, nst):
+                        eri3_i_a = m_full[:no, a].T                        # (naux, i)
+                        eri3_r_a = m_full[:, a].T                          # (naux, r)
+                        braket1_ri = eri3_r_m.T @ (chi_wp @ eri3_i_a)      # (r, i)
+                        braket2_ri = eri3_r_a.T @ eri3_i_m                 # (r, i), chi_wwp = 1
+                        for r in range(nst):
+                            for i in range(no):
+                                d1 = z[iz] + isignp * 1j * omega_p[k] - energy_g[r]
+                                d2 = isignp * 1j * omega_p[k] + energy_g[i] - energy_g[a]
+                                s += weight_p[k] * braket1_ri[r, i] / d1 * braket2_ri[r, i] / d2 / (2.0 * PI)
+                    eri3_a_m = m_full[no:, m].T                            # (naux, a)
+                    for i in range(no):
+                        eri3_a_i = m_full[no:, i].T                        # (naux, a)
+                        eri3_r_i = m_full[:, i].T                          # (naux, r)
+                        braket1_ra = eri3_r_m.T @ (chi_wp @ eri3_a_i)      # (r, a)
+                        braket2_ra = eri3_r_i.T @ eri3_a_m                 # (r, a)
+                        for a in range(no, nst):
+                            for r in range(nst):
+                                d1 = z[iz] + isignp * 1j * omega_p[k] - energy_g[r]
+                                d2 = isignp * 1j * omega_p[k] + energy_g[a] - energy_g[i]
+                                s -= (weight_p[k] * braket1_ra[r, a - no] / d1 * braket2_ra[r, a - no] / d2
+                                      / (2.0 * PI))
+                    out[ip, iz] += s
+    return factor_sosex * out

@@ -106,6 +106,7 @@ def test_bad_arguments_return_status_not_abort(lib):
     assert lib.rigw_create(None, 0, 0) == 1
     assert lib.rigw_g0w0(None, None, None) == 1
     assert lib.rigw_sox_selfenergy_imag(None, None, None) == 1
+    assert lib.rigw_sosex_selfenergy_imag(None, None, None, None) == 1
     assert lib.rigw_version() == 1
 
 
@@ -170,3 +171,26 @@ def test_sox_problem_layout_matches_ctypes(tmp_path):
     assert int(out["S"]) == C.sizeof(SoxProblem)
     for f in fields:
         assert int(out[f"X {f}"]) == getattr(SoxProblem, f).offset, f
+
+
+def test_sosex_problem_layout_matches_ctypes(tmp_path):
+    from molgw_b200.rigw import SosexProblem
+    fields = [f for f, _ in SosexProblem._fields_]
+    body = "".join(f'  printf("X {f} %zu\\n", offsetof(rigw_sosex_problem, {f}));\n' for f in fields)
+    src = tmp_path / "sosex.c"
+    src.write_text(textwrap.dedent(f"""
+        #include <stdio.h>
+        #include <stddef.h>
+        #include "rigw.h"
+        int main(void) {{
+          printf("S %zu\\n", sizeof(rigw_sosex_problem));
+        {body}  return 0;
+        }}
+    """))
+    exe = tmp_path / "sosex"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in
+               subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if line)
+    assert int(out["S"]) == C.sizeof(SosexProblem)
+    for f in fields:
+        assert int(out[f"X {f}"]) == getattr(SosexProblem, f).offset, f
