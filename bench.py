@@ -481,7 +481,9 @@ def run_sox_line(args):
     (element x point)/s over Nocc^2 Nvirt + Nocc Nvirt (Nvirt+1)/2 elements per
     state; the oracle's Sigma^SOX timed on the host cores beside it.  value = the
     whole GW+SOX solve (W, Sigma_c, Sigma^SOX, Pade, QP) per second on the 840
-    instance through the host-pointer calls.  One JSON line."""
+    instance through the host-pointer calls.  "sosex": Sigma^SOSEX from the
+    resident W on the 840 instance with its full window tensor
+    (synth.with_window), timed and checked against the oracle.  One JSON line."""
     import torch
     from threadpoolctl import threadpool_limits
     from molgw_b200 import build, synth
@@ -536,6 +538,35 @@ def run_sox_line(args):
         walls.append((time.perf_counter() - t0) * 1e3)
     gw = eng.g0w0(inst)
     shift = float(np.abs(res.energy_qp_g - gw.energy_qp_g).max() * HA_EV)
+    # Sigma^SOSEX from the resident W on the same instance with a full window tensor
+    inst_w, m_full = synth.with_window(synth.single_instance_840(), seed=3)
+    m_full = pinned_copy(m_full)
+    z = efermi_of(inst_w) + 1j * inst_w.step_sigma_calc * np.arange(inst_w.nomega_sigma_calc)
+    _, _, wpol = eng.polarizability_grid_scalapack(inst_w)
+    try:
+        eng.sosex_selfenergy_imag_grid(wpol, inst_w, m_full, z)
+        stats, walls_x = [], []
+        for _ in range(3):
+            t0 = time.perf_counter()
+            out = eng.sosex_selfenergy_imag_grid(wpol, inst_w, m_full, z)
+            walls_x.append((time.perf_counter() - t0) * 1e3)
+            stats.append(eng.last_stats())
+    finally:
+        wpol.release()
+    st = min(stats, key=lambda s: s["total_ms"])
+    no, e = inst_w.nocc, inst_w.energy
+    om, wt = o.imaginary_quad_grid(inst_w.nomega)
+    with threadpool_limits(limits=os.cpu_count() or 1):
+        t0 = time.perf_counter()
+        sf = o.polarizability_grid(inst_w.m_ia, e[:no], e[no:], inst_w.occupation[:no], inst_w.occupation[no:], om, wt)
+        ref = o.sosex_selfenergy_imag(e, m_full, no, list(range(inst_w.nsemin - 1, inst_w.nsemax)), sf.chi, sf.omega,
+                                      sf.weight_quad, z)
+        cpu_ms = (time.perf_counter() - t0) * 1e3
+    sosex = {"instance": "840 (window tensor 350 MB, page-locked)", "wall_ms": float(min(walls_x)),
+             "device_ms": st["total_ms"], "upload_transpose_ms": st["stage_ms"][0],
+             "products_and_k_ms": st["stage_ms"][1], "sums_ms": st["stage_ms"][3],
+             "max_abs_diff_vs_oracle_rel": float(np.abs(out - ref).max() / np.abs(ref).max()),
+             "oracle_ms_incl_w": cpu_ms}
     eng.close()
     ms = float(np.median(walls))
     line = {"metric": "GW+SOX solves/s", "value": 1e3 / ms, "unit": "solves/s", "n_gpus": 1,
@@ -545,7 +576,7 @@ def run_sox_line(args):
                                    "page-locked host memory), Nocc=21 Nvirt=207 Naux=840, 32 imaginary frequencies, "
                                    "50 evaluation points",
                        "fp64_peak_tflops": fp64_peak},
-            "sox_qp_shift_ev": shift, "cases": cases}
+            "sox_qp_shift_ev": shift, "cases": cases, "sosex": sosex}
     print(json.dumps(line), flush=True)
 
 
