@@ -29,6 +29,8 @@ the same BLAS/LAPACK call sequence (through SciPy's bundled OpenBLAS):
                               src/m_selfenergy_evaluation.f90:494-503)
 * ``sosex_selfenergy_imag``   src/m_g3w2_selfenergy.f90:2200-2478 (GW+SOSEX on the
                               imaginary axis, after SOX, :498-500)
+* ``g3w2_selfenergy_imag``    src/m_g3w2_selfenergy.f90:2018-2196 (GW+G3W2 on the
+                              imaginary axis, after SOSEX, :501-503)
 
 Pinning: the reference's own known answer that needs no Gaussian integrals is
 the analytic RPA correlation energy of bulk LiH from the shipped CC4S tensor
@@ -550,7 +552,7 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
               exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
               ncore_w: int = 0, energy_g: np.ndarray | None = None, sox: bool = False,
               m_ov_g: np.ndarray | None = None, factor_sosex: float | None = None,
-              m_full: np.ndarray | None = None) -> G0W0Result:
+              m_full: np.ndarray | None = None, g3w2: bool = False) -> G0W0Result:
     """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
     (src/m_selfenergy_evaluation.f90:214-246, 587-611).
 
@@ -567,7 +569,8 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     (default ``m_ia``, the W window, when both windows start at the same state).
     ``factor_sosex``: GW+SOSEX_PADE (GW+2SOSEX_PADE with 2), SOX and then
     factor_sosex x SOSEX added (:496-500); ``m_full`` is the G-window tensor
-    [nstate_G, nstate_G, naux].
+    [nstate_G, nstate_G, naux].  ``g3w2``: the G3W2 term added last (:501-503);
+    GW+G3W2_PADE is sox=True, factor_sosex=2, g3w2=True.
     """
     eg = energy if energy_g is None else energy_g
     occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
@@ -591,6 +594,11 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
         sig = list(range(rng.nsemin - 1 - rng.ncore_g, rng.nsemax - rng.ncore_g))
         se.sigma_calc += sosex_selfenergy_imag(window, m_full, rng.nhomo_g - rng.ncore_g, sig, sf.chi, sf.omega,
                                                sf.weight_quad, se.omega_calc, factor_sosex).T
+    if g3w2:
+        window = eg[rng.ncore_g: rng.ncore_g + m_sigma.shape[1]]
+        sig = list(range(rng.nsemin - 1 - rng.ncore_g, rng.nsemax - rng.ncore_g))
+        se.sigma_calc += g3w2_selfenergy_imag(window, m_full, sig, sf.chi, sf.omega, sf.weight_quad,
+                                              se.omega_calc).T
     if technique == "pade":
         se_pade_fit(se, eta)
     else:
@@ -817,3 +825,72 @@ def sosex_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, nocc: 
                                       / (2.0 * PI))
                     out[ip, iz] += s
     return factor_sosex * out
+
+
+def g3w2_selfenergy_imag(energy_g: np.ndarray, m_full: np.ndarray, sig_states, chi: np.ndarray,
+                         omega_p: np.ndarray, weight_p: np.ndarray, omega_calc: np.ndarray) -> np.ndarray:
+    """G (W-v) G (W-v) G on the evaluation points of the imaginary axis,
+    g3w2_selfenergy_imag_grid (src/m_g3w2_selfenergy.f90:2018-2196), one spin,
+    diagonal (q = p), with W - v = ``chi`` [nomega', naux, naux] on wpol_imag's grid.
+
+    braket1(u,v,w) = (v w|W(i w')-v|u p), braket2(u,v,w) = (u v|W(i w'')-v|w p)
+    (:2100-2110), and the four sign pairs (s', s'') of :2113-2146 sum
+    1 / [(z + s' i w' - e_u)(z + s' i w' + s'' i w'' - e_v)(z + s'' i w'' - e_w)].
+    Each term is a product of one factor per state index, so the sum over
+    (u, v, w) is a trilinear contraction of braket1 * braket2 with three vectors;
+    braket1 depends on w' only and braket2 on w'' only.  Returns
+    w' w'' (-1/(2 pi))^2 sum (...) as [nsig, nomega_calc] complex."""
+    ng = m_full.shape[0]
+    e = energy_g[:ng]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    mflat = m_full.reshape(ng * ng, -1)
+    out = np.zeros((len(sig_states), z.size), dtype=np.complex128)
+    for ip, p in enumerate(sig_states):
+        # (v w|chi_k|u p) and (u v|chi_k|w p) for every frequency k, [k][u][v][w]
+        x = np.stack([m_full[:, p] @ chi[k].T for k in range(len(omega_p))])      # [k][u][P]
+        b1 = np.stack([(mflat @ x[k].T).reshape(ng, ng, ng).transpose(2, 0, 1) for k in range(len(omega_p))])
+        b2 = np.stack([(mflat @ x[k].T).reshape(ng, ng, ng) for k in range(len(omega_p))])
+        for k1, (w1, o1) in enumerate(zip(weight_p, omega_p)):
+            for k2, (w2, o2) in enumerate(zip(weight_p, omega_p)):
+                bb = b1[k1] * b2[k2]
+                for iz, zz in enumerate(z):
+                    acc = 0.0 + 0.0j
+                    for s1 in (1.0, -1.0):
+                        a = 1.0 / (zz + s1 * 1j * o1 - e)
+                        for s2 in (1.0, -1.0):
+                            b = 1.0 / (zz + s1 * 1j * o1 + s2 * 1j * o2 - e)
+                            c = 1.0 / (zz + s2 * 1j * o2 - e)
+                            acc += np.einsum("uvw,u,v,w->", bb, a, b, c)
+                    out[ip, iz] += w1 * w2 * acc
+    return out / (2.0 * PI) ** 2
+
+
+def g3w2_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, sig_states, chi: np.ndarray,
+                               omega_p: np.ndarray, weight_p: np.ndarray, omega_calc: np.ndarray) -> np.ndarray:
+    """Loop-for-loop restatement of g3w2_selfenergy_imag_grid
+    (src/m_g3w2_selfenergy.f90:2082-2158) for small cases."""
+    ng = m_full.shape[0]
+    e = energy_g[:ng]
+    z = np.asarray(omega_calc, dtype=np.complex128)
+    out = np.zeros((len(sig_states), z.size), dtype=np.complex128)
+    for ip, p in enumerate(sig_states):
+        q = p
+        for k1 in range(len(omega_p)):
+            for k2 in range(len(omega_p)):
+                chi_omegap_up = chi[k1] @ m_full[:, p].T          # (naux, u)
+                chi_omegapp_wq = chi[k2] @ m_full[:, q].T         # (naux, w)
+                wp, wpp = 1j * omega_p[k1], 1j * omega_p[k2]
+                for u in range(ng):
+                    for v in range(ng):
+                        for w in range(ng):
+                            braket1 = m_full[v, w] @ chi_omegap_up[:, u]
+                            braket2 = m_full[u, v] @ chi_omegapp_wq[:, w]
+                            for iz in range(z.size):
+                                zz = z[iz]
+                                d = 1.0 / ((zz + wp - e[u]) * (zz + wp + wpp - e[v]) * (zz + wpp - e[w]))
+                                d += 1.0 / ((zz - wp - e[u]) * (zz - wp + wpp - e[v]) * (zz + wpp - e[w]))
+                                d += 1.0 / ((zz + wp - e[u]) * (zz + wp - wpp - e[v]) * (zz - wpp - e[w]))
+                                d += 1.0 / ((zz - wp - e[u]) * (zz - wp - wpp - e[v]) * (zz - wpp - e[w]))
+                                out[ip, iz] += (weight_p[k1] * weight_p[k2] * braket1 * braket2 * d
+                                                * (-1.0 / (2.0 * PI)) ** 2)
+    return out
