@@ -37,6 +37,16 @@ sys.path.insert(0, str(ROOT))
 HA_EV = 27.21138505
 METRIC = "G0W0 solves/s"
 WORKLOAD = "single synthetic RI-GW instance Nocc=21 Nvirt=207 Naux=840, 32 imaginary frequencies"
+DATA = ("synthetic (seeded PCG64 seed 2 + rank; energies U[-30,-8]/U[0.5,40] eV, M ~ N(0,s^2) scaled so "
+        "max eig eps(i0) = 1.8)")
+
+
+def bench_config(precision: str, world: int) -> dict:
+    """The ``config`` of the default line, printed identically by both arms."""
+    return {"workload": WORKLOAD, "precision": precision,
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
+            "l2": "flushed between solves (512 MiB write)", "sigma_states": "HOMO, LUMO",
+            "nomega_sigma_calc": 50, "nomega_sigma": 101}
 
 
 def parse():
@@ -47,9 +57,15 @@ def parse():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="fp64", choices=["fp64", "bf16x3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--batch-count", type=int, default=32,
+    ap.add_argument("--batch-count", type=int, default=256,
                     help="molecules of the ragged batch measured beside the single instance (0: skip)")
-    ap.add_argument("--batch-reps", type=int, default=2)
+    ap.add_argument("--batch-reps", type=int, default=2, help="timed repetitions of the split-precision batch")
+    ap.add_argument("--batch-reps-fp64", type=int, default=1, help="timed repetitions of the FP64 batch")
+    ap.add_argument("--serving-window", type=float, default=10.0,
+                    help="seconds of Poisson arrivals at --serve-rate in the default line's serving block (0: skip)")
+    ap.add_argument("--serving-stable-rate", type=float, default=8.0,
+                    help="arrival rate (req/s) of the sustainable-load run of the serving block")
+    ap.add_argument("--serving-stable-window", type=float, default=20.0)
     ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep", "aomo", "sox"])
     ap.add_argument("--sweep-reps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -84,58 +100,109 @@ def oracle_solve(inst):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
-    Q = ("timestamp,index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    """SM clock, power and clock-event reasons sampled during the timed region.
 
-    def __init__(self, gpu_index: int):
-        self.gpu = gpu_index
-        self.proc = None
-        # the raw samples go to $RIGW_CLOCKS_CSV (a directory) or the system temp directory
-        import tempfile
-        base = Path(os.environ.get("RIGW_CLOCKS_CSV", tempfile.gettempdir()))
-        self.path = base / f"clocks_rank{gpu_index}.csv"
+    NVML is read from a thread every 10 ms (read-only queries), so a timed region
+    of a tenth of a second still holds several samples; ``nvidia-smi -lms 200``
+    is the fallback when NVML cannot be loaded.  The GPU is found by the PCI bus
+    id of the CUDA device, so the samples are of the GPU that runs the work."""
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+
+    def __init__(self, cuda_index: int, period_s: float = 0.01):
+        self.cuda_index = cuda_index
+        self.period = period_s
+        self.samples = []            # (time, sm_mhz, max_mhz, power_w, reasons)
+        self.thread = None
+        self.smi = None
+
+    def _handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            pr = torch.cuda.get_device_properties(self.cuda_index)
+            bus = f"{pr.pci_domain_id:08x}:{pr.pci_bus_id:02x}:{pr.pci_device_id:02x}.0"
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.cuda_index)
 
     def start(self):
+        import threading
         try:
-            self.path.parent.mkdir(exist_ok=True)
-            self.f = open(self.path, "w")
-            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
-                                          "-i", str(self.gpu), "-lms", "200"], stdout=self.f,
-                                         stderr=subprocess.DEVNULL)
+            nv, h = self._handle()
+            bits = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            return self._start_smi()
+        self.stop_flag = threading.Event()
+
+        def loop():
+            while not self.stop_flag.is_set():
+                try:
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    pw = nv.nvmlDeviceGetPowerUsage(h) * 1e-3
+                    rs = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((time.time(), sm, mx, pw,
+                                         tuple(n for n, b in zip(self.NAMES, bits) if rs & b)))
+                except Exception:
+                    pass
+                self.stop_flag.wait(self.period)
+        self.thread = threading.Thread(target=loop, daemon=True)
+        self.thread.start()
+
+    def _start_smi(self):
+        import tempfile
+        q = ("timestamp,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        self.path = Path(os.environ.get("RIGW_CLOCKS_CSV", tempfile.gettempdir())) / f"clocks_{os.getpid()}.csv"
+        try:
+            self.f = open(self.path, "w")
+            self.smi = subprocess.Popen(["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                         "-i", str(self.cuda_index), "-lms", "200"], stdout=self.f,
+                                        stderr=subprocess.DEVNULL)
+        except Exception:
+            self.smi = None
 
     def mark(self, which: str):
         """Wall-clock bounds of the timed region (samples outside it are not used)."""
         setattr(self, which, time.time())
 
-    def stop(self) -> dict:
-        if self.proc is None:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        self.proc.wait(timeout=10)
+    def _collect_smi(self):
+        import datetime
+        self.smi.terminate()
+        self.smi.wait(timeout=10)
         self.f.close()
-        rows = [r.split(", ") for r in self.path.read_text().strip().splitlines() if r.strip()]
-        rows = [r[1:] for r in rows if len(r) >= 10 and self._in_region(r[0])]
-        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[k] for r in rows for k in range(4) if r[5 + k].strip() == "Active"})
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(rows), "window": "samples taken inside the timed region"}
+        for r in self.path.read_text().strip().splitlines():
+            c = [x.strip() for x in r.split(",")]
+            if len(c) < 8:
+                continue
+            try:
+                t = datetime.datetime.strptime(c[0], "%Y/%m/%d %H:%M:%S.%f").timestamp()
+                self.samples.append((t, float(c[1]), float(c[2]), float(c[3]),
+                                     tuple(n for n, v in zip(self.NAMES, c[4:8]) if v == "Active")))
+            except ValueError:
+                continue
 
-    def _in_region(self, stamp: str) -> bool:
+    def stop(self) -> dict:
+        if self.thread is not None:
+            self.stop_flag.set()
+            self.thread.join(timeout=5)
+            src = "NVML every 10 ms"
+        elif self.smi is not None:
+            self._collect_smi()
+            src = "nvidia-smi every 200 ms"
+        else:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["clock sampling unavailable"]}
         t0, t1 = getattr(self, "begin", None), getattr(self, "end", None)
-        if t0 is None or t1 is None:
-            return True
-        try:
-            import datetime
-            t = datetime.datetime.strptime(stamp.strip(), "%Y/%m/%d %H:%M:%S.%f").timestamp()
-        except ValueError:
-            return True
-        return t0 - 0.25 <= t <= t1 + 0.25
+        rows = [r for r in self.samples if t0 is None or t1 is None or t0 <= r[0] <= t1]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0, "source": src}
+        return {"sm_mhz": statistics.median(r[1] for r in rows), "sm_max_mhz": max(r[2] for r in rows),
+                "reasons": sorted({n for r in rows for n in r[4]}), "samples": len(rows),
+                "power_w_max": max(r[3] for r in rows), "source": src,
+                "window": "samples taken inside the timed region"}
 
 
 def measured_fp64_peak(torch) -> float:
@@ -176,7 +243,7 @@ def compact_tuning(rep: dict) -> dict:
         "candidates": len(rep["candidates"])}
 
 
-def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
+def run_batched(eng, count: int, reps: int, flush_l2, reps_fp64: int | None = None) -> dict:
     """The ragged batch (Nocc ~ U{5..60}, Nvirt = round(Nocc*U[8,10]), Naux =
     4(Nocc+Nvirt), 32 frequencies, seeds 4..) in one call, split precision and
     FP64, QP-only outputs; inputs generated and kept in device memory."""
@@ -197,7 +264,7 @@ def run_batched(eng, count: int, reps: int, flush_l2) -> dict:
         tuning[name] = compact_tuning(eng.autotune(insts[:8], prec, devs[:8], qp_only=True))
         eng.g0w0_batch(insts, prec, devs, qp_only=True)
         dev_ms, wall_ms, stage_ms = [], [], []
-        for _ in range(reps):
+        for _ in range(reps if (name == "bf16x3" or reps_fp64 is None) else reps_fp64):
             flush_l2()
             t0 = time.perf_counter()
             o = eng.g0w0_batch(insts, prec, devs, qp_only=True)
@@ -336,6 +403,43 @@ def run_serve_line(args):
                                    "48 frequencies", "rate": args.serve_rate, "duration_s": args.serve_duration},
             "serving": res}
     print(json.dumps(line), flush=True)
+
+
+def run_serving_block(args) -> dict:
+    """The serving block of the default line (BASELINE config 5 in a shorter
+    window): Poisson arrivals at ``--serve-rate`` req/s for ``--serving-window``
+    s into the request loop, split precision and FP64 on the same arrivals, then
+    a sustainable rate (``--serving-stable-rate``) in split precision.  p50/p99
+    latency per lane and solves/s per precision; the QP difference in meV
+    between the split and FP64 results of the requests both runs completed
+    (same arrival schedule, same inputs)."""
+    import torch
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64
+
+    def run(rate, window, prec, grace):
+        r = run_serving(rate, window, prec, args.serve_workers, args.serve_batch, grace=grace)
+        r.pop("pool")
+        outs = r.pop("outputs")
+        r.pop("loop_stats", None)
+        torch.cuda.empty_cache()
+        return r, outs
+
+    res = {"note": "latency = completion - scheduled arrival; requests unfinished at the end of the grace "
+                   "period enter with their latency so far (lower bound)"}
+    split, so = run(args.serve_rate, args.serving_window, RIGW_BF16X3, 5.0)
+    f64, fo = run(args.serve_rate, args.serving_window, RIGW_FP64, 5.0)
+    both = [(a, b) for a, b in zip(so, fo) if a is not None and b is not None]
+    res["overload"] = {"rate": args.serve_rate, "window_s": args.serving_window, "bf16x3": split, "fp64": f64,
+                       "speedup_split_vs_fp64": split["solves_per_s"] / f64["solves_per_s"],
+                       "qp_max_diff_mev_split_vs_fp64": max(
+                           (float(np.abs(a.energy_qp_g - b.energy_qp_g).max() * HA_EV * 1e3) for a, b in both),
+                           default=None),
+                       "compared_requests": len(both)}
+    if args.serving_stable_rate > 0:
+        stable, _ = run(args.serving_stable_rate, args.serving_stable_window, RIGW_BF16X3, 10.0)
+        res["stable"] = {"rate": args.serving_stable_rate, "window_s": args.serving_stable_window,
+                         "bf16x3": stable}
+    return res
 
 
 def run_sweep_line(args):
@@ -601,8 +705,8 @@ def run_reference(args, rank, world):
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": mean * 1e3, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, PCG64 seed 2)",
-        "config": {"workload": WORKLOAD, "precision": "fp64", "parallelism": "host threads (OpenBLAS)"},
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": DATA,
+        "config": bench_config("fp64", args.gpus),
         "latency_ms": {"p50": float(np.percentile(times, 50) * 1e3), "p99": float(np.percentile(times, 99) * 1e3)},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": cores, "kind": "port",
                          "sample": "full G0W0 solves of the same instance (CPU restatement of MOLGW's "
@@ -754,9 +858,15 @@ def main():
     batched = None
     if args.batch_count > 0 and world == 1:
         try:
-            batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2)
+            batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2, args.batch_reps_fp64)
         except Exception as exc:    # reported, not hidden
             batched = {"error": str(exc)}
+    serving = None
+    if args.serving_window > 0 and world == 1:
+        try:
+            serving = run_serving_block(args)
+        except Exception as exc:    # reported, not hidden
+            serving = {"error": str(exc)}
 
     if rank == 0:
         fp64_peak = measured_fp64_peak(torch)
@@ -775,13 +885,9 @@ def main():
             "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64" if precision == RIGW_FP64 else "bf16x3+f64",
-            "data": "synthetic (seeded PCG64; energies U[-30,-8]/U[0.5,40] eV, M ~ N(0,s^2) scaled so "
-                    "max eig eps(i0) = 1.8)",
-            "config": {"workload": WORKLOAD, "precision": args.precision,
-                       "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
-                       "l2": "flushed between solves (512 MiB write)", "sigma_states": "HOMO, LUMO",
-                       "nomega_sigma_calc": inst.nomega_sigma_calc, "nomega_sigma": inst.nomega_sigma,
-                       "tuning": tune_main},
+            "data": DATA,
+            "config": bench_config(args.precision, world),
+            "tuning": tune_main,
             "latency_ms": {"p50": float(np.percentile(dev_ms, 50)), "p99": float(np.percentile(dev_ms, 99))},
             "stage_ms": {"pack": stages[0], "chi0": stages[1], "eps_factor_solve": stages[2],
                          "sigma_qp": stages[3]},
@@ -793,6 +899,7 @@ def main():
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
             "other_precision": alt,
             "batched": batched,
+            "serving": serving,
         }
         if alt and "chi0_ms" in alt and alt["precision"] == "bf16x3":
             # the tcgen05 kernel does 3 bf16 products of the chi0 contraction

@@ -339,7 +339,8 @@ RIGW_API int rigw_server_destroy(rigw_server* srv);
  * would also synchronize the device).  Every array is a CUDA device pointer
  * owned by the caller: sigma_calc [nsig][nomega_sigma_calc][2], e_sig [nsig],
  * exchange_m_vxc [nsig] or NULL, omega_calc [nomega_sigma_calc][2] or NULL
- * (then efermi + i*step_sigma_calc*(k-1)); outputs energy_qp_g, energy_qp_z
+ * (then point k is efermi + i*step_sigma_calc*k, k = 0 .. nomega_sigma_calc-1;
+ * RIGW_HOMOLUMO needs the caller's points); outputs energy_qp_g, energy_qp_z
  * (or NULL), zz (or NULL) [nsig] and sigma [nsig][2*(nomega_sigma/2)+1][2] (or
  * NULL).  ``stream`` is a cudaStream_t (NULL: default stream); the call returns
  * after the work on it is done.  Intermediates live in a fixed 1.06 MiB

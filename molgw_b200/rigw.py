@@ -84,6 +84,15 @@ class SosexProblem(C.Structure):
     ]
 
 
+def _vertex_w_inst(inst):
+    """The instance whose W window the vertex path factors: on that path the
+    reference calls gw_selfenergy_grid with energy_g (src/m_selfenergy_evaluation.f90:496),
+    and that routine builds W from the energies it is given
+    (src/m_gw_selfenergy_grid.f90:604), so the W energies are energy_g."""
+    eg = getattr(inst, "energy_g", None)
+    return inst if eg is None else replace(inst, energy=np.asarray(eg, dtype=np.float64))
+
+
 def efermi_of(inst) -> float:
     """se_init's efermi from the energies in G: half-way between the highest
     energy of state nhomo_G and the lowest of state nhomo_G + 1 over the spin
@@ -504,8 +513,10 @@ class Engine:
         """GW+SOX on the imaginary axis (postscf 'GW+SOX_PADE'): W and Sigma_c on
         the evaluation points, Sigma^SOX added to sigma_calc, then the
         Pade continuation and the QP equation (src/m_selfenergy_evaluation.f90:494-503,
-        587-611; the imaginary-axis vertex path exists for imaginary_axis_pade only)."""
-        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        587-611; the imaginary-axis vertex path exists for imaginary_axis_pade only).
+        W is built from energy_g when it is set, as gw_selfenergy_grid does with the
+        energies it is given (src/m_gw_selfenergy_grid.f90:604)."""
+        erpa, egw, wpol = self.polarizability_grid_scalapack(_vertex_w_inst(inst), precision)
         try:
             sigma = self.gw_selfenergy_imag_scalapack(wpol, inst)
         finally:
@@ -547,8 +558,9 @@ class Engine:
         """GW+SOSEX on the imaginary axis (postscf 'GW+SOSEX_PADE'; factor_sosex = 2
         for 'GW+2SOSEX_PADE'): W, then Sigma_c + Sigma^SOX + factor_sosex Sigma^SOSEX
         on the evaluation points, then the Pade continuation and the QP equation
-        (src/m_selfenergy_evaluation.f90:494-503)."""
-        erpa, egw, wpol = self.polarizability_grid_scalapack(inst, precision)
+        (src/m_selfenergy_evaluation.f90:494-503).  W is built from energy_g when it
+        is set (src/m_gw_selfenergy_grid.f90:604)."""
+        erpa, egw, wpol = self.polarizability_grid_scalapack(_vertex_w_inst(inst), precision)
         oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
         cg = getattr(inst, "ncore_g", 0)
         no = getattr(inst, "ncore_w", 0) + inst.nocc - cg

@@ -562,7 +562,10 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     ``energy_g`` (default ``energy``) are the energies in G, as read from
     ENERGY_QP under force_energy_qp (:164-181): se%init and the Sigma sum take
     them, W (energy_w = energy for GW) and the energy0 of the QP equation
-    (find_qp_energy_*(se, ..., energy, ...), :587-590) keep ``energy``.
+    (find_qp_energy_*(se, ..., energy, ...), :587-590) keep ``energy``.  On the
+    vertex path (``sox``, ``factor_sosex`` or ``g3w2``) the reference calls
+    gw_selfenergy_grid with energy_g (:496), which builds its own W from that
+    argument (src/m_gw_selfenergy_grid.f90:604), so W there takes ``energy_g``.
 
     ``sox``: GW+SOX_PADE, Sigma^SOX from energy_g added to sigma_calc before the
     fit (:494-503); ``m_ov_g`` is the occupied x empty block of the G window
@@ -573,10 +576,11 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     GW+G3W2_PADE is sox=True, factor_sosex=2, g3w2=True.
     """
     eg = energy if energy_g is None else energy_g
+    ew = eg if (sox or factor_sosex is not None or g3w2) else energy
     occ_w = occupation[ncore_w:ncore_w + m_ia.shape[0]]
-    e_occ = energy[ncore_w:ncore_w + m_ia.shape[0]]
+    e_occ = ew[ncore_w:ncore_w + m_ia.shape[0]]
     nlumo = ncore_w + m_ia.shape[0]
-    e_virt = energy[nlumo:nlumo + m_ia.shape[1]]
+    e_virt = ew[nlumo:nlumo + m_ia.shape[1]]
     occ_v = occupation[nlumo:nlumo + m_ia.shape[1]]
     omega, weight = imaginary_quad_grid(nomega_chi_imag)
     sf = polarizability_grid(m_ia, e_occ, e_virt, occ_w, occ_v, omega, weight)

@@ -76,4 +76,6 @@ def main(ref: Path):
 
 
 if __name__ == "__main__":
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path("/root/reference"))
+    if len(sys.argv) != 2:
+        sys.exit("usage: python tests/golden/make_golden.py <path of the MOLGW source tree>")
+    main(Path(sys.argv[1]))

@@ -83,3 +83,19 @@ def test_gw_plus_sosex_qp_matches_oracle(engine):
                       eta=inst.eta, sox=True, factor_sosex=2.0, m_full=mf)
     assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
     assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6
+
+
+def test_gw_plus_sosex_builds_w_from_energy_g(engine):
+    """energy_g != energy: the vertex path's W takes energy_g (src/m_gw_selfenergy_grid.f90:604)."""
+    from dataclasses import replace
+    inst, mf = _case((5, 37, 51, 8), seed=21)
+    eg = inst.energy + np.random.default_rng(2).uniform(-0.05, 0.05, inst.nstate)
+    out = engine.gw_sosex_imag(replace(inst, energy_g=eg), mf, factor_sosex=2.0)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng,
+                      nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma,
+                      nomega_sigma_calc=inst.nomega_sigma_calc, step_sigma_calc=inst.step_sigma_calc,
+                      eta=inst.eta, energy_g=eg, sox=True, factor_sosex=2.0, m_full=mf)
+    assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
+    assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6

@@ -81,3 +81,19 @@ def test_sox_device_pointers_match_host_pointers(engine):
         "m_ov": torch.from_numpy(np.ascontiguousarray(inst.m_ia)).cuda(),
         "m_pq": torch.from_numpy(np.ascontiguousarray(inst.m_sigma)).cuda()})
     assert np.array_equal(host, dev)
+
+
+def test_gw_plus_sox_builds_w_from_energy_g(engine):
+    """energy_g != energy: the vertex path's W takes energy_g (src/m_gw_selfenergy_grid.f90:604)."""
+    from dataclasses import replace
+    inst = synth.make_instance(5, 37, 51, 8, seed=4)
+    eg = inst.energy + np.random.default_rng(1).uniform(-0.05, 0.05, inst.nstate)
+    out = engine.gw_sox_imag(replace(inst, energy_g=eg))
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng,
+                      nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma,
+                      nomega_sigma_calc=inst.nomega_sigma_calc, step_sigma_calc=inst.step_sigma_calc,
+                      eta=inst.eta, energy_g=eg, sox=True)
+    assert np.abs(out.sigma_calc - ref.sigma_calc.T).max() <= 1e-9 * np.abs(ref.sigma_calc).max()
+    assert np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV <= 1e-6

@@ -65,3 +65,34 @@ def test_gw_plus_sox_moves_the_qp_energies():
 def gws_points(inst):
     from molgw_b200.rigw import efermi_of
     return efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
+
+
+def test_vertex_path_builds_w_from_energy_g():
+    """On the vertex path the reference calls gw_selfenergy_grid with energy_g
+    (src/m_selfenergy_evaluation.f90:496), which builds W from that argument
+    (src/m_gw_selfenergy_grid.f90:604).  With energy_g != energy, the GW+SOX
+    sigma_calc equals W, Sigma_c and the SOX loop form all taken from energy_g,
+    and differs from a W built from energy."""
+    inst, mf = synth.with_window(synth.make_instance(3, 12, 20, 8, seed=5), seed=6)
+    no = inst.nocc
+    eg = inst.energy + np.random.default_rng(3).uniform(-0.05, 0.05, inst.nstate)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    kw = dict(nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma,
+              nomega_sigma_calc=inst.nomega_sigma_calc, step_sigma_calc=inst.step_sigma_calc, eta=inst.eta)
+    res = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng,
+                      energy_g=eg, sox=True, **kw)
+    omega, weight = o.imaginary_quad_grid(inst.nomega)
+    occ = inst.occupation
+
+    def by_hand(ew):
+        sf = o.polarizability_grid(inst.m_ia, ew[:no], ew[no:], occ[:no], occ[no:], omega, weight)
+        se = o.se_init_imaginary_axis(eg, rng, "pade", inst.nomega_sigma, inst.step_sigma,
+                                      inst.nomega_sigma_calc, inst.step_sigma_calc)
+        sig = list(range(inst.nsemin - 1, inst.nsemax))
+        gw = o.gw_selfenergy_imag(eg, inst.m_sigma, sf, se.omega_calc, 1)
+        return gw + o.sox_selfenergy_imag_loops(eg, mf, no, sig, se.omega_calc).T
+
+    ref = by_hand(eg)
+    assert np.abs(res.sigma_calc - ref).max() <= 1e-12 * np.abs(ref).max()
+    assert np.abs(by_hand(inst.energy) - ref).max() > 1e-6 * np.abs(ref).max()
