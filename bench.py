@@ -863,6 +863,10 @@ def main():
             batched = {"error": str(exc)}
     serving = None
     if args.serving_window > 0 and world == 1:
+        # the request loop sizes its worker arenas from free memory: release this
+        # context's plan arenas and the batch inputs first
+        eng.close()
+        torch.cuda.empty_cache()
         try:
             serving = run_serving_block(args)
         except Exception as exc:    # reported, not hidden

@@ -108,7 +108,7 @@ typedef struct rigw_problem {
   int technique;             /* rigw_technique                                            */
   int nomega_sigma_calc;     /* Sigma evaluation points (<= 128)                          */
   double step_sigma_calc;
-  const double* omega_calc;  /* [nomega_sigma_calc][2] complex points; NULL: efermi + i*step*(k-1) */
+  const double* omega_calc;  /* [nomega_sigma_calc][2] complex points; NULL: efermi + i*step*k, k from 0 */
   int nomega_sigma;          /* real grid has 2*(nomega_sigma/2)+1 points                 */
   double step_sigma;
   double eta;

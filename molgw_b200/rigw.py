@@ -379,8 +379,10 @@ class Engine:
 
     # ---------------------------------------------------------------- fused
     def g0w0_batch(self, insts, precision=RIGW_FP64, device_arrays=None,
-                   qp_only: bool = False) -> list[G0W0Output]:
-        """One call for many molecules; ``precision`` is one code for all or one per molecule."""
+                   qp_only: bool = False, freq: tuple | None = None) -> list[G0W0Output]:
+        """One call for many molecules; ``precision`` is one code for all or one per molecule.
+        ``freq`` = (omega, weight): the imaginary frequencies and quadrature weights
+        of W in place of the Gauss-Legendre grid (wpol%omega, wpol%weight_quad)."""
         n = len(insts)
         precs = list(precision) if isinstance(precision, (list, tuple)) else [precision] * n
         probs = (Problem * n)()
@@ -388,7 +390,7 @@ class Engine:
         keep, bufs = [], []
         for i, inst in enumerate(insts):
             p, k = self.make_problem(inst, precs[i], device_arrays[i] if device_arrays else None,
-                                     qp_only=qp_only)
+                                     qp_only=qp_only, freq=freq)
             probs[i] = p
             keep.append(k)
             r, b = self._alloc_result(p)
@@ -421,8 +423,9 @@ class Engine:
                 "default_ms": rep.default_ms,
                 "tuned_ms": rep.tuned_ms, "candidates": cands}
 
-    def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False) -> G0W0Output:
-        return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None, qp_only)[0]
+    def g0w0(self, inst, precision: int = RIGW_FP64, device_arrays=None, qp_only: bool = False,
+             freq: tuple | None = None) -> G0W0Output:
+        return self.g0w0_batch([inst], precision, [device_arrays] if device_arrays else None, qp_only, freq)[0]
 
     # ---------------------------------------------------------------- drop-in pieces
     def polarizability_grid_scalapack(self, inst, precision: int = RIGW_FP64):

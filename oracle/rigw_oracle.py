@@ -552,7 +552,8 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
               exchange_m_vxc: np.ndarray | None = None, technique: str = "pade",
               ncore_w: int = 0, energy_g: np.ndarray | None = None, sox: bool = False,
               m_ov_g: np.ndarray | None = None, factor_sosex: float | None = None,
-              m_full: np.ndarray | None = None, g3w2: bool = False) -> G0W0Result:
+              m_full: np.ndarray | None = None, g3w2: bool = False,
+              freq: tuple | None = None, mu_origin: float = -100.0) -> G0W0Result:
     """Path of selfenergy_evaluation for imaginary_axis_pade / _homolumo
     (src/m_selfenergy_evaluation.f90:214-246, 587-611).
 
@@ -574,6 +575,10 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     factor_sosex x SOSEX added (:496-500); ``m_full`` is the G-window tensor
     [nstate_G, nstate_G, naux].  ``g3w2``: the G3W2 term added last (:501-503);
     GW+G3W2_PADE is sox=True, factor_sosex=2, g3w2=True.
+    ``freq`` = (omega, weight) replaces the Gauss-Legendre grid of W (wpol%omega,
+    wpol%weight_quad), e.g. a subset of it for one rank of the frequency split.
+    ``mu_origin``: the input variable of that name, the origin of the imaginary
+    axis of the evaluation points when > -99 (src/m_selfenergy_tools.f90:573-585).
     """
     eg = energy if energy_g is None else energy_g
     ew = eg if (sox or factor_sosex is not None or g3w2) else energy
@@ -582,10 +587,10 @@ def g0w0_imag(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_si
     nlumo = ncore_w + m_ia.shape[0]
     e_virt = ew[nlumo:nlumo + m_ia.shape[1]]
     occ_v = occupation[nlumo:nlumo + m_ia.shape[1]]
-    omega, weight = imaginary_quad_grid(nomega_chi_imag)
+    omega, weight = imaginary_quad_grid(nomega_chi_imag) if freq is None else freq
     sf = polarizability_grid(m_ia, e_occ, e_virt, occ_w, occ_v, omega, weight)
     se = se_init_imaginary_axis(eg, rng, technique, nomega_sigma, step_sigma,
-                                nomega_sigma_calc, step_sigma_calc)
+                                nomega_sigma_calc, step_sigma_calc, mu_origin=mu_origin)
     se.sigma_calc[:] = gw_selfenergy_imag(eg, m_sigma, sf, se.omega_calc, rng.ncore_g + 1)
     if sox:
         mov = m_ia if m_ov_g is None else m_ov_g
