@@ -17,6 +17,7 @@ constexpr int kChainPairs = 4;                 // (problem, frequency) pairs per
 constexpr int kSplitGroup = 8;                 // frequencies sharing one bf16 hi/lo split buffer
 constexpr size_t kSplitWholeBytes = size_t(1) << 30;   // below this, one buffer for all frequencies
 constexpr size_t kSplitProblemBytes = size_t(4) << 30; // split buffer of one problem at most (>= one frequency)
+constexpr size_t kSplitL2Bytes = size_t(48) << 20;     // split buffers that stay resident in the 126 MB L2
 constexpr int kSplitT = 256;                   // transitions per item of the split / slice kernels
 
 // Device-side error flags (bitmask written with atomicOr, read by the host after a stage).

@@ -240,6 +240,19 @@ Dims dims_of(const Shape& sh, PlanMode mode) {
   return d;
 }
 
+}  // namespace
+
+// Bytes of one frequency's split operands (bf16 hi/lo, or the Ozaki slices).
+size_t split_bytes_per_frequency(const Shape& sh) {
+  if (sh.precision == RIGW_FP64) return 0;
+  const int npad = round_up(sh.naux, kPanel);
+  const int nia = sh.nocc * sh.nvirt + sh.nocc2 * sh.nvirt2;
+  const int nia_pad = round_up(std::max(nia, 1), is_ozaki(sh.precision) ? 128 : 64);
+  return size_t(npad) * nia_pad * (is_ozaki(sh.precision) ? ozaki_slices(sh.precision) : 4);
+}
+
+namespace {
+
 // Transitions per item of the split / slice / row-max kernels: wide items for
 // large problems (fewer items to build), 64 otherwise (enough CTAs to fill the GPU).
 int split_item_t(const Dims& d) { return (size_t(d.nia_pad / 64) * (d.npad / 64) >= 8192) ? kSplitT : 64; }

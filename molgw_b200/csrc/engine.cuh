@@ -105,6 +105,8 @@ struct Tuning {
 // Precision class of a batch (tunings are kept per mode and class):
 // 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed.
 int precision_class(const std::vector<Shape>& shapes);
+// Bytes of one frequency's split operands of a problem (0 for FP64).
+size_t split_bytes_per_frequency(const Shape& sh);
 
 enum PlanMode : int {
   kPlanFused = 0,      // chi0 -> eps -> factor -> [I | M_sigma] solve -> Sigma -> QP

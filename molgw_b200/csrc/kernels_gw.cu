@@ -138,71 +138,116 @@ __global__ void __launch_bounds__(256) mnorm_kernel(const ProbDev* __restrict__ 
 
 // ---------------------------------------------------------------------------
 // Diagonal block of panel k: A_kk = U^T U (upper Cholesky, in place) and
-// W = U^-1 (to winv), blocked in shared memory.  One CTA of kDiagThreads threads
-// per (prob, frequency).  Shared memory holds the block (U in its upper
-// triangle, W^T in its strictly lower triangle), 1/U(i,i), dense copies of the
-// four 32x32 diagonal blocks of W^T and a scratch for the W products.
-// For each 32-row block j (right-looking):
-//   a. one warp factors and inverts A_jj in registers: Gaussian elimination of
-//      [A_jj | I] (lane l owns column l; the identity part lives in the strictly
-//      lower triangle) leaves D L^T above and L^-1 below the diagonal,
-//      A_jj = L D L^T; U_jj = D^-1/2 (D L^T), W_jj = U_jj^-1 = L^-T D^-1/2;
-//   b. the rest of the 32 rows: U_j,rest = W_jj^T A_j,rest          (DMMA);
-//   c. trailing update A_rest,rest -= U_j,rest^T U_j,rest, upper part (DMMA).
-// Then the off-diagonal blocks of W by increasing distance from the diagonal:
-//   W_ab = -W_aa (sum_{a<m<b} U_am W_mb + U_ab W_bb)                 (DMMA).
-constexpr int kDiagLd = kPanel + 4;      // shared row stride of the block (doubles)
-constexpr int kDiagPb = 32;              // rows per block
-constexpr int kDiagNb = kPanel / kDiagPb;
-constexpr int kDiagTld = kDiagPb + 1;    // row stride of the 32x32 scratch blocks
+// W = U^-1 (to winv).  One CTA of kDiagThreads threads per (prob, frequency);
+// the block lives in shared memory (U in its upper triangle, W^T in its
+// strictly lower triangle, W(i,i) = 1/U(i,i) in invd).
+//
+// Right-looking over 8-wide leaves j with a one-leaf lookahead:
+//   a. warp 0 factors and inverts the 8x8 leaf A_jj in registers (lanes 0..7
+//      own its columns; Gaussian elimination of [A_jj | I] leaves D L^T above
+//      and L^-1 below the diagonal; U_jj = D^-1/2 (D L^T), W_jj = L^-T D^-1/2);
+//   b. all warps: U_j,rest = W_jj^T A_j,rest, one 8x8 DMMA tile per warp;
+//   c. all warps: A_rest,rest -= U_j,rest^T U_j,rest on the upper 8x8 tiles.
+//      Warp 0 takes the next leaf's diagonal tile first and factors that leaf
+//      (step a of j + 1) while warps 1..7 finish the update.
+// Then W by recursive doubling over blocks of 8, 16, 32, 64 rows: for each
+// pair of diagonal blocks (F, G), T = U_FG W_GG and W_FG = -W_FF T (DMMA).
+// Two barriers per leaf and two per doubling level; the serial part of the
+// block is sixteen 8-step eliminations.
+constexpr int kDiagLd = kPanel + 8;      // row stride of the block (doubles): == 8 (mod 32), so the
+                                         // DMMA fragment loads (8 rows x 4 columns) hit distinct banks
+constexpr int kDiagTl = 72;              // row stride of the product scratch (== 8 mod 32)
+constexpr int kLeaf = 8;
+constexpr int kNLeaf = kPanel / kLeaf;
 constexpr int kDiagWarps = kDiagThreads / 32;
 
-// One 8x8 tile C += X Y with X (8 x K) and Y (K x 8) in shared memory:
-// X(r, k) = xs[r * xr + k * xk], Y(k, c) = ys[k * yk + c * yc].  Lane (g, q):
-// c0 = C(g, 2q), c1 = C(g, 2q + 1).
-RIGW_DEVICE_INLINE void smem_tile_mma(double& c0, double& c1, const double* xs, int xr, int xk, const double* ys,
-                                      int yk, int yc, int K, int lane) {
-  const int g = lane >> 2, q = lane & 3;
-  const double* xp = xs + g * xr + q * xk;
-  const double* yp = ys + q * yk + g * yc;
-#pragma unroll 4
-  for (int k0 = 0; k0 < K; k0 += 4) dmma_8x8x4(c0, c1, xp[k0 * xk], yp[k0 * yk]);
-}
-
-// Step a for the 32x32 block at (j0, j0), one warp, lane l owning column l.
-// Kept out of line: its 32-double column then stays in registers.
-__device__ __noinline__ void diag_block_factor(double* S, double* wdt, int j0, double* piv, double* invd, int* err) {
-  const int lane = threadIdx.x & 31;
-  double col[kDiagPb];
+// Steps a of the leaf at rows/columns j0 .. j0+7; all 32 lanes of the calling
+// warp take part (lanes 8..31 repeat lanes 0..7 and store nothing).
+__device__ __noinline__ void leaf8_factor(double* S, int j0, double* piv, double* invd, int* err) {
+  const int lane = threadIdx.x & 31, c = lane & 7;
+  const bool owner = lane < kLeaf;
+  double col[kLeaf];
+#pragma unroll
+  for (int i = 0; i < kLeaf; ++i) col[i] = (i <= c) ? S[(j0 + i) * kDiagLd + j0 + c] : 0.0;
   double myd = 0.0;
 #pragma unroll
-  for (int i = 0; i < kDiagPb; ++i) col[i] = (i <= lane) ? S[(j0 + i) * kDiagLd + j0 + lane] : 0.0;
-#pragma unroll
-  for (int j = 0; j < kDiagPb; ++j) {
+  for (int j = 0; j < kLeaf; ++j) {
     const double d = __shfl_sync(0xffffffffu, col[j], j);
-    // row j of the block, A(j,i) held by lane i: every shuffle is issued before the
-    // updates, so that their latencies overlap instead of pairing with each update
-    double aj[kDiagPb];
+    double aj[kLeaf];
 #pragma unroll
-    for (int i = j + 1; i < kDiagPb; ++i) aj[i] = __shfl_sync(0xffffffffu, col[j], i);
-    const double xj = ((lane == j) ? 1.0 : col[j]) * __drcp_rn(d);   // multiplier row j
+    for (int i = j + 1; i < kLeaf; ++i) aj[i] = __shfl_sync(0xffffffffu, col[j], i);   // A(j, i)
+    const double xj = ((c == j) ? 1.0 : col[j]) * __drcp_rn(d);
 #pragma unroll
-    for (int i = j + 1; i < kDiagPb; ++i)
-      if (lane >= i || lane <= j) col[i] -= aj[i] * xj;
-    if (lane == j) myd = d;
+    for (int i = j + 1; i < kLeaf; ++i)
+      if (c >= i || c <= j) col[i] -= aj[i] * xj;
+    if (c == j) myd = d;
   }
   const double r = 1.0 / sqrt(myd);
-  piv[j0 + lane] = myd;
-  invd[j0 + lane] = r;
-  if (!(myd > 0.0)) atomicOr(err, kErrNotSPD);
-  // row i <= lane: U(i, lane); row i > lane: W(lane, i) stored transposed;
-  // wdt[i][lane] = W^T(i, lane) densely (zero above the diagonal)
-#pragma unroll
-  for (int i = 0; i < kDiagPb; ++i) {
-    const double v = col[i] * __shfl_sync(0xffffffffu, r, i);
-    S[(j0 + i) * kDiagLd + j0 + lane] = v;
-    wdt[i * kDiagTld + lane] = (i > lane) ? v : (i == lane ? r : 0.0);
+  if (owner) {
+    piv[j0 + c] = myd;
+    invd[j0 + c] = r;
+    if (!(myd > 0.0)) atomicOr(err, kErrNotSPD);
   }
+  // row i <= c: U(i, c); row i > c: W(c, i) = W^T(i, c)
+#pragma unroll
+  for (int i = 0; i < kLeaf; ++i) {
+    const double v = col[i] * __shfl_sync(0xffffffffu, r, i);
+    if (owner) S[(j0 + i) * kDiagLd + j0 + c] = v;
+  }
+}
+
+// W(r, c) of the finished part: r < c stored at S[c][r], the diagonal in invd.
+RIGW_DEVICE_INLINE double w_at(const double* S, const double* invd, int r, int c) {
+  const double s = S[c * kDiagLd + r], d = invd[r];   // both in bounds for any r, c < kPanel
+  return (r < c) ? s : (r == c ? d : 0.0);
+}
+
+// Trailing-update tile (rt, ct) of leaf j0: A_rt,ct -= U_j,rt^T U_j,ct (8x8, K = 8).
+RIGW_DEVICE_INLINE void leaf8_update_tile(double* S, int j0, int rt, int ct, int g, int q) {
+  double c0 = 0.0, c1 = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < 2; ++ks) {
+    const int k = 4 * ks + q;
+    dmma_8x8x4(c0, c1, S[(j0 + k) * kDiagLd + 8 * rt + g], S[(j0 + k) * kDiagLd + 8 * ct + g]);
+  }
+  double2* d = reinterpret_cast<double2*>(S + (8 * rt + g) * kDiagLd + 8 * ct + 2 * q);
+  double2 v = *d;
+  v.x -= c0;
+  v.y -= c1;
+  *d = v;
+}
+
+// Two independent update tiles: their DMMA chains and shared-memory accesses overlap.
+RIGW_DEVICE_INLINE void leaf8_update_tile2(double* S, int j0, int rt0, int ct0, int rt1, int ct1, int g, int q) {
+  double a0 = 0.0, a1 = 0.0, b0 = 0.0, b1 = 0.0;
+#pragma unroll
+  for (int ks = 0; ks < 2; ++ks) {
+    const double* row = S + (j0 + 4 * ks + q) * kDiagLd;
+    const double x0 = row[8 * rt0 + g], y0 = row[8 * ct0 + g], x1 = row[8 * rt1 + g], y1 = row[8 * ct1 + g];
+    dmma_8x8x4(a0, a1, x0, y0);
+    dmma_8x8x4(b0, b1, x1, y1);
+  }
+  double2* d0 = reinterpret_cast<double2*>(S + (8 * rt0 + g) * kDiagLd + 8 * ct0 + 2 * q);
+  double2* d1 = reinterpret_cast<double2*>(S + (8 * rt1 + g) * kDiagLd + 8 * ct1 + 2 * q);
+  double2 v0 = *d0, v1 = *d1;
+  v0.x -= a0;
+  v0.y -= a1;
+  v1.x -= b0;
+  v1.y -= b1;
+  *d0 = v0;
+  *d1 = v1;
+}
+
+// The upper 8x8 tiles (rt <= ct) of the block listed from the bottom right:
+// index t -> m = 15 - rt with m(m+1)/2 <= t < (m+1)(m+2)/2, ct = rt + t - m(m+1)/2.
+// The tiles of leaf jb's trailing update (rt > jb) are the first n(n+1)/2 with
+// n = 15 - jb, and the next leaf's diagonal tile is index n(n-1)/2.
+RIGW_DEVICE_INLINE void tri_tile(int t, int& rt, int& ct) {
+  int m = int((sqrtf(8.0f * float(t) + 1.0f) - 1.0f) * 0.5f);
+  if ((m + 1) * (m + 2) / 2 <= t) ++m;
+  if (m * (m + 1) / 2 > t) --m;
+  rt = (kNLeaf - 1) - m;
+  ct = rt + t - m * (m + 1) / 2;
 }
 
 __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* __restrict__ probs,
@@ -214,14 +259,13 @@ __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* 
   double* A = p.eps + size_t(w) * ld * ld + size_t(k) * kPanel * ld + size_t(k) * kPanel;
   extern __shared__ double dsm[];
   double* S = dsm;                                   // [kPanel][kDiagLd]
-  double* WdT = S + kPanel * kDiagLd;                // [kDiagNb][kDiagPb][kDiagTld] dense W_jj^T
-  double* T = WdT + kDiagNb * kDiagPb * kDiagTld;    // [kDiagNb-1][kDiagPb][kDiagTld]
-  double* piv = T + (kDiagNb - 1) * kDiagPb * kDiagTld;   // [kPanel]
+  double* Tb = S + kPanel * kDiagLd;                 // [64][kDiagTl] products of the W doubling
+  double* piv = Tb + 64 * kDiagTl;                   // [kPanel] pivots D
   double* invd = piv + kPanel;                       // [kPanel] 1/U(i,i) = W(i,i)
   const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
   const int g = lane >> 2, q = lane & 3;
-  // the block: asynchronous 16-byte copies of whole rows (all in flight at once),
-  // then zeros below the diagonal
+  // the block: asynchronous 16-byte copies of whole rows, all in flight at once
+  // (the lower triangle is loaded too and never read)
   for (int c = t; c < kPanel * kPanel / 2; c += kDiagThreads) {
     const int i = c / (kPanel / 2), l = (c % (kPanel / 2)) * 2;
     cp_async16(S + i * kDiagLd + l, A + size_t(i) * ld + l, 16);
@@ -229,113 +273,116 @@ __global__ void __launch_bounds__(kDiagThreads) chol_diag_kernel(const ProbDev* 
   cp_async_commit();
   cp_async_wait<0>();
   __syncthreads();
-  for (int idx = t; idx < kPanel * kPanel; idx += kDiagThreads) {
-    const int i = idx / kPanel, l = idx % kPanel;
-    if (l < i) S[i * kDiagLd + l] = 0.0;
-  }
+
+  if (warp == 0) leaf8_factor(S, 0, piv, invd, p.err);
   __syncthreads();
-
-  for (int jb = 0; jb < kDiagNb; ++jb) {
-    const int j0 = jb * kDiagPb;
-    double* wdt = WdT + jb * kDiagPb * kDiagTld;
-    if (warp == 0) diag_block_factor(S, wdt, j0, piv, invd, p.err);
-    __syncthreads();
-    const int base = j0 + kDiagPb, n = kPanel - base;
-    if (n == 0) break;
-    // b. U_j,rest = W_jj^T A_j,rest: 4 x n/8 tiles, at most 6 per warp; the
-    //    results replace A_j,rest after every warp has read it
-    {
-      constexpr int kMaxTiles = 4 * (kPanel - kDiagPb) / 8 / kDiagWarps;
-      double r0[kMaxTiles], r1[kMaxTiles];
-      const int ntile = 4 * (n / 8);
-#pragma unroll
-      for (int u = 0; u < kMaxTiles; ++u) {
-        r0[u] = r1[u] = 0.0;
-        const int tile = warp + kDiagWarps * u;
-        if (tile < ntile) {
-          const int rt = tile & 3, ct = tile >> 2;
-          smem_tile_mma(r0[u], r1[u], wdt + 8 * rt * kDiagTld, kDiagTld, 1, S + j0 * kDiagLd + base + 8 * ct,
-                        kDiagLd, 1, kDiagPb, lane);
-        }
-      }
-      __syncthreads();
-#pragma unroll
-      for (int u = 0; u < kMaxTiles; ++u) {
-        const int tile = warp + kDiagWarps * u;
-        if (tile < ntile) {
-          const int rt = tile & 3, ct = tile >> 2;
-          double* c = S + (j0 + 8 * rt + g) * kDiagLd + base + 8 * ct + 2 * q;
-          c[0] = r0[u];
-          c[1] = r1[u];
-        }
-      }
-      __syncthreads();
-    }
-    // c. A_rest,rest -= U_j,rest^T U_j,rest on the upper 8x8 tiles
-    {
-      const int nt = n / 8;
-      for (int tile = warp; tile < nt * nt; tile += kDiagWarps) {
-        const int rt = tile / nt, ct = tile % nt;
-        if (rt > ct) continue;
-        double c0 = 0.0, c1 = 0.0;
-        smem_tile_mma(c0, c1, S + j0 * kDiagLd + base + 8 * rt, 1, kDiagLd, S + j0 * kDiagLd + base + 8 * ct,
-                      kDiagLd, 1, kDiagPb, lane);
-        const int row = base + 8 * rt + g, col = base + 8 * ct + 2 * q;
-        if (row <= col) S[row * kDiagLd + col] -= c0;
-        if (row <= col + 1) S[row * kDiagLd + col + 1] -= c1;
-      }
-      __syncthreads();
-    }
-  }
-
-  // Off-diagonal blocks of W; W(r, c) (r < c) is kept at S[c][r].
-  for (int lev = 1; lev < kDiagNb; ++lev) {
-    const int ntile = (kDiagNb - lev) * 16;          // 16 tiles of 8x8 per 32x32 block
-    for (int tile = warp; tile < ntile; tile += kDiagWarps) {   // T_a = sum_{a<m<b} U_am W_mb + U_ab W_bb
-      const int a = tile >> 4, rt = (tile >> 2) & 3, ct = tile & 3;
-      const int b = a + lev;
+  for (int jb = 0; jb < kNLeaf - 1; ++jb) {
+    const int j0 = jb * kLeaf;
+    const int nb = kNLeaf - 1 - jb;                  // tiles right of the leaf
+    // b. U_j,ct = W_jj^T A_j,ct; W_jj^T(m, k) = W(j0 + k, j0 + m)
+    for (int tt = warp; tt < nb; tt += kDiagWarps) {
+      const int ct = jb + 1 + tt;
       double c0 = 0.0, c1 = 0.0;
-      if (lev > 1)
-        smem_tile_mma(c0, c1, S + (a * kDiagPb + 8 * rt) * kDiagLd + (a + 1) * kDiagPb, kDiagLd, 1,
-                      S + (b * kDiagPb + 8 * ct) * kDiagLd + (a + 1) * kDiagPb, 1, kDiagLd, (lev - 1) * kDiagPb, lane);
-      smem_tile_mma(c0, c1, S + (a * kDiagPb + 8 * rt) * kDiagLd + b * kDiagPb, kDiagLd, 1,
-                    WdT + (b * kDiagPb + 8 * ct) * kDiagTld, 1, kDiagTld, kDiagPb, lane);
-      double* tp = T + (a * kDiagPb + 8 * rt + g) * kDiagTld + 8 * ct + 2 * q;
-      tp[0] = c0;
-      tp[1] = c1;
+#pragma unroll
+      for (int ks = 0; ks < 2; ++ks) {
+        const int kk = 4 * ks + q;
+        dmma_8x8x4(c0, c1, w_at(S, invd, j0 + kk, j0 + g), S[(j0 + kk) * kDiagLd + 8 * ct + g]);
+      }
+      __syncwarp();
+      *reinterpret_cast<double2*>(S + (j0 + g) * kDiagLd + 8 * ct + 2 * q) = make_double2(c0, c1);
     }
     __syncthreads();
-    for (int tile = warp; tile < ntile; tile += kDiagWarps) {   // W_ab = -W_aa T_a
-      const int a = tile >> 4, rt = (tile >> 2) & 3, ct = tile & 3;
-      const int b = a + lev;
-      double c0 = 0.0, c1 = 0.0;
-      smem_tile_mma(c0, c1, WdT + a * kDiagPb * kDiagTld + 8 * rt, 1, kDiagTld, T + a * kDiagPb * kDiagTld + 8 * ct,
-                    kDiagTld, 1, kDiagPb, lane);
-      const int r = a * kDiagPb + 8 * rt + g, c = b * kDiagPb + 8 * ct + 2 * q;
-      S[c * kDiagLd + r] = -c0;
-      S[(c + 1) * kDiagLd + r] = -c1;
+    // c. trailing update; warp 0: the next leaf's diagonal tile, then that leaf
+    if (warp == 0) {
+      leaf8_update_tile(S, j0, jb + 1, jb + 1, g, q);
+      __syncwarp();
+      leaf8_factor(S, j0 + kLeaf, piv, invd, p.err);
+    } else {
+      // tiles 0 .. n(n+1)/2 - 1 except the next leaf's diagonal tile n(n-1)/2,
+      // two per iteration
+      const int ntile = nb * (nb + 1) / 2 - 1, skip = nb * (nb - 1) / 2;
+      constexpr int kStride = kDiagWarps - 1;
+      for (int u = warp - 1; u < ntile; u += 2 * kStride) {
+        int r0, c0, r1, c1;
+        tri_tile(u < skip ? u : u + 1, r0, c0);
+        const int u1 = u + kStride;
+        if (u1 < ntile) {
+          tri_tile(u1 < skip ? u1 : u1 + 1, r1, c1);
+          leaf8_update_tile2(S, j0, r0, c0, r1, c1, g, q);
+        } else {
+          leaf8_update_tile(S, j0, r0, c0, g, q);
+        }
+      }
     }
     __syncthreads();
   }
 
+  // W by recursive doubling: pairs (F, G) of diagonal blocks of b rows
+  for (int b = kLeaf; b < kPanel; b *= 2) {
+    const int nt = b / kLeaf, ntiles = (kPanel / (2 * b)) * nt * nt;
+    for (int tt = warp; tt < ntiles; tt += kDiagWarps) {        // T = U_FG W_GG
+      const int pr = tt / (nt * nt), ti = (tt / nt) % nt, tj = tt % nt;
+      const int F0 = 2 * pr * b, G0 = F0 + b;
+      // two accumulator chains (k-tiles of 8 split in halves) overlap the DMMA latency
+      double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+      for (int k0 = 0; k0 < 8 * tj + 8; k0 += 8) {
+        const int ka = k0 + q, kb = k0 + 4 + q;
+        dmma_8x8x4(c0, c1, S[(F0 + 8 * ti + g) * kDiagLd + G0 + ka], w_at(S, invd, G0 + ka, G0 + 8 * tj + g));
+        dmma_8x8x4(e0, e1, S[(F0 + 8 * ti + g) * kDiagLd + G0 + kb], w_at(S, invd, G0 + kb, G0 + 8 * tj + g));
+      }
+      *reinterpret_cast<double2*>(Tb + (pr * b + 8 * ti + g) * kDiagTl + 8 * tj + 2 * q) =
+          make_double2(c0 + e0, c1 + e1);
+    }
+    __syncthreads();
+    for (int tt = warp; tt < ntiles; tt += kDiagWarps) {        // W_FG = -W_FF T, stored transposed
+      const int pr = tt / (nt * nt), ti = (tt / nt) % nt, tj = tt % nt;
+      const int F0 = 2 * pr * b, G0 = F0 + b;
+      double c0 = 0.0, c1 = 0.0, e0 = 0.0, e1 = 0.0;
+      for (int k0 = 8 * ti; k0 < b; k0 += 8) {
+        const int ka = k0 + q, kb = k0 + 4 + q;
+        dmma_8x8x4(c0, c1, w_at(S, invd, F0 + 8 * ti + g, F0 + ka), Tb[(pr * b + ka) * kDiagTl + 8 * tj + g]);
+        dmma_8x8x4(e0, e1, w_at(S, invd, F0 + 8 * ti + g, F0 + kb), Tb[(pr * b + kb) * kDiagTl + 8 * tj + g]);
+      }
+      S[(G0 + 8 * tj + 2 * q) * kDiagLd + F0 + 8 * ti + g] = -(c0 + e0);
+      S[(G0 + 8 * tj + 2 * q + 1) * kDiagLd + F0 + 8 * ti + g] = -(c1 + e1);
+    }
+    __syncthreads();
+  }
+
+  // U back into eps (upper triangle); W to winv, dense row-major: the strictly
+  // lower 32x32 blocks are zeros, the upper ones go through a per-warp
+  // transposition tile (warps 0..3, in the product scratch) so that both the
+  // shared reads and the global writes are contiguous
   double* W = p.winv + (size_t(w) * p.npanel + k) * kPanel * kPanel;
 #pragma unroll 4
   for (int idx = t; idx < kPanel * kPanel; idx += kDiagThreads) {
     const int i = idx / kPanel, l = idx % kPanel;
     if (l >= i) A[size_t(i) * ld + l] = S[i * kDiagLd + l];
-    // W[i][l] = U^-1(i,l): stored transposed at S[l][i] for i < l
-    W[idx] = (i < l) ? S[l * kDiagLd + i] : (i == l ? invd[i] : 0.0);
+    else if ((i >> 5) > (l >> 5)) W[idx] = 0.0;
   }
-  if (t < 32) {
+  if (warp < 4) {
+    double* tr = Tb + warp * 32 * 33;
+    int n = 0;
+    for (int bi = 0; bi < kPanel / 32; ++bi)
+      for (int bj = bi; bj < kPanel / 32; ++bj) {
+        if (n++ % 4 != warp) continue;
+        const int i0 = 32 * bi, l0 = 32 * bj;
+        for (int rr = 0; rr < 32; ++rr) tr[lane * 33 + rr] = w_at(S, invd, i0 + lane, l0 + rr);
+        __syncwarp();
+        for (int rr = 0; rr < 32; ++rr) W[(i0 + rr) * kPanel + l0 + lane] = tr[rr * 33 + lane];
+        __syncwarp();
+      }
+  }
+  if (warp == 4) {
     double sl = 0.0;
-    for (int m = t; m < kPanel; m += 32) sl += log(piv[m]);
+    for (int m = lane; m < kPanel; m += 32) sl += log(piv[m]);
     sl = warp_sum(sl);
-    if (t == 0) p.logdet[size_t(w) * p.npanel + k] = sl;
+    if (lane == 0) p.logdet[size_t(w) * p.npanel + k] = sl;
   }
 }
 
 size_t chol_diag_smem_bytes() {
-  return (size_t(kPanel) * kDiagLd + size_t(2 * kDiagNb - 1) * kDiagPb * kDiagTld + 2 * kPanel) * sizeof(double);
+  return (size_t(kPanel) * kDiagLd + size_t(64) * kDiagTl + 2 * kPanel) * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------

@@ -302,6 +302,19 @@ Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* 
     return Status::ok();
   };
   if (any_fp64) RIGW_TRY(try_field(&Tuning::chi0_rows, {64, 128}, 1));
+  // split precision: frequencies per hi/lo buffer, including a group whose
+  // buffers stay resident in L2 between the split and the tensor-core launch
+  bool any_split = false;
+  size_t per_w = 0;
+  for (const Shape& sh : shapes)
+    if (sh.precision != RIGW_FP64) {
+      any_split = true;
+      per_w += split_bytes_per_frequency(sh);
+    }
+  if (any_split) {
+    const int g_l2 = int(std::max<size_t>(1, kSplitL2Bytes / std::max<size_t>(per_w, 1)));
+    RIGW_TRY(try_field(&Tuning::split_group, {g_l2, 8}, 1));
+  }
   RIGW_TRY(try_field(&Tuning::update_rows, {64, 128}, 2));
   RIGW_TRY(try_field(&Tuning::chains, {1, 2, 4}, 2));
   RIGW_TRY(try_field(&Tuning::panel_group, {2, 8, 16}, 2));

@@ -60,3 +60,26 @@ def allreduce_partials(sigma_calc: np.ndarray, energies: np.ndarray, group=None)
     n = sigma_calc.size
     sig = flat[:n].reshape(sigma_calc.shape) + 1j * flat[n:2 * n].reshape(sigma_calc.shape)
     return sig, flat[2 * n:]
+
+
+def g0w0_frequency_sharded(engine, inst, precision: int = 0, group=None):
+    """One molecule's G0W0 over the ranks of ``group``: this rank's share of the
+    Gauss-Legendre frequencies (``frequency_shard``) through W and Sigma_c on its
+    GPU (``Engine.frequency_partials``), one all-reduce of the partial Sigma_c and
+    energies, then the Pade continuation and the QP equation on the sum (every
+    rank holds the same result).  The sequence of gw_selfenergy_grid under the
+    poorman split (src/m_gw_selfenergy_grid.f90:626, 658, 325)."""
+    import torch.distributed as dist
+    rank = dist.get_rank(group) if dist.is_initialized() else 0
+    world = dist.get_world_size(group) if dist.is_initialized() else 1
+    idx = frequency_shard(inst.nomega, rank, world)
+    if idx.size:
+        sigma, energies = engine.frequency_partials(inst, idx, precision)
+    else:                               # more ranks than frequencies: this rank adds zeros
+        sigma = np.zeros((inst.nsig, inst.nomega_sigma_calc), dtype=np.complex128)
+        energies = np.zeros(2)
+    if world > 1:
+        sigma, energies = allreduce_partials(sigma, energies, group)
+    out = engine.qp_solve(inst, sigma)
+    out.erpa, out.egw = float(energies[0]), float(energies[1])
+    return out

@@ -79,3 +79,59 @@ def test_shard_molecules_balances_a_ragged_batch():
     assert sorted(i for s in shards for i in s) == list(range(64))
     loads = [sum(parallel.solve_cost(*sizes[i]) for i in s) for s in shards]
     assert max(loads) / min(loads) < 1.1
+
+
+class _OracleEngine:
+    """Stand-in for the library context on CPU: the oracle's partial W / Sigma_c
+    and its Pade + QP, so that the host logic of the sharded path runs on gloo."""
+
+    def frequency_partials(self, inst, idx, precision=0):
+        return _partial(inst, np.asarray(idx))
+
+    def qp_solve(self, inst, sigma):
+        from types import SimpleNamespace
+        rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                           selfenergy_state_max=inst.nsemax)
+        se = o.se_init_imaginary_axis(inst.energy, rng, "pade", 101, 0.025, 20, 0.075)
+        se.sigma_calc[:] = sigma.T
+        o.se_pade_fit(se, 0.01)
+        eqp, _, _, _ = o.find_qp_energy_graphical(se, np.zeros(inst.nsig), inst.energy[inst.nsemin - 1:inst.nsemax])
+        return SimpleNamespace(sigma_calc=sigma, energy_qp_g=eqp, erpa=None, egw=None)
+
+
+def _sharded_worker(rank, world, port, q):
+    import torch.distributed as dist
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        inst = synth.make_instance(4, 24, 40, 3, seed=98)   # 3 frequencies over 4 ranks: one rank has none
+        inst.nomega_sigma_calc = 20
+        out = parallel.g0w0_frequency_sharded(_OracleEngine(), inst)
+        q.put((rank, out.sigma_calc, out.erpa, out.egw, out.energy_qp_g))
+    finally:
+        dist.destroy_process_group()
+
+
+def test_sharded_g0w0_host_logic_on_four_ranks():
+    """parallel.g0w0_frequency_sharded on 4 gloo ranks for 3 frequencies (one rank
+    owns none and contributes zeros): every rank ends with the full Sigma_c, the
+    full energies and the QP energies of the one-rank solve."""
+    world = 4
+    port = _free_port()
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_sharded_worker, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    res = [q.get(timeout=120) for _ in range(world)]
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    inst = synth.make_instance(4, 24, 40, 3, seed=98)
+    inst.nomega_sigma_calc = 20
+    full_sig, full_en = _partial(inst, np.arange(inst.nomega))
+    ref = _OracleEngine().qp_solve(inst, full_sig)
+    for _, sig, erpa, egw, eqp in res:
+        assert np.abs(sig - full_sig).max() < 1e-13 * np.abs(full_sig).max()
+        assert abs(erpa - full_en[0]) < 1e-12 and abs(egw - full_en[1]) < 1e-12
+        assert np.abs(eqp - ref.energy_qp_g).max() * 27.21138505 < 1e-6   # eV; three frequencies: Pade amplifies 1e-13 noise
