@@ -24,6 +24,7 @@
  *                               (GW+SOX_PADE: added to sigma_calc before the Pade fit,
  *                               src/m_selfenergy_evaluation.f90:494-503)
  *   rigw_sosex_selfenergy_imag  sosex_selfenergy_imag_grid    src/m_g3w2_selfenergy.f90:2200-2478
+ *   rigw_g3w2_selfenergy_imag   g3w2_selfenergy_imag_grid     src/m_g3w2_selfenergy.f90:2018-2196
  *                               (GW+SOSEX_PADE: added after SOX, src/m_selfenergy_evaluation.f90:498-500)
  */
 #ifndef RIGW_H
@@ -253,6 +254,29 @@ typedef struct rigw_sosex_problem {
 /* sigma_sosex: [nsig][nomega_calc][2], overwritten. */
 RIGW_API int rigw_sosex_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_sosex_problem* prob,
                                         double* sigma_sosex);
+
+/* G (W-v) G (W-v) G on the evaluation points, one spin channel, diagonal
+ * (g3w2_selfenergy_imag_grid), with W - v from the resident factors of ``wpol``
+ * (its frequency grid and weights are wpol_imag's).  Over the states u, v, w
+ * of the G window:
+ *   Sigma_p(z) = (2 pi)^-2 sum_{k', k''} w_k' w_k'' (v w|W_k'-v|u p) (u v|W_k''-v|w p)
+ *      sum_{s', s'' = +-1} 1 / [(z + s' i w_k' - e_u)(z + s' i w_k' + s'' i w_k'' - e_v)(z + s'' i w_k'' - e_w)].
+ * m_full must be symmetric in its two state indices (real orbitals).  The wpol
+ * must hold the identity part of the solve (not RIGW_PROBLEM_QP_ONLY). */
+typedef struct rigw_g3w2_problem {
+  int naux;
+  int nstate;                /* states of the G window, ncore_G+1 .. nvirtual_G-1          */
+  const double* m_full;      /* [nstate][nstate][naux] = eri_3center_mo(naux, q, r) over the window */
+  int nsig;                  /* Sigma states nsemin..nsemax                                */
+  int sig_first;             /* window index (0-based) of nsemin: nsemin - ncore_G - 1     */
+  const double* energy;      /* [nstate] energy_g over the window (Ha)                     */
+  int nomega_calc;
+  const double* omega_calc;  /* [nomega_calc][2] complex points                            */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS (m_full, sigma_g3w2 on the device) */
+} rigw_g3w2_problem;
+/* sigma_g3w2: [nsig][nomega_calc][2], overwritten. */
+RIGW_API int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g3w2_problem* prob,
+                                       double* sigma_g3w2);
 
 /* ---- fused solves ----------------------------------------------------------- */
 RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result);

@@ -217,6 +217,15 @@ int rigw_sosex_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_
   return finish(ctx, rigw::sosex_selfenergy_imag(ctx->impl, wpol->impl, *prob, sigma_sosex));
 }
 
+int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g3w2_problem* prob,
+                              double* sigma_g3w2) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!wpol || !prob || !sigma_g3w2) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::g3w2_selfenergy_imag(ctx->impl, wpol->impl, *prob, sigma_g3w2));
+}
+
 int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux, const int* index_basis,
                         const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                         int nstate_min, int nstate_max, double* out) {

@@ -453,6 +453,132 @@ sosex_sigma_kernel(const double* __restrict__ K, const double* __restrict__ omeg
   }
 }
 
+// ---------------------------------------------------------------------------
+// G3W2 on the imaginary axis (g3w2_selfenergy_imag_grid, src/m_g3w2_selfenergy.f90:2018-2196).
+// For one Sigma state p, with X_k[Q][u] = sum_P W~_k[P][Q] M(u, p, P):
+//   Gn_k[v][w][u] = (v w|W_k - v|u p) = sum_Q M(v, w, Q) X_k[Q][u]
+//   Gp_k[v][w][u] = (u v|W_k - v|w p) = sum_Q X_k[Q][w] M(v, u, Q)     (M symmetric in its states)
+//   Sigma_p(z) = (2 pi)^-2 sum_{k', k''} w' w'' sum_v sum_u sum_{s', s''} a_u(z, s') b_v(z, s', s'')
+//                sum_w c_w(z, s'') Gn_k'[v][w][u] Gp_k''[v][w][u]
+// with a_u = 1/(z + s' i w' - e_u), b_v = 1/(z + s' i w' + s'' i w'' - e_v),
+// c_w = 1/(z + s'' i w'' - e_w).  One block per (k', k'', kG3Z points): every
+// thread owns states u, keeps the inner sums over w in registers for the
+// block's points and both s'', and the products with a_u b_v; one block sum at
+// the end.  Both tensors are read along u, so the loads are coalesced.
+constexpr int kG3Z = 4;
+
+struct G3w2Args {
+  const double* gn;    // [nwp][ng][wq][wq]
+  const double* gp;    // [nwp][ng][wq][wq]
+  long long sk;        // doubles per frequency: ng * wq * wq
+  int ng, wq;
+  const double* e;     // [ng] energy_g over the window
+  const double* om;    // [nwp] imaginary frequencies
+  const double* wt;    // [nwp] quadrature weights
+  int nwp;
+  const double* z;     // [nz][2]
+  int nz;
+  double* partial;     // [nwp * nwp][nz][2]
+};
+
+RIGW_DEVICE_INLINE void crecip(double x, double y, double& r, double& i) {
+  const double inv = 1.0 / fma(x, x, y * y);
+  r = x * inv;
+  i = -y * inv;
+}
+
+__global__ void __launch_bounds__(kSosexThreads) g3w2_contract_kernel(G3w2Args a) {
+  extern __shared__ double csm[];   // [ng][kG3Z][2 (s'')][2]: c_w(z, s'')
+  __shared__ double red[kSosexThreads / 32][2];
+  const int k1 = blockIdx.x / a.nwp, k2 = blockIdx.x % a.nwp;
+  const int z0 = blockIdx.y * kG3Z, nzc = min(kG3Z, a.nz - z0);
+  const double w1 = a.om[k1], w2 = a.om[k2];
+  for (int idx = threadIdx.x; idx < a.ng * kG3Z * 2; idx += kSosexThreads) {
+    const int w = idx / (kG3Z * 2), zi = (idx >> 1) % kG3Z, s2 = idx & 1;
+    double cr = 0.0, ci = 0.0;
+    if (zi < nzc) crecip(a.z[2 * (z0 + zi)] - a.e[w], a.z[2 * (z0 + zi) + 1] + (s2 ? -w2 : w2), cr, ci);
+    csm[2 * idx] = cr;
+    csm[2 * idx + 1] = ci;
+  }
+  __syncthreads();
+  double accr[kG3Z], acci[kG3Z];
+#pragma unroll
+  for (int zi = 0; zi < kG3Z; ++zi) accr[zi] = acci[zi] = 0.0;
+  const double* g1 = a.gn + k1 * a.sk;
+  const double* g2 = a.gp + k2 * a.sk;
+  const long long wq2 = (long long)a.wq * a.wq;
+  for (int u = threadIdx.x; u < a.ng; u += kSosexThreads) {
+    double ar[kG3Z][2], ai[kG3Z][2];
+#pragma unroll
+    for (int zi = 0; zi < kG3Z; ++zi)
+#pragma unroll
+      for (int s1 = 0; s1 < 2; ++s1)
+        crecip(a.z[2 * (z0 + min(zi, nzc - 1))] - a.e[u], a.z[2 * (z0 + min(zi, nzc - 1)) + 1] + (s1 ? -w1 : w1),
+               ar[zi][s1], ai[zi][s1]);
+    for (int v = 0; v < a.ng; ++v) {
+      double fr[kG3Z][2], fi[kG3Z][2];
+#pragma unroll
+      for (int zi = 0; zi < kG3Z; ++zi) fr[zi][0] = fr[zi][1] = fi[zi][0] = fi[zi][1] = 0.0;
+      const double* p1 = g1 + v * wq2 + u;
+      const double* p2 = g2 + v * wq2 + u;
+      for (int w = 0; w < a.ng; ++w) {
+        const double h = p1[(long long)w * a.wq] * p2[(long long)w * a.wq];
+        const double* c = csm + w * kG3Z * 4;
+#pragma unroll
+        for (int zi = 0; zi < kG3Z; ++zi)
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            fr[zi][s2] = fma(h, c[(zi * 2 + s2) * 2], fr[zi][s2]);
+            fi[zi][s2] = fma(h, c[(zi * 2 + s2) * 2 + 1], fi[zi][s2]);
+          }
+      }
+      const double ev = a.e[v];
+#pragma unroll
+      for (int zi = 0; zi < kG3Z; ++zi) {
+        const double zr = a.z[2 * (z0 + min(zi, nzc - 1))] - ev, zm = a.z[2 * (z0 + min(zi, nzc - 1)) + 1];
+#pragma unroll
+        for (int s1 = 0; s1 < 2; ++s1)
+#pragma unroll
+          for (int s2 = 0; s2 < 2; ++s2) {
+            double br, bi;
+            crecip(zr, zm + (s1 ? -w1 : w1) + (s2 ? -w2 : w2), br, bi);
+            const double tr = ar[zi][s1] * br - ai[zi][s1] * bi, ti = ar[zi][s1] * bi + ai[zi][s1] * br;
+            accr[zi] += tr * fr[zi][s2] - ti * fi[zi][s2];
+            acci[zi] += tr * fi[zi][s2] + ti * fr[zi][s2];
+          }
+      }
+    }
+  }
+  const double scale = a.wt[k1] * a.wt[k2] / (4.0 * kPi * kPi);
+  for (int zi = 0; zi < nzc; ++zi) {
+    double sr = accr[zi], si = acci[zi];
+    block_sum2(sr, si, red);
+    if (threadIdx.x == 0) {
+      double* o = a.partial + ((long long)blockIdx.x * a.nz + z0 + zi) * 2;
+      o[0] = scale * sr;
+      o[1] = scale * si;
+    }
+    __syncthreads();   // red is reused by the next point
+  }
+}
+
+// out[iz] = sum over the frequency pairs of the partial sums, in a fixed order.
+__global__ void __launch_bounds__(kSosexThreads) g3w2_reduce_kernel(const double* __restrict__ partial, int npair,
+                                                                     int nz, double* __restrict__ out) {
+  __shared__ double red[kSosexThreads / 32][2];
+  const int iz = blockIdx.x;
+  double sr = 0.0, si = 0.0;
+  for (int j = threadIdx.x; j < npair; j += kSosexThreads) {
+    sr += partial[((long long)j * nz + iz) * 2];
+    si += partial[((long long)j * nz + iz) * 2 + 1];
+  }
+  block_sum2(sr, si, red);
+  if (threadIdx.x == 0) {
+    out[2 * iz] = sr;
+    out[2 * iz + 1] = si;
+  }
+}
+
 Status upload_items(Context& c, DeviceBuffer* buf, const std::vector<GemmItem>& items, const char* what) {
   if (items.empty()) return Status::ok();
   RIGW_TRY(buf->allocate(&c, items.size() * sizeof(GemmItem), what));
@@ -676,6 +802,185 @@ Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem
   st.total_ms = double(t01) + t12 + t23;
   st.kernel_launches = launches;
   st.chunks = (nsig + pc - 1) / pc;
+  st.waves = 1;
+  st.device_bytes_in_use = c.in_use;
+  st.device_bytes_peak = c.peak;
+  c.last_stats = st;
+  return Status::ok();
+}
+
+Status g3w2_selfenergy_imag(Context& c, const Wpol& w, const rigw_g3w2_problem& pr, double* sigma) {
+  const int ng = pr.nstate, naux = pr.naux, nsig = pr.nsig, nz = pr.nomega_calc;
+  if (ng <= 0 || naux <= 0 || nsig <= 0 || nz <= 0 || nz > 65535 || !pr.m_full || !pr.energy || !pr.omega_calc ||
+      !sigma || pr.sig_first < 0 || pr.sig_first + nsig > ng)
+    return Status::fail(RIGW_ERR_ARG, "g3w2_selfenergy_imag: invalid arguments");
+  const ProbDev& pd = w.plan->problems()[0].dev;
+  if (naux != pd.naux) return Status::fail(RIGW_ERR_ARG, "g3w2_selfenergy_imag: naux differs from the polarizability");
+  if (!pd.want_identity)
+    return Status::fail(RIGW_ERR_UNSUPPORTED, "g3w2_selfenergy_imag: the polarizability was solved without W (QP-only)");
+  const int wq = ng + (ng & 1), naux_e = naux + (naux & 1), npad = pd.npad, nwp = pd.nomega;
+  const long long ldm = (long long)wq * wq, sk = (long long)ng * ldm;
+  const size_t smem = size_t(ng) * kG3Z * 4 * sizeof(double);
+  if (ldm >= (1LL << 31) || smem > 200 * 1024)
+    return Status::fail(RIGW_ERR_ARG, "g3w2_selfenergy_imag: window of %d states beyond the contraction's limit", ng);
+  // Gn and Gp of every frequency stay resident for the frequency pairs
+  const size_t need = (size_t(2) * nwp * sk + size_t(nwp) * npad * npad + size_t(nwp) * naux_e * wq +
+                       size_t(naux) * ldm + size_t(nwp) * nwp * nz * 2) * 8;
+  if (c.budget > 0 && need > (c.budget > c.in_use ? c.budget - c.in_use : 0))
+    return Status::fail(RIGW_ERR_NOMEM, "g3w2_selfenergy_imag: %zu bytes needed beyond the HBM budget", need);
+  NvtxRange range("G3W2 self-energy");
+  const bool on_dev = (pr.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
+  cudaStream_t s = c.stream;
+  struct Events {
+    cudaEvent_t e[4] = {};
+    ~Events() {
+      for (cudaEvent_t x : e)
+        if (x) cudaEventDestroy(x);
+    }
+  } ev;
+  for (cudaEvent_t& x : ev.e) RIGW_CUDA_TRY(cudaEventCreate(&x));
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[0], s));
+
+  // window tensor, transposed once: Mft[P][a * wq + b]
+  DeviceBuffer b_in, b_mft, b_e, b_z;
+  const double* min = pr.m_full;
+  if (!on_dev) {
+    RIGW_TRY(b_in.allocate(&c, size_t(ng) * ng * naux * 8, "g3w2 window tensor"));
+    RIGW_CUDA_TRY(cudaMemcpyAsync(b_in.data(), pr.m_full, size_t(ng) * ng * naux * 8, cudaMemcpyHostToDevice, s));
+    min = reinterpret_cast<const double*>(b_in.data());
+  }
+  RIGW_TRY(b_mft.allocate(&c, size_t(naux) * ldm * 8, "g3w2 window tensor^T"));
+  double* mft = reinterpret_cast<double*>(b_mft.data());
+  RIGW_CUDA_TRY(cudaMemsetAsync(mft, 0, size_t(naux) * ldm * 8, s));
+  sox_transpose_kernel<<<dim3(unsigned(((long long)ng * ng + 31) / 32), unsigned((naux + 31) / 32)), dim3(32, 8), 0,
+                         s>>>(min, (long long)ng * ng, naux, TransposeMap{ng, wq, ng, 0, ng, 0}, mft, ldm);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  int launches = 1;
+  RIGW_TRY(b_e.allocate(&c, size_t(ng) * 8, "g3w2 energies"));
+  RIGW_TRY(b_z.allocate(&c, size_t(nz) * 16, "g3w2 omega_calc"));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_e.data(), pr.energy, size_t(ng) * 8, cudaMemcpyDefault, s));
+  RIGW_CUDA_TRY(cudaMemcpyAsync(b_z.data(), pr.omega_calc, size_t(nz) * 16, cudaMemcpyDefault, s));
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[1], s));
+
+  DeviceBuffer b_wt, b_x, b_gn, b_gp, b_part, b_out, b_iw;
+  RIGW_TRY(b_wt.allocate(&c, size_t(nwp) * npad * npad * 8, "g3w2 W~"));
+  RIGW_TRY(b_x.allocate(&c, size_t(nwp) * naux_e * wq * 8, "g3w2 X"));
+  RIGW_TRY(b_gn.allocate(&c, size_t(nwp) * sk * 8, "g3w2 Gn"));
+  RIGW_TRY(b_gp.allocate(&c, size_t(nwp) * sk * 8, "g3w2 Gp"));
+  RIGW_TRY(b_part.allocate(&c, size_t(nwp) * nwp * nz * 16, "g3w2 partial sums"));
+  double* wt = reinterpret_cast<double*>(b_wt.data());
+  double* dx = reinterpret_cast<double*>(b_x.data());
+  double* gn = reinterpret_cast<double*>(b_gn.data());
+  double* gp = reinterpret_cast<double*>(b_gp.data());
+  double* out = sigma;
+  if (!on_dev) {
+    RIGW_TRY(b_out.allocate(&c, size_t(nsig) * nz * 16, "g3w2 sigma"));
+    out = reinterpret_cast<double*>(b_out.data());
+  }
+  // W~_k = Y_k^T Y_k - 1 for every frequency (Y_k = U_k^-T, the identity part of the resident solve)
+  std::vector<GemmItem> iw;
+  for (int k = 0; k < nwp; ++k) {
+    const double* y = pd.rhs + size_t(k) * npad * pd.ldb;
+    for (int i0 = 0; i0 < npad; i0 += 128)
+      for (int j0 = 0; j0 < npad; j0 += 128) {
+        GemmItem g{};
+        g.A = y + i0;
+        g.lda = pd.ldb;
+        g.B = y + j0;
+        g.ldb = pd.ldb;
+        g.C = wt + size_t(k) * npad * npad + size_t(i0) * npad + j0;
+        g.ldc = npad;
+        g.m = std::min(128, npad - i0);
+        g.n = std::min(128, npad - j0);
+        g.k = npad;
+        g.flags = kSubIdentity;
+        g.diag = i0 - j0;
+        g.alpha = 1.0;
+        iw.push_back(g);
+      }
+  }
+  RIGW_TRY(upload_items(c, &b_iw, iw, "g3w2 W~ items"));
+  launch_dgemm_128x128(reinterpret_cast<const GemmItem*>(b_iw.data()), int(iw.size()), 1, s);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  ++launches;
+  if (smem > 48 * 1024)
+    RIGW_CUDA_TRY(cudaFuncSetAttribute(g3w2_contract_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem)));
+  for (int ml = 0; ml < nsig; ++ml) {
+    const long long colp = (long long)(pr.sig_first + ml) * wq;   // columns of M(p, .) in Mft
+    std::vector<GemmItem> ix, ig;
+    for (int k = 0; k < nwp; ++k) {
+      double* xk = dx + size_t(k) * naux_e * wq;
+      // X_k[Q][u] = sum_P W~_k[P][Q] M(p, u, P)
+      for (int q0 = 0; q0 < naux_e; q0 += 128)
+        for (int u0 = 0; u0 < wq; u0 += 128) {
+          GemmItem g{};
+          g.A = wt + size_t(k) * npad * npad + q0;
+          g.lda = npad;
+          g.B = mft + colp + u0;
+          g.ldb = int(ldm);
+          g.C = xk + size_t(q0) * wq + u0;
+          g.ldc = wq;
+          g.m = std::min(128, naux_e - q0);
+          g.n = std::min(128, wq - u0);
+          g.k = naux;
+          g.alpha = 1.0;
+          ix.push_back(g);
+        }
+      for (int v = 0; v < ng; ++v)
+        for (int w0 = 0; w0 < wq; w0 += 64)
+          for (int u0 = 0; u0 < wq; u0 += 128) {
+            GemmItem g{};
+            g.m = std::min(64, wq - w0);
+            g.n = std::min(128, wq - u0);
+            g.k = naux;
+            g.alpha = 1.0;
+            g.ldc = wq;
+            // Gn_k[v][w][u] = sum_Q M(v, w, Q) X_k[Q][u]
+            g.A = mft + (long long)v * wq + w0;
+            g.lda = int(ldm);
+            g.B = xk + u0;
+            g.ldb = wq;
+            g.C = gn + size_t(k) * sk + (size_t(v) * wq + w0) * wq + u0;
+            ig.push_back(g);
+            // Gp_k[v][w][u] = sum_Q X_k[Q][w] M(v, u, Q)
+            g.A = xk + w0;
+            g.lda = wq;
+            g.B = mft + (long long)v * wq + u0;
+            g.ldb = int(ldm);
+            g.C = gp + size_t(k) * sk + (size_t(v) * wq + w0) * wq + u0;
+            ig.push_back(g);
+          }
+    }
+    DeviceBuffer b_ix, b_ig;
+    RIGW_TRY(upload_items(c, &b_ix, ix, "g3w2 X items"));
+    RIGW_TRY(upload_items(c, &b_ig, ig, "g3w2 G items"));
+    launch_dgemm_128x128(reinterpret_cast<const GemmItem*>(b_ix.data()), int(ix.size()), 1, s);
+    launch_dgemm_64x128(reinterpret_cast<const GemmItem*>(b_ig.data()), int(ig.size()), 1, s);
+    RIGW_CUDA_TRY(cudaGetLastError());
+    G3w2Args a{gn, gp, sk, ng, wq, reinterpret_cast<const double*>(b_e.data()), pd.omega, pd.weight, nwp,
+               reinterpret_cast<const double*>(b_z.data()), nz, reinterpret_cast<double*>(b_part.data())};
+    g3w2_contract_kernel<<<dim3(unsigned(nwp * nwp), unsigned((nz + kG3Z - 1) / kG3Z)), kSosexThreads, smem, s>>>(a);
+    g3w2_reduce_kernel<<<nz, kSosexThreads, 0, s>>>(reinterpret_cast<const double*>(b_part.data()), nwp * nwp, nz,
+                                                     out + size_t(ml) * nz * 2);
+    RIGW_CUDA_TRY(cudaGetLastError());
+    launches += 4;
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));   // the item buffers of this state are released below
+  }
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[2], s));
+  if (!on_dev) RIGW_CUDA_TRY(cudaMemcpyAsync(sigma, out, size_t(nsig) * nz * 16, cudaMemcpyDeviceToHost, s));
+  RIGW_CUDA_TRY(cudaEventRecord(ev.e[3], s));
+  RIGW_CUDA_TRY(cudaEventSynchronize(ev.e[3]));
+  float t01 = 0.0f, t12 = 0.0f, t23 = 0.0f;
+  cudaEventElapsedTime(&t01, ev.e[0], ev.e[1]);
+  cudaEventElapsedTime(&t12, ev.e[1], ev.e[2]);
+  cudaEventElapsedTime(&t23, ev.e[2], ev.e[3]);
+  rigw_stats st{};
+  st.stage_ms[0] = t01;   // upload and transpose of the window tensor
+  st.stage_ms[1] = t12;   // W~, X, Gn, Gp products and the frequency-pair contractions
+  st.stage_ms[3] = t23;   // download
+  st.total_ms = double(t01) + t12 + t23;
+  st.kernel_launches = launches;
+  st.chunks = nsig;
   st.waves = 1;
   st.device_bytes_in_use = c.in_use;
   st.device_bytes_peak = c.peak;

@@ -84,6 +84,13 @@ class SosexProblem(C.Structure):
     ]
 
 
+class G3w2Problem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nstate", C.c_int), ("m_full", _dp), ("nsig", C.c_int), ("sig_first", C.c_int),
+        ("energy", _dp), ("nomega_calc", C.c_int), ("omega_calc", _dp), ("flags", C.c_int),
+    ]
+
+
 def _vertex_w_inst(inst):
     """The instance whose W window the vertex path factors: on that path the
     reference calls gw_selfenergy_grid with energy_g (src/m_selfenergy_evaluation.f90:496),
@@ -171,6 +178,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_qp_solve.argtypes = [C.c_void_p, C.POINTER(Problem), _dp, C.POINTER(Result)]
     lib.rigw_sox_selfenergy_imag.argtypes = [C.c_void_p, C.POINTER(SoxProblem), _dp]
     lib.rigw_sosex_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SosexProblem), _dp]
+    lib.rigw_g3w2_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(G3w2Problem), _dp]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -512,21 +520,22 @@ class Engine:
                     "rigw_sox_selfenergy_imag")
         return out[..., 0] + 1j * out[..., 1]
 
-    def gw_sox_imag(self, inst, precision: int = RIGW_FP64, m_ov=None) -> G0W0Output:
+    def gw_sox_imag(self, inst, precision: int = RIGW_FP64, m_ov=None, efermi: float | None = None) -> G0W0Output:
         """GW+SOX on the imaginary axis (postscf 'GW+SOX_PADE'): W and Sigma_c on
         the evaluation points, Sigma^SOX added to sigma_calc, then the
         Pade continuation and the QP equation (src/m_selfenergy_evaluation.f90:494-503,
         587-611; the imaginary-axis vertex path exists for imaginary_axis_pade only).
         W is built from energy_g when it is set, as gw_selfenergy_grid does with the
         energies it is given (src/m_gw_selfenergy_grid.f90:604)."""
+        ef = efermi_of(inst) if efermi is None else efermi
         erpa, egw, wpol = self.polarizability_grid_scalapack(_vertex_w_inst(inst), precision)
+        oc = ef + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
         try:
-            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst)
+            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst, omega_calc=oc)
         finally:
             wpol.release()
-        oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
         sigma = sigma + self.sox_selfenergy_imag_grid(inst, oc, m_ov)
-        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc)
+        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc, efermi=ef)
         out.erpa, out.egw = erpa, egw
         return out
 
@@ -557,25 +566,57 @@ class Engine:
                     "rigw_sosex_selfenergy_imag")
         return out[..., 0] + 1j * out[..., 1]
 
-    def gw_sosex_imag(self, inst, m_full, precision: int = RIGW_FP64, factor_sosex: float = 1.0) -> G0W0Output:
+    def gw_sosex_imag(self, inst, m_full, precision: int = RIGW_FP64, factor_sosex: float = 1.0,
+                      efermi: float | None = None, g3w2: bool = False) -> G0W0Output:
         """GW+SOSEX on the imaginary axis (postscf 'GW+SOSEX_PADE'; factor_sosex = 2
         for 'GW+2SOSEX_PADE'): W, then Sigma_c + Sigma^SOX + factor_sosex Sigma^SOSEX
         on the evaluation points, then the Pade continuation and the QP equation
         (src/m_selfenergy_evaluation.f90:494-503).  W is built from energy_g when it
         is set (src/m_gw_selfenergy_grid.f90:604)."""
+        ef = efermi_of(inst) if efermi is None else efermi
         erpa, egw, wpol = self.polarizability_grid_scalapack(_vertex_w_inst(inst), precision)
-        oc = efermi_of(inst) + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
+        oc = ef + 1j * inst.step_sigma_calc * np.arange(inst.nomega_sigma_calc)
         cg = getattr(inst, "ncore_g", 0)
         no = getattr(inst, "ncore_w", 0) + inst.nocc - cg
         try:
-            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst)
+            sigma = self.gw_selfenergy_imag_scalapack(wpol, inst, omega_calc=oc)
             sigma = sigma + self.sosex_selfenergy_imag_grid(wpol, inst, m_full, oc, factor_sosex)
+            if g3w2:
+                sigma = sigma + self.g3w2_selfenergy_imag_grid(wpol, inst, m_full, oc)
         finally:
             wpol.release()
         sigma = sigma + self.sox_selfenergy_imag_grid(inst, oc, m_full[:no, no:])
-        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc)
+        out = self.qp_solve(inst, sigma, RIGW_PADE, omega_calc=oc, efermi=ef)
         out.erpa, out.egw = erpa, egw
         return out
+
+    def g3w2_selfenergy_imag_grid(self, wpol: "WPol", inst, m_full, omega_calc) -> np.ndarray:
+        """G (W-v) G (W-v) G on the evaluation points ``omega_calc`` for the Sigma
+        states of ``inst`` (g3w2_selfenergy_imag_grid, src/m_g3w2_selfenergy.f90:2018-2196),
+        [nsig, nomega_calc] complex, with W from the resident factors of ``wpol``.
+        ``m_full`` is the window tensor [nstate_G, nstate_G, naux]."""
+        cg = getattr(inst, "ncore_g", 0)
+        mf = np.ascontiguousarray(m_full, dtype=np.float64)
+        ng = mf.shape[0]
+        e = inst.energy if getattr(inst, "energy_g", None) is None else inst.energy_g
+        ew = np.ascontiguousarray(np.asarray(e, dtype=np.float64)[cg:cg + ng])
+        oc = np.ascontiguousarray(np.stack([np.real(omega_calc), np.imag(omega_calc)], -1), dtype=np.float64)
+        gp = G3w2Problem()
+        gp.naux, gp.nstate = inst.naux, ng
+        gp.m_full, gp.energy, gp.omega_calc = _ptr(mf), _ptr(ew), _ptr(oc)
+        gp.nsig = inst.nsemax - inst.nsemin + 1
+        gp.sig_first = inst.nsemin - 1 - cg
+        gp.nomega_calc = oc.shape[0]
+        out = np.zeros((gp.nsig, gp.nomega_calc, 2))
+        self._check(self._lib.rigw_g3w2_selfenergy_imag(self._h, wpol.handle, C.byref(gp), _ptr(out)),
+                    "rigw_g3w2_selfenergy_imag")
+        return out[..., 0] + 1j * out[..., 1]
+
+    def gw_g3w2_imag(self, inst, m_full, precision: int = RIGW_FP64, efermi: float | None = None) -> G0W0Output:
+        """GW+G3W2 on the imaginary axis (postscf 'GW+G3W2_PADE'): Sigma_c, SOX,
+        2 SOSEX and G3W2 added to sigma_calc before the Pade fit
+        (src/m_selfenergy_evaluation.f90:494-503)."""
+        return self.gw_sosex_imag(inst, m_full, precision, factor_sosex=2.0, efermi=efermi, g3w2=True)
 
     def frequency_partials(self, inst, freq_index, precision: int = RIGW_FP64):
         """The share of one rank in MOLGW's frequency split ("poorman",
