@@ -66,6 +66,11 @@ def parse():
     ap.add_argument("--serving-stable-rate", type=float, default=8.0,
                     help="arrival rate (req/s) of the sustainable-load run of the serving block")
     ap.add_argument("--serving-stable-window", type=float, default=20.0)
+    ap.add_argument("--sweep-block", type=int, default=1,
+                    help="1: add the precision-sweep instance (FP64, BF16x3, Ozaki 4) to the default line")
+    ap.add_argument("--parallel", default="replicas", choices=["replicas", "frequencies"],
+                    help="N > 1: independent replicas (weak scaling) or the frequencies of one molecule "
+                         "sharded over the ranks with one all-reduce of Sigma_c (strong scaling)")
     ap.add_argument("--workload", default="single", choices=["single", "serve", "sweep", "aomo", "sox"])
     ap.add_argument("--sweep-reps", type=int, default=2)
     ap.add_argument("--serve-rate", type=float, default=200.0)
@@ -442,6 +447,41 @@ def run_serving_block(args) -> dict:
     return res
 
 
+def run_sweep_block(fp64_peak: float, bf16_peak: float) -> dict:
+    """The precision-sweep instance of the default line (Nocc=100, Nvirt=1100,
+    Naux=4000, 48 frequencies, seed 3, in device memory): one timed solve each in
+    FP64, BF16x3 and Ozaki INT8 with 4 slices after one untimed solve, QP-only
+    outputs, QP energies in meV and E_RPA against the FP64 solve of the same run."""
+    import torch
+    from molgw_b200 import synth
+    from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64, RIGW_OZAKI, Engine
+    no, nv, na, nw = 100, 1100, 4000, 48
+    inst, dev = synth.make_instance_device(no, nv, na, nw, 3)
+    torch.cuda.synchronize()
+    f_chi0 = float(nw) * na * (na + 1) * (no * nv)
+    out, ref = {}, None
+    for name, prec, products, peak in (("fp64", RIGW_FP64, 1, fp64_peak), ("bf16x3", RIGW_BF16X3, 3, bf16_peak),
+                                       ("ozaki4", RIGW_OZAKI(4), 10, 2.0 * bf16_peak)):
+        eng = Engine(0)
+        eng.g0w0(inst, prec, dev, qp_only=True)
+        o = eng.g0w0(inst, prec, dev, qp_only=True)
+        st = eng.last_stats()
+        eng.close()
+        if ref is None:
+            ref = o
+        ach = f_chi0 / (st["stage_ms"][1] * 1e-3) / 1e12
+        out[name] = {"ms_per_solve": st["total_ms"], "solves_per_s": 1e3 / st["total_ms"],
+                     "stage_ms": st["stage_ms"], "chi0_tflops_algorithmic": ach,
+                     "chi0_frac_of_peak": ach * products / peak, "tensor_products": products,
+                     "qp_diff_mev_vs_fp64": float(np.abs(o.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3),
+                     "erpa_rel_diff_vs_fp64": float(abs(o.erpa - ref.erpa) / abs(ref.erpa))}
+    del dev
+    torch.cuda.empty_cache()
+    out["speedup_bf16x3_vs_fp64"] = out["fp64"]["ms_per_solve"] / out["bf16x3"]["ms_per_solve"]
+    out["workload"] = "Nocc=100 Nvirt=1100 Naux=4000, 48 imaginary frequencies, QP-only (precision sweep instance)"
+    return out
+
+
 def run_sweep_line(args):
     """`--workload sweep`: the precision sweep on one large instance (Nocc=100,
     Nvirt=1100, Naux=4000, 48 frequencies, seed 3, generated in device memory):
@@ -684,6 +724,49 @@ def run_sox_line(args):
     print(json.dumps(line), flush=True)
 
 
+def run_frequency_sharded(args, rank, world, local):
+    """`--parallel frequencies`: each step is one G0W0 solve of the 21/207/840/32
+    instance with its 32 frequencies sharded over the ranks (round robin, MOLGW's
+    poorman split): W and Sigma_c of the rank's frequencies on its GPU, one NCCL
+    all-reduce of the partial Sigma_c and energies, the QP equation on the sum
+    (parallel.g0w0_frequency_sharded; the library calls are synchronous, so
+    CUDA events recorded after a device synchronisation bracket the whole step).
+    Strong scaling: the total work per step is fixed."""
+    import torch
+    import torch.distributed as dist
+    from molgw_b200 import parallel, synth
+    from molgw_b200.rigw import RIGW_FP64, Engine
+    inst = synth.single_instance_840()
+    eng = Engine(local)
+    ref = eng.g0w0(inst) if rank == 0 else None
+    for _ in range(args.warmup):
+        parallel.g0w0_frequency_sharded(eng, inst, RIGW_FP64)
+    dist.barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(args.steps):
+        out = parallel.g0w0_frequency_sharded(eng, inst, RIGW_FP64)
+    torch.cuda.synchronize()
+    e1.record()
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], device="cuda", dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    eng.close()
+    if rank == 0:
+        line = {"metric": METRIC, "value": args.steps / (total_ms * 1e-3), "unit": "solves/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": total_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64", "data": DATA,
+                "config": {**bench_config("fp64", world), "parallelism": f"frequencies over {world} ranks"},
+                "qp_diff_mev_vs_one_gpu": float(np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3),
+                "timing": "CUDA events around the steps after device synchronisation (synchronous library calls), "
+                          "max over ranks"}
+        print(json.dumps(line), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def run_reference(args, rank, world):
     """CPU restatement of the MOLGW path on the host cores (rank 0 only)."""
     if rank != 0:
@@ -756,6 +839,9 @@ def main():
         dist.barrier()
     from molgw_b200.rigw import RIGW_BF16X3, RIGW_FP64, Engine
 
+    if args.parallel == "frequencies" and world > 1:
+        run_frequency_sharded(args, rank, world, local)
+        return
     precision = RIGW_FP64 if args.precision == "fp64" else RIGW_BF16X3
     inst = synth.single_instance_840(seed=2 + rank)
     eng = Engine(local)
@@ -861,6 +947,15 @@ def main():
             batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2, args.batch_reps_fp64)
         except Exception as exc:    # reported, not hidden
             batched = {"error": str(exc)}
+    sweep = None
+    if args.sweep_block and world == 1:
+        eng.close()
+        torch.cuda.empty_cache()
+        try:
+            peaks0 = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()) if (ROOT / "MEASURED_PEAKS.json").exists() else {}
+            sweep = run_sweep_block(measured_fp64_peak(torch), float(peaks0.get("bf16_tflops", 1590.0)))
+        except Exception as exc:    # reported, not hidden
+            sweep = {"error": str(exc)}
     serving = None
     if args.serving_window > 0 and world == 1:
         # the request loop sizes its worker arenas from free memory: release this
@@ -903,6 +998,7 @@ def main():
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
             "other_precision": alt,
             "batched": batched,
+            "sweep": sweep,
             "serving": serving,
         }
         if alt and "chi0_ms" in alt and alt["precision"] == "bf16x3":
