@@ -447,6 +447,59 @@ def run_serving_block(args) -> dict:
     return res
 
 
+def run_ao_to_qp_block(reps: int = 3) -> dict:
+    """From the AO tensor to the QP energies for the 21/207/840/32 workload:
+    B(mu nu, P) over all 26 106 pairs of nbf = 228 functions (N(0, s^2), s the
+    scale of the 840 instance's M, so that M = C B C^T has its statistics), C
+    orthonormal, the instance's energies; wall time per solve from a page-locked
+    host AO tensor.  "device": Engine.g0w0_from_ao (one upload of the AO tensor,
+    both transforms and the solve on the device).  "host": the two host-pointer
+    transforms (each uploads the AO tensor) and the host-pointer solve (uploads M)."""
+    import torch
+    from molgw_b200 import synth
+    from molgw_b200.rigw import Engine
+    inst = synth.single_instance_840()
+    nbf, naux, nocc = inst.nstate, inst.naux, inst.nocc
+    rng = np.random.default_rng(228)
+    pairs = np.array([(k, l) for l in range(1, nbf + 1) for k in range(1, l + 1)], dtype=np.int32)
+    eri3 = pinned_copy(rng.standard_normal((naux, len(pairs))) * float(inst.m_ia.std()))
+    c = np.linalg.qr(rng.standard_normal((nbf, nbf)))[0].T.copy()
+    grid = dict(nomega_sigma=inst.nomega_sigma, step_sigma=inst.step_sigma, nomega_sigma_calc=inst.nomega_sigma_calc,
+                step_sigma_calc=inst.step_sigma_calc, eta=inst.eta)
+    eng = Engine(0)
+
+    def device_path():
+        return eng.g0w0_from_ao(eri3, pairs, c, inst.energy, inst.occupation, inst.nomega, inst.nsemin,
+                                inst.nsemax, **grid)
+
+    def host_path():
+        from dataclasses import replace
+        m_ia = eng.calculate_eri_3center_mo(eri3, pairs, c, nocc + 1, nbf, 1, nocc)
+        m_pm = eng.calculate_eri_3center_mo(eri3, pairs, c, 1, nbf, inst.nsemin, inst.nsemax)
+        return eng.g0w0(replace(inst, m_ia=m_ia, m_sigma=m_pm))
+
+    res = {}
+    outs = {}
+    for name, fn in (("device", device_path), ("host", host_path)):
+        fn()
+        walls = []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            outs[name] = fn()
+            walls.append((time.perf_counter() - t0) * 1e3)
+        res[name] = {"wall_ms": float(np.median(walls)), "solves_per_s": 1e3 / float(np.median(walls))}
+    eng.close()
+    small = 8 * (2 * nbf + nbf * nbf * 2)
+    res["device"]["h2d_bytes"] = int(eri3.nbytes) + small
+    res["host"]["h2d_bytes"] = 2 * int(eri3.nbytes) + small + 8 * naux * (nocc * (nbf - nocc) + 2 * nbf)
+    res["qp_diff_mev_device_vs_host"] = float(np.abs(outs["device"].energy_qp_g - outs["host"].energy_qp_g).max()
+                                              * HA_EV * 1e3)
+    res["workload"] = (f"AO tensor of nbf={nbf}, Naux={naux} ({len(pairs)} pairs, {eri3.nbytes / 1e6:.0f} MB, "
+                       "page-locked) to QP energies, Nocc=21, 32 frequencies, FP64")
+    return res
+
+
 def run_sweep_block(fp64_peak: float, bf16_peak: float) -> dict:
     """The precision-sweep instance of the default line (Nocc=100, Nvirt=1100,
     Naux=4000, 48 frequencies, seed 3, in device memory): one timed solve each in
@@ -947,6 +1000,15 @@ def main():
             batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2, args.batch_reps_fp64)
         except Exception as exc:    # reported, not hidden
             batched = {"error": str(exc)}
+    ao_to_qp = None
+    if world == 1:
+        # the blocks below use their own contexts: release this one's plan arenas first
+        eng.close()
+        torch.cuda.empty_cache()
+        try:
+            ao_to_qp = run_ao_to_qp_block()
+        except Exception as exc:    # reported, not hidden
+            ao_to_qp = {"error": str(exc)}
     sweep = None
     if args.sweep_block and world == 1:
         eng.close()
@@ -998,6 +1060,7 @@ def main():
             "hbm_peak_gbs_measured": peaks.get("hbm_gbs"),
             "other_precision": alt,
             "batched": batched,
+            "ao_to_qp": ao_to_qp,
             "sweep": sweep,
             "serving": serving,
         }

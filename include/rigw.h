@@ -194,6 +194,15 @@ RIGW_API int rigw_eri_3center_mo_precision(rigw_ctx* ctx, int nbf, int nstate, i
                                            const int* index_basis, const double* eri3, const double* c_matrix,
                                            int mstate_min, int mstate_max, int nstate_min, int nstate_max,
                                            double* out, int precision);
+/* The same with ``flags``: RIGW_PROBLEM_DEVICE_POINTERS reads eri3 and writes out
+ * in device memory (index_basis and c_matrix stay host arrays), so that the MO
+ * tensor can go straight into rigw_g0w0 / rigw_polarizability_imag in device-
+ * pointer mode, as polarizability_grid_scalapack calls the transform itself
+ * (src/m_gw_selfenergy_grid.f90:92): the AO tensor crosses PCIe once. */
+RIGW_API int rigw_eri_3center_mo_ex(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux,
+                                    const int* index_basis, const double* eri3, const double* c_matrix,
+                                    int mstate_min, int mstate_max, int nstate_min, int nstate_max, double* out,
+                                    int precision, int flags);
 
 /* chi0, eps(iw) = 1 - chi0 and its factorization for every frequency; keeps the
  * factors resident on the device in *wpol.  Uses the W-window fields of

@@ -246,4 +246,14 @@ int rigw_eri_3center_mo_precision(rigw_ctx* ctx, int nbf, int nstate, int npair,
                                           mstate_min, mstate_max, nstate_min, nstate_max, out, precision));
 }
 
+int rigw_eri_3center_mo_ex(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux, const int* index_basis,
+                           const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
+                           int nstate_min, int nstate_max, double* out, int precision, int flags) {
+  if (!ctx) return RIGW_ERR_ARG;
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::eri_3center_mo(ctx->impl, nbf, nstate, npair, naux, index_basis, eri3, c_matrix,
+                                          mstate_min, mstate_max, nstate_min, nstate_max, out, precision, flags));
+}
+
 }  // extern "C"

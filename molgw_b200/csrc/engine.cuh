@@ -276,7 +276,7 @@ Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem
 Status g3w2_selfenergy_imag(Context& c, const Wpol& w, const rigw_g3w2_problem& pr, double* sigma);
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
-                      int nstate_min, int nstate_max, double* out, int precision);
+                      int nstate_min, int nstate_max, double* out, int precision, int flags = 0);
 bool bf16x3_available();
 Status validate_batch(int n, const rigw_problem* probs, std::vector<Shape>* shapes);
 Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* res);

@@ -119,9 +119,12 @@ Status run_tc_items(Context& c, const std::vector<TcItem>& items, bool ozaki = f
 
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
-                      int nstate_min, int nstate_max, double* out, int precision) {
+                      int nstate_min, int nstate_max, double* out, int precision, int flags) {
   if (nbf <= 0 || nstate <= 0 || npair <= 0 || naux <= 0 || !index_basis || !eri3 || !c_matrix || !out)
     return Status::fail(RIGW_ERR_ARG, "eri_3center_mo: invalid arguments");
+  // RIGW_PROBLEM_DEVICE_POINTERS: the AO tensor is read and the MO tensor written
+  // in device memory (index_basis and c_matrix, both small, stay host arrays)
+  const bool on_dev = (flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
   NvtxRange range("3-center AO to MO transform");
   if (precision != RIGW_FP64 && precision != RIGW_BF16X3 && !is_ozaki(precision))
     return Status::fail(RIGW_ERR_UNSUPPORTED, "eri_3center_mo: precision %d (FP64, BF16X3 or OZAKI(3..7))",
@@ -152,7 +155,7 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   RIGW_TRY(b_ctm.allocate(&c, ctm.size() * 8, "aomo ctm"));
   RIGW_TRY(b_ctn.allocate(&c, ctn.size() * 8, "aomo ctn"));
   RIGW_TRY(b_idx.allocate(&c, size_t(2) * npair * sizeof(int), "aomo index"));
-  RIGW_TRY(b_eri.allocate(&c, size_t(pc) * npair * 8, "aomo eri3 chunk"));
+  if (!on_dev) RIGW_TRY(b_eri.allocate(&c, size_t(pc) * npair * 8, "aomo eri3 chunk"));
   RIGW_TRY(b_full.allocate(&c, size_t(nbf) * nbf * pcp * 8, "aomo unpacked"));
   RIGW_TRY(b_t.allocate(&c, size_t(ncp) * nbf * pcp * 8, "aomo half"));
   RIGW_TRY(b_out.allocate(&c, size_t(ncp) * mcp * pcp * 8, "aomo out chunk"));
@@ -217,11 +220,13 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
   for (int p0 = 0; p0 < naux; p0 += pc) {
     const int cnt = std::min(pc, naux - p0);
     RIGW_CUDA_TRY(cudaEventRecord(ev.e[0], s));
-    RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), eri3 + size_t(p0) * npair, size_t(cnt) * npair * 8,
-                                  cudaMemcpyHostToDevice, s));
+    const double* chunk = eri3 + size_t(p0) * npair;
+    if (!on_dev) {
+      RIGW_CUDA_TRY(cudaMemcpyAsync(b_eri.data(), chunk, size_t(cnt) * npair * 8, cudaMemcpyHostToDevice, s));
+      chunk = reinterpret_cast<const double*>(b_eri.data());
+    }
     RIGW_CUDA_TRY(cudaMemsetAsync(dfull, 0, size_t(nbf) * nbf * pcp * 8, s));
-    AomoUnpackItem it{reinterpret_cast<const double*>(b_eri.data()), reinterpret_cast<const int*>(b_idx.data()),
-                      dfull, cnt, pcp, npair, nbf, 0};
+    AomoUnpackItem it{chunk, reinterpret_cast<const int*>(b_idx.data()), dfull, cnt, pcp, npair, nbf, 0};
     RIGW_CUDA_TRY(cudaMemcpyAsync(b_item.data(), &it, sizeof(it), cudaMemcpyHostToDevice, s));
     dim3 grid((npair + 31) / 32, (cnt + 31) / 32);
     aomo_unpack_kernel<<<grid, 256, 0, s>>>(reinterpret_cast<const AomoUnpackItem*>(b_item.data()));
@@ -341,7 +346,7 @@ Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, cons
     for (int n = 0; n < nc; ++n)
       RIGW_CUDA_TRY(cudaMemcpy2DAsync(out + (size_t(n) * mc) * naux + p0, size_t(naux) * 8,
                                       dout + size_t(n) * mcp * pcp, size_t(pcp) * 8, size_t(cnt) * 8, mc,
-                                      cudaMemcpyDeviceToHost, s));
+                                      on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s));
     RIGW_CUDA_TRY(cudaEventRecord(ev.e[3], s));
     RIGW_CUDA_TRY(cudaStreamSynchronize(s));
     stage[0] += elapsed(0, 1);

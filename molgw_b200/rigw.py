@@ -168,6 +168,8 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_imag_grid.argtypes = [C.c_int, _dp, _dp]
     lib.rigw_eri_3center_mo.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
                                         _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp]
+    lib.rigw_eri_3center_mo_ex.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int),
+                                           _dp, _dp, C.c_int, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int]
     lib.rigw_eri_3center_mo_precision.argtypes = [C.c_void_p, C.c_int, C.c_int, C.c_int, C.c_int,
                                                   C.POINTER(C.c_int), _dp, _dp, C.c_int, C.c_int, C.c_int,
                                                   C.c_int, _dp, C.c_int]
@@ -260,6 +262,7 @@ class Engine:
             raise RigwError(rc, f"rigw_create(device={device})")
         self._h = h
         self._keep = []
+        self.device = device
 
     def close(self):
         if self._h:
@@ -726,18 +729,59 @@ class Engine:
             wpol.release()
         return outs
 
-    def calculate_eri_3center_mo(self, eri3: np.ndarray, index_basis: np.ndarray, c_matrix: np.ndarray,
+    def calculate_eri_3center_mo(self, eri3, index_basis: np.ndarray, c_matrix: np.ndarray,
                                  m_min: int, m_max: int, n_min: int, n_max: int,
-                                 precision: int = RIGW_FP64) -> np.ndarray:
-        naux, npair = eri3.shape
+                                 precision: int = RIGW_FP64):
+        """calculate_eri_3center_mo (src/m_eri_ao_mo.f90:416-582): eri3 [naux, npair]
+        (pair-packed, diagonal x0.5), c_matrix [nstate, nbf]; returns [n, m, naux].
+        When ``eri3`` is a CUDA tensor the transform reads it in place and returns a
+        CUDA tensor (RIGW_PROBLEM_DEVICE_POINTERS): nothing crosses PCIe."""
+        naux, npair = int(eri3.shape[0]), int(eri3.shape[1])
         nstate, nbf = c_matrix.shape
         idx = np.ascontiguousarray(index_basis, dtype=np.int32)
-        out = np.zeros((n_max - n_min + 1, m_max - m_min + 1, naux))
+        cm = np.ascontiguousarray(c_matrix, dtype=np.float64)
+        shape = (n_max - n_min + 1, m_max - m_min + 1, naux)
+        if hasattr(eri3, "is_cuda") and eri3.is_cuda:
+            import torch
+            out = torch.empty(shape, dtype=torch.float64, device=eri3.device)
+            self._check(self._lib.rigw_eri_3center_mo_ex(
+                self._h, nbf, nstate, npair, naux, idx.ctypes.data_as(C.POINTER(C.c_int)), _ptr(eri3), _ptr(cm),
+                m_min, m_max, n_min, n_max, _ptr(out), precision, RIGW_PROBLEM_DEVICE_POINTERS),
+                "rigw_eri_3center_mo_ex")
+            return out
+        out = np.zeros(shape)
         self._check(self._lib.rigw_eri_3center_mo_precision(
             self._h, nbf, nstate, npair, naux, idx.ctypes.data_as(C.POINTER(C.c_int)),
-            _ptr(np.ascontiguousarray(eri3)), _ptr(np.ascontiguousarray(c_matrix)), m_min, m_max, n_min, n_max,
+            _ptr(np.ascontiguousarray(eri3)), _ptr(cm), m_min, m_max, n_min, n_max,
             _ptr(out), precision), "rigw_eri_3center_mo_precision")
         return out
+
+    def g0w0_from_ao(self, eri3, index_basis: np.ndarray, c_matrix: np.ndarray, energy: np.ndarray,
+                     occupation: np.ndarray, nomega: int, nsemin: int, nsemax: int, precision: int = RIGW_FP64,
+                     aomo_precision: int = RIGW_FP64, **grid) -> G0W0Output:
+        """The drop-in path from the AO tensor: the W-window transform (m empty, n
+        occupied) and the Sigma transform (m all states, n the Sigma states) on the
+        device, then the solve in device-pointer mode, as
+        polarizability_grid_scalapack / gw_selfenergy_imag_scalapack call
+        calculate_eri_3center_mo themselves (src/m_gw_selfenergy_grid.f90:92, 270).
+        ``eri3`` is [naux, npair], host memory (uploaded once) or a CUDA tensor."""
+        import torch
+        from .synth import GWInstance
+        dev = eri3 if (hasattr(eri3, "is_cuda") and eri3.is_cuda) else \
+            torch.from_numpy(np.ascontiguousarray(eri3, dtype=np.float64)).to(f"cuda:{self.device}")
+        e = np.ascontiguousarray(energy, dtype=np.float64)
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        nstate = e.size
+        nocc = int(np.sum(occ > 0))
+        m_ia = self.calculate_eri_3center_mo(dev, index_basis, c_matrix, nocc + 1, nstate, 1, nocc, aomo_precision)
+        m_pm = self.calculate_eri_3center_mo(dev, index_basis, c_matrix, 1, nstate, nsemin, nsemax, aomo_precision)
+        inst = GWInstance(nocc=nocc, nvirt=nstate - nocc, naux=int(dev.shape[0]), nomega=nomega, energy=e,
+                          occupation=occ, m_ia=None, m_sigma=None, nsemin=nsemin, nsemax=nsemax, **grid)
+        small = {"e_occ": e[:nocc], "e_virt": e[nocc:], "occ_occ": occ[:nocc], "occ_virt": occ[nocc:], "e_p": e,
+                 "e_sig": e[nsemin - 1:nsemax], "occ_sig": occ[nsemin - 1:nsemax]}
+        arrays = {k: torch.from_numpy(np.ascontiguousarray(v)).to(dev.device) for k, v in small.items()}
+        arrays.update(m_ia=m_ia, m_pm=m_pm)
+        return self.g0w0(inst, precision, device_arrays=arrays)
 
 
 class WPol:
