@@ -145,6 +145,7 @@ Status Context::init(int dev, size_t budget_bytes, int want_priority, bool block
   uint64_t keep = ~uint64_t(0);
   RIGW_CUDA_TRY(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
   RIGW_CUDA_TRY(prepare_dgemm_kernels());
+  RIGW_CUDA_TRY(prepare_syrk_f64_tma());
   RIGW_CUDA_TRY(prepare_tc_kernels());
   RIGW_CUDA_TRY(prepare_ozaki_kernels());
   RIGW_CUDA_TRY(cudaFuncSetAttribute(chol_diag_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -357,7 +358,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       pp.off_in_omega = L.take(size_t(sh.nomega) * D);
       pp.off_in_weight = L.take(size_t(sh.nomega) * D);
       off[i].mp = L.take(size_t(d.nia_pad) * d.npad * D);
-      if (sh.precision == RIGW_BF16X3) {
+      if (sh.precision == RIGW_FP64) {
+        off[i].tmap = L.take(256);   // tensor maps of mp and dscale (TMA-staged FP64 chi0)
+      } else if (sh.precision == RIGW_BF16X3) {
         off[i].xs = L.take(size_t(split_group(sh)) * 2 * d.npad * d.nia_pad * 2);
         off[i].tmap = L.take(128);
       } else if (is_ozaki(sh.precision)) {
@@ -476,6 +479,11 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       }
       p.tnorm = dp(off[i].tnorm);
       p.dscale = dp(off[i].dscale);
+      if (sh.precision == RIGW_FP64) {
+        alignas(64) unsigned char maps[256];
+        RIGW_TRY(make_f64_tmaps(maps, p.mp, d.npad, d.nia_pad, p.dscale, sh.nomega));
+        RIGW_CUDA_TRY(cudaMemcpyAsync(base + off[i].tmap, maps, sizeof(maps), cudaMemcpyHostToDevice, ctx->stream));
+      }
       p.eps = dp(off[i].eps);
       p.winv = dp(off[i].winv);
       p.logdet = dp(off[i].logdet);
@@ -613,7 +621,28 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         // diagonal BMC x BMC block lies below it, and end at naux
         if (npad > sh.naux)
           for (int w = 0; w < sh.nomega; ++w) wl_pad_.push_back({i, w, 0, 0});
-        for (int ti = 0; ti < sh.naux; ti += BMC)
+        // 64-row items: the TMA-staged kernel (its operands by TMA from the tensor
+        // maps of mp and dscale); 128-row items (a tuner candidate): the cp.async engine
+        if (BMC == 64)
+          for (int ti = 0; ti < sh.naux; ti += BMC)
+            for (int tj = ti; tj < sh.naux; tj += BMN) {
+              F64SyrkItem f{};
+              f.tmap_m = base + off[i].tmap;
+              f.tmap_d = base + off[i].tmap + 128;
+              f.C = p.eps + size_t(ti) * npad + tj;
+              f.err = p.err;
+              f.ti = ti;
+              f.tj = tj;
+              f.m = std::min(BMC, sh.naux - ti);
+              f.n = std::min(BMN, sh.naux - tj);
+              f.ktiles = p.nia_pad / 16;
+              f.ldc = npad;
+              f.diag = ti - tj;
+              f.nw = sh.nomega;
+              f.sC = (long long)npad * npad;
+              fl_syrk_.push_back(f);
+            }
+        for (int ti = 0; BMC != 64 && ti < sh.naux; ti += BMC)
           for (int tj = ti; tj < sh.naux; tj += BMN) {
             GemmItem g{};
             g.A = p.mp + ti;
@@ -750,6 +779,9 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 
   // chi0 items longest first: the block scheduler hands out CTAs in index order,
   // so a ragged batch ends on short tiles (results do not depend on the order)
+  std::stable_sort(fl_syrk_.begin(), fl_syrk_.end(), [](const F64SyrkItem& a, const F64SyrkItem& b) {
+    return double(a.ktiles) * a.m * a.n * std::max(a.nw, 1) > double(b.ktiles) * b.m * b.n * std::max(b.nw, 1);
+  });
   std::stable_sort(gl_syrk_.begin(), gl_syrk_.end(), [](const GemmItem& a, const GemmItem& b) {
     return double(a.k) * a.m * a.n * std::max(a.nw, 1) > double(b.k) * b.m * b.n * std::max(b.nw, 1);
   });
@@ -786,6 +818,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
       for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const GemmItem*>(src)[j].nw);
     if (kind == 13 || kind == 20 || kind == 21)
       for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const TcItem*>(src)[j].nw);
+    if (kind == 22)
+      for (size_t j = 0; j < n; ++j) ny = std::max(ny, static_cast<const F64SyrkItem*>(src)[j].nw);
     pend.push_back({kind, src, elem * n, int(n), arg, stream, wait_ev, rec_ev, ny});
     return true;
   };
@@ -793,6 +827,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   add(2, wl_rhs_.data(), sizeof(WorkItem), wl_rhs_.size(), 0);
   add(3, wl_mnorm_.data(), sizeof(WorkItem), wl_mnorm_.size(), 0);
   add(1, gl_syrk_.data(), sizeof(GemmItem), gl_syrk_.size(), 0);
+  add(22, fl_syrk_.data(), sizeof(F64SyrkItem), fl_syrk_.size(), 0);
   for (size_t g = 0; g < wl_split_.size(); ++g) {
     add(12, wl_split_[g].data(), sizeof(WorkItem), wl_split_[g].size(), 0);
     add(13, tl_syrk_[g].data(), sizeof(TcItem), tl_syrk_[g].size(), 0);
@@ -880,7 +915,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
 static int stage_of(int kind) {
   switch (kind) {
     case 0: case 2: case 3: return 0;
-    case 1: case 12: case 13: case 15: case 16: case 17: case 18: case 19: case 20: case 21: return 1;
+    case 1: case 12: case 13: case 15: case 16: case 17: case 18: case 19: case 20: case 21: case 22: return 1;
     case -1: case 4: case 5: case 6: case 14: return 2;
     default: return 3;
   }
@@ -912,6 +947,7 @@ void Plan::record(cudaStream_t s0, int stage) {
       case 16: pad_eps_kernel<<<L.count, 256, 0, s>>>(probs_dev_, wl); break;
       case 12: launch_split_bf16x3(probs_dev_, wl, L.count, s); break;
       case 13: launch_syrk_bf16x3(reinterpret_cast<const TcItem*>(lb + L.off), L.count, L.ny, s); break;
+      case 22: launch_syrk_f64_tma(reinterpret_cast<const F64SyrkItem*>(lb + L.off), L.count, L.ny, s); break;
       case 17: launch_ozaki_zero(probs_dev_, wl, L.count, s); break;
       case 18: launch_ozaki_rowmax(probs_dev_, wl, L.count, s); break;
       case 19: launch_ozaki_slice(probs_dev_, wl, L.count, s); break;

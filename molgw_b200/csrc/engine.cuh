@@ -168,6 +168,7 @@ class Plan {
   std::vector<WorkItem> wl_pack_, wl_rhs_, wl_mnorm_, wl_energy_, wl_vchiv_, wl_sigma_, wl_pade_;
   std::vector<std::vector<WorkItem>> wl_diag_;
   std::vector<GemmItem> gl_syrk_;
+  std::vector<F64SyrkItem> fl_syrk_;              // FP64 chi0, TMA-staged (64-row items)
   std::vector<std::vector<WorkItem>> wl_split_;   // per frequency group
   std::vector<std::vector<TcItem>> tl_syrk_;
   std::vector<WorkItem> wl_ozzero_, wl_rowmax_;    // Ozaki: row maxima over every frequency
@@ -283,6 +284,9 @@ Status solve_batch(Context& c, int n, const rigw_problem* probs, rigw_result* re
 Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* rep);
 size_t available_bytes(Context& c);
 Status make_split_tmap(void* host_map, const void* xs, int kpad, long long rows);
+// The two tensor maps of the TMA-staged FP64 chi0 (256 bytes at host_maps):
+// mp [nia_pad][npad] in 16 x 16 boxes with 128-byte swizzle, dscale [nomega][nia_pad] in 16 x 1 boxes.
+Status make_f64_tmaps(void* host_maps, const double* mp, int npad, int nia_pad, const double* dscale, int nomega);
 // box_bytes 128: 128-byte swizzle (syrk_ozaki_kernel); 64: 64-byte swizzle (syrk_ozaki_fused_kernel)
 Status make_ozaki_tmap(void* host_map, const void* xq, int kpad, long long rows, int box_bytes = 128);
 

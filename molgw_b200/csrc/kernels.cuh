@@ -97,6 +97,24 @@ constexpr int kOzaFusedMaxSlices = 4;
 cudaError_t prepare_ozaki_kernels();
 cudaError_t prepare_tc_kernels();
 
+// FP64 chi0 with TMA-staged operands (syrk_f64_tma.cu): one 64 x 128 upper tile
+// of eps(iw) = 1 + sum_t M[t][i] D_w(t) M[t][j] per CTA, frequency = blockIdx.y.
+struct F64SyrkItem {
+  const void* tmap_m;   // CUtensorMap of mp [nia_pad][npad] (16 x 16 boxes, 128-byte swizzle)
+  const void* tmap_d;   // CUtensorMap of dscale [nomega][nia_pad] (16 x 1 boxes)
+  double* C;            // &eps[0][ti][tj]
+  int* err;
+  int ti, tj;           // first auxiliary row (A) and column (B) of the tile
+  int m, n;             // rows and columns stored (<= 64, <= 128, even)
+  int ktiles;           // nia_pad / 16
+  int ldc;              // npad
+  int diag;             // ti - tj: identity where col - row == diag
+  int nw;               // frequencies (grid y)
+  long long sC;         // doubles between the eps blocks of two frequencies
+};
+void launch_syrk_f64_tma(const F64SyrkItem* items, int n, int ny, cudaStream_t s);
+cudaError_t prepare_syrk_f64_tma();
+
 // Host-side launchers of the DMMA tile engine (gemm_f64.cu).
 // grid (n items) x (ny frequencies): CTAs with blockIdx.y >= item.nw return at once
 void launch_dgemm_128x128(const GemmItem* items, int n, int ny, cudaStream_t s);
