@@ -447,6 +447,56 @@ def run_serving_block(args) -> dict:
     return res
 
 
+def h2o_instance():
+    """The H2O cc-pVDZ G0W0@HF workload (HF in cc-pVDZ with cc-pVDZ-RI, 24
+    functions, 84 auxiliary functions, 5 occupied, 16 frequencies, HOMO and
+    LUMO) from its committed fixture, with the oracle's QP energies stored there."""
+    from molgw_b200.synth import GWInstance
+    d = np.load(ROOT / "tests" / "golden" / "h2o_ccpvdz.npz")
+    c, b3 = d["c_matrix"], d["b3_ao"]
+    m = np.einsum("ip,jq,ijP->pqP", c, c, b3, optimize=True)
+    nocc = int(np.sum(d["occupation"] > 0))
+    grid = {k: v for k, v in json.loads(str(d["workload_grid"])).items() if k != "nomega"}
+    inst = GWInstance(nocc=nocc, nvirt=m.shape[0] - nocc, naux=m.shape[2], nomega=16, energy=d["energy"].copy(),
+                      occupation=d["occupation"].copy(), m_ia=np.ascontiguousarray(m[:nocc, nocc:]),
+                      m_sigma=np.ascontiguousarray(m[nocc - 1:nocc + 1]), nsemin=nocc, nsemax=nocc + 1, **grid)
+    return inst, d["oracle_qp"]
+
+
+def run_h2o_block(reps: int = 20, batch: int = 256) -> dict:
+    """The H2O cc-pVDZ workload: one FP64 solve at a time through the host-pointer
+    C ABI (wall time per call, host buffers, copies inside) and ``batch`` copies
+    in one batched call; QP energies against the oracle's, stored in the fixture."""
+    import torch
+    from molgw_b200.rigw import Engine
+    inst, ref_qp = h2o_instance()
+    eng = Engine(0)
+    for _ in range(3):
+        out = eng.g0w0(inst)
+    walls, dev = [], []
+    for _ in range(reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        out = eng.g0w0(inst)
+        walls.append((time.perf_counter() - t0) * 1e3)
+        dev.append(eng.last_stats()["total_ms"])
+    eng.g0w0_batch([inst] * batch)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    outs = eng.g0w0_batch([inst] * batch)
+    bwall = time.perf_counter() - t0
+    eng.close()
+    err = max(float(np.abs(o.energy_qp_g - ref_qp).max()) for o in [out] + outs) * HA_EV * 1e3
+    return {"workload": "H2O HF cc-pVDZ (24 bf) / cc-pVDZ-RI (84), 5 occupied, 16 Gauss-Legendre frequencies, "
+                        "HOMO+LUMO, FP64; inputs from the oracle's Gaussian front end (pinned on the reference's "
+                        "H2O SCF and RI-MP2 known answers)",
+            "single_wall_ms": float(np.median(walls)), "single_device_ms": float(np.median(dev)),
+            "single_solves_per_s": 1e3 / float(np.median(walls)),
+            "batch": batch, "batch_solves_per_s": batch / bwall,
+            "homo_lumo_ev": [float(out.energy_qp_g[0] * HA_EV), float(out.energy_qp_g[1] * HA_EV)],
+            "qp_error_mev_vs_oracle": err}
+
+
 def run_ao_to_qp_block(reps: int = 3) -> dict:
     """From the AO tensor to the QP energies for the 21/207/840/32 workload:
     B(mu nu, P) over all 26 106 pairs of nbf = 228 functions (N(0, s^2), s the
@@ -1000,7 +1050,7 @@ def main():
             batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2, args.batch_reps_fp64)
         except Exception as exc:    # reported, not hidden
             batched = {"error": str(exc)}
-    ao_to_qp = None
+    ao_to_qp = h2o = None
     if world == 1:
         # the blocks below use their own contexts: release this one's plan arenas first
         eng.close()
@@ -1009,6 +1059,10 @@ def main():
             ao_to_qp = run_ao_to_qp_block()
         except Exception as exc:    # reported, not hidden
             ao_to_qp = {"error": str(exc)}
+        try:
+            h2o = run_h2o_block()
+        except Exception as exc:    # reported, not hidden
+            h2o = {"error": str(exc)}
     sweep = None
     if args.sweep_block and world == 1:
         eng.close()
@@ -1061,6 +1115,7 @@ def main():
             "other_precision": alt,
             "batched": batched,
             "ao_to_qp": ao_to_qp,
+            "h2o": h2o,
             "sweep": sweep,
             "serving": serving,
         }
@@ -1086,6 +1141,15 @@ def main():
             out = outs[-1]
             line["qp_error_mev_vs_oracle"] = float(np.abs(out.energy_qp_g - ref.energy_qp_g).max() * HA_EV * 1e3)
             line["homo_lumo_ev"] = [float(out.ehomo * HA_EV), float(out.elumo * HA_EV)]
+            if h2o and "error" not in h2o:
+                hinst, _ = h2o_instance()
+                with threadpool_limits(limits=cores):
+                    t0 = time.perf_counter()
+                    for _ in range(5):
+                        oracle_solve(hinst)
+                    dt = (time.perf_counter() - t0) / 5
+                h2o["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": cores, "kind": "port",
+                                       "sample": "five G0W0 solves of the H2O workload, CPU restatement"}
         print(json.dumps(line), flush=True)
     eng.close()
     if world > 1:

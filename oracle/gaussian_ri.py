@@ -38,8 +38,11 @@ What it restates, and from where:
 """
 from __future__ import annotations
 
+import ctypes
+import subprocess
 from dataclasses import dataclass, field
 from math import comb, factorial, sqrt, pi
+from pathlib import Path
 
 import numpy as np
 from scipy import special
@@ -171,6 +174,7 @@ class BasisFunctions:
     prims: list                    # per Cartesian function: (center, exps, coefs incl. primitive norms, (i,j,k))
     cart_to_pure: np.ndarray       # [nbf_pure, nbf_cart]
     shell_of: list                 # pure function -> shell index
+    shells: list = field(default_factory=list)
 
 
 def build_functions(shells: list[Shell]) -> BasisFunctions:
@@ -192,9 +196,9 @@ def build_functions(shells: list[Shell]) -> BasisFunctions:
     for start, tb in blocks:
         T[r:r + tb.shape[0], start:start + tb.shape[1]] = tb
         r += tb.shape[0]
-    bf = BasisFunctions(prims, T, shell_of)
+    bf = BasisFunctions(prims, T, shell_of, list(shells))
     # every pure function normalized to one (the contraction then too)
-    s = bf.cart_to_pure @ overlap_cart(bf) @ bf.cart_to_pure.T
+    s = bf.cart_to_pure @ (_c_one_body(bf, [])[0] if _c_available() else overlap_cart(bf)) @ bf.cart_to_pure.T
     bf.cart_to_pure = bf.cart_to_pure / np.sqrt(np.diag(s))[:, None]
     return bf
 
@@ -326,7 +330,7 @@ def overlap_cart(bf: BasisFunctions) -> np.ndarray:
     return S
 
 
-def one_body(bf: BasisFunctions, nuclei) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+def one_body_py(bf: BasisFunctions, nuclei) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
     """Overlap, kinetic and nuclear-attraction matrices over the pure functions;
     ``nuclei`` = [(Z, (x, y, z)), ...]."""
     n = len(bf.prims)
@@ -366,7 +370,7 @@ def _single_list(bf: BasisFunctions, i: int):
     return out
 
 
-def coulomb_2center(aux: BasisFunctions) -> np.ndarray:
+def coulomb_2center_py(aux: BasisFunctions) -> np.ndarray:
     """(P|Q) over the pure auxiliary functions."""
     n = len(aux.prims)
     L = [_single_list(aux, i) for i in range(n)]
@@ -379,7 +383,7 @@ def coulomb_2center(aux: BasisFunctions) -> np.ndarray:
     return X @ V @ X.T
 
 
-def coulomb_3center(bf: BasisFunctions, aux: BasisFunctions) -> np.ndarray:
+def coulomb_3center_py(bf: BasisFunctions, aux: BasisFunctions) -> np.ndarray:
     """(mu nu|P) over pure functions, [nbf, nbf, naux]."""
     n, na = len(bf.prims), len(aux.prims)
     LA = [_single_list(aux, k) for k in range(na)]
@@ -409,6 +413,103 @@ def coulomb_4center(bf: BasisFunctions) -> np.ndarray:
                     out[a, b, c, d] = out[c, d, a, b] = v
     X = bf.cart_to_pure
     return np.einsum("ai,bj,ck,dl,ijkl->abcd", X, X, X, X, out, optimize=True)
+
+
+# ----------------------------------------------------------------------------- the same integrals in C
+# gto_ints.c restates the scheme above over whole shells (one Boys evaluation
+# per primitive combination); the Python functions stay as its cross-check.
+_LIB_PATH = Path(__file__).with_name("libgto_ints.so")
+_SRC_PATH = Path(__file__).with_name("gto_ints.c")
+_lib = None
+
+
+class _CShell(ctypes.Structure):
+    _fields_ = [("x", ctypes.c_double), ("y", ctypes.c_double), ("z", ctypes.c_double),
+                ("l", ctypes.c_int), ("nprim", ctypes.c_int),
+                ("a", ctypes.POINTER(ctypes.c_double)), ("c", ctypes.POINTER(ctypes.c_double))]
+
+
+def build_library(force: bool = False) -> Path:
+    """Compile gto_ints.c next to it (gcc -O2); a no-op when the library is newer."""
+    if force or not _LIB_PATH.exists() or _LIB_PATH.stat().st_mtime < _SRC_PATH.stat().st_mtime:
+        subprocess.run(["gcc", "-O2", "-shared", "-fPIC", str(_SRC_PATH), "-o", str(_LIB_PATH), "-lm"], check=True)
+    return _LIB_PATH
+
+
+def _c_available() -> bool:
+    global _lib
+    if _lib is None:
+        try:
+            build_library()
+            _lib = ctypes.CDLL(str(_LIB_PATH))
+        except (OSError, subprocess.CalledProcessError, FileNotFoundError):
+            _lib = False
+    return bool(_lib)
+
+
+def _c_shells(shells: list[Shell]):
+    """ctypes shell array; coefficients carry the common primitive norm of each shell."""
+    arr = (_CShell * len(shells))()
+    keep = []
+    for k, sh in enumerate(shells):
+        a = np.ascontiguousarray(sh.alpha, dtype=float)
+        c = np.ascontiguousarray([ck * primitive_norm(ak, (sh.am, 0, 0)) for ak, ck in zip(sh.alpha, sh.coeff)],
+                                 dtype=float)
+        keep += [a, c]
+        x, y, z = (float(v) for v in sh.center)
+        arr[k] = _CShell(x, y, z, sh.am, len(a), a.ctypes.data_as(ctypes.POINTER(ctypes.c_double)),
+                         c.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+    return arr, keep
+
+
+def _ptr(x: np.ndarray):
+    return x.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _c_one_body(bf: BasisFunctions, nuclei):
+    """Cartesian S, T, V from the C library."""
+    arr, keep = _c_shells(bf.shells)
+    n = len(bf.prims)
+    S, T, V = (np.zeros((n, n)) for _ in range(3))
+    zc = np.array([float(z) for z, _ in nuclei] or [0.0])
+    xyz = np.array([list(map(float, c)) for _, c in nuclei] or [[0.0, 0.0, 0.0]]).ravel()
+    _lib.gto_one_body(len(bf.shells), arr, len(nuclei), _ptr(zc), _ptr(xyz), _ptr(S), _ptr(T), _ptr(V))
+    return S, T, V
+
+
+def one_body(bf: BasisFunctions, nuclei) -> tuple[np.ndarray, np.ndarray, np.ndarray]:
+    """Overlap, kinetic and nuclear-attraction matrices over the pure functions;
+    ``nuclei`` = [(Z, (x, y, z)), ...] in Bohr."""
+    if not _c_available():
+        return one_body_py(bf, nuclei)
+    S, T, V = _c_one_body(bf, nuclei)
+    X = bf.cart_to_pure
+    return X @ S @ X.T, X @ T @ X.T, X @ V @ X.T
+
+
+def coulomb_2center(aux: BasisFunctions) -> np.ndarray:
+    """(P|Q) over the pure auxiliary functions."""
+    if not _c_available():
+        return coulomb_2center_py(aux)
+    arr, keep = _c_shells(aux.shells)
+    n = len(aux.prims)
+    V = np.zeros((n, n))
+    _lib.gto_coulomb2(len(aux.shells), arr, _ptr(V))
+    X = aux.cart_to_pure
+    return X @ V @ X.T
+
+
+def coulomb_3center(bf: BasisFunctions, aux: BasisFunctions) -> np.ndarray:
+    """(mu nu|P) over pure functions, [nbf, nbf, naux]."""
+    if not _c_available():
+        return coulomb_3center_py(bf, aux)
+    arr, keep = _c_shells(bf.shells)
+    arra, keepa = _c_shells(aux.shells)
+    n, na = len(bf.prims), len(aux.prims)
+    out = np.zeros((n, n, na))
+    _lib.gto_coulomb3(len(bf.shells), arr, len(aux.shells), arra, _ptr(out))
+    X, Y = bf.cart_to_pure, aux.cart_to_pure
+    return np.einsum("ai,bj,ijk,ck->abc", X, X, out, Y, optimize=True)
 
 
 # ----------------------------------------------------------------------------- RI and SCF
@@ -509,3 +610,63 @@ def atom_ri_hf(basis_text: str, z: int, nelec: int | None = None):
                "aux_shells": [(s.am, float(s.alpha[0])) for s in aux_shells], "bf": bf, "aux": aux,
                "S": S, "H": T + V}
     return scf, mo_3center(scf), details
+
+
+BOHR_A = 0.52917721092             # src/m_definitions.f90:43
+HA_EV = 27.21138505                # src/m_definitions.f90:44
+
+
+def nuclear_repulsion(nuclei) -> float:
+    e = 0.0
+    for i, (zi, ci) in enumerate(nuclei):
+        for zj, cj in nuclei[:i]:
+            e += zi * zj / float(np.linalg.norm(np.asarray(ci, float) - np.asarray(cj, float)))
+    return e
+
+
+def molecule_ri_hf(atoms, basis: dict, auxil: dict | None = None, charge: int = 0, tol: float = 1e-12):
+    """RI-RHF of a molecule.  ``atoms`` = [(Z, (x, y, z) in Angstrom), ...]
+    (the reference's default length_unit, src/input_variables.f90:502);
+    ``basis`` / ``auxil`` map Z to the text of a basis file in the reference's
+    format; ``auxil`` None builds the PAuto auxiliary basis per atom.  Shells
+    are listed atom by atom in input order, as the reference does
+    (src/m_basis_set.f90:90-340).  Returns (SCFResult, M [nstate, nstate,
+    nauxil] over the MOs, details)."""
+    nuclei = [(int(z), np.asarray(xyz, float) / BOHR_A) for z, xyz in atoms]
+    shells, aux_shells = [], []
+    for z, c in nuclei:
+        sh = parse_basis_file(basis[z], center=tuple(c))
+        shells += sh
+        aux_shells += parse_basis_file(auxil[z], center=tuple(c)) if auxil else pauto_auxiliary(sh, z)
+    bf = build_functions(shells)
+    aux = build_functions(aux_shells)
+    S, T, V = one_body(bf, nuclei)
+    v2 = coulomb_2center(aux)
+    sqrtinv, eig = inverse_sqrt_metric(v2)
+    b3 = np.einsum("ijQ,QP->ijP", coulomb_3center(bf, aux), sqrtinv, optimize=True)
+    nelec = sum(z for z, _ in nuclei) - charge
+    e_nn = nuclear_repulsion(nuclei)
+    scf = rhf_ri(S, T + V, b3, nelec, e_nn=e_nn, tol=tol)
+    scf.metric_eigenvalues = eig
+    details = {"nbf": S.shape[0], "naux_basis": v2.shape[0], "nauxil": b3.shape[2], "e_nn": e_nn,
+               "bf": bf, "aux": aux, "S": S, "H": T + V}
+    return scf, mo_3center(scf), details
+
+
+def element_core(z: int) -> int:
+    """Frozen core states per all-electron atom, frozencore='molgw'
+    (element_core, src/m_elements.f90:40-68)."""
+    return 0 if z <= 4 else 1 if z <= 12 else 5 if z <= 30 else 9 if z <= 48 else 18
+
+
+def rimp2_energy(energy: np.ndarray, m: np.ndarray, nocc: int, ncore: int = 0) -> float:
+    """Closed-shell RI-MP2 correlation energy from the MO 3-center tensor
+    M[p, q, P] (mp2_energy_ri, src/m_mp2_energy.f90:25-143): the ring term
+    2 sum (ia|jb)^2 / D and the exchange term -sum (ia|jb)(ib|ja) / D over
+    i, j in ncore..nocc-1 and a, b >= nocc, D = e_i + e_j - e_a - e_b."""
+    e = np.asarray(energy, float)
+    mia = m[ncore:nocc, nocc:, :]
+    iajb = np.einsum("iaP,jbP->iajb", mia, mia, optimize=True)
+    eo, ev = e[ncore:nocc], e[nocc:]
+    d = eo[:, None, None, None] + eo[None, None, :, None] - ev[None, :, None, None] - ev[None, None, None, :]
+    return float(np.sum(iajb * (2.0 * iajb - iajb.transpose(0, 3, 2, 1)) / d))

@@ -1,0 +1,73 @@
+"""The oracle's Gaussian front end on H2O with multi-center integrals, pinned on
+known answers of the reference's test suite, and the H2O cc-pVDZ G0W0@HF
+workload built on it.
+
+* tests/inputs/h2o_rt_tddft_hf_PC2B.in: HF in cc-pVDZ with cc-pVDZ-RI, the
+  basis pair of the workload: SCF total energy (testsuite:789-790, 1e-7 Ha);
+* tests/inputs/h2o_mp3.in: HF in cc-pVDZ with cc-pVTZ-RI (141 auxiliary
+  functions up to g), frozencore='molgw': SCF total energy and the RI-MP2
+  correlation energy (testsuite:782-784, 1e-7 Ha).  RI-MP2 sums over every
+  (ia|jb) of the MO 3-center tensor and the orbital energies, the inputs that
+  chi0 consumes.
+
+CPU only; the front end takes well under a second per molecule."""
+import numpy as np
+import pytest
+
+from oracle import gaussian_ri as g
+from oracle import rigw_oracle as o
+from tests import h2o_case
+from tests.conftest import HA_EV
+
+
+@pytest.fixture(scope="module")
+def h2o():
+    return h2o_case.load()
+
+
+@pytest.mark.parametrize("case", ["h2o_rt_tddft_hf_PC2B.in", "h2o_mp3.in"])
+def test_front_end_reproduces_the_scf_energy(h2o, case):
+    scf, m, det = h2o_case.front_end(h2o, case)
+    ref, tol = h2o["cases"][case]["known_answers"]["SCF Total Energy"]
+    assert abs(scf.energy - ref) < tol
+    assert det["nauxil"] == det["naux_basis"]                 # no metric eigenvalue below 1e-6
+    assert np.abs(scf.fock_mo_diag - scf.e_orb).max() < 1e-9  # Sigma_x - V_xc of HF vanishes
+
+
+def test_front_end_reproduces_the_frozen_core_rimp2_energy(h2o):
+    case = h2o["cases"]["h2o_mp3.in"]
+    assert case["frozencore"].lower() == "molgw" and case["auxil_basis"] == "cc-pVTZ-RI"
+    scf, m, det = h2o_case.front_end(h2o, "h2o_mp3.in")
+    assert det["nauxil"] == 141
+    ncore = sum(g.element_core(z) for z, _ in case["atoms"])
+    assert ncore == 1
+    nocc = int(np.sum(scf.occupation > 0))
+    emp2 = g.rimp2_energy(scf.e_orb, m, nocc, ncore)
+    ref, tol = case["known_answers"]["MP2 Energy"]
+    assert abs(emp2 - ref) < tol
+    ref_tot, tol_tot = case["known_answers"]["MP2 Total Energy"]
+    assert abs(scf.energy + emp2 - ref_tot) < tol_tot
+
+
+def test_workload_front_end_matches_the_fixture(h2o):
+    scf, m, det = h2o_case.front_end(h2o)
+    assert (det["nbf"], det["nauxil"]) == (24, 84)
+    assert int(np.sum(scf.occupation > 0)) == 5
+    assert abs(scf.energy - float(h2o["scf_energy"])) < 1e-10
+    assert np.allclose(scf.e_orb, h2o["energy"], atol=1e-10)
+    # M is defined up to the sign of each MO: compare sign-free contractions
+    mf = h2o["m_full"]
+    assert np.allclose(np.einsum("pqP,pqP->pq", m, m), np.einsum("pqP,pqP->pq", mf, mf), atol=1e-10)
+    assert np.allclose(np.einsum("ppP,qqP->pq", m, m), np.einsum("ppP,qqP->pq", mf, mf), atol=1e-10)
+
+
+def test_workload_oracle_g0w0_matches_the_fixture(h2o):
+    inst = h2o_case.instance(h2o)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    ref = o.g0w0_imag(inst.energy, inst.occupation, inst.m_ia, inst.m_sigma, inst.nomega, rng, **h2o_case.grid(h2o))
+    assert abs(ref.erpa - float(h2o["oracle_erpa"])) < 1e-10
+    assert np.abs(ref.energy_qp_g - h2o["oracle_qp"]).max() * HA_EV < 1e-7
+    # G0W0@HF moves the HOMO up and the LUMO down (screening)
+    homo, lumo = ref.energy_qp_g * HA_EV
+    assert inst.energy[4] * HA_EV < homo < 0.0 < lumo < inst.energy[5] * HA_EV
