@@ -71,3 +71,25 @@ def test_workload_oracle_g0w0_matches_the_fixture(h2o):
     # G0W0@HF moves the HOMO up and the LUMO down (screening)
     homo, lumo = ref.energy_qp_g * HA_EV
     assert inst.energy[4] * HA_EV < homo < 0.0 < lumo < inst.energy[5] * HA_EV
+
+
+def test_pade_conditioning_on_the_workload_grid(h2o):
+    """The Thiele continuation through the workload's 50 imaginary points
+    amplifies rounding-sized noise: relative noise of 1e-14 in Sigma_c moves the
+    QP HOMO by more than 1e-6 eV, yet stays inside the suite's 1e-4 eV.  This is
+    why QP energies on the GPU are held to 1e-4 eV and Sigma_c to 1e-9."""
+    inst = h2o_case.instance(h2o)
+    gr = h2o_case.grid(h2o)
+    rng = o.selfenergy_set_state_range(inst.nstate, inst.occupation, selfenergy_state_min=inst.nsemin,
+                                       selfenergy_state_max=inst.nsemax)
+    se = o.se_init_imaginary_axis(inst.energy, rng, "pade", gr["nomega_sigma"], gr["step_sigma"],
+                                  gr["nomega_sigma_calc"], gr["step_sigma_calc"])
+    sig = h2o["oracle_sigma_calc"]
+    noise = np.random.default_rng(0)
+    shifts = []
+    for _ in range(10):
+        se.sigma_calc[:] = sig * (1.0 + 1e-14 * noise.standard_normal(sig.shape))
+        o.se_pade_fit(se, gr["eta"])
+        eqp, _, _, _ = o.find_qp_energy_graphical(se, np.zeros(2), inst.energy[inst.nsemin - 1:inst.nsemax])
+        shifts.append(np.abs(eqp - h2o["oracle_qp"]).max() * HA_EV)
+    assert 1e-6 < max(shifts) < 1e-4
