@@ -82,13 +82,21 @@ def lmax_abs(lmax_obs: int, z: int) -> int:
     return max(lmax_obs + AUTO_AUXIL_LMAXINC, 2 * lval)
 
 
-def pauto_auxiliary(shells: list[Shell], z: int) -> list[Shell]:
-    """PAuto auxiliary basis of one center (init_auxil_basis_set_auto,
-    src/m_basis_set.f90:638-831): one uncontracted shell per (exponent, am)."""
+def pauto_auxiliary(shells: list[Shell], z: int, pauto: bool = True) -> list[Shell]:
+    """PAuto (or, with ``pauto`` False, Auto) auxiliary basis of one center
+    (init_auxil_basis_set_auto, src/m_basis_set.f90:638-831): one uncontracted
+    shell per (exponent, am).  PAuto takes every sum of two primitive exponents
+    and angular momenta of the center as a candidate, Auto every primitive
+    exponent and angular momentum doubled (:733-758)."""
     cand_e, cand_l = [], []
     lmax_obs = 0
     for si in shells:
         lmax_obs = max(lmax_obs, si.am)
+        if not pauto:
+            for ai in si.alpha:
+                cand_e.append(2.0 * ai)
+                cand_l.append(2 * si.am)
+            continue
         for sj in shells:
             for ai in si.alpha:
                 for aj in sj.alpha:
@@ -624,11 +632,12 @@ def nuclear_repulsion(nuclei) -> float:
     return e
 
 
-def molecule_ri_hf(atoms, basis: dict, auxil: dict | None = None, charge: int = 0, tol: float = 1e-12):
+def molecule_ri_hf(atoms, basis: dict, auxil: dict | str | None = None, charge: int = 0, tol: float = 1e-12):
     """RI-RHF of a molecule.  ``atoms`` = [(Z, (x, y, z) in Angstrom), ...]
     (the reference's default length_unit, src/input_variables.f90:502);
     ``basis`` / ``auxil`` map Z to the text of a basis file in the reference's
-    format; ``auxil`` None builds the PAuto auxiliary basis per atom.  Shells
+    format; ``auxil`` None (or "PAUTO") builds the PAuto auxiliary basis per
+    atom, "AUTO" the Auto one.  Shells
     are listed atom by atom in input order, as the reference does
     (src/m_basis_set.f90:90-340).  Returns (SCFResult, M [nstate, nstate,
     nauxil] over the MOs, details)."""
@@ -637,7 +646,10 @@ def molecule_ri_hf(atoms, basis: dict, auxil: dict | None = None, charge: int = 
     for z, c in nuclei:
         sh = parse_basis_file(basis[z], center=tuple(c))
         shells += sh
-        aux_shells += parse_basis_file(auxil[z], center=tuple(c)) if auxil else pauto_auxiliary(sh, z)
+        if isinstance(auxil, dict):
+            aux_shells += parse_basis_file(auxil[z], center=tuple(c))
+        else:
+            aux_shells += pauto_auxiliary(sh, z, pauto=(auxil or "PAUTO").upper() == "PAUTO")
     bf = build_functions(shells)
     aux = build_functions(aux_shells)
     S, T, V = one_body(bf, nuclei)

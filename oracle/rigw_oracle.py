@@ -903,3 +903,157 @@ def g3w2_selfenergy_imag_loops(energy_g: np.ndarray, m_full: np.ndarray, sig_sta
                                 out[ip, iz] += (weight_p[k1] * weight_p[k2] * braket1 * braket2 * d
                                                 * (-1.0 / (2.0 * PI)) ** 2)
     return out
+
+
+# ---------------------------------------------------------------------------
+# Contour deformation (postscf G0W0_CONTOUR)
+# ---------------------------------------------------------------------------
+TOL_LOW_EIGVAL = 1.0e-3        # src/m_spectral_function.f90:783
+
+
+def vsqrt_chi_vsqrt_lowrank(m_ia: np.ndarray, e_occ: np.ndarray, e_virt: np.ndarray, occ_occ: np.ndarray,
+                            occ_virt: np.ndarray, omega: np.ndarray) -> list:
+    """sf_vsqrt_chi_vsqrt_rpa with low_rank (src/m_spectral_function.f90:779-921)
+    at the complex frequencies ``omega``: chi0 = M F M^T with F =
+    REAL(2 docc de / (omega^2 - de^2)) (:861-872, DGEMM('N','T') :880-881),
+    diagonalized (:895), eigenvalues turned into lambda / (1 - lambda) (:898) and
+    those with |.| <= 1e-3 dropped (:899-913).  Returns per frequency
+    (eigvec [naux, neig], eigval [neig]) of v^1/2 chi v^1/2."""
+    nocc, nvirt, naux = m_ia.shape
+    docc = (occ_occ[:, None] - occ_virt[None, :]).reshape(-1)
+    de = (e_virt[None, :] - e_occ[:, None]).reshape(-1)
+    m_t = np.asfortranarray(m_ia.reshape(nocc * nvirt, naux).T)
+    out = []
+    for w in omega:
+        factor = np.real(2.0 * docc * de / (w * w - de * de))
+        chi0 = sblas.dgemm(1.0, np.asfortranarray(m_t * factor[None, :]), m_t, trans_b=1)
+        eigval, eigvec = sla.eigh(chi0, driver="ev")                   # DSYEV('V')
+        eigval = eigval / (1.0 - eigval)
+        keep = np.abs(eigval) > TOL_LOW_EIGVAL
+        out.append((eigvec[:, keep].copy(), eigval[keep].copy()))
+    return out
+
+
+def real_linear_grid(nomega: int, omega_max: float) -> np.ndarray:
+    """sf_init(REAL_LINEAR) frequencies (src/m_spectral_function.f90:308-316)."""
+    return np.array([k / (nomega - 1) * omega_max for k in range(nomega)])
+
+
+def nearest_real_frequency(omega_real: np.ndarray, omega: float) -> int:
+    """sf_interpolate_vsqrt_chi_vsqrt (src/m_spectral_function.f90:925-950): no
+    interpolation, the first closest grid point (MINLOC)."""
+    if omega > omega_real.max() or omega < omega_real.min():
+        raise ValueError("requested frequency out of range")
+    return int(np.argmin(np.abs(omega_real - omega)))
+
+
+@dataclass
+class ContourResult:
+    sigma: np.ndarray            # [2*nomega+1, nsig] complex, real grid around energy0
+    omega: np.ndarray            # se%omega (real)
+    omega_real: np.ndarray       # the real frequencies of W
+    de_max: float
+    nrank_imag: list             # kept eigenpairs per imaginary frequency
+    nrank_real: list
+    energy_qp_g: np.ndarray
+    energy_qp_z: np.ndarray
+    zz: np.ndarray
+    ehomo: float
+    elumo: float
+    nsemin: int
+    nsemax: int
+
+
+def gw_selfenergy_contour(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_sigma: np.ndarray,
+                          rng: StateRange, ncore_w: int, nomega_chi_imag: int, nomega_chi_real: int,
+                          nomega_sigma: int, step_sigma: float, eta: float):
+    """gw_selfenergy_contour (src/m_gw_selfenergy_grid.f90:342-551) for one spin.
+
+    ``m_ia`` is the W window [nocc_w, nvirt_w, naux] from state ncore_w+1;
+    ``m_sigma`` is [nsig, prange, naux] over p = ncore_G+1 .. nvirtual_G-1.
+    The self-energy is evaluated on se%omega = step_sigma * (-n..n) around
+    energy0 = energy of the Sigma states (src/m_selfenergy_tools.f90:658-663, 679-680).
+    Returns (sigma [2n+1, nsig], se_omega, omega_real, de_max, w_imag, w_real)."""
+    nom = nomega_sigma // 2
+    se_omega = step_sigma * np.arange(-nom, nom + 1)
+    energy0 = energy[rng.nsemin - 1: rng.nsemax]
+    nocc_w, nvirt_w = m_ia.shape[:2]
+    occ_w, e_occ = occupation[ncore_w:ncore_w + nocc_w], energy[ncore_w:ncore_w + nocc_w]
+    e_virt = energy[ncore_w + nocc_w: ncore_w + nocc_w + nvirt_w]
+    occ_v = occupation[ncore_w + nocc_w: ncore_w + nocc_w + nvirt_w]
+    wimag, wquad = imaginary_quad_grid(nomega_chi_imag)
+    w_imag = vsqrt_chi_vsqrt_lowrank(m_ia, e_occ, e_virt, occ_w, occ_v, 1j * wimag)
+    # largest real frequency needed (:390-414)
+    de_max = 0.0
+    for s in range(len(energy0)):
+        for p in range(rng.ncore_g + 1, rng.nhomo_g + 1):
+            for om in se_omega:
+                de = energy[p - 1] - (energy0[s] + om)
+                if de < -eta:
+                    continue
+                de_max = max(de_max, de)
+        for p in range(rng.nlumo_g, rng.nvirtual_g):
+            for om in se_omega:
+                de = energy0[s] + om - energy[p - 1]
+                if de < -eta:
+                    continue
+                de_max = max(de_max, de)
+    omega_real = real_linear_grid(nomega_chi_real, de_max)
+    w_real = vsqrt_chi_vsqrt_lowrank(m_ia, e_occ, e_virt, occ_w, occ_v, omega_real.astype(complex))
+    prange = rng.nvirtual_g - rng.ncore_g - 1
+    sigma = np.zeros((2 * nom + 1, len(energy0)), dtype=complex)
+    for s in range(len(energy0)):
+        eri3 = np.asfortranarray(m_sigma[s, :prange].T)                 # [naux, prange]
+        # imaginary-axis integral (:440-478)
+        for iw in range(nomega_chi_imag):
+            vec, val = w_imag[iw]
+            if val.size == 0:
+                continue
+            tmp2 = sblas.dgemm(1.0, vec, eri3, trans_a=1)                # DGEMM('T','N')
+            vchiv = np.sum(tmp2 ** 2 * val[:, None], axis=0)
+            for pl in range(prange):
+                p = pl + rng.ncore_g + 1
+                x = energy0[s] + se_omega - energy[p - 1]
+                mask = np.abs(x) > eta
+                term = (1.0 / (x + 1j * wimag[iw]) + 1.0 / (x - 1j * wimag[iw])) * vchiv[pl] / (2.0 * PI)
+                sigma[mask, s] -= wquad[iw] * term[mask]
+        # residues of the occupied states (:481-508) and of the empty states (:511-538)
+        for pl in range(prange):
+            p = pl + rng.ncore_g + 1
+            occupied = p < rng.nlumo_g
+            empty = p > rng.nhomo_g
+            for io, om in enumerate(se_omega):
+                for kind, on in ((-1.0, occupied), (1.0, empty)):
+                    if not on:
+                        continue
+                    de = energy[p - 1] - (energy0[s] + om) if kind < 0 else energy0[s] + om - energy[p - 1]
+                    if de < -eta:
+                        continue
+                    vec, val = w_real[nearest_real_frequency(omega_real, abs(de))]
+                    tmp = eri3[:, pl] @ vec
+                    factor = 0.5 if abs(de) < eta else 1.0
+                    sigma[io, s] += kind * np.sum(tmp ** 2 * val) * factor
+    return sigma, se_omega, omega_real, de_max, w_imag, w_real
+
+
+def g0w0_contour(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_sigma: np.ndarray,
+                 rng: StateRange, ncore_w: int, nomega_chi_imag: int, nomega_chi_real: int,
+                 nomega_sigma: int = 51, step_sigma: float = 0.01, eta: float = 0.001,
+                 exchange_m_vxc: np.ndarray | None = None) -> ContourResult:
+    """selfenergy_evaluation for contour_deformation (src/m_selfenergy_evaluation.f90:239-240):
+    Sigma on the real grid, then the linearized and graphical QP energies and
+    HOMO/LUMO over the Sigma states (:587-611)."""
+    sigma, se_omega, omega_real, de_max, w_imag, w_real = gw_selfenergy_contour(
+        energy, occupation, m_ia, m_sigma, rng, ncore_w, nomega_chi_imag, nomega_chi_real, nomega_sigma,
+        step_sigma, eta)
+    e0 = energy[rng.nsemin - 1: rng.nsemax]
+    se = SelfEnergyGrid(omega=se_omega.astype(complex), omega_calc=np.zeros(0, complex), energy0=e0.copy(),
+                        sigma=sigma)
+    xc = np.zeros_like(e0) if exchange_m_vxc is None else exchange_m_vxc
+    eqp_z, _ = find_qp_energy_linearization(se, xc, e0)
+    eqp_g, zz_g, _, _ = find_qp_energy_graphical(se, xc, e0)
+    full = energy.copy()
+    full[rng.nsemin - 1: rng.nsemax] = eqp_g
+    ehomo, elumo = output_homolumo(occupation, full, rng.nsemin, rng.nsemax)
+    return ContourResult(sigma, se_omega, omega_real, de_max, [v.size for _, v in w_imag],
+                         [v.size for _, v in w_real], eqp_g, eqp_z, zz_g, ehomo, elumo, rng.nsemin, rng.nsemax)

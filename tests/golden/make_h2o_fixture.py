@@ -7,11 +7,15 @@ Run next to the MOLGW sources:
 
 It reads from the MOLGW tree:
 
-* ``basis/{O,H}_cc-pVDZ``, ``{O,H}_cc-pVDZ-RI`` and ``{O,H}_cc-pVTZ-RI``;
+* ``basis/{O,H}_cc-pVDZ``, ``{O,H}_cc-pVTZ``, ``{O,H}_cc-pVDZ-RI`` and
+  ``{O,H}_cc-pVTZ-RI``;
 * ``tests/inputs/h2o_rt_tddft_hf_PC2B.in`` (HF, cc-pVDZ / cc-pVDZ-RI) and
   ``tests/inputs/h2o_mp3.in`` (HF, cc-pVDZ / cc-pVTZ-RI, frozencore='molgw'):
   their geometries, bases and their known answers in ``tests/inputs/testsuite``
-  (SCF total energy and the RI-MP2 correlation energy, 1e-7 Ha).
+  (SCF total energy and the RI-MP2 correlation energy, 1e-7 Ha);
+* ``tests/inputs/h2o_gw_contour.in`` (HF, cc-pVTZ with the Auto auxiliary basis,
+  G0W0 by contour deformation, frozencore='molgw'): geometry, basis, GW settings
+  and known answers (SCF total energy 1e-7 Ha, HOMO and LUMO 1e-4 eV).
 
 The workload itself is H2O with O at (0, 0, 0) and the H atoms at
 (0, +-0.757, 0.587) Angstrom, HF in cc-pVDZ (24 functions) with cc-pVDZ-RI (84
@@ -25,7 +29,8 @@ Writes ``h2o_ccpvdz.npz`` next to this script: the basis texts, per case the
 geometry and known answers, and for the workload the orbital energies and
 occupations, the MO coefficients, the AO 3-center tensor B(mu nu, P) (metric
 folded in; the MO tensor M[p, q, P] = sum C B C follows), the SCF energy, and the
-oracle's G0W0 output (E_RPA, E_GW, QP energies).  The tests read only this
+oracle's G0W0 output (E_RPA, E_GW, QP energies); for the contour input, the
+oracle's QP energies and Sigma on its real grid.  The tests read only this
 fixture (and recompute the front end from its basis texts).
 """
 from __future__ import annotations
@@ -41,15 +46,19 @@ sys.path.insert(0, str(HERE.parent.parent))
 
 from tests.golden.make_he_fixture import read_known_answers  # noqa: E402
 
-PIN_INPUTS = ("h2o_rt_tddft_hf_PC2B.in", "h2o_mp3.in")
+PIN_INPUTS = ("h2o_rt_tddft_hf_PC2B.in", "h2o_mp3.in", "h2o_gw_contour.in")
+CONTOUR_KEYS = ("nomega_chi_imag", "nomega_chi_real", "step_sigma", "nomega_sigma", "selfenergy_state_range",
+                "eta", "postscf")
 WORKLOAD_ATOMS = [(8, (0.0, 0.0, 0.0)), (1, (0.0, 0.757, 0.587)), (1, (0.0, -0.757, 0.587))]
 WORKLOAD_GRID = dict(nomega=16, nomega_sigma=101, step_sigma=0.025, nomega_sigma_calc=50, step_sigma_calc=0.075,
                      eta=0.01)
 SYMBOL = {1: "H", 8: "O"}
+ZOF = {v.upper(): k for k, v in SYMBOL.items()}
 
 
 def read_case(path: Path) -> dict:
-    """Namelist values (basis, auxil_basis, frozencore, natom) and the atom lines."""
+    """Namelist values (basis, auxil_basis, frozencore, natom, GW settings) and
+    the atom lines (atomic number or element symbol, then x y z in Angstrom)."""
     text = path.read_text()
     head, tail = text.split("\n/", 1)
     vals = {}
@@ -62,16 +71,17 @@ def read_case(path: Path) -> dict:
     atoms = []
     for line in tail.strip().splitlines()[:natom]:
         z, x, y, zz = line.split()[:4]
-        atoms.append((int(float(z)), (float(x), float(y), float(zz))))
+        zn = ZOF[z.upper()] if z.upper() in ZOF else int(float(z))
+        atoms.append((zn, (float(x), float(y), float(zz))))
     return {"basis": vals["basis"], "auxil_basis": vals["auxil_basis"], "frozencore": vals.get("frozencore", "no"),
-            "atoms": atoms}
+            "atoms": atoms, "settings": {k: vals[k] for k in CONTOUR_KEYS if k in vals}}
 
 
 def main(molgw: Path):
     from oracle import gaussian_ri as g
     from oracle import rigw_oracle as o
     basis = {}
-    for name in ("cc-pVDZ", "cc-pVDZ-RI", "cc-pVTZ-RI"):
+    for name in ("cc-pVDZ", "cc-pVTZ", "cc-pVDZ-RI", "cc-pVTZ-RI"):
         basis[name] = {str(z): (molgw / "basis" / f"{s}_{name}").read_text() for z, s in SYMBOL.items()}
     cases = {}
     for name in PIN_INPUTS:
@@ -89,14 +99,25 @@ def main(molgw: Path):
     grid = {k: v for k, v in WORKLOAD_GRID.items() if k != "nomega"}
     ref = o.g0w0_imag(scf.e_orb, scf.occupation, m[:nocc, nocc:], m[nocc - 1:nocc + 1], WORKLOAD_GRID["nomega"],
                       rng, **grid)
+    contour = contour_run(cases["h2o_gw_contour.in"], basis)
     np.savez_compressed(
         HERE / "h2o_ccpvdz.npz", basis=np.array(json.dumps(basis)), cases=np.array(json.dumps(cases)),
         workload_atoms=np.array(json.dumps(WORKLOAD_ATOMS)), workload_grid=np.array(json.dumps(WORKLOAD_GRID)),
         energy=scf.e_orb, occupation=scf.occupation, c_matrix=scf.c, b3_ao=scf.b3,
         scf_energy=scf.energy, nauxil=det["nauxil"], oracle_erpa=ref.erpa, oracle_egw=ref.egw,
-        oracle_qp=ref.energy_qp_g, oracle_sigma_calc=ref.sigma_calc)
+        oracle_qp=ref.energy_qp_g, oracle_sigma_calc=ref.sigma_calc,
+        contour_qp=contour.energy_qp_g, contour_sigma=contour.sigma, contour_de_max=contour.de_max)
     print("wrote", HERE / "h2o_ccpvdz.npz", "E_SCF =", scf.energy, "nauxil =", det["nauxil"],
-          "QP HOMO/LUMO (eV) =", ref.energy_qp_g * g.HA_EV)
+          "QP HOMO/LUMO (eV) =", ref.energy_qp_g * g.HA_EV, "contour QP (eV) =", contour.energy_qp_g * g.HA_EV)
+
+
+def contour_run(case: dict, basis: dict):
+    from oracle import rigw_oracle as o
+    from tests.h2o_case import contour_inputs
+    scf, m, rng, ncore, m_ia, m_sig, st = contour_inputs(case, basis)
+    return o.g0w0_contour(scf.e_orb, scf.occupation, m_ia, m_sig, rng, ncore, st["nomega_chi_imag"],
+                          st["nomega_chi_real"], nomega_sigma=st["nomega_sigma"], step_sigma=st["step_sigma"],
+                          eta=st["eta"])
 
 
 if __name__ == "__main__":

@@ -8,7 +8,12 @@ workload built on it.
   functions up to g), frozencore='molgw': SCF total energy and the RI-MP2
   correlation energy (testsuite:782-784, 1e-7 Ha).  RI-MP2 sums over every
   (ia|jb) of the MO 3-center tensor and the orbital energies, the inputs that
-  chi0 consumes.
+  chi0 consumes;
+* tests/inputs/h2o_gw_contour.in: HF in cc-pVTZ (58 functions) with the Auto
+  auxiliary basis (231 functions), frozencore='molgw', G0W0 by contour
+  deformation with 16 imaginary and 6 real frequencies and the low-rank W:
+  SCF total energy (1e-7 Ha) and the HOMO and LUMO QP energies (1e-4 eV),
+  testsuite:777-780.
 
 CPU only; the front end takes well under a second per molecule."""
 import numpy as np
@@ -25,7 +30,7 @@ def h2o():
     return h2o_case.load()
 
 
-@pytest.mark.parametrize("case", ["h2o_rt_tddft_hf_PC2B.in", "h2o_mp3.in"])
+@pytest.mark.parametrize("case", ["h2o_rt_tddft_hf_PC2B.in", "h2o_mp3.in", "h2o_gw_contour.in"])
 def test_front_end_reproduces_the_scf_energy(h2o, case):
     scf, m, det = h2o_case.front_end(h2o, case)
     ref, tol = h2o["cases"][case]["known_answers"]["SCF Total Energy"]
@@ -93,3 +98,19 @@ def test_pade_conditioning_on_the_workload_grid(h2o):
         eqp, _, _, _ = o.find_qp_energy_graphical(se, np.zeros(2), inst.energy[inst.nsemin - 1:inst.nsemax])
         shifts.append(np.abs(eqp - h2o["oracle_qp"]).max() * HA_EV)
     assert 1e-6 < max(shifts) < 1e-4
+
+
+def test_contour_deformation_reproduces_the_known_qp_energies(h2o):
+    case = h2o["cases"]["h2o_gw_contour.in"]
+    assert case["auxil_basis"].upper() == "AUTO" and case["settings"]["postscf"].lower() == "g0w0_contour"
+    scf, m, rng, ncore, m_ia, m_sig, st = h2o_case.contour_inputs(case, h2o["basis"])
+    assert (scf.e_orb.size, m.shape[2], ncore, rng.nsemin, rng.nsemax) == (58, 231, 1, 4, 6)
+    res = o.g0w0_contour(scf.e_orb, scf.occupation, m_ia, m_sig, rng, ncore, st["nomega_chi_imag"],
+                         st["nomega_chi_real"], nomega_sigma=st["nomega_sigma"], step_sigma=st["step_sigma"],
+                         eta=st["eta"])
+    for label, value in (("GW HOMO energy", res.ehomo), ("GW LUMO energy", res.elumo)):
+        ref, tol = case["known_answers"][label]
+        assert abs(value * HA_EV - ref) < tol
+    assert np.abs(res.energy_qp_g - h2o["contour_qp"]).max() * HA_EV < 1e-8
+    # the low-rank filter drops eigenpairs: all of them at the highest imaginary frequency
+    assert res.nrank_imag[-1] < res.nrank_imag[0] <= min(m.shape[2], m_ia.shape[0] * m_ia.shape[1])
