@@ -26,6 +26,9 @@
  *   rigw_sosex_selfenergy_imag  sosex_selfenergy_imag_grid    src/m_g3w2_selfenergy.f90:2200-2478
  *   rigw_g3w2_selfenergy_imag   g3w2_selfenergy_imag_grid     src/m_g3w2_selfenergy.f90:2018-2196
  *                               (GW+SOSEX_PADE: added after SOX, src/m_selfenergy_evaluation.f90:498-500)
+ *   rigw_gw_selfenergy_contour  gw_selfenergy_contour         src/m_gw_selfenergy_grid.f90:342-551
+ *                               + sf_vsqrt_chi_vsqrt_rpa(low_rank) src/m_spectral_function.f90:779-921
+ *                               + the QP equation of G0W0_CONTOUR, src/m_selfenergy_evaluation.f90:239-240,587-611
  */
 #ifndef RIGW_H
 #define RIGW_H
@@ -286,6 +289,55 @@ typedef struct rigw_g3w2_problem {
 /* sigma_g3w2: [nsig][nomega_calc][2], overwritten. */
 RIGW_API int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g3w2_problem* prob,
                                        double* sigma_g3w2);
+
+/* ---- contour deformation ------------------------------------------------------
+ * G0W0 by contour deformation (postscf G0W0_CONTOUR), one spin channel
+ * (gw_selfenergy_contour): W from the eigenpairs of v^1/2 chi0 v^1/2 at
+ * nomega_imag Gauss-Legendre imaginary frequencies and at nomega_real real
+ * frequencies spread linearly over 0 .. de_max, keeping the eigenvalues
+ * lambda / (1 - lambda) with |.| > 1e-3 (the low-rank W); Sigma_c on the real grid
+ * se%omega = step_sigma * (-n .. n), n = nomega_sigma / 2, around energy0 of each
+ * state: the imaginary-axis integral plus the residues of the occupied and
+ * empty states, W taken at the real frequency closest to the pole (no
+ * interpolation); then the linearized and graphical QP energies.  de_max is
+ * the largest pole distance over the states and the grid, as the reference
+ * computes it. */
+typedef struct rigw_contour_problem {
+  int naux;
+  int nocc_w, nvirt_w;          /* W window: occupied ncore_W+1..nhomo_W, empty nlumo_W..nvirtual_W-1 */
+  const double* m_ia;           /* [nocc_w][nvirt_w][naux] = eri_3center_mo(naux, a, i)        */
+  const double* e_occ_w;        /* [nocc_w] host, energies of the W window (Ha)                 */
+  const double* e_virt_w;       /* [nvirt_w] host                                               */
+  const double* occ_occ_w;      /* [nocc_w] host, occupations                                   */
+  const double* occ_virt_w;     /* [nvirt_w] host                                               */
+  int nomega_imag;              /* nomega_chi_imag (>= 1)                                       */
+  int nomega_real;              /* nomega_chi_real (>= 2)                                       */
+  int nstate_p;                 /* states p of the sum: ncore_G+1 .. nvirtual_G-1               */
+  int p_occ_end;                /* p index (0-based) below which the occupied residues run:
+                                   nlumo_G - ncore_G - 1                                        */
+  int p_empty_begin;            /* p index from which the empty residues run: nhomo_G - ncore_G */
+  const double* energy_p;       /* [nstate_p] host, energies of the states p (energy_g)         */
+  int nsig;                     /* Sigma states nsemin..nsemax                                  */
+  const double* m_pm;           /* [nsig][nstate_p][naux] = eri_3center_mo(naux, p, m)          */
+  const double* energy0;        /* [nsig] host, se%energy0: energy_g of the Sigma states         */
+  const double* energy_qp0;     /* [nsig] host, energies of the QP equation (the mean-field
+                                   energy of find_qp_energy_*), or NULL: energy0                 */
+  const double* exchange_m_vxc; /* [nsig] host, Sigma_x - V_xc, or NULL for zero                */
+  int nomega_sigma;             /* se%omega has 2 * (nomega_sigma / 2) + 1 points               */
+  double step_sigma;
+  double eta;
+  int flags;                    /* RIGW_PROBLEM_DEVICE_POINTERS: m_ia and m_pm in device memory  */
+} rigw_contour_problem;
+typedef struct rigw_contour_result {
+  double* sigma;                /* [nsig][2n+1][2] host, or NULL                                */
+  double* energy_qp_g;          /* [nsig] graphical QP energies, or NULL                        */
+  double* energy_qp_z;          /* [nsig] linearized QP energies, or NULL                       */
+  double* zz;                   /* [nsig] Z of the graphical solution, or NULL                  */
+  int* rank;                    /* [nomega_imag + nomega_real] eigenpairs kept, or NULL         */
+  double* omega_real;           /* [nomega_real] the real frequencies of W, or NULL             */
+  double de_max;                /* out: the largest real frequency                              */
+} rigw_contour_result;
+RIGW_API int rigw_gw_selfenergy_contour(rigw_ctx* ctx, const rigw_contour_problem* prob, rigw_contour_result* result);
 
 /* ---- fused solves ----------------------------------------------------------- */
 RIGW_API int rigw_g0w0(rigw_ctx* ctx, const rigw_problem* prob, rigw_result* result);

@@ -226,6 +226,14 @@ int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g
   return finish(ctx, rigw::g3w2_selfenergy_imag(ctx->impl, wpol->impl, *prob, sigma_g3w2));
 }
 
+int rigw_gw_selfenergy_contour(rigw_ctx* ctx, const rigw_contour_problem* prob, rigw_contour_result* result) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!prob || !result) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::gw_selfenergy_contour(ctx->impl, *prob, *result));
+}
+
 int rigw_eri_3center_mo(rigw_ctx* ctx, int nbf, int nstate, int npair, int naux, const int* index_basis,
                         const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                         int nstate_min, int nstate_max, double* out) {

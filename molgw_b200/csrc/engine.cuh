@@ -275,6 +275,7 @@ Status wpol_chi(Context& c, const Wpol& w, double* chi);
 Status sox_selfenergy_imag(Context& c, const rigw_sox_problem& pr, double* sigma_sox);
 Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem& pr, double* sigma);
 Status g3w2_selfenergy_imag(Context& c, const Wpol& w, const rigw_g3w2_problem& pr, double* sigma);
+Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_contour_result& res);
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                       int nstate_min, int nstate_max, double* out, int precision, int flags = 0);

@@ -2,6 +2,7 @@
 // problem table and a work list, so one launch covers all frequencies of all
 // molecules of a batch.
 #include "kernels.cuh"
+#include "qp_tools.cuh"
 
 namespace rigw {
 
@@ -570,70 +571,10 @@ __global__ void __launch_bounds__(256) pade_qp_kernel(const ProbDev* __restrict_
   }
   __syncthreads();
   if (tid != 0) return;
-  const double e0 = p.e_sig[s];
-  const double xc = p.xc_sig ? p.xc_sig[s] : 0.0;
-  const int h = p.nsigma_half;
-  double eqp_z, zlin;
-  if (h > 0) {
-    const double w_p = p.efermi + p.step_sigma * 1.0, w_m = p.efermi - p.step_sigma * 1.0;
-    double z = (sr[h + 1].re - sr[h - 1].re) / (w_p - w_m);
-    z = 1.0 / (1.0 - z);
-    z = fmin(fmax(z, 0.0), 1.0);
-    zlin = z;
-    eqp_z = z * (e0 + sr[h].re + xc);
-  } else {
-    zlin = 1.0;
-    eqp_z = e0 + sr[h].re + xc;
-  }
-  double eqp_g, zg;
-  if (h > 0) {
-    double zw[4] = {-1.0, -1.0, -1.0, -1.0};
-    double ef[4] = {0.0, 0.0, 0.0, 0.0};
-    double xprev = p.efermi + p.step_sigma * (0 - h);
-    double fprev = sr[0].re + xc + e0;
-    for (int j = 1; j < nreal; ++j) {
-      const double x = p.efermi + p.step_sigma * (j - h);
-      const double f = sr[j].re + xc + e0;
-      const double g0 = fprev - xprev, g1 = f - x;
-      if (g0 * g1 < 0.0) {
-        const double zz = 1.0 / (1.0 - (f - fprev) / (x - xprev));
-        if (zz >= 0.00001 && zz > zw[3]) {
-          int jf = 0;
-          while (!(zz > zw[jf])) ++jf;
-          for (int m = 3; m > jf; --m) {
-            zw[m] = zw[m - 1];
-            ef[m] = ef[m - 1];
-          }
-          zw[jf] = zz;
-          const double gp = (g1 - g0) / (x - xprev);
-          ef[jf] = xprev - g0 / gp;
-        }
-      }
-      xprev = x;
-      fprev = f;
-    }
-    int iq = 0;
-    for (int m = 1; m < 4; ++m)
-      if (zw[m] > zw[iq]) iq = m;
-    if (zw[iq] > 1.0e-6) {
-      eqp_g = ef[iq];
-      zg = zw[iq];
-    } else {
-      eqp_g = e0;
-      zg = 1.0;
-    }
-    int nfixed = 0;
-    for (int m = 0; m < 4; ++m) nfixed += zw[m] > 0.0;
-    if (nfixed == 0) eqp_g = e0 + sr[h].re + xc;
-  } else {
-    eqp_g = e0 + sr[h].re + xc;
-    zg = 1.0;
-  }
   double* q = p.qp + 4 * s;
-  q[0] = eqp_g;
-  q[1] = eqp_z;
-  q[2] = zg;
-  q[3] = zlin;
+  qp_on_real_grid(reinterpret_cast<const double*>(sr), p.nsigma_half, p.efermi, p.step_sigma, 0.0, p.e_sig[s],
+                  p.xc_sig ? p.xc_sig[s] : 0.0, q);
+  const double eqp_g = q[0], eqp_z = q[1];
   if (!isfinite(eqp_g) || !isfinite(eqp_z)) atomicOr(p.err, kErrNonFinite);
 }
 

@@ -91,6 +91,40 @@ class G3w2Problem(C.Structure):
     ]
 
 
+class ContourProblem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nocc_w", C.c_int), ("nvirt_w", C.c_int), ("m_ia", _dp), ("e_occ_w", _dp),
+        ("e_virt_w", _dp), ("occ_occ_w", _dp), ("occ_virt_w", _dp), ("nomega_imag", C.c_int),
+        ("nomega_real", C.c_int), ("nstate_p", C.c_int), ("p_occ_end", C.c_int), ("p_empty_begin", C.c_int),
+        ("energy_p", _dp), ("nsig", C.c_int), ("m_pm", _dp), ("energy0", _dp), ("energy_qp0", _dp),
+        ("exchange_m_vxc", _dp), ("nomega_sigma", C.c_int), ("step_sigma", C.c_double), ("eta", C.c_double),
+        ("flags", C.c_int),
+    ]
+
+
+class ContourResult(C.Structure):
+    _fields_ = [
+        ("sigma", _dp), ("energy_qp_g", _dp), ("energy_qp_z", _dp), ("zz", _dp), ("rank", C.POINTER(C.c_int)),
+        ("omega_real", _dp), ("de_max", C.c_double),
+    ]
+
+
+@dataclass
+class ContourOutput:
+    """Result of Engine.g0w0_contour (fields as in the oracle's ContourResult)."""
+    sigma: np.ndarray            # [2n+1, nsig] complex, Sigma_c on se%omega around energy0
+    omega: np.ndarray            # se%omega
+    omega_real: np.ndarray       # the real frequencies of W
+    de_max: float
+    rank: np.ndarray             # kept eigenpairs per frequency (imaginary, then real)
+    energy_qp_g: np.ndarray
+    energy_qp_z: np.ndarray
+    zz: np.ndarray
+    ehomo: float
+    elumo: float
+    device_ms: float
+
+
 def _vertex_w_inst(inst):
     """The instance whose W window the vertex path factors: on that path the
     reference calls gw_selfenergy_grid with energy_g (src/m_selfenergy_evaluation.f90:496),
@@ -181,6 +215,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_sox_selfenergy_imag.argtypes = [C.c_void_p, C.POINTER(SoxProblem), _dp]
     lib.rigw_sosex_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SosexProblem), _dp]
     lib.rigw_g3w2_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(G3w2Problem), _dp]
+    lib.rigw_gw_selfenergy_contour.argtypes = [C.c_void_p, C.POINTER(ContourProblem), C.POINTER(ContourResult)]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -755,6 +790,85 @@ class Engine:
             _ptr(np.ascontiguousarray(eri3)), _ptr(cm), m_min, m_max, n_min, n_max,
             _ptr(out), precision), "rigw_eri_3center_mo_precision")
         return out
+
+    def g0w0_contour(self, energy: np.ndarray, occupation: np.ndarray, m_ia, m_sigma, nsemin: int, nsemax: int,
+                     nomega_imag: int, nomega_real: int, nomega_sigma: int, step_sigma: float, eta: float = 0.001,
+                     ncore_w: int = 0, ncore_g: int = 0, energy_g: np.ndarray | None = None,
+                     exchange_m_vxc: np.ndarray | None = None) -> ContourOutput:
+        """G0W0 by contour deformation for one spin channel (postscf G0W0_CONTOUR:
+        gw_selfenergy_contour, src/m_gw_selfenergy_grid.f90:342-551, then the QP
+        equation, src/m_selfenergy_evaluation.f90:587-611) through
+        rigw_gw_selfenergy_contour.
+
+        ``m_ia`` is the W window [nocc_w, nvirt_w, naux] from state ncore_w+1;
+        ``m_sigma`` is [nsig, nstate - ncore_g, naux] over the states p =
+        ncore_g+1 .. nstate for the Sigma states nsemin..nsemax (1-based).  Both
+        may be CUDA tensors (RIGW_PROBLEM_DEVICE_POINTERS).  ``energy_g`` (default
+        ``energy``) is the energy of G and W and se%energy0; the QP equation
+        keeps ``energy``."""
+        e = np.ascontiguousarray(energy, dtype=np.float64)
+        occ = np.ascontiguousarray(occupation, dtype=np.float64)
+        eg = e if energy_g is None else np.ascontiguousarray(energy_g, dtype=np.float64)
+        nstate = e.size
+        on_dev = hasattr(m_ia, "is_cuda") and m_ia.is_cuda
+        if not on_dev:
+            m_ia = np.ascontiguousarray(m_ia, dtype=np.float64)
+            m_sigma = np.ascontiguousarray(m_sigma, dtype=np.float64)
+        nocc_w, nvirt_w, naux = (int(x) for x in m_ia.shape)
+        nsig = nsemax - nsemin + 1
+        nstate_p = nstate - ncore_g
+        if tuple(int(x) for x in m_sigma.shape) != (nsig, nstate_p, naux):
+            raise ValueError("g0w0_contour: m_sigma must be [nsig, nstate - ncore_g, naux]")
+        # HOMO / LUMO of G (selfenergy_set_state_range, src/m_selfenergy_tools.f90:96-109)
+        empty = 1.0e-5
+        nhomo = max([1] + [p + 1 for p in range(nstate) if not occ[p] < empty])
+        nlumo = min([100000] + [p + 1 for p in range(nstate) if not occ[p] > empty])
+        keep = []
+        cp = ContourProblem()
+        cp.naux, cp.nocc_w, cp.nvirt_w = naux, nocc_w, nvirt_w
+        arrays = {
+            "e_occ_w": eg[ncore_w:ncore_w + nocc_w], "e_virt_w": eg[ncore_w + nocc_w:ncore_w + nocc_w + nvirt_w],
+            "occ_occ_w": occ[ncore_w:ncore_w + nocc_w],
+            "occ_virt_w": occ[ncore_w + nocc_w:ncore_w + nocc_w + nvirt_w],
+            "energy_p": eg[ncore_g:], "energy0": eg[nsemin - 1:nsemax], "energy_qp0": e[nsemin - 1:nsemax]}
+        if exchange_m_vxc is not None:
+            arrays["exchange_m_vxc"] = np.asarray(exchange_m_vxc, dtype=np.float64)
+        for k, v in arrays.items():
+            v = np.ascontiguousarray(v, dtype=np.float64)
+            keep.append(v)
+            setattr(cp, k, _ptr(v))
+        if on_dev:
+            cp.m_ia, cp.m_pm = C.cast(m_ia.data_ptr(), _dp), C.cast(m_sigma.data_ptr(), _dp)
+            cp.flags = RIGW_PROBLEM_DEVICE_POINTERS
+        else:
+            cp.m_ia, cp.m_pm = _ptr(m_ia), _ptr(m_sigma)
+        cp.nomega_imag, cp.nomega_real = nomega_imag, nomega_real
+        cp.nstate_p = nstate_p
+        cp.p_occ_end = max(0, min(nstate_p, nlumo - ncore_g - 1))
+        cp.p_empty_begin = max(0, min(nstate_p, nhomo - ncore_g))
+        cp.nsig = nsig
+        cp.nomega_sigma, cp.step_sigma, cp.eta = nomega_sigma, step_sigma, eta
+        h = nomega_sigma // 2
+        sig = np.zeros((nsig, 2 * h + 1, 2))
+        eqp_g, eqp_z, zz = np.zeros(nsig), np.zeros(nsig), np.zeros(nsig)
+        rank = np.zeros(nomega_imag + nomega_real, dtype=np.int32)
+        omr = np.zeros(nomega_real)
+        cr = ContourResult()
+        cr.sigma, cr.energy_qp_g, cr.energy_qp_z, cr.zz = _ptr(sig), _ptr(eqp_g), _ptr(eqp_z), _ptr(zz)
+        cr.rank = rank.ctypes.data_as(C.POINTER(C.c_int))
+        cr.omega_real = _ptr(omr)
+        self._check(self._lib.rigw_gw_selfenergy_contour(self._h, C.byref(cp), C.byref(cr)),
+                    "rigw_gw_selfenergy_contour")
+        full = e.copy()
+        full[nsemin - 1:nsemax] = eqp_g
+        ehomo, elumo = -np.inf, np.inf
+        for st in range(nsemin, nsemax + 1):
+            if occ[st - 1] / 2.0 > empty:
+                ehomo = max(ehomo, full[st - 1])
+            if occ[st - 1] / 2.0 < 1.0 - empty:
+                elumo = min(elumo, full[st - 1])
+        return ContourOutput(sig[..., 0].T + 1j * sig[..., 1].T, step_sigma * np.arange(-h, h + 1), omr,
+                             cr.de_max, rank, eqp_g, eqp_z, zz, ehomo, elumo, self.last_stats()["total_ms"])
 
     def g0w0_from_ao(self, eri3, index_basis: np.ndarray, c_matrix: np.ndarray, energy: np.ndarray,
                      occupation: np.ndarray, nomega: int, nsemin: int, nsemax: int, precision: int = RIGW_FP64,

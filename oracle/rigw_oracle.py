@@ -1039,16 +1039,19 @@ def gw_selfenergy_contour(energy: np.ndarray, occupation: np.ndarray, m_ia: np.n
 def g0w0_contour(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m_sigma: np.ndarray,
                  rng: StateRange, ncore_w: int, nomega_chi_imag: int, nomega_chi_real: int,
                  nomega_sigma: int = 51, step_sigma: float = 0.01, eta: float = 0.001,
-                 exchange_m_vxc: np.ndarray | None = None) -> ContourResult:
+                 exchange_m_vxc: np.ndarray | None = None, energy_g: np.ndarray | None = None) -> ContourResult:
     """selfenergy_evaluation for contour_deformation (src/m_selfenergy_evaluation.f90:239-240):
     Sigma on the real grid, then the linearized and graphical QP energies and
-    HOMO/LUMO over the Sigma states (:587-611)."""
+    HOMO/LUMO over the Sigma states (:587-611).  ``energy_g`` (default
+    ``energy``) seeds se%energy0 (se%init with energy_g, :185) and goes into
+    gw_selfenergy_contour (W and the poles); the QP equation keeps ``energy``."""
+    eg = energy if energy_g is None else energy_g
     sigma, se_omega, omega_real, de_max, w_imag, w_real = gw_selfenergy_contour(
-        energy, occupation, m_ia, m_sigma, rng, ncore_w, nomega_chi_imag, nomega_chi_real, nomega_sigma,
+        eg, occupation, m_ia, m_sigma, rng, ncore_w, nomega_chi_imag, nomega_chi_real, nomega_sigma,
         step_sigma, eta)
     e0 = energy[rng.nsemin - 1: rng.nsemax]
-    se = SelfEnergyGrid(omega=se_omega.astype(complex), omega_calc=np.zeros(0, complex), energy0=e0.copy(),
-                        sigma=sigma)
+    se = SelfEnergyGrid(omega=se_omega.astype(complex), omega_calc=np.zeros(0, complex),
+                        energy0=eg[rng.nsemin - 1: rng.nsemax].copy(), sigma=sigma)
     xc = np.zeros_like(e0) if exchange_m_vxc is None else exchange_m_vxc
     eqp_z, _ = find_qp_energy_linearization(se, xc, e0)
     eqp_g, zz_g, _, _ = find_qp_energy_graphical(se, xc, e0)

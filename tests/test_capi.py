@@ -194,3 +194,29 @@ def test_sosex_problem_layout_matches_ctypes(tmp_path):
     assert int(out["S"]) == C.sizeof(SosexProblem)
     for f in fields:
         assert int(out[f"X {f}"]) == getattr(SosexProblem, f).offset, f
+
+
+@pytest.mark.parametrize("cname,pyname", [("rigw_contour_problem", "ContourProblem"),
+                                          ("rigw_contour_result", "ContourResult")])
+def test_contour_layouts_match_ctypes(tmp_path, cname, pyname):
+    from molgw_b200 import rigw
+    cls = getattr(rigw, pyname)
+    fields = [f for f, _ in cls._fields_]
+    body = "".join(f'  printf("X {f} %zu\\n", offsetof({cname}, {f}));\n' for f in fields)
+    src = tmp_path / "contour.c"
+    src.write_text(textwrap.dedent(f"""
+        #include <stdio.h>
+        #include <stddef.h>
+        #include "rigw.h"
+        int main(void) {{
+          printf("S %zu\\n", sizeof({cname}));
+        {body}  return 0;
+        }}
+    """))
+    exe = tmp_path / "contour"
+    subprocess.run(["gcc", "-std=c99", "-I", str(ROOT / "include"), str(src), "-o", str(exe)], check=True)
+    out = dict(line.rsplit(" ", 1) for line in
+               subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split("\n") if line)
+    assert int(out["S"]) == C.sizeof(cls)
+    for f in fields:
+        assert int(out[f"X {f}"]) == getattr(cls, f).offset, f
