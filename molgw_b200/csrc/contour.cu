@@ -4,7 +4,7 @@
 //   chi0(w) = M^T F(w) M, F_t = REAL(2 docc de / (w^2 - de^2))   (DMMA, lower tiles, mirrored)
 //           at nomega_imag Gauss-Legendre imaginary frequencies and nomega_real
 //           real frequencies 0 .. de_max                          (src/m_spectral_function.f90:779-921)
-//   chi0(w) = V diag(lambda) V^T                                  (parallel Jacobi, one CTA per frequency)
+//   chi0(w) = V diag(lambda) V^T                                  (block Jacobi, eigh_jacobi.cu)
 //   g_k = lambda_k / (1 - lambda_k), dropped where |g_k| <= 1e-3   (the low-rank W)
 //   v(w, m, p) = sum_k g_k (V_k . M_mp)^2                         (DMMA Z = V^T M^T, then a weighted
 //                                                                   column sum of squares)
@@ -13,14 +13,9 @@
 //                  closest to |de| (no interpolation, :440-538)
 //   QP: linearized and graphical on that real grid (qp_tools.cuh).
 //
-// The eigensolver is the two-sided cyclic Jacobi method (Jacobi 1846; Rutishauser's
-// rotation formula) with the round-robin pairing of Brent and Luk (1985): each
-// round rotates n/2 disjoint index pairs at once, n - 1 rounds make a sweep.
-// With that pairing the first members of consecutive pairs are consecutive
-// indices (the second members count down), so the row pass (rows a, b, all
-// columns) and the column pass (all rows, columns a, b) both read consecutive
-// addresses across a warp.  A rotation is skipped when |a_pq| <= 1e-14 ||A||_F;
-// the sweeps stop when one rotates nothing (normwise accuracy, as DSYEV's).
+// The auxiliary dimension is padded with zeros to a multiple of 64 (the block
+// size of the eigensolver); the padded rows and columns stay decoupled and give
+// zero eigenvalues, which the low-rank filter drops.
 #include <algorithm>
 #include <cmath>
 #include <vector>
@@ -31,19 +26,15 @@
 namespace rigw {
 namespace {
 
-constexpr int kJacThreads = 1024;
-constexpr int kJacMaxSweeps = 60;
-constexpr double kJacRelTol = 1.0e-14;
 constexpr double kTolLowEigval = 1.0e-3;   // TOL_LOW_EIGVAL, src/m_spectral_function.f90:783
 constexpr double kPi = 3.14159265358979323;
 
 enum ContourErr : int {
-  kCErrJacobi = 1,      // an eigensolver ran out of sweeps
   kCErrRange = 2,       // a residue asked for a real frequency outside 0 .. de_max
   kCErrNonFinite = 4,   // non-finite QP energy
 };
 
-inline long long round_up2(long long v) { return (v + 1) / 2 * 2; }
+inline long long round_up(long long v, long long a) { return (v + a - 1) / a * a; }
 
 // F[w][t] = REAL(2 docc de / (omega_w^2 - de^2)) (src/m_spectral_function.f90:861-872);
 // om2[w] is the real part of omega_w^2 (-y^2 on the imaginary axis, x^2 on the real one).
@@ -94,105 +85,6 @@ __global__ void contour_mirror_kernel(double* __restrict__ A, int n, long long s
     const int r = rt * 32 + y, c = ct * 32 + threadIdx.x;
     if (r < n && c < n && r < c) a[size_t(r) * n + c] = t[threadIdx.x][y];
   }
-}
-
-// Pair k of round r of the round-robin ordering over m (even) indices.
-RIGW_DEVICE_INLINE void round_robin_pair(int r, int k, int m, int& a, int& b) {
-  if (k == 0) {
-    a = 0;
-    b = 1 + r;
-  } else {
-    a = 1 + (r + k) % (m - 1);
-    b = 1 + (r - k + (m - 1)) % (m - 1);
-  }
-}
-
-// Eigen-decomposition of the symmetric n x n matrix blockIdx.x (n even): on
-// return its diagonal holds the eigenvalues and V (row-major, V[i][k] =
-// component i of eigenvector k) the eigenvectors.  Both stay in global memory
-// (L2-resident at the sizes of this path); the rotation parameters of a round
-// live in shared memory (n doubles).
-__global__ void __launch_bounds__(kJacThreads) jacobi_eigh_kernel(double* __restrict__ Aall,
-                                                                  double* __restrict__ Vall, int n, long long sA,
-                                                                  int* __restrict__ status) {
-  double* A = Aall + size_t(blockIdx.x) * sA;
-  double* V = Vall + size_t(blockIdx.x) * sA;
-  extern __shared__ double jac_smem[];
-  double* cs = jac_smem;
-  double* sn = jac_smem + n / 2;
-  __shared__ double red[32];
-  const int tid = threadIdx.x, nt = blockDim.x, half = n / 2;
-  const long long nn = (long long)n * n;
-  double acc = 0.0;
-  for (long long idx = tid; idx < nn; idx += nt) {
-    const double x = A[idx];
-    acc += x * x;
-    V[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
-  }
-  acc = warp_sum(acc);
-  if ((tid & 31) == 0) red[tid >> 5] = acc;
-  __syncthreads();
-  if (tid < 32) {
-    double v = tid < (nt >> 5) ? red[tid] : 0.0;
-    v = warp_sum(v);
-    if (tid == 0) red[0] = v;
-  }
-  __syncthreads();
-  const double tau = kJacRelTol * sqrt(red[0]);
-  bool converged = false;
-  for (int sweep = 0; sweep < kJacMaxSweeps && !converged; ++sweep) {
-    int did = 0;
-    for (int r = 0; r < n - 1; ++r) {
-      for (int k = tid; k < half; k += nt) {
-        int a, b;
-        round_robin_pair(r, k, n, a, b);
-        const double apq = A[size_t(a) * n + b];
-        double c = 1.0, s = 0.0;
-        if (fabs(apq) > tau) {
-          const double app = A[size_t(a) * n + a], aqq = A[size_t(b) * n + b];
-          const double th = (aqq - app) / (2.0 * apq);
-          const double t = fabs(th) < 1.0e150 ? copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0)) : 0.5 / th;
-          c = 1.0 / sqrt(t * t + 1.0);
-          s = t * c;
-          did = 1;
-        }
-        cs[k] = c;
-        sn[k] = s;
-      }
-      __syncthreads();
-      // rows a and b of every rotating pair: A <- J^T A
-      for (long long idx = tid; idx < (long long)half * n; idx += nt) {
-        const int k = int(idx / n), j = int(idx % n);
-        const double s = sn[k];
-        if (s == 0.0) continue;
-        const double c = cs[k];
-        int a, b;
-        round_robin_pair(r, k, n, a, b);
-        const double xa = A[size_t(a) * n + j], xb = A[size_t(b) * n + j];
-        A[size_t(a) * n + j] = c * xa - s * xb;
-        A[size_t(b) * n + j] = s * xa + c * xb;
-      }
-      __syncthreads();
-      // columns a and b of A and V: A <- A J, V <- V J
-      for (long long idx = tid; idx < (long long)half * n; idx += nt) {
-        const int i = int(idx / half), k = int(idx % half);
-        const double s = sn[k];
-        if (s == 0.0) continue;
-        const double c = cs[k];
-        int a, b;
-        round_robin_pair(r, k, n, a, b);
-        const double xa = A[size_t(i) * n + a], xb = A[size_t(i) * n + b];
-        A[size_t(i) * n + a] = c * xa - s * xb;
-        A[size_t(i) * n + b] = s * xa + c * xb;
-        const double va = V[size_t(i) * n + a], vb = V[size_t(i) * n + b];
-        V[size_t(i) * n + a] = c * va - s * vb;
-        V[size_t(i) * n + b] = s * va + c * vb;
-      }
-      __syncthreads();
-    }
-    converged = !__syncthreads_or(did);
-  }
-  if (!converged && tid == 0) atomicOr(status, kCErrJacobi);
 }
 
 // g[w][k] = lambda_k / (1 - lambda_k) where |.| > 1e-3, else 0 (src/m_spectral_function.f90:898-913);
@@ -324,8 +216,8 @@ Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_co
   const bool on_dev = (pr.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
   const int h = pr.nomega_sigma / 2, nrs = 2 * h + 1;
   const int nw = nimag + nreal;
-  const long long npad = round_up2(naux), ntrans = (long long)no * nv, ntp = round_up2(ntrans);
-  const long long ncols = (long long)nsig * np, ncp = round_up2(ncols);
+  const long long npad = round_up(naux, 64), ntrans = (long long)no * nv, ntp = round_up(ntrans, 2);
+  const long long ncols = (long long)nsig * np, ncp = round_up(ncols, 2);
   if (npad * npad >= (1LL << 31) || ntp >= (1LL << 31) || npad * ncp >= (1LL << 31) || npad > 16384)
     return Status::fail(RIGW_ERR_ARG, "gw_selfenergy_contour: dimensions beyond the supported range");
 
@@ -389,7 +281,8 @@ Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_co
   int* status = reinterpret_cast<int*>(b_status.data());
   int* rank = status + 1;
   double *d_eo = sm, *d_ev = d_eo + no, *d_oo = d_ev + nv, *d_ov = d_oo + no, *d_ep = d_ov + nv;
-  double *d_e0 = d_ep + np, *d_eq = d_e0 + nsig, *d_xc = d_eq + nsig, *d_y = d_xc + nsig, *d_wq = d_y + nimag, *d_omr = d_wq + nimag;
+  double *d_e0 = d_ep + np, *d_eq = d_e0 + nsig, *d_xc = d_eq + nsig, *d_y = d_xc + nsig;
+  double *d_wq = d_y + nimag, *d_omr = d_wq + nimag;
   double* d_om2 = d_omr + nreal;
 
   // inputs
@@ -409,16 +302,22 @@ Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_co
   std::copy(om2.begin(), om2.end(), small.begin() + (d_om2 - sm));
   RIGW_CUDA_TRY(cudaMemcpyAsync(sm, small.data(), nsmall * 8, cudaMemcpyHostToDevice, s));
   RIGW_CUDA_TRY(cudaMemsetAsync(status, 0, size_t(nw + 1) * sizeof(int), s));
-  const cudaMemcpyKind kind = on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
-  RIGW_CUDA_TRY(cudaMemsetAsync(mt, 0, size_t(ntp) * npad * 8, s));
-  RIGW_CUDA_TRY(cudaMemcpy2DAsync(mt, size_t(npad) * 8, pr.m_ia, size_t(naux) * 8, size_t(naux) * 8, size_t(ntrans),
-                                  kind, s));
+  // the host tensors go up contiguous (one copy each); the pitched copy into the
+  // padded layout runs device to device
+  const double* mia = pr.m_ia;
   const double* mpm = pr.m_pm;
   if (!on_dev) {
-    RIGW_TRY(b_mpm.allocate(&c, size_t(ncols) * naux * 8, "contour M_sigma"));
-    RIGW_CUDA_TRY(cudaMemcpyAsync(b_mpm.data(), pr.m_pm, size_t(ncols) * naux * 8, cudaMemcpyHostToDevice, s));
-    mpm = reinterpret_cast<const double*>(b_mpm.data());
+    RIGW_TRY(b_mpm.allocate(&c, size_t(ncols + ntrans) * naux * 8, "contour M uploads"));
+    double* up = reinterpret_cast<double*>(b_mpm.data());
+    RIGW_CUDA_TRY(cudaMemcpyAsync(up, pr.m_pm, size_t(ncols) * naux * 8, cudaMemcpyHostToDevice, s));
+    RIGW_CUDA_TRY(cudaMemcpyAsync(up + size_t(ncols) * naux, pr.m_ia, size_t(ntrans) * naux * 8,
+                                  cudaMemcpyHostToDevice, s));
+    mpm = up;
+    mia = up + size_t(ncols) * naux;
   }
+  RIGW_CUDA_TRY(cudaMemsetAsync(mt, 0, size_t(ntp) * npad * 8, s));
+  RIGW_CUDA_TRY(cudaMemcpy2DAsync(mt, size_t(npad) * 8, mia, size_t(naux) * 8, size_t(naux) * 8, size_t(ntrans),
+                                  cudaMemcpyDeviceToDevice, s));
   RIGW_CUDA_TRY(cudaMemsetAsync(mT, 0, size_t(npad) * ncp * 8, s));
   int launches = 0;
   contour_transpose_kernel<<<dim3(unsigned((naux + 31) / 32), unsigned((ncols + 31) / 32)), dim3(32, 8), 0, s>>>(
@@ -481,14 +380,11 @@ Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_co
   RIGW_CUDA_TRY(cudaEventRecord(ev.e[2], s));
 
   // eigenpairs, low-rank weights
-  const size_t jac_smem = size_t(npad) * 8;
-  if (jac_smem > 48 * 1024)
-    RIGW_CUDA_TRY(cudaFuncSetAttribute(jacobi_eigh_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(jac_smem)));
-  jacobi_eigh_kernel<<<nw, kJacThreads, jac_smem, s>>>(chi, vv, int(npad), npad * npad, status);
+  int sweeps = 0;
+  RIGW_TRY(eigh_jacobi_batched(c, chi, vv, int(npad), nw, s, &sweeps, &launches));
   contour_lowrank_kernel<<<nw, 256, 0, s>>>(chi, int(npad), npad * npad, g, rank);
   RIGW_CUDA_TRY(cudaGetLastError());
-  launches += 2;
+  launches += 1;
   RIGW_CUDA_TRY(cudaEventRecord(ev.e[3], s));
 
   // v(w, m, p), Sigma on the real grids, QP
@@ -527,9 +423,6 @@ Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_co
                                 s));
   RIGW_CUDA_TRY(cudaEventRecord(ev.e[4], s));
   RIGW_CUDA_TRY(cudaEventSynchronize(ev.e[4]));
-  if (host_status[0] & kCErrJacobi)
-    return Status::fail(RIGW_ERR_NUMERIC, "gw_selfenergy_contour: eigensolver did not converge in %d sweeps",
-                        kJacMaxSweeps);
   if (host_status[0] & kCErrRange)
     return Status::fail(RIGW_ERR_NUMERIC, "gw_selfenergy_contour: requested real frequency out of range");
   if (host_status[0] & kCErrNonFinite)

@@ -1,0 +1,301 @@
+// Batched symmetric eigensolver: block two-sided Jacobi.
+//
+// The matrix (n a multiple of 64) is cut into nb = n / 32 block rows.  A sweep
+// visits every pair of blocks (I, J) once in the round-robin order of Brent and
+// Luk (1985): each round takes nb/2 disjoint pairs, nb - 1 rounds make a sweep.
+// For a pair, the 64 x 64 subproblem S = [A_II A_IJ; A_JI A_JJ] is diagonalized
+// in shared memory by the scalar cyclic Jacobi method (Rutishauser's rotation
+// formula, round-robin pairs of its 64 indices, to convergence), which gives the
+// orthogonal Q with Q^T S Q diagonal.  The whole matrix is then updated with
+// that rotation embedded at the rows / columns of I and J:
+//   rows    A[IJ, :] <- Q^T A[IJ, :]     (eigh_pair_kernel, right after the solve)
+//   columns A[:, IJ] <- A[:, IJ] Q,  V[:, IJ] <- V[:, IJ] Q   (eigh_col_kernel)
+// Rotations of different pairs act on disjoint rows (columns), so a round is two
+// launches over all pairs and all matrices of the batch.  The products are
+// 64-wide and stream the matrix once per round, against once per single
+// rotation in the scalar method.
+//
+// A subproblem whose off-diagonal entries are all <= tau = 1e-14 ||A||_F is
+// left alone, one with a larger entry is solved down to tau/4; the sweeps stop
+// when one leaves every pair alone (normwise accuracy, as DSYEV's).  The eigenvalues are then the diagonal of A and V[i][k] is
+// component i of eigenvector k.  Every loop is bounded: a subproblem that does
+// not converge in 40 inner sweeps, or a matrix in 40 outer sweeps, returns
+// RIGW_ERR_NUMERIC.
+#include <vector>
+
+#include "engine.cuh"
+
+namespace rigw {
+namespace {
+
+constexpr int kB = 32;            // block size
+constexpr int kS = 2 * kB;        // subproblem size
+constexpr int kLd = kS + 1;       // shared-memory row stride (conflict-free columns)
+constexpr int kThreads = 256;
+constexpr int kInnerMaxSweeps = 40;
+constexpr int kOuterMaxSweeps = 40;
+constexpr double kRelTol = 1.0e-14;
+constexpr size_t kPairSmem = size_t(3 * kS * kLd + kS) * sizeof(double);   // S, Q, tile, rotations
+constexpr size_t kColSmem = size_t(2 * kS * kLd) * sizeof(double);         // Q, tile
+
+// Pair k of round r of the round-robin ordering over m (even) indices.
+RIGW_DEVICE_INLINE void rr_pair(int r, int k, int m, int& a, int& b) {
+  if (k == 0) {
+    a = 0;
+    b = 1 + r;
+  } else {
+    a = 1 + (r + k) % (m - 1);
+    b = 1 + (r - k + (m - 1)) % (m - 1);
+  }
+}
+
+// Row or column of the full matrix of index i (0..63) of the subproblem of blocks I, J.
+RIGW_DEVICE_INLINE int sub_index(int i, int I, int J) { return i < kB ? I * kB + i : J * kB + (i - kB); }
+
+// V = I and tau = 1e-14 ||A||_F for matrix blockIdx.x.
+__global__ void __launch_bounds__(1024) eigh_init_kernel(const double* __restrict__ Aall, double* __restrict__ Vall,
+                                                         int n, long long sA, double* __restrict__ tau) {
+  const double* A = Aall + size_t(blockIdx.x) * sA;
+  double* V = Vall + size_t(blockIdx.x) * sA;
+  __shared__ double red[32];
+  const long long nn = (long long)n * n;
+  double acc = 0.0;
+  for (long long idx = threadIdx.x; idx < nn; idx += blockDim.x) {
+    const double x = A[idx];
+    acc += x * x;
+    V[idx] = (idx / n == idx % n) ? 1.0 : 0.0;
+  }
+  acc = warp_sum(acc);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    double v = threadIdx.x < (blockDim.x >> 5) ? red[threadIdx.x] : 0.0;
+    v = warp_sum(v);
+    if (threadIdx.x == 0) tau[blockIdx.x] = kRelTol * sqrt(v);
+  }
+}
+
+// Cyclic Jacobi on the 64 x 64 symmetric S (stride kLd) in shared memory,
+// accumulating the rotations into Q (starts as the identity).  Returns true on
+// convergence (a sweep without rotation).
+__device__ bool inner_jacobi(double* S, double* Q, double* cs, double* sn, double tau) {
+  const int tid = threadIdx.x;
+  for (int sweep = 0; sweep < kInnerMaxSweeps; ++sweep) {
+    int did = 0;
+    for (int r = 0; r < kS - 1; ++r) {
+      if (tid < kS / 2) {
+        int a, b;
+        rr_pair(r, tid, kS, a, b);
+        const double apq = S[a * kLd + b];
+        double c = 1.0, s = 0.0;
+        if (fabs(apq) > tau) {
+          const double th = (S[b * kLd + b] - S[a * kLd + a]) / (2.0 * apq);
+          const double t = fabs(th) < 1.0e150 ? copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0)) : 0.5 / th;
+          c = 1.0 / sqrt(t * t + 1.0);
+          s = t * c;
+          did = 1;
+        }
+        cs[tid] = c;
+        sn[tid] = s;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < (kS / 2) * kS; idx += kThreads) {   // rows a, b
+        const int k = idx / kS, j = idx % kS;
+        const double s = sn[k];
+        if (s == 0.0) continue;
+        const double c = cs[k];
+        int a, b;
+        rr_pair(r, k, kS, a, b);
+        const double xa = S[a * kLd + j], xb = S[b * kLd + j];
+        S[a * kLd + j] = c * xa - s * xb;
+        S[b * kLd + j] = s * xa + c * xb;
+      }
+      __syncthreads();
+      for (int idx = tid; idx < kS * (kS / 2); idx += kThreads) {   // columns a, b of S and Q
+        const int i = idx / (kS / 2), k = idx % (kS / 2);
+        const double s = sn[k];
+        if (s == 0.0) continue;
+        const double c = cs[k];
+        int a, b;
+        rr_pair(r, k, kS, a, b);
+        const double xa = S[i * kLd + a], xb = S[i * kLd + b];
+        S[i * kLd + a] = c * xa - s * xb;
+        S[i * kLd + b] = s * xa + c * xb;
+        const double qa = Q[i * kLd + a], qb = Q[i * kLd + b];
+        Q[i * kLd + a] = c * qa - s * qb;
+        Q[i * kLd + b] = s * qa + c * qb;
+      }
+      __syncthreads();
+    }
+    if (!__syncthreads_or(did)) return true;
+  }
+  return false;
+}
+
+// One CTA per (pair k of round r, matrix w = blockIdx.y): solve the subproblem,
+// store its Q, rotate the 64 rows of the pair.  flags[w][k] says whether the
+// pair rotated; rot[w] whether any pair of matrix w did.
+__global__ void __launch_bounds__(kThreads) eigh_pair_kernel(double* __restrict__ Aall, double* __restrict__ Qbuf,
+                                                             int* __restrict__ flags, int* __restrict__ rot,
+                                                             const double* __restrict__ tau, int n, long long sA,
+                                                             int r, int* __restrict__ status) {
+  extern __shared__ double smem[];
+  double* S = smem;
+  double* Q = S + kS * kLd;
+  double* T = Q + kS * kLd;
+  double* cs = T + kS * kLd;
+  double* sn = cs + kS / 2;
+  const int w = blockIdx.y, k = blockIdx.x, tid = threadIdx.x;
+  const int nb = n / kB, npairs = nb / 2;
+  double* A = Aall + size_t(w) * sA;
+  int I, J;
+  rr_pair(r, k, nb, I, J);
+  const double tw = tau[w];
+  int big = 0;
+  for (int idx = tid; idx < kS * kS; idx += kThreads) {
+    const int i = idx / kS, j = idx % kS;
+    const double x = A[size_t(sub_index(i, I, J)) * n + sub_index(j, I, J)];
+    S[i * kLd + j] = x;
+    Q[i * kLd + j] = (i == j) ? 1.0 : 0.0;
+    if (i != j && fabs(x) > tw) big = 1;
+  }
+  if (!__syncthreads_or(big)) {
+    if (tid == 0) flags[w * npairs + k] = 0;
+    return;
+  }
+  // hysteresis: inside a flagged subproblem rotate down to tau/4, so that an
+  // entry just above tau is not left just below it by the other rotations and
+  // recreated above it by the rounding of the 64-wide updates
+  if (!inner_jacobi(S, Q, cs, sn, 0.25 * tw) && tid == 0) atomicOr(status, 1);
+  if (tid == 0) {
+    flags[w * npairs + k] = 1;
+    atomicOr(rot + w, 1);
+  }
+  double* qg = Qbuf + (size_t(w) * npairs + k) * kS * kS;
+  for (int idx = tid; idx < kS * kS; idx += kThreads) qg[idx] = Q[(idx / kS) * kLd + idx % kS];
+  // rows: A[IJ, c0:c0+64] <- Q^T A[IJ, c0:c0+64]
+  const int ty = tid / 16, tx = tid % 16;
+  for (int c0 = 0; c0 < n; c0 += kS) {
+    __syncthreads();   // the previous tile's reads are done
+    for (int idx = tid; idx < kS * kS; idx += kThreads) {
+      const int i = idx / kS, j = idx % kS;
+      T[i * kLd + j] = A[size_t(sub_index(i, I, J)) * n + c0 + j];
+    }
+    __syncthreads();
+    double acc[4][4] = {};
+    for (int kk = 0; kk < kS; ++kk) {
+      double q[4], t[4];
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii) q[ii] = Q[kk * kLd + ty + 16 * ii];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) t[jj] = T[kk * kLd + tx + 16 * jj];
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(q[ii], t[jj], acc[ii][jj]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        A[size_t(sub_index(ty + 16 * ii, I, J)) * n + c0 + tx + 16 * jj] = acc[ii][jj];
+  }
+}
+
+// One CTA per (pair, 64-row chunk) x matrix: A[rows, IJ] <- A[rows, IJ] Q and
+// the same for V, for the pairs of round r that rotated.
+__global__ void __launch_bounds__(kThreads) eigh_col_kernel(double* __restrict__ Aall, double* __restrict__ Vall,
+                                                            const double* __restrict__ Qbuf,
+                                                            const int* __restrict__ flags, int n, long long sA,
+                                                            int r) {
+  extern __shared__ double smem[];
+  double* Q = smem;
+  double* T = Q + kS * kLd;
+  const int nb = n / kB, npairs = nb / 2;
+  const int w = blockIdx.y, k = blockIdx.x % npairs, chunk = blockIdx.x / npairs, tid = threadIdx.x;
+  if (!flags[w * npairs + k]) return;
+  int I, J;
+  rr_pair(r, k, nb, I, J);
+  const double* qg = Qbuf + (size_t(w) * npairs + k) * kS * kS;
+  for (int idx = tid; idx < kS * kS; idx += kThreads) Q[(idx / kS) * kLd + idx % kS] = qg[idx];
+  const int i0 = chunk * kS;
+  const int ty = tid / 16, tx = tid % 16;
+  for (int m = 0; m < 2; ++m) {
+    double* M = (m == 0 ? Aall : Vall) + size_t(w) * sA;
+    __syncthreads();
+    for (int idx = tid; idx < kS * kS; idx += kThreads) {
+      const int i = idx / kS, j = idx % kS;
+      T[i * kLd + j] = M[size_t(i0 + i) * n + sub_index(j, I, J)];
+    }
+    __syncthreads();
+    double acc[4][4] = {};
+    for (int kk = 0; kk < kS; ++kk) {
+      double t[4], q[4];
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii) t[ii] = T[(ty + 16 * ii) * kLd + kk];
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) q[jj] = Q[kk * kLd + tx + 16 * jj];
+#pragma unroll
+      for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(t[ii], q[jj], acc[ii][jj]);
+    }
+#pragma unroll
+    for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj)
+        M[size_t(i0 + ty + 16 * ii) * n + sub_index(tx + 16 * jj, I, J)] = acc[ii][jj];
+  }
+}
+
+}  // namespace
+
+Status eigh_jacobi_batched(Context& c, double* A, double* V, int n, int nw, cudaStream_t s, int* sweeps,
+                           int* launches) {
+  if (n <= 0 || n % kS != 0 || nw <= 0)
+    return Status::fail(RIGW_ERR_ARG, "eigh_jacobi_batched: n must be a positive multiple of %d", kS);
+  // per device (cheap): the current device is the context's
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(eigh_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPairSmem)));
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(eigh_col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kColSmem)));
+  const int nb = n / kB, npairs = nb / 2, chunks = n / kS;
+  const long long sA = (long long)n * n;
+  DeviceBuffer b_q, b_aux;
+  RIGW_TRY(b_q.allocate(&c, size_t(nw) * npairs * kS * kS * 8, "eigensolver block rotations"));
+  const size_t aux_bytes = size_t(nw) * 8 + size_t(nw) * npairs * 4 + size_t(nw) * 4 + 4;
+  RIGW_TRY(b_aux.allocate(&c, aux_bytes, "eigensolver flags"));
+  double* qbuf = reinterpret_cast<double*>(b_q.data());
+  double* tau = reinterpret_cast<double*>(b_aux.data());
+  int* flags = reinterpret_cast<int*>(tau + nw);
+  int* rot = flags + size_t(nw) * npairs;
+  int* status = rot + nw;
+  RIGW_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), s));
+  eigh_init_kernel<<<nw, 1024, 0, s>>>(A, V, n, sA, tau);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  int nl = 1;
+  std::vector<int> host_rot(nw + 1);
+  bool converged = false;
+  int sweep = 0;
+  for (; sweep < kOuterMaxSweeps && !converged; ++sweep) {
+    RIGW_CUDA_TRY(cudaMemsetAsync(rot, 0, size_t(nw) * sizeof(int), s));
+    for (int r = 0; r < nb - 1; ++r) {
+      eigh_pair_kernel<<<dim3(npairs, nw), kThreads, kPairSmem, s>>>(A, qbuf, flags, rot, tau, n, sA, r, status);
+      eigh_col_kernel<<<dim3(npairs * chunks, nw), kThreads, kColSmem, s>>>(A, V, qbuf, flags, n, sA, r);
+      nl += 2;
+    }
+    RIGW_CUDA_TRY(cudaGetLastError());
+    RIGW_CUDA_TRY(cudaMemcpyAsync(host_rot.data(), rot, size_t(nw + 1) * sizeof(int), cudaMemcpyDeviceToHost, s));
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+    if (host_rot[nw] != 0)
+      return Status::fail(RIGW_ERR_NUMERIC, "eigh_jacobi_batched: a subproblem did not converge in %d sweeps",
+                          kInnerMaxSweeps);
+    converged = true;
+    for (int w = 0; w < nw; ++w) converged = converged && host_rot[w] == 0;
+  }
+  if (!converged)
+    return Status::fail(RIGW_ERR_NUMERIC, "eigh_jacobi_batched: no convergence in %d sweeps", kOuterMaxSweeps);
+  if (sweeps) *sweeps = sweep;
+  if (launches) *launches += nl;
+  return Status::ok();
+}
+
+}  // namespace rigw

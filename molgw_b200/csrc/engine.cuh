@@ -276,6 +276,11 @@ Status sox_selfenergy_imag(Context& c, const rigw_sox_problem& pr, double* sigma
 Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem& pr, double* sigma);
 Status g3w2_selfenergy_imag(Context& c, const Wpol& w, const rigw_g3w2_problem& pr, double* sigma);
 Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_contour_result& res);
+// Eigenpairs of nw symmetric n x n matrices (n a multiple of 64, row-major, A[w] at A + w n^2):
+// on return the diagonal of A[w] holds the eigenvalues and V[w][i][k] is component i of
+// eigenvector k (eigh_jacobi.cu).  Adds its kernel launches to *launches.
+Status eigh_jacobi_batched(Context& c, double* A, double* V, int n, int nw, cudaStream_t s, int* sweeps,
+                           int* launches);
 Status eri_3center_mo(Context& c, int nbf, int nstate, int npair, int naux, const int* index_basis,
                       const double* eri3, const double* c_matrix, int mstate_min, int mstate_max,
                       int nstate_min, int nstate_max, double* out, int precision, int flags = 0);
