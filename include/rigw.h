@@ -348,15 +348,17 @@ RIGW_API int rigw_g0w0_batch(rigw_ctx* ctx, int nprob, const rigw_problem* probs
  * No routine of the reference corresponds to this.  Times launch-shape
  * candidates on the given batch (which must fit the device in one plan): the
  * row height of the FP64 chi0 and trailing-update tiles (64 or 128 rows x 128
- * columns) and the number of frequency chains (the split-precision buffer size
- * follows the free memory of each batch and is not tuned).  The fastest shapes are kept in the context for every later
- * batch of the same precision class (FP64, BF16x3, Ozaki, mixed); results of a
- * solve do not depend on them beyond floating-point summation order. */
+ * columns), the number of frequency chains, the panels per trailing update and,
+ * for split precision, the frequencies per split buffer (automatic, a group
+ * whose buffers fit in L2, or 8).  The fastest shapes are kept in the context
+ * for every later batch of the same precision class (FP64, BF16x3, Ozaki,
+ * mixed); results of a solve do not depend on them beyond floating-point
+ * summation order. */
 #define RIGW_TUNE_MAX_CANDIDATES 16
 typedef struct rigw_tune_report {
   int chi0_rows;             /* FP64 chi0 tile rows chosen (64 or 128)                    */
   int update_rows;           /* trailing-update tile rows chosen (64 or 128)              */
-  int split_group;           /* frequencies per split buffer (0: automatic, not tuned)    */
+  int split_group;           /* frequencies per split buffer (0: automatic)               */
   int chains;                /* frequency chains (0: automatic)                           */
   int panel_group;           /* panels per trailing update of the factorization (2..32)   */
   int precision_class;       /* 0 FP64, 1 BF16x3, 2 Ozaki INT8, 3 mixed                    */

@@ -9,9 +9,10 @@ integral + residues) and the QP equation.
   (tests/inputs/testsuite:777-780), Sigma_c within 1e-9 (relative to its
   largest entry) and the QP energies within 1e-6 eV of the oracle, the same
   eigenpairs kept at every frequency.
-* Seeded synthetic instances against the oracle: an even and an odd auxiliary
-  size (the device pads to even), frozen core in W and G, energy_g != energy
-  (se%energy0 and the poles from energy_g, the QP equation from energy).
+* Seeded synthetic instances against the oracle: auxiliary sizes 70, 61 and
+  300 (the device pads to a multiple of 64: 2 and 5 block pairs per round of
+  the eigensolver), frozen core in W and G, energy_g != energy (se%energy0 and
+  the poles from energy_g, the QP equation from energy).
 * Device-pointer mode equals host mode bitwise.
 
 Sigma_c on the real grid needs no continuation, so the QP energies are well
@@ -81,7 +82,7 @@ def test_h2o_contour_reproduces_the_known_answers(engine):
     assert np.abs(out.sigma - h2o_case.load()["contour_sigma"]).max() < 1e-9 * np.abs(ref.sigma).max()
 
 
-@pytest.mark.parametrize("naux", [70, 61])
+@pytest.mark.parametrize("naux", [70, 61, 300])
 def test_synthetic_matches_the_oracle(engine, naux):
     e, occ, m = _synthetic(6, 40, naux, seed=naux)
     ref, out, _, _ = _both(engine, e, occ, m, ncore=1, nsemin=5, nsemax=8, nimag=12, nreal=8, nomega_sigma=21,
