@@ -9,13 +9,12 @@
 // orthogonal Q.  (Solving S to convergence instead changes neither the number
 // of outer sweeps nor the result: on the test matrices both take 11 outer
 // sweeps at n = 512, the single inner sweep with a quarter of the inner work.)
-// The whole matrix is then updated with that rotation embedded at the rows /
-// columns of I and J:
-//   rows    A[IJ, :] <- Q^T A[IJ, :]     (eigh_pair_kernel, right after the solve)
-//   columns A[:, IJ] <- A[:, IJ] Q,  V[:, IJ] <- V[:, IJ] Q   (eigh_col_kernel)
-// Rotations of different pairs act on disjoint rows (columns), so a round is two
-// launches over all pairs and all matrices of the batch.  The products are
-// 64-wide and stream the matrix once per round, against once per single
+// The whole matrix is then updated with the round's rotation J (the pairs' Q
+// embedded at their rows and columns): every row and column belongs to exactly
+// one pair, so tile (p, q) of J^T A J is Q_p^T A[P, Q] Q_q and depends only on
+// tile (p, q) of A (eigh_apply_kernel, one CTA per upper tile, plus V <- V J by
+// 64-row chunks).  A round is two launches over all pairs and all matrices of
+// the batch; the update streams A and V once per round, against once per single
 // rotation in the scalar method.
 //
 // A subproblem whose off-diagonal entries are all <= tau = 1e-14 ||A||_F is
@@ -37,8 +36,8 @@ constexpr int kLd = kS + 1;       // shared-memory row stride (conflict-free col
 constexpr int kThreads = 256;
 constexpr int kOuterMaxSweeps = 60;
 constexpr double kRelTol = 1.0e-14;
-constexpr size_t kPairSmem = size_t(3 * kS * kLd + kS + kS / 2) * sizeof(double);   // S, Q, tile, rotations, pairs
-constexpr size_t kColSmem = size_t(2 * kS * kLd) * sizeof(double);         // Q, tile
+constexpr size_t kPairSmem = size_t(2 * kS * kLd + kS + kS / 2) * sizeof(double);   // S, Q, rotations, pairs
+constexpr size_t kApplySmem = size_t(3 * kS * kLd) * sizeof(double);                // tile, two rotations
 
 // Pair k of round r of the round-robin ordering over m (even) indices.
 RIGW_DEVICE_INLINE void rr_pair(int r, int k, int m, int& a, int& b) {
@@ -133,23 +132,22 @@ __device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn,
   }
 }
 
-// One CTA per (pair k of round r, matrix w = blockIdx.y): solve the subproblem,
-// store its Q, rotate the 64 rows of the pair.  flags[w][k] says whether the
-// pair rotated; rot[w] whether any pair of matrix w did.
-__global__ void __launch_bounds__(kThreads) eigh_pair_kernel(double* __restrict__ Aall, double* __restrict__ Qbuf,
-                                                             int* __restrict__ flags, int* __restrict__ rot,
-                                                             const double* __restrict__ tau, int n, long long sA,
-                                                             int r) {
+// One CTA per (pair k of round r, matrix w = blockIdx.y): one sweep on the
+// subproblem, its Q to Qbuf.  flags[w][k] says whether the pair rotated;
+// rot[w] whether any pair of matrix w did.
+__global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __restrict__ Aall,
+                                                             double* __restrict__ Qbuf, int* __restrict__ flags,
+                                                             int* __restrict__ rot, const double* __restrict__ tau,
+                                                             int n, long long sA, int r) {
   extern __shared__ double smem[];
   double* S = smem;
   double* Q = S + kS * kLd;
-  double* T = Q + kS * kLd;
-  double* cs = T + kS * kLd;
+  double* cs = Q + kS * kLd;
   double* sn = cs + kS / 2;
   int* pab = reinterpret_cast<int*>(sn + kS / 2);
   const int w = blockIdx.y, k = blockIdx.x, tid = threadIdx.x;
   const int nb = n / kB, npairs = nb / 2;
-  double* A = Aall + size_t(w) * sA;
+  const double* A = Aall + size_t(w) * sA;
   int I, J;
   rr_pair(r, k, nb, I, J);
   const double tw = tau[w];
@@ -175,78 +173,107 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(double* __restrict_
   }
   double* qg = Qbuf + (size_t(w) * npairs + k) * kS * kS;
   for (int idx = tid; idx < kS * kS; idx += kThreads) qg[idx] = Q[(idx / kS) * kLd + idx % kS];
-  // rows: A[IJ, c0:c0+64] <- Q^T A[IJ, c0:c0+64]
-  const int ty = tid / 16, tx = tid % 16;
-  for (int c0 = 0; c0 < n; c0 += kS) {
-    __syncthreads();   // the previous tile's reads are done
-    for (int idx = tid; idx < kS * kS; idx += kThreads) {
-      const int i = idx / kS, j = idx % kS;
-      T[i * kLd + j] = A[size_t(sub_index(i, I, J)) * n + c0 + j];
-    }
-    __syncthreads();
-    double acc[4][4] = {};
-    for (int kk = 0; kk < kS; ++kk) {
-      double q[4], t[4];
-#pragma unroll
-      for (int ii = 0; ii < 4; ++ii) q[ii] = Q[kk * kLd + ty + 16 * ii];
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) t[jj] = T[kk * kLd + tx + 16 * jj];
-#pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(q[ii], t[jj], acc[ii][jj]);
-    }
-#pragma unroll
-    for (int ii = 0; ii < 4; ++ii)
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-        A[size_t(sub_index(ty + 16 * ii, I, J)) * n + c0 + tx + 16 * jj] = acc[ii][jj];
-  }
 }
 
-// One CTA per (pair, 64-row chunk) x matrix: A[rows, IJ] <- A[rows, IJ] Q and
-// the same for V, for the pairs of round r that rotated.
-__global__ void __launch_bounds__(kThreads) eigh_col_kernel(double* __restrict__ Aall, double* __restrict__ Vall,
-                                                            const double* __restrict__ Qbuf,
-                                                            const int* __restrict__ flags, int n, long long sA,
-                                                            int r) {
-  extern __shared__ double smem[];
-  double* Q = smem;
-  double* T = Q + kS * kLd;
-  const int nb = n / kB, npairs = nb / 2;
-  const int w = blockIdx.y, k = blockIdx.x % npairs, chunk = blockIdx.x / npairs, tid = threadIdx.x;
-  if (!flags[w * npairs + k]) return;
-  int I, J;
-  rr_pair(r, k, nb, I, J);
-  const double* qg = Qbuf + (size_t(w) * npairs + k) * kS * kS;
-  for (int idx = tid; idx < kS * kS; idx += kThreads) Q[(idx / kS) * kLd + idx % kS] = qg[idx];
-  const int i0 = chunk * kS;
-  const int ty = tid / 16, tx = tid % 16;
-  for (int m = 0; m < 2; ++m) {
-    double* M = (m == 0 ? Aall : Vall) + size_t(w) * sA;
-    __syncthreads();
-    for (int idx = tid; idx < kS * kS; idx += kThreads) {
-      const int i = idx / kS, j = idx % kS;
-      T[i * kLd + j] = M[size_t(i0 + i) * n + sub_index(j, I, J)];
-    }
-    __syncthreads();
-    double acc[4][4] = {};
-    for (int kk = 0; kk < kS; ++kk) {
-      double t[4], q[4];
+// out = X^T T (transpose_x) or T X, 64 x 64 in shared memory, 4 x 4 outputs per
+// thread (rows ty + 16 ii, columns tx + 16 jj); the result goes back into T.
+RIGW_DEVICE_INLINE void tile_product(double* T, const double* X, bool transpose_x) {
+  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
+  double acc[4][4] = {};
+  for (int kk = 0; kk < kS; ++kk) {
+    double u[4], v[4];
+    if (transpose_x) {   // sum_k X[k][i] T[k][j]
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii) t[ii] = T[(ty + 16 * ii) * kLd + kk];
+      for (int ii = 0; ii < 4; ++ii) u[ii] = X[kk * kLd + ty + 16 * ii];
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) q[jj] = Q[kk * kLd + tx + 16 * jj];
+      for (int jj = 0; jj < 4; ++jj) v[jj] = T[kk * kLd + tx + 16 * jj];
+    } else {             // sum_k T[i][k] X[k][j]
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii)
+      for (int ii = 0; ii < 4; ++ii) u[ii] = T[(ty + 16 * ii) * kLd + kk];
 #pragma unroll
-        for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(t[ii], q[jj], acc[ii][jj]);
+      for (int jj = 0; jj < 4; ++jj) v[jj] = X[kk * kLd + tx + 16 * jj];
     }
 #pragma unroll
     for (int ii = 0; ii < 4; ++ii)
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj)
-        M[size_t(i0 + ty + 16 * ii) * n + sub_index(tx + 16 * jj, I, J)] = acc[ii][jj];
+      for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(u[ii], v[jj], acc[ii][jj]);
+  }
+  __syncthreads();   // every read of T is done
+#pragma unroll
+  for (int ii = 0; ii < 4; ++ii)
+#pragma unroll
+    for (int jj = 0; jj < 4; ++jj) T[(ty + 16 * ii) * kLd + tx + 16 * jj] = acc[ii][jj];
+  __syncthreads();
+}
+
+// The rotation of round r applied to the whole matrix in one pass: every row
+// and every column belongs to exactly one pair, so output tile (p, q) of
+// J^T A J is Q_p^T A[P, Q] Q_q and depends only on input tile (p, q).  CTA t <
+// ntri takes the upper tile (p, q), p <= q, of A (writing (q, p) as its
+// transpose, which keeps A exactly symmetric); CTA t >= ntri a (64-row chunk,
+// pair q) tile of V: V[chunk, Q] <- V[chunk, Q] Q_q.  Tiles whose pairs did not
+// rotate are skipped (their Q is the identity).
+__global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict__ Aall, double* __restrict__ Vall,
+                                                              const double* __restrict__ Qbuf,
+                                                              const int* __restrict__ flags, int n, long long sA,
+                                                              int r) {
+  extern __shared__ double smem[];
+  double* T = smem;
+  double* Qa = T + kS * kLd;
+  double* Qb = Qa + kS * kLd;
+  const int nb = n / kB, npairs = nb / 2, ntri = npairs * (npairs + 1) / 2;
+  const int w = blockIdx.y, tid = threadIdx.x;
+  const int* fl = flags + w * npairs;
+  const double* qw = Qbuf + size_t(w) * npairs * kS * kS;
+  int t = blockIdx.x;
+  if (t < ntri) {
+    int p = 0;
+    while (t >= npairs - p) {   // row p of the upper triangle holds npairs - p tiles
+      t -= npairs - p;
+      ++p;
+    }
+    const int q = p + t;
+    const bool fp = fl[p] != 0, fq = fl[q] != 0;
+    if (!fp && !fq) return;
+    int Ip, Jp, Iq, Jq;
+    rr_pair(r, p, nb, Ip, Jp);
+    rr_pair(r, q, nb, Iq, Jq);
+    double* A = Aall + size_t(w) * sA;
+    for (int idx = tid; idx < kS * kS; idx += kThreads) {
+      const int i = idx / kS, j = idx % kS;
+      T[i * kLd + j] = A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)];
+      if (fp) Qa[i * kLd + j] = qw[size_t(p) * kS * kS + idx];
+      if (fq) Qb[i * kLd + j] = qw[size_t(q) * kS * kS + idx];
+    }
+    __syncthreads();
+    if (fp) tile_product(T, Qa, true);
+    if (fq) tile_product(T, Qb, false);
+    for (int idx = tid; idx < kS * kS; idx += kThreads) {
+      const int i = idx / kS, j = idx % kS;
+      // diagonal tile: the upper half mirrored, so the tile stays exactly symmetric
+      const double x = (p == q && i > j) ? T[j * kLd + i] : T[i * kLd + j];
+      A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)] = x;
+      if (p != q) A[size_t(sub_index(j, Iq, Jq)) * n + sub_index(i, Ip, Jp)] = x;
+    }
+    return;
+  }
+  t -= ntri;
+  const int q = t % npairs, chunk = t / npairs;
+  if (!fl[q]) return;
+  int Iq, Jq;
+  rr_pair(r, q, nb, Iq, Jq);
+  double* V = Vall + size_t(w) * sA;
+  const int i0 = chunk * kS;
+  for (int idx = tid; idx < kS * kS; idx += kThreads) {
+    const int i = idx / kS, j = idx % kS;
+    T[i * kLd + j] = V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)];
+    Qb[i * kLd + j] = qw[size_t(q) * kS * kS + idx];
+  }
+  __syncthreads();
+  tile_product(T, Qb, false);
+  for (int idx = tid; idx < kS * kS; idx += kThreads) {
+    const int i = idx / kS, j = idx % kS;
+    V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)] = T[i * kLd + j];
   }
 }
 
@@ -258,8 +285,8 @@ Status eigh_jacobi_batched(Context& c, double* A, double* V, int n, int nw, cuda
     return Status::fail(RIGW_ERR_ARG, "eigh_jacobi_batched: n must be a positive multiple of %d", kS);
   // per device (cheap): the current device is the context's
   RIGW_CUDA_TRY(cudaFuncSetAttribute(eigh_pair_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kPairSmem)));
-  RIGW_CUDA_TRY(cudaFuncSetAttribute(eigh_col_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kColSmem)));
-  const int nb = n / kB, npairs = nb / 2, chunks = n / kS;
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(eigh_apply_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(kApplySmem)));
+  const int nb = n / kB, npairs = nb / 2, chunks = n / kS, ntri = npairs * (npairs + 1) / 2;
   const long long sA = (long long)n * n;
   DeviceBuffer b_q, b_aux;
   RIGW_TRY(b_q.allocate(&c, size_t(nw) * npairs * kS * kS * 8, "eigensolver block rotations"));
@@ -279,7 +306,7 @@ Status eigh_jacobi_batched(Context& c, double* A, double* V, int n, int nw, cuda
     RIGW_CUDA_TRY(cudaMemsetAsync(rot, 0, size_t(nw) * sizeof(int), s));
     for (int r = 0; r < nb - 1; ++r) {
       eigh_pair_kernel<<<dim3(npairs, nw), kThreads, kPairSmem, s>>>(A, qbuf, flags, rot, tau, n, sA, r);
-      eigh_col_kernel<<<dim3(npairs * chunks, nw), kThreads, kColSmem, s>>>(A, V, qbuf, flags, n, sA, r);
+      eigh_apply_kernel<<<dim3(ntri + npairs * chunks, nw), kThreads, kApplySmem, s>>>(A, V, qbuf, flags, n, sA, r);
       nl += 2;
     }
     RIGW_CUDA_TRY(cudaGetLastError());
