@@ -26,6 +26,8 @@
  *   rigw_sosex_selfenergy_imag  sosex_selfenergy_imag_grid    src/m_g3w2_selfenergy.f90:2200-2478
  *   rigw_g3w2_selfenergy_imag   g3w2_selfenergy_imag_grid     src/m_g3w2_selfenergy.f90:2018-2196
  *                               (GW+SOSEX_PADE: added after SOX, src/m_selfenergy_evaluation.f90:498-500)
+ *   rigw_gw_density_matrix_imag gw_density_matrix_imag        src/m_mbpt_density_matrix.f90:491-640
+ *                               (pt_density_matrix GW_IMAGINARY, src/m_dm_mbpt_driver.f90:117-122)
  *   rigw_gw_selfenergy_contour  gw_selfenergy_contour         src/m_gw_selfenergy_grid.f90:342-551
  *                               + sf_vsqrt_chi_vsqrt_rpa(low_rank) src/m_spectral_function.f90:779-921
  *                               + the QP equation of G0W0_CONTOUR, src/m_selfenergy_evaluation.f90:239-240,587-611
@@ -289,6 +291,32 @@ typedef struct rigw_g3w2_problem {
 /* sigma_g3w2: [nsig][nomega_calc][2], overwritten. */
 RIGW_API int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g3w2_problem* prob,
                                        double* sigma_g3w2);
+
+/* ---- GW density matrix from the imaginary axis ----------------------------------
+ * Correction to the MO density matrix of one spin channel (gw_density_matrix_imag),
+ * with v^1/2 chi v^1/2 of the resident factors of ``wpol`` (its frequencies and
+ * weights are wpol_imag's), for p, q in the Sigma range of the window:
+ *   P_pq = -spin_fact 2/(2 pi)^2 sum_k w_k sum_s w_s sum_m (p m|W_k - v|q m)
+ *          Re{ [1/(i s - e~_m + i w_k) + 1/(i s - e~_m - i w_k)] / ((i s - e~_p)(i s - e~_q)) },
+ * e~ = e - mu, the s grid Gauss-Legendre on [0, 1) mapped to [0, inf) with
+ * alpha = beta = 1 (nomega_sigma points).  P is symmetric and zero outside the
+ * Sigma range; adding diag(occupation) and transforming to the AO basis gives
+ * the correlated density matrix (update_density_matrix). */
+typedef struct rigw_dm_problem {
+  int naux;
+  int nstate;                /* window ncore_G+1 .. nvirtual_G-1                           */
+  const double* m_full;      /* [nstate][nstate][naux] = eri_3center_mo(naux, q, r) over the window */
+  int nsig;                  /* Sigma states nsemin..nsemax                                */
+  int sig_first;             /* window index (0-based) of nsemin                           */
+  const double* energy;      /* [nstate] host, energies of the window (Ha)                */
+  double mu;                 /* centre of the HOMO-LUMO gap (Ha)                          */
+  int nomega_sigma;          /* points of the density-matrix frequency grid (<= 256)      */
+  double spin_fact;          /* 2 for nspin = 1                                            */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS (m_full, p_matrix on the device) */
+} rigw_dm_problem;
+/* p_matrix: [nstate][nstate] over the window, overwritten. */
+RIGW_API int rigw_gw_density_matrix_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_dm_problem* prob,
+                                         double* p_matrix);
 
 /* ---- contour deformation ------------------------------------------------------
  * G0W0 by contour deformation (postscf G0W0_CONTOUR), one spin channel

@@ -226,6 +226,15 @@ int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g
   return finish(ctx, rigw::g3w2_selfenergy_imag(ctx->impl, wpol->impl, *prob, sigma_g3w2));
 }
 
+int rigw_gw_density_matrix_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_dm_problem* prob,
+                                double* p_matrix) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!wpol || !prob || !p_matrix) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::gw_density_matrix_imag(ctx->impl, wpol->impl, *prob, p_matrix));
+}
+
 int rigw_gw_selfenergy_contour(rigw_ctx* ctx, const rigw_contour_problem* prob, rigw_contour_result* result) {
   if (!ctx) return RIGW_ERR_ARG;
   if (!prob || !result) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));

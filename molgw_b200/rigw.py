@@ -91,6 +91,14 @@ class G3w2Problem(C.Structure):
     ]
 
 
+class DmProblem(C.Structure):
+    _fields_ = [
+        ("naux", C.c_int), ("nstate", C.c_int), ("m_full", _dp), ("nsig", C.c_int), ("sig_first", C.c_int),
+        ("energy", _dp), ("mu", C.c_double), ("nomega_sigma", C.c_int), ("spin_fact", C.c_double),
+        ("flags", C.c_int),
+    ]
+
+
 class ContourProblem(C.Structure):
     _fields_ = [
         ("naux", C.c_int), ("nocc_w", C.c_int), ("nvirt_w", C.c_int), ("m_ia", _dp), ("e_occ_w", _dp),
@@ -216,6 +224,7 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_sosex_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(SosexProblem), _dp]
     lib.rigw_g3w2_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(G3w2Problem), _dp]
     lib.rigw_gw_selfenergy_contour.argtypes = [C.c_void_p, C.POINTER(ContourProblem), C.POINTER(ContourResult)]
+    lib.rigw_gw_density_matrix_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(DmProblem), _dp]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -649,6 +658,40 @@ class Engine:
         self._check(self._lib.rigw_g3w2_selfenergy_imag(self._h, wpol.handle, C.byref(gp), _ptr(out)),
                     "rigw_g3w2_selfenergy_imag")
         return out[..., 0] + 1j * out[..., 1]
+
+    def gw_density_matrix_imag(self, inst, m_full, nomega_sigma: int, precision: int = RIGW_FP64,
+                               spin_fact: float = 2.0):
+        """pt_density_matrix='GW_IMAGINARY' (src/m_dm_mbpt_driver.f90:117-122): W on
+        the imaginary grid of ``inst`` (rigw_polarizability_imag), then the
+        correction to the MO density matrix (rigw_gw_density_matrix_imag) for the
+        Sigma range of ``inst``.  ``m_full`` is the window tensor [nstate_G,
+        nstate_G, naux] over the states ncore_g+1 ..; mu is the centre of the
+        HOMO-LUMO gap (src/m_mbpt_density_matrix.f90:571).  Returns the
+        correction [nstate, nstate] (zero on the core rows and columns) and E_RPA."""
+        cg = getattr(inst, "ncore_g", 0)
+        mf = np.ascontiguousarray(m_full, dtype=np.float64)
+        ng = mf.shape[0]
+        e = np.asarray(inst.energy, dtype=np.float64)
+        occ = np.asarray(inst.occupation, dtype=np.float64)
+        nhomo = max([1] + [p + 1 for p in range(e.size) if not occ[p] < 1.0e-5])
+        mu = 0.5 * (e[nhomo] + e[nhomo - 1])
+        erpa, _, wpol = self.polarizability_grid_scalapack(inst, precision)
+        try:
+            ew = np.ascontiguousarray(e[cg:cg + ng])
+            dp = DmProblem()
+            dp.naux, dp.nstate = inst.naux, ng
+            dp.m_full, dp.energy = _ptr(mf), _ptr(ew)
+            dp.nsig = inst.nsemax - inst.nsemin + 1
+            dp.sig_first = inst.nsemin - 1 - cg
+            dp.mu, dp.nomega_sigma, dp.spin_fact = mu, nomega_sigma, spin_fact
+            pw = np.zeros((ng, ng))
+            self._check(self._lib.rigw_gw_density_matrix_imag(self._h, wpol.handle, C.byref(dp), _ptr(pw)),
+                        "rigw_gw_density_matrix_imag")
+        finally:
+            wpol.release()
+        out = np.zeros((e.size, e.size))
+        out[cg:cg + ng, cg:cg + ng] = pw
+        return out, erpa
 
     def gw_g3w2_imag(self, inst, m_full, precision: int = RIGW_FP64, efermi: float | None = None) -> G0W0Output:
         """GW+G3W2 on the imaginary axis (postscf 'GW+G3W2_PADE'): Sigma_c, SOX,

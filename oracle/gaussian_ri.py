@@ -185,7 +185,11 @@ class BasisFunctions:
     shells: list = field(default_factory=list)
 
 
-def build_functions(shells: list[Shell]) -> BasisFunctions:
+def build_functions(shells: list[Shell], pure: bool = True) -> BasisFunctions:
+    """Contracted functions of the shells: pure (real solid harmonics) or, with
+    ``pure`` False (gaussian_type='CART'), the Cartesian monomials themselves,
+    each normalized on its own (the (nx, ny, nz) part of the normalization,
+    src/m_cart_to_pure.f90:262-279)."""
     prims, blocks, shell_of = [], [], []
     ncart = 0
     for si, sh in enumerate(shells):
@@ -197,15 +201,15 @@ def build_functions(shells: list[Shell]) -> BasisFunctions:
             coef = np.array([ck * primitive_norm(a, (sh.am, 0, 0)) for a, ck in zip(sh.alpha, sh.coeff)])
             prims.append((sh.center, sh.alpha.copy(), coef, c))
             ncart += 1
-        blocks.append((start, solid_harmonic_coeffs(sh.am)))
-        shell_of += [si] * (2 * sh.am + 1)
+        blocks.append((start, solid_harmonic_coeffs(sh.am) if pure else np.eye(len(carts))))
+        shell_of += [si] * ((2 * sh.am + 1) if pure else len(carts))
     T = np.zeros((len(shell_of), ncart))
     r = 0
     for start, tb in blocks:
         T[r:r + tb.shape[0], start:start + tb.shape[1]] = tb
         r += tb.shape[0]
     bf = BasisFunctions(prims, T, shell_of, list(shells))
-    # every pure function normalized to one (the contraction then too)
+    # every function normalized to one (the contraction then too)
     s = bf.cart_to_pure @ (_c_one_body(bf, [])[0] if _c_available() else overlap_cart(bf)) @ bf.cart_to_pure.T
     bf.cart_to_pure = bf.cart_to_pure / np.sqrt(np.diag(s))[:, None]
     return bf
@@ -632,12 +636,14 @@ def nuclear_repulsion(nuclei) -> float:
     return e
 
 
-def molecule_ri_hf(atoms, basis: dict, auxil: dict | str | None = None, charge: int = 0, tol: float = 1e-12):
+def molecule_ri_hf(atoms, basis: dict, auxil: dict | str | None = None, charge: int = 0, tol: float = 1e-12,
+                   cart: bool = False):
     """RI-RHF of a molecule.  ``atoms`` = [(Z, (x, y, z) in Angstrom), ...]
     (the reference's default length_unit, src/input_variables.f90:502);
     ``basis`` / ``auxil`` map Z to the text of a basis file in the reference's
     format; ``auxil`` None (or "PAUTO") builds the PAuto auxiliary basis per
-    atom, "AUTO" the Auto one.  Shells
+    atom, "AUTO" the Auto one.  ``cart``: Cartesian functions for both bases
+    (gaussian_type='CART'), else pure ones.  Shells
     are listed atom by atom in input order, as the reference does
     (src/m_basis_set.f90:90-340).  Returns (SCFResult, M [nstate, nstate,
     nauxil] over the MOs, details)."""
@@ -650,8 +656,8 @@ def molecule_ri_hf(atoms, basis: dict, auxil: dict | str | None = None, charge: 
             aux_shells += parse_basis_file(auxil[z], center=tuple(c))
         else:
             aux_shells += pauto_auxiliary(sh, z, pauto=(auxil or "PAUTO").upper() == "PAUTO")
-    bf = build_functions(shells)
-    aux = build_functions(aux_shells)
+    bf = build_functions(shells, pure=not cart)
+    aux = build_functions(aux_shells, pure=not cart)
     S, T, V = one_body(bf, nuclei)
     v2 = coulomb_2center(aux)
     sqrtinv, eig = inverse_sqrt_metric(v2)
@@ -661,7 +667,7 @@ def molecule_ri_hf(atoms, basis: dict, auxil: dict | str | None = None, charge: 
     scf = rhf_ri(S, T + V, b3, nelec, e_nn=e_nn, tol=tol)
     scf.metric_eigenvalues = eig
     details = {"nbf": S.shape[0], "naux_basis": v2.shape[0], "nauxil": b3.shape[2], "e_nn": e_nn,
-               "bf": bf, "aux": aux, "S": S, "H": T + V}
+               "bf": bf, "aux": aux, "S": S, "H": T + V, "T": T, "V": V}
     return scf, mo_3center(scf), details
 
 
@@ -682,3 +688,28 @@ def rimp2_energy(energy: np.ndarray, m: np.ndarray, nocc: int, ncore: int = 0) -
     eo, ev = e[ncore:nocc], e[nocc:]
     d = eo[:, None, None, None] + eo[None, None, :, None] - ev[None, :, None, None] - ev[None, None, None, :]
     return float(np.sum(iajb * (2.0 * iajb - iajb.transpose(0, 3, 2, 1)) / d))
+
+
+def correlated_dm_energies(scf: SCFResult, details: dict, p_corr_mo: np.ndarray, spin_fact: float = 2.0) -> dict:
+    """Energies of the correlated density matrix (get_dm_mbpt,
+    src/m_dm_mbpt_driver.f90:228-249): P_AO = C (P_corr + diag(occupation)) C^T
+    (update_density_matrix, src/m_mbpt_density_matrix.f90:840-880), kinetic and
+    nuclear energies as traces, the RI Hartree energy 1/2 sum J P, and the RI
+    exchange energy 1/2 sum K P with K built from the eigenvectors of P_AO whose
+    eigenvalues are >= 1e-5 (get_c_matrix_from_p_matrix,
+    src/m_hamiltonian_tools.f90:1356-1412; setup_exchange_ri,
+    src/m_hamiltonian_twobodies.f90:707-784)."""
+    c = scf.c
+    p_mo = p_corr_mo + np.diag(scf.occupation)
+    p_ao = c @ p_mo @ c.T
+    b3 = scf.b3
+    jmat = np.einsum("ijP,P->ij", b3, np.einsum("klP,kl->P", b3, p_ao))
+    w, u = np.linalg.eigh(-p_ao)
+    w = -w
+    nocc = int(np.max(np.nonzero(w >= 1.0e-5)[0])) + 1 if np.any(w >= 1.0e-5) else 0
+    ct = u[:, :nocc] * np.sqrt(np.maximum(w[:nocc], 0.0) / spin_fact)
+    tmp = np.einsum("mnP,ni->imP", b3, ct, optimize=True)
+    kmat = -np.einsum("imP,inP->mn", tmp, tmp, optimize=True)
+    return {"kinetic": float(np.sum(details["T"] * p_ao)), "nucleus": float(np.sum(details["V"] * p_ao)),
+            "hartree": 0.5 * float(np.sum(jmat * p_ao)), "exchange": 0.5 * float(np.sum(kmat * p_ao)),
+            "trace_mo": float(np.trace(p_mo)), "p_ao": p_ao}

@@ -1060,3 +1060,44 @@ def g0w0_contour(energy: np.ndarray, occupation: np.ndarray, m_ia: np.ndarray, m
     ehomo, elumo = output_homolumo(occupation, full, rng.nsemin, rng.nsemax)
     return ContourResult(sigma, se_omega, omega_real, de_max, [v.size for _, v in w_imag],
                          [v.size for _, v in w_real], eqp_g, eqp_z, zz_g, ehomo, elumo, rng.nsemin, rng.nsemax)
+
+
+# ---------------------------------------------------------------------------
+# GW density matrix from the imaginary axis (pt_density_matrix GW_IMAGINARY)
+# ---------------------------------------------------------------------------
+def gw_density_matrix_imag(energy: np.ndarray, m_window: np.ndarray, sf: SpectralFunction, rng: StateRange,
+                           nomega_sigma: int, spin_fact: float = 2.0) -> np.ndarray:
+    """gw_density_matrix_imag (src/m_mbpt_density_matrix.f90:491-640), one spin.
+
+    ``m_window`` is M[p, q, P] over the states ncore_G+1 .. nvirtual_G-1 (the
+    rows and columns of eri_3center_mo); ``sf`` holds chi = v^1/2 chi v^1/2 on
+    the imaginary grid of W (wpol%chi, wpol%omega, wpol%weight_quad).  The
+    frequency integral of the density matrix runs on a second Gauss-Legendre
+    grid of nomega_sigma points mapped with alpha = beta = 1 (:555-567), around
+    mu, the centre of the HOMO-LUMO gap (:571).  Returns the correction to the
+    MO density matrix, [nstate, nstate], symmetric, zero outside the Sigma range."""
+    nstate = energy.size
+    x, ws = coeffs_gausslegint(0.0, 1.0, nomega_sigma)
+    ws = ws / (2.0 ** 1.0 - 1.0) * 1.0 * (1.0 - x) ** (-2.0) * 1.0
+    om_s = 1.0 / (2.0 ** 1.0 - 1.0) * (1.0 / (1.0 - x) - 1.0) * 1.0
+    mu = 0.5 * (energy[rng.nhomo_g] + energy[rng.nhomo_g - 1])
+    c0 = rng.ncore_g
+    mrange = rng.nvirtual_g - rng.ncore_g - 1
+    em = energy[c0:c0 + mrange] - mu
+    p = np.zeros((nstate, nstate))
+    zs = 1j * om_s
+    for q in range(rng.nsemin, rng.nsemax + 1):
+        eri3_q = m_window[:mrange, q - 1 - c0, :].T                       # [naux, mrange]
+        for iw in range(len(sf.omega)):
+            chi_eri3_q = sf.chi[iw] @ eri3_q                              # DGEMM('N','N')
+            yw = 1j * sf.omega[iw]
+            g = (1.0 / (zs[:, None] - em[None, :] + yw) + 1.0 / (zs[:, None] - em[None, :] - yw))   # [s, m]
+            for pp in range(q, rng.nsemax + 1):
+                eri3_p = m_window[:mrange, pp - 1 - c0, :].T
+                v = np.sum(eri3_p * chi_eri3_q, axis=0)                   # [m]
+                k = g / (zs[:, None] - (energy[pp - 1] - mu)) / (zs[:, None] - (energy[q - 1] - mu))
+                p[pp - 1, q - 1] -= spin_fact * 2.0 / (2.0 * PI) ** 2 * np.sum(
+                    sf.weight_quad[iw] * ws[:, None] * v[None, :] * k.real)
+    iu = np.triu_indices(nstate, 1)
+    p[iu] = p.T[iu]
+    return p

@@ -196,7 +196,7 @@ def test_sosex_problem_layout_matches_ctypes(tmp_path):
         assert int(out[f"X {f}"]) == getattr(SosexProblem, f).offset, f
 
 
-@pytest.mark.parametrize("cname,pyname", [("rigw_contour_problem", "ContourProblem"),
+@pytest.mark.parametrize("cname,pyname", [("rigw_contour_problem", "ContourProblem"), ("rigw_dm_problem", "DmProblem"),
                                           ("rigw_contour_result", "ContourResult")])
 def test_contour_layouts_match_ctypes(tmp_path, cname, pyname):
     from molgw_b200 import rigw
