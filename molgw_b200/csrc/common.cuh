@@ -11,7 +11,7 @@ namespace rigw {
 
 constexpr double kPi = 3.14159265358979323;   // src/m_definitions.f90:50
 constexpr int kPanel = 128;                    // Cholesky panel width (rows of one U block row)
-constexpr int kMaxChains = 4;                  // frequency chains of the factorization stage (tuner's range)
+constexpr int kMaxChains = 8;                  // frequency chains of the factorization stage (tuner's range)
 constexpr int kAutoChains = 2;                 // chains without a tuning
 constexpr int kChainPairs = 4;                 // (problem, frequency) pairs per chain at least
 constexpr int kSplitGroup = 8;                 // frequencies sharing one bf16 hi/lo split buffer

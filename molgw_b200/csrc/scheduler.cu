@@ -316,7 +316,7 @@ Status autotune(Context& c, int n, const rigw_problem* probs, rigw_tune_report* 
     RIGW_TRY(try_field(&Tuning::split_group, {g_l2, 8}, 1));
   }
   RIGW_TRY(try_field(&Tuning::update_rows, {64, 128}, 2));
-  RIGW_TRY(try_field(&Tuning::chains, {1, 2, 4}, 2));
+  RIGW_TRY(try_field(&Tuning::chains, {1, 2, 4, 8}, 2));
   RIGW_TRY(try_field(&Tuning::panel_group, {2, 8, 16}, 2));
   c.tuned[{int(kPlanFused), cls}] = best;
   c.plan_cache.clear();

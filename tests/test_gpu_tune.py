@@ -28,7 +28,7 @@ def test_autotune_keeps_results_and_reports_candidates(precision):
     eng.close()
     assert rep["chi0_rows"] in (64, 128) and rep["update_rows"] in (64, 128)
     # split classes also time an L2-resident frequency group and a group of 8
-    assert rep["chains"] in (0, 1, 2, 4)
+    assert rep["chains"] in (0, 1, 2, 4, 8)
     assert rep["split_group"] == 0 if precision == RIGW_FP64 else rep["split_group"] >= 0
     assert rep["precision_class"] == (0 if precision == RIGW_FP64 else (1 if precision == RIGW_BF16X3 else 2))
     assert len(rep["candidates"]) >= 3
