@@ -26,6 +26,11 @@
  *   rigw_sosex_selfenergy_imag  sosex_selfenergy_imag_grid    src/m_g3w2_selfenergy.f90:2200-2478
  *   rigw_g3w2_selfenergy_imag   g3w2_selfenergy_imag_grid     src/m_g3w2_selfenergy.f90:2018-2196
  *                               (GW+SOSEX_PADE: added after SOX, src/m_selfenergy_evaluation.f90:498-500)
+ *   rigw_eri_2center            calculate_eri_2center (LIBCINT int2c2e) src/m_eri_calculate.f90:1049-1262
+ *   rigw_eri_3center_raw        the 3-center shell loop of calculate_eri_3center_scalapack
+ *                               (LIBCINT int3c2e)              src/m_eri_calculate.f90:1584-1850
+ *   rigw_eri_3center            calculate_eri_3center_scalapack with the metric and the
+ *                               x0.5 diagonal convention       src/m_eri_calculate.f90:1584-1950
  *   rigw_gw_density_matrix_imag gw_density_matrix_imag        src/m_mbpt_density_matrix.f90:491-640
  *                               (pt_density_matrix GW_IMAGINARY, src/m_dm_mbpt_driver.f90:117-122)
  *   rigw_gw_selfenergy_contour  gw_selfenergy_contour         src/m_gw_selfenergy_grid.f90:342-551
@@ -291,6 +296,42 @@ typedef struct rigw_g3w2_problem {
 /* sigma_g3w2: [nsig][nomega_calc][2], overwritten. */
 RIGW_API int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g3w2_problem* prob,
                                        double* sigma_g3w2);
+
+/* ---- RI Coulomb integrals --------------------------------------------------------
+ * Gaussian shells of the orbital and auxiliary bases (angular momentum <= 4).  The
+ * coefficients are the reference's shell coefficients: the normalized contraction
+ * coefficient of each primitive times (2/pi)^{3/4} 2^l alpha^{(2l+3)/4}, i.e. the
+ * x^l component normalized up to the (nx, ny, nz) factor, which the library
+ * applies with the pure (real solid harmonics, m = -l..l) or Cartesian (x^l
+ * first, nx from l down and nz from 0 up) transform of each shell. */
+typedef struct rigw_shell {
+  double center[3];          /* Bohr                                                       */
+  int am;
+  int nprim;
+  const double* alpha;       /* [nprim] exponents                                          */
+  const double* coeff;       /* [nprim] shell coefficients as above                        */
+} rigw_shell;
+typedef struct rigw_ri_problem {
+  int nshell;                /* orbital basis (ignored by rigw_eri_2center)                */
+  const rigw_shell* shells;
+  int pure;                  /* 1: pure functions, 0: Cartesian                            */
+  int nshell_aux;            /* auxiliary basis                                            */
+  const rigw_shell* aux_shells;
+  int pure_aux;
+  int npair;                 /* basis-function pairs kept (screening is the caller's)      */
+  const int* index_basis;    /* [npair][2] 1-based (index_basis of src/m_eri.f90:252-320)  */
+  int flags;                 /* RIGW_PROBLEM_DEVICE_POINTERS: outputs in device memory     */
+} rigw_ri_problem;
+/* (P|Q): v2 [naux_basis][naux_basis]. */
+RIGW_API int rigw_eri_2center(rigw_ctx* ctx, const rigw_ri_problem* prob, double* v2);
+/* (mu nu|P) without the metric: eri3 [naux_basis][npair]. */
+RIGW_API int rigw_eri_3center_raw(rigw_ctx* ctx, const rigw_ri_problem* prob, double* eri3);
+/* eri_3center(pair, P) = sum_Q (mu nu|Q) (Q|P)^-1/2 with diagonal pairs halved, as the
+ * reference stores it: eri3 [nauxil_kept][npair] (room for naux_basis rows); (P|Q) is
+ * diagonalized on the device and eigenvalues <= 1e-6 dropped (*nauxil_kept returns the
+ * count).  The kept eigenpairs come in the eigensolver's order: the result equals the
+ * reference's up to an orthogonal transformation of the auxiliary index. */
+RIGW_API int rigw_eri_3center(rigw_ctx* ctx, const rigw_ri_problem* prob, double* eri3, int* nauxil_kept);
 
 /* ---- GW density matrix from the imaginary axis ----------------------------------
  * Correction to the MO density matrix of one spin channel (gw_density_matrix_imag),

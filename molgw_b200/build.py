@@ -11,7 +11,8 @@ CSRC = HERE / "csrc"
 LIB = HERE / "librigw.so"
 SOURCES = ["capi.cu", "engine.cu", "ops.cu", "gemm_f64.cu", "kernels_gw.cu", "kernels_aomo.cu",
            "syrk_bf16x3.cu", "syrk_ozaki.cu", "syrk_f64_tma.cu", "qp_noalloc.cu", "scheduler.cu", "serve.cu", "sox.cu",
-           "contour.cu", "eigh_jacobi.cu", "dm.cu"]
+           "contour.cu", "eigh_jacobi.cu", "dm.cu",
+           "ri_ints.cu"]
 NVCC_FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-lineinfo", "-O3", "-std=c++17",
               "-Xcompiler", "-fPIC", "-Xcompiler", "-fvisibility=hidden", "--expt-relaxed-constexpr"]
 

@@ -226,6 +226,30 @@ int rigw_g3w2_selfenergy_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_g
   return finish(ctx, rigw::g3w2_selfenergy_imag(ctx->impl, wpol->impl, *prob, sigma_g3w2));
 }
 
+int rigw_eri_2center(rigw_ctx* ctx, const rigw_ri_problem* prob, double* v2) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!prob || !v2) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::ri_integrals(ctx->impl, *prob, 2, v2, nullptr));
+}
+
+int rigw_eri_3center_raw(rigw_ctx* ctx, const rigw_ri_problem* prob, double* eri3) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!prob || !eri3) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::ri_integrals(ctx->impl, *prob, 3, eri3, nullptr));
+}
+
+int rigw_eri_3center(rigw_ctx* ctx, const rigw_ri_problem* prob, double* eri3, int* nauxil_kept) {
+  if (!ctx) return RIGW_ERR_ARG;
+  if (!prob || !eri3 || !nauxil_kept) return finish(ctx, Status::fail(RIGW_ERR_ARG, "null argument"));
+  std::lock_guard<std::mutex> lock(ctx->impl.mu);
+  cudaSetDevice(ctx->impl.device);
+  return finish(ctx, rigw::ri_integrals(ctx->impl, *prob, 0, eri3, nauxil_kept));
+}
+
 int rigw_gw_density_matrix_imag(rigw_ctx* ctx, const rigw_wpol* wpol, const rigw_dm_problem* prob,
                                 double* p_matrix) {
   if (!ctx) return RIGW_ERR_ARG;

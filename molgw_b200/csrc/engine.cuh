@@ -277,6 +277,8 @@ Status sosex_selfenergy_imag(Context& c, const Wpol& w, const rigw_sosex_problem
 Status g3w2_selfenergy_imag(Context& c, const Wpol& w, const rigw_g3w2_problem& pr, double* sigma);
 Status gw_selfenergy_contour(Context& c, const rigw_contour_problem& pr, rigw_contour_result& res);
 Status gw_density_matrix_imag(Context& c, const Wpol& w, const rigw_dm_problem& pr, double* p_matrix);
+// RI integrals (ri_ints.cu): what = 2 (P|Q), 3 (mu nu|P) raw, 0 eri_3center with the metric.
+Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out, int* nkept);
 // Eigenpairs of nw symmetric n x n matrices (n a multiple of 64, row-major, A[w] at A + w n^2):
 // on return the diagonal of A[w] holds the eigenvalues and V[w][i][k] is component i of
 // eigenvector k (eigh_jacobi.cu).  Adds its kernel launches to *launches.

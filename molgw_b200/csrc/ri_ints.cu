@@ -1,0 +1,606 @@
+// RI Coulomb integrals on the device: (P|Q) over the auxiliary basis and (mu nu|P)
+// over the orbital-basis pairs, then B(mu nu, P) = sum_Q (mu nu|Q) (Q|P)^-1/2 in the
+// pair-packed layout the AO->MO transform reads (calculate_eri_2center /
+// calculate_eri_3center_scalapack, src/m_eri_calculate.f90:1049-1262, 1584-1950).
+//
+// The integrals follow the McMurchie-Davidson scheme (Helgaker, Jorgensen, Olsen,
+// "Molecular Electronic-Structure Theory", ch. 9): Hermite expansion coefficients
+// E^{ij}_t of the Gaussian products and Hermite Coulomb integrals R_tuv from the
+// Boys function.  One CTA per (orbital shell pair, auxiliary shell) or (auxiliary
+// shell pair): for every primitive pair/triple the E tables and the R table
+// (level-by-level recursion in shared memory, two cubes) are built once and every
+// Cartesian component of the block reads them; the Cartesian block is then
+// transformed to pure functions (real solid harmonics) or normalized per
+// component (CART) in shared memory and stored.
+//
+// The metric: (P|Q) is diagonalized by the device eigensolver (eigh_jacobi.cu),
+// eigenvalues <= 1e-6 are dropped (TOO_LOW_EIGENVAL, src/m_eri.f90:27) and
+// (P|Q)^-1/2 = V[:, kept] / sqrt(lambda[kept]).  The kept eigenpairs are taken in
+// the eigensolver's order; B is defined up to that orthogonal transformation of
+// the auxiliary index, like the reference's (every product M M^T downstream is
+// invariant to it).
+#include <cmath>
+#include <vector>
+
+#include "engine.cuh"
+
+namespace rigw {
+namespace {
+
+constexpr int kRiLmax = 4;                                   // highest angular momentum of a shell
+constexpr int kRiNc = (kRiLmax + 1) * (kRiLmax + 2) / 2;     // Cartesian components (15)
+constexpr int kRiL3 = 3 * kRiLmax;                           // highest Hermite order (12)
+constexpr int kRiNR = kRiL3 + 1;
+constexpr int kRiThreads = 128;
+constexpr double kRiTooLowEigval = 1.0e-6;
+
+struct DevShell {
+  double x, y, z;
+  int l, nprim, p0, f0;   // angular momentum, primitives, first primitive, first function
+};
+
+struct RiArgs {
+  const DevShell* sh;     // orbital shells
+  const DevShell* ax;     // auxiliary shells
+  const double* alpha;    // primitives of both bases
+  const double* coeff;
+  const double* trans;    // per l and basis: [nfun][ncart] transforms, at toff[l] (orbital), toff[5 + l] (aux)
+  const int* toff;
+  const int* shellpair;   // [nsp][2] orbital shell pairs (A >= B)
+  const int* pairmap;     // [nbf][nbf] pair index or -1
+  double* out;            // 3-center: [naux][npair]; 2-center: [naux][naux]
+  int nbf, naux, npair;
+  int pure_orb, pure_aux;
+};
+
+RIGW_DEVICE_INLINE int ncart(int l) { return (l + 1) * (l + 2) / 2; }
+RIGW_DEVICE_INLINE int nfun(int l, int pure) { return pure ? 2 * l + 1 : ncart(l); }
+
+// Cartesian component c of shell l: nx from l down, nz from 0 up (the reference's order).
+RIGW_DEVICE_INLINE void cart_comp(int l, int c, int& nx, int& ny, int& nz) {
+  int k = 0;
+  for (int x = l; x >= 0; --x)
+    for (int z = 0; z <= l - x; ++z) {
+      if (k == c) {
+        nx = x;
+        ny = l - x - z;
+        nz = z;
+        return;
+      }
+      ++k;
+    }
+  nx = ny = nz = 0;
+}
+
+// Boys function F_m(T), m = 0..mmax: series for the highest order and downward
+// recursion; for large T the asymptotic F_0 and upward recursion.
+__device__ void boys(int mmax, double T, double* F) {
+  if (T < 1.0e-14) {
+    for (int m = 0; m <= mmax; ++m) F[m] = 1.0 / (2 * m + 1) - T / (2 * m + 3);
+    return;
+  }
+  const double e = exp(-T);
+  if (T > 50.0 && T > 2.0 * mmax) {
+    F[0] = 0.5 * sqrt(3.14159265358979323846 / T);
+    for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
+    return;
+  }
+  double term = 1.0 / (2 * mmax + 1), sum = term;
+  for (int k = 1; k < 4000; ++k) {
+    term *= 2.0 * T / (2 * mmax + 2 * k + 1);
+    sum += term;
+    if (term < 1.0e-17 * sum) break;
+  }
+  F[mmax] = e * sum;
+  for (int m = mmax; m > 0; --m) F[m - 1] = (2.0 * T * F[m] + e) / (2 * m - 1);
+}
+
+// E^{ij}_t along one axis for i <= imax, j <= jmax (Q = A - B), into E[(i * (kRiLmax+1) + j) * (2*kRiLmax+1) + t].
+constexpr int kEi = kRiLmax + 1, kEt = 2 * kRiLmax + 1;
+__device__ void hermite_e(int imax, int jmax, double a, double b, double qx, double* E) {
+  const double p = a + b, mu = a * b / p;
+  const double xpa = -b / p * qx, xpb = a / p * qx, h = 0.5 / p;
+  E[0] = exp(-mu * qx * qx);
+  for (int i = 0; i <= imax; ++i)
+    for (int j = 0; j <= jmax; ++j) {
+      if (i == 0 && j == 0) continue;
+      const int tp = i + j - 1;
+      for (int t = 0; t <= i + j; ++t) {
+        double v;
+        if (i > 0) {
+          const double* Ep = E + ((i - 1) * kEi + j) * kEt;
+          v = (t <= tp ? xpa * Ep[t] : 0.0) + (t + 1 <= tp ? (t + 1) * Ep[t + 1] : 0.0);
+          if (t > 0) v += h * Ep[t - 1];
+        } else {
+          const double* Ep = E + (i * kEi + j - 1) * kEt;
+          v = (t <= tp ? xpb * Ep[t] : 0.0) + (t + 1 <= tp ? (t + 1) * Ep[t + 1] : 0.0);
+          if (t > 0) v += h * Ep[t - 1];
+        }
+        E[(i * kEi + j) * kEt + t] = v;
+      }
+    }
+}
+
+RIGW_DEVICE_INLINE int ridx(int t, int u, int v) { return (t * kRiNR + u) * kRiNR + v; }
+
+// R_tuv of order 0 for t + u + v <= L into R0 (cube of kRiNR^3), the whole CTA
+// working level by level with two cubes; F holds F_0..F_L.
+__device__ void hermite_r(int L, double p, double X, double Y, double Z, const double* F, double* R0, double* R1) {
+  // level n = L: only R^{(L)}_000
+  double* cur = (L & 1) ? R1 : R0;   // ends in R0 at n = 0
+  if (threadIdx.x == 0) cur[0] = pow(-2.0 * p, L) * F[L];
+  __syncthreads();
+  for (int n = L - 1; n >= 0; --n) {
+    double* nxt = (cur == R0) ? R1 : R0;
+    const int lim = L - n;
+    const double fac = pow(-2.0 * p, n) * F[n];
+    for (int idx = threadIdx.x; idx < kRiNR * kRiNR * kRiNR; idx += blockDim.x) {
+      const int t = idx / (kRiNR * kRiNR), u = (idx / kRiNR) % kRiNR, v = idx % kRiNR;
+      if (t + u + v > lim) continue;
+      double val;
+      if (t + u + v == 0) {
+        val = fac;
+      } else if (t > 0) {
+        val = X * cur[ridx(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[ridx(t - 2, u, v)] : 0.0);
+      } else if (u > 0) {
+        val = Y * cur[ridx(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[ridx(t, u - 2, v)] : 0.0);
+      } else {
+        val = Z * cur[ridx(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[ridx(t, u, v - 2)] : 0.0);
+      }
+      nxt[idx] = val;
+    }
+    __syncthreads();
+    cur = nxt;
+  }
+}
+
+// Shared memory of the integral kernels (doubles).
+constexpr int kSmemR = 2 * kRiNR * kRiNR * kRiNR;           // two R cubes
+constexpr int kSmemE = 3 * kEi * kEi * kEt;                 // E tables of the bra pair
+constexpr int kSmemF = 3 * kEi * kEi * kEt;                 // E tables of the ket (single function: j = 0)
+constexpr int kSmemAcc = kRiNc * kRiNc * kRiNc;             // Cartesian block
+constexpr int kSmemBoys = kRiNR + 1;
+constexpr size_t kRiSmemBytes = size_t(kSmemR + kSmemE + kSmemF + 2 * kSmemAcc + kSmemBoys) * sizeof(double);
+
+// Cartesian block of one shell triple (bra A, B; ket Q, a single function) or,
+// with B == nullptr, one auxiliary pair (bra P as a single function, ket Q).
+__device__ void shell_block(const DevShell& A, const DevShell* B, const DevShell& Q, const double* alpha,
+                            const double* coeff, double* smem, int na, int nb, int nq) {
+  double* R0 = smem;
+  double* R1 = R0 + kRiNR * kRiNR * kRiNR;
+  double* E = R1 + kRiNR * kRiNR * kRiNR;
+  double* Fk = E + kSmemE;
+  double* acc = Fk + kSmemF;
+  double* F = acc + 2 * kSmemAcc;
+  const int tid = threadIdx.x;
+  const int lb = B ? B->l : 0;
+  const int nblk = na * nb * nq;
+  for (int i = tid; i < nblk; i += blockDim.x) acc[i] = 0.0;
+  const int L = A.l + lb + Q.l;
+  const int pbn = B ? B->nprim : 1;
+  for (int pa = 0; pa < A.nprim; ++pa)
+    for (int pb = 0; pb < pbn; ++pb) {
+      const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0;
+      const double cab = coeff[A.p0 + pa] * (B ? coeff[B->p0 + pb] : 1.0);
+      const double XB[3] = {B ? B->x : A.x, B ? B->y : A.y, B ? B->z : A.z};
+      const double XA[3] = {A.x, A.y, A.z};
+      const double p = a + b;
+      const double P[3] = {(a * XA[0] + b * XB[0]) / p, (a * XA[1] + b * XB[1]) / p, (a * XA[2] + b * XB[2]) / p};
+      __syncthreads();   // the previous pair's E tables are no longer read
+      if (tid < 3) hermite_e(A.l, lb, a, b, XA[tid] - XB[tid], E + tid * kEi * kEi * kEt);
+      for (int pq = 0; pq < Q.nprim; ++pq) {
+        const double q = alpha[Q.p0 + pq];
+        const double pref = cab * coeff[Q.p0 + pq] * 2.0 * pow(3.14159265358979323846, 2.5) / (p * q * sqrt(p + q));
+        const double al = p * q / (p + q);
+        const double X = P[0] - Q.x, Y = P[1] - Q.y, Z = P[2] - Q.z;
+        __syncthreads();   // the previous triple's R and ket tables are no longer read
+        if (tid >= 32 && tid < 35) hermite_e(Q.l, 0, q, 0.0, 0.0, Fk + (tid - 32) * kEi * kEi * kEt);
+        if (tid == 64) boys(L, al * (X * X + Y * Y + Z * Z), F);
+        __syncthreads();
+        hermite_r(L, al, X, Y, Z, F, R0, R1);   // ends with a barrier, result in R0
+        for (int o = tid; o < nblk; o += blockDim.x) {
+          const int i = o / (nb * nq), j = (o / nq) % nb, k = o % nq;
+          int ix, iy, iz, jx = 0, jy = 0, jz = 0, kx, ky, kz;
+          cart_comp(A.l, i, ix, iy, iz);
+          if (B) cart_comp(lb, j, jx, jy, jz);
+          cart_comp(Q.l, k, kx, ky, kz);
+          const double* Ex = E + (ix * kEi + jx) * kEt;
+          const double* Ey = E + kEi * kEi * kEt + (iy * kEi + jy) * kEt;
+          const double* Ez = E + 2 * kEi * kEi * kEt + (iz * kEi + jz) * kEt;
+          const double* Fx = Fk + (kx * kEi) * kEt;
+          const double* Fy = Fk + kEi * kEi * kEt + (ky * kEi) * kEt;
+          const double* Fz = Fk + 2 * kEi * kEi * kEt + (kz * kEi) * kEt;
+          double tot = 0.0;
+          for (int t = 0; t <= ix + jx; ++t)
+            for (int u = 0; u <= iy + jy; ++u)
+              for (int v = 0; v <= iz + jz; ++v) {
+                const double e1 = Ex[t] * Ey[u] * Ez[v];
+                if (e1 == 0.0) continue;
+                double s = 0.0;
+                for (int t2 = 0; t2 <= kx; ++t2)
+                  for (int u2 = 0; u2 <= ky; ++u2)
+                    for (int v2 = 0; v2 <= kz; ++v2) {
+                      const double e2 = Fx[t2] * Fy[u2] * Fz[v2];
+                      s += (((t2 + u2 + v2) & 1) ? -e2 : e2) * R0[ridx(t + t2, u + u2, v + v2)];
+                    }
+                tot += e1 * s;
+              }
+          acc[o] += pref * tot;
+        }
+      }
+    }
+  __syncthreads();
+}
+
+// Transform of the Cartesian block acc[na][nb][nq] to functions: out[fa][fb][fq]
+// = sum Ta[fa][i] Tb[fb][j] Tq[fq][k] acc[i][j][k] (three passes through tmp).
+__device__ void transform_block(const double* Ta, int fa, int na, const double* Tb, int fb, int nb, const double* Tq,
+                                int fq, int nq, double* acc, double* tmp) {
+  const int tid = threadIdx.x;
+  // k: tmp[i][j][q] = sum_k Tq[q][k] acc[i][j][k]
+  for (int o = tid; o < na * nb * fq; o += blockDim.x) {
+    const int i = o / (nb * fq), j = (o / fq) % nb, q = o % fq;
+    double s = 0.0;
+    for (int k = 0; k < nq; ++k) s += Tq[q * nq + k] * acc[(i * nb + j) * nq + k];
+    tmp[o] = s;
+  }
+  __syncthreads();
+  // j: acc[i][b][q] = sum_j Tb[b][j] tmp[i][j][q]
+  for (int o = tid; o < na * fb * fq; o += blockDim.x) {
+    const int i = o / (fb * fq), bb = (o / fq) % fb, q = o % fq;
+    double s = 0.0;
+    for (int j = 0; j < nb; ++j) s += Tb[bb * nb + j] * tmp[(i * nb + j) * fq + q];
+    acc[o] = s;
+  }
+  __syncthreads();
+  // i: tmp[a][b][q] = sum_i Ta[a][i] acc[i][b][q]
+  for (int o = tid; o < fa * fb * fq; o += blockDim.x) {
+    const int aa = o / (fb * fq), bb = (o / fq) % fb, q = o % fq;
+    double s = 0.0;
+    for (int i = 0; i < na; ++i) s += Ta[aa * na + i] * acc[(i * fb + bb) * fq + q];
+    tmp[o] = s;
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(kRiThreads) ri_3center_kernel(RiArgs a) {
+  extern __shared__ double smem[];
+  const int sp = blockIdx.x, qs = blockIdx.y;
+  const DevShell A = a.sh[a.shellpair[2 * sp]], B = a.sh[a.shellpair[2 * sp + 1]], Q = a.ax[qs];
+  const int na = ncart(A.l), nb = ncart(B.l), nq = ncart(Q.l);
+  shell_block(A, &B, Q, a.alpha, a.coeff, smem, na, nb, nq);
+  double* acc = smem + kSmemR + kSmemE + kSmemF;
+  double* tmp = acc + kSmemAcc;
+  const int fa = nfun(A.l, a.pure_orb), fb = nfun(B.l, a.pure_orb), fq = nfun(Q.l, a.pure_aux);
+  transform_block(a.trans + a.toff[A.l], fa, na, a.trans + a.toff[B.l], fb, nb, a.trans + a.toff[5 + Q.l], fq, nq,
+                  acc, tmp);
+  for (int o = threadIdx.x; o < fa * fb * fq; o += blockDim.x) {
+    const int i = o / (fb * fq), j = (o / fq) % fb, k = o % fq;
+    const int mu = A.f0 + i, nu = B.f0 + j;
+    if (mu < nu) continue;   // A == B: (mu nu|P) = (nu mu|P), stored once
+    const int pr = a.pairmap[mu * a.nbf + nu];
+    if (pr >= 0) a.out[(size_t)(Q.f0 + k) * a.npair + pr] = tmp[o];
+  }
+}
+
+__global__ void __launch_bounds__(kRiThreads) ri_2center_kernel(RiArgs a) {
+  extern __shared__ double smem[];
+  const int ps = blockIdx.x, qs = blockIdx.y;
+  if (qs > ps) return;
+  const DevShell P = a.ax[ps], Q = a.ax[qs];
+  const int np = ncart(P.l), nq = ncart(Q.l);
+  shell_block(P, nullptr, Q, a.alpha, a.coeff, smem, np, 1, nq);
+  double* acc = smem + kSmemR + kSmemE + kSmemF;
+  double* tmp = acc + kSmemAcc;
+  const double one = 1.0;
+  const int fp = nfun(P.l, a.pure_aux), fq = nfun(Q.l, a.pure_aux);
+  transform_block(a.trans + a.toff[5 + P.l], fp, np, &one, 1, 1, a.trans + a.toff[5 + Q.l], fq, nq, acc, tmp);
+  for (int o = threadIdx.x; o < fp * fq; o += blockDim.x) {
+    const int i = o / fq, k = o % fq;
+    a.out[(size_t)(P.f0 + i) * a.naux + Q.f0 + k] = tmp[o];
+    a.out[(size_t)(Q.f0 + k) * a.naux + P.f0 + i] = tmp[o];
+  }
+}
+
+// sqrtinv[P][c] = V[P][k_c] / sqrt(lambda_{k_c}) for the kept eigenpairs, in order;
+// A holds the eigenvalues on its diagonal (n x n, padded).
+__global__ void ri_sqrtinv_kernel(const double* __restrict__ A, const double* __restrict__ V, int n, int naux,
+                                  const int* __restrict__ kept, int nkept, double* __restrict__ out, int ldo) {
+  const int c = blockIdx.x;
+  const int k = kept[c];
+  const double s = 1.0 / sqrt(A[(size_t)k * n + k]);
+  for (int p = threadIdx.x; p < naux; p += blockDim.x) out[(size_t)p * ldo + c] = V[(size_t)p * n + k] * s;
+}
+
+// Halve the diagonal pairs (the reference's convention, src/m_eri_calculate.f90:1841,1854).
+__global__ void ri_halve_diag_kernel(double* __restrict__ raw, int naux, int npair, const int* __restrict__ diag,
+                                     int ndiag) {
+  const int p = blockIdx.y;
+  for (int d = blockIdx.x * blockDim.x + threadIdx.x; d < ndiag; d += gridDim.x * blockDim.x)
+    raw[(size_t)p * npair + diag[d]] *= 0.5;
+}
+
+// ---- host: solid harmonics and the basis upload
+double dfact(int n) {
+  double r = 1.0;
+  for (int k = n; k > 1; k -= 2) r *= k;
+  return r;
+}
+double binom(int n, int k) {
+  if (k < 0 || k > n) return 0.0;
+  double r = 1.0;
+  for (int i = 1; i <= k; ++i) r = r * (n - k + i) / i;
+  return r;
+}
+double fact(int n) {
+  double r = 1.0;
+  for (int k = 2; k <= n; ++k) r *= k;
+  return r;
+}
+
+// Transform of shell l acting on monomials of the common normalization
+// (2/pi)^{3/4} 2^l alpha^{(2l+3)/4} (the reference's shell coefficients): pure:
+// real solid harmonics m = -l..l (Helgaker et al. eq. 6.4.73) over sqrt((2l-1)!!);
+// Cartesian: 1 / sqrt((2nx-1)!! (2ny-1)!! (2nz-1)!!) (src/m_cart_to_pure.f90:262-279).
+std::vector<double> shell_transform(int l, bool pure) {
+  const int nc = (l + 1) * (l + 2) / 2;
+  std::vector<int> cx, cy, cz;
+  for (int x = l; x >= 0; --x)
+    for (int z = 0; z <= l - x; ++z) {
+      cx.push_back(x);
+      cy.push_back(l - x - z);
+      cz.push_back(z);
+    }
+  auto index = [&](int x, int y, int z) {
+    for (int k = 0; k < nc; ++k)
+      if (cx[k] == x && cy[k] == y && cz[k] == z) return k;
+    return -1;
+  };
+  if (!pure) {
+    std::vector<double> t(size_t(nc) * nc, 0.0);
+    for (int k = 0; k < nc; ++k) t[size_t(k) * nc + k] = 1.0 / std::sqrt(dfact(2 * cx[k] - 1) * dfact(2 * cy[k] - 1) *
+                                                                        dfact(2 * cz[k] - 1));
+    return t;
+  }
+  const int nf = 2 * l + 1;
+  std::vector<double> t(size_t(nf) * nc, 0.0);
+  for (int row = 0; row < nf; ++row) {
+    const int m = row - l, am = std::abs(m);
+    const double vm = m >= 0 ? 0.0 : 0.5;
+    const double nlm = 1.0 / (std::pow(2.0, am) * fact(l)) *
+                       std::sqrt(2.0 * fact(l + am) * fact(l - am) / (m == 0 ? 2.0 : 1.0));
+    for (int tt = 0; tt <= (l - am) / 2; ++tt)
+      for (int u = 0; u <= tt; ++u) {
+        const double vtop = std::floor(am / 2.0 - vm) + vm;
+        for (double v = vm; v <= vtop + 1e-9; v += 1.0) {
+          const int iv2 = int(std::lround(2 * v));
+          const double sgn = (int(std::lround(tt + v - vm)) % 2 == 0) ? 1.0 : -1.0;
+          const double c = sgn * std::pow(0.25, tt) * binom(l, tt) * binom(l - tt, am + tt) * binom(tt, u) * binom(am, iv2);
+          const int ex = int(std::lround(2 * tt + am - 2 * (u + v))), ey = int(std::lround(2 * (u + v))),
+                    ez = l - 2 * tt - am;
+          const int k = index(ex, ey, ez);
+          if (k >= 0) t[size_t(row) * nc + k] += nlm * c / std::sqrt(dfact(2 * l - 1));
+        }
+      }
+  }
+  return t;
+}
+
+struct RiBasis {
+  std::vector<DevShell> sh, ax;
+  std::vector<double> alpha, coeff, trans;
+  std::vector<int> toff, shellpair, pairmap, diag;
+  int nbf = 0, naux = 0;
+};
+
+Status build_basis(const rigw_ri_problem& pr, RiBasis& b) {
+  auto add = [&](const rigw_shell* src, int n, std::vector<DevShell>& dst, bool pure, int& nf) -> Status {
+    for (int i = 0; i < n; ++i) {
+      const rigw_shell& s = src[i];
+      if (s.am < 0 || s.am > kRiLmax || s.nprim <= 0 || !s.alpha || !s.coeff)
+        return Status::fail(RIGW_ERR_ARG, "ri integrals: shell %d: angular momentum beyond %d or no primitives", i,
+                            kRiLmax);
+      DevShell d{};
+      d.x = s.center[0];
+      d.y = s.center[1];
+      d.z = s.center[2];
+      d.l = s.am;
+      d.nprim = s.nprim;
+      d.p0 = int(b.alpha.size());
+      d.f0 = nf;
+      for (int k = 0; k < s.nprim; ++k) {
+        b.alpha.push_back(s.alpha[k]);
+        b.coeff.push_back(s.coeff[k]);
+      }
+      nf += pure ? 2 * s.am + 1 : (s.am + 1) * (s.am + 2) / 2;
+      dst.push_back(d);
+    }
+    return Status::ok();
+  };
+  RIGW_TRY(add(pr.shells, pr.nshell, b.sh, pr.pure != 0, b.nbf));
+  RIGW_TRY(add(pr.aux_shells, pr.nshell_aux, b.ax, pr.pure_aux != 0, b.naux));
+  b.toff.assign(10, 0);
+  for (int basis = 0; basis < 2; ++basis)
+    for (int l = 0; l <= kRiLmax; ++l) {
+      b.toff[basis * 5 + l] = int(b.trans.size());
+      const std::vector<double> t = shell_transform(l, basis == 0 ? pr.pure != 0 : pr.pure_aux != 0);
+      b.trans.insert(b.trans.end(), t.begin(), t.end());
+    }
+  for (int A = 0; A < int(b.sh.size()); ++A)
+    for (int B = 0; B <= A; ++B) {
+      b.shellpair.push_back(A);
+      b.shellpair.push_back(B);
+    }
+  if (pr.npair > 0) {
+    b.pairmap.assign(size_t(b.nbf) * b.nbf, -1);
+    for (int k = 0; k < pr.npair; ++k) {
+      const int i = pr.index_basis[2 * k] - 1, j = pr.index_basis[2 * k + 1] - 1;
+      if (i < 0 || j < 0 || i >= b.nbf || j >= b.nbf)
+        return Status::fail(RIGW_ERR_ARG, "ri integrals: pair %d outside the basis", k);
+      b.pairmap[size_t(i) * b.nbf + j] = k;
+      b.pairmap[size_t(j) * b.nbf + i] = k;
+      if (i == j) b.diag.push_back(k);
+    }
+  }
+  return Status::ok();
+}
+
+template <class T>
+Status upload(Context& c, DeviceBuffer& buf, const std::vector<T>& v, const char* name, cudaStream_t s) {
+  RIGW_TRY(buf.allocate(&c, std::max<size_t>(v.size(), 1) * sizeof(T), name));
+  if (!v.empty()) RIGW_CUDA_TRY(cudaMemcpyAsync(buf.data(), v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
+  return Status::ok();
+}
+
+}  // namespace
+
+Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out, int* nkept_out) {
+  if (pr.nshell_aux <= 0 || !pr.aux_shells || (what != 2 && (pr.nshell <= 0 || !pr.shells || pr.npair <= 0 ||
+                                                             !pr.index_basis)) || !out)
+    return Status::fail(RIGW_ERR_ARG, "ri integrals: invalid arguments");
+  NvtxRange range(what == 2 ? "2-center integrals" : "3-center integrals");
+  RiBasis b;
+  RIGW_TRY(build_basis(pr, b));
+  cudaStream_t s = c.stream;
+  const bool on_dev = (pr.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
+  DeviceBuffer b_sh, b_ax, b_al, b_co, b_tr, b_to, b_sp, b_pm, b_out, b_v2, b_vec, b_kept, b_diag, b_items;
+  RIGW_TRY(upload(c, b_sh, b.sh, "ri shells", s));
+  RIGW_TRY(upload(c, b_ax, b.ax, "ri auxiliary shells", s));
+  RIGW_TRY(upload(c, b_al, b.alpha, "ri exponents", s));
+  RIGW_TRY(upload(c, b_co, b.coeff, "ri coefficients", s));
+  RIGW_TRY(upload(c, b_tr, b.trans, "ri transforms", s));
+  RIGW_TRY(upload(c, b_to, b.toff, "ri transform offsets", s));
+  RiArgs a{};
+  a.sh = reinterpret_cast<const DevShell*>(b_sh.data());
+  a.ax = reinterpret_cast<const DevShell*>(b_ax.data());
+  a.alpha = reinterpret_cast<const double*>(b_al.data());
+  a.coeff = reinterpret_cast<const double*>(b_co.data());
+  a.trans = reinterpret_cast<const double*>(b_tr.data());
+  a.toff = reinterpret_cast<const int*>(b_to.data());
+  a.nbf = b.nbf;
+  a.naux = b.naux;
+  a.npair = pr.npair;
+  a.pure_orb = pr.pure != 0;
+  a.pure_aux = pr.pure_aux != 0;
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(kRiSmemBytes)));
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_2center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     int(kRiSmemBytes)));
+  const int nax = int(b.ax.size());
+  if (what == 2 || what == 0) {
+    // (P|Q); for the metric, into a matrix padded to a multiple of 64 for the eigensolver
+    const int n = what == 2 ? b.naux : int((b.naux + 63) / 64 * 64);
+    double* v2 = nullptr;
+    if (what == 2 && on_dev) {
+      v2 = out;
+    } else {
+      RIGW_TRY(b_v2.allocate(&c, size_t(n) * n * 8, "ri (P|Q)"));
+      v2 = reinterpret_cast<double*>(b_v2.data());
+    }
+    RIGW_CUDA_TRY(cudaMemsetAsync(v2, 0, size_t(n) * n * 8, s));
+    RiArgs a2 = a;
+    a2.out = v2;
+    a2.naux = n;   // row stride
+    ri_2center_kernel<<<dim3(nax, nax), kRiThreads, kRiSmemBytes, s>>>(a2);
+    RIGW_CUDA_TRY(cudaGetLastError());
+    if (what == 2) {
+      if (!on_dev) RIGW_CUDA_TRY(cudaMemcpyAsync(out, v2, size_t(n) * n * 8, cudaMemcpyDeviceToHost, s));
+      RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+      return Status::ok();
+    }
+  }
+  // (mu nu|P) over the pairs: [naux][npair]
+  const int nsp = int(b.shellpair.size() / 2);
+  RIGW_TRY(upload(c, b_sp, b.shellpair, "ri shell pairs", s));
+  RIGW_TRY(upload(c, b_pm, b.pairmap, "ri pair map", s));
+  a.shellpair = reinterpret_cast<const int*>(b_sp.data());
+  a.pairmap = reinterpret_cast<const int*>(b_pm.data());
+  double* raw = nullptr;
+  if (what == 3 && on_dev) {
+    raw = out;
+  } else {
+    RIGW_TRY(b_out.allocate(&c, size_t(b.naux) * pr.npair * 8, "ri (mu nu|P)"));
+    raw = reinterpret_cast<double*>(b_out.data());
+  }
+  a.out = raw;
+  ri_3center_kernel<<<dim3(nsp, nax), kRiThreads, kRiSmemBytes, s>>>(a);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  if (what == 3) {
+    if (!on_dev)
+      RIGW_CUDA_TRY(cudaMemcpyAsync(out, raw, size_t(b.naux) * pr.npair * 8, cudaMemcpyDeviceToHost, s));
+    RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+    return Status::ok();
+  }
+  // the metric: eigenpairs of (P|Q), kept where lambda > 1e-6
+  const int n = int((b.naux + 63) / 64 * 64);
+  double* v2 = reinterpret_cast<double*>(b_v2.data());
+  RIGW_TRY(b_vec.allocate(&c, size_t(n) * n * 8, "ri metric eigenvectors"));
+  double* vec = reinterpret_cast<double*>(b_vec.data());
+  int sweeps = 0, launches = 0;
+  RIGW_TRY(eigh_jacobi_batched(c, v2, vec, n, 1, s, &sweeps, &launches));
+  std::vector<double> diag(size_t(n) * n);
+  RIGW_CUDA_TRY(cudaMemcpyAsync(diag.data(), v2, size_t(n) * n * 8, cudaMemcpyDeviceToHost, s));
+  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  // the padding rows and columns are zero: their eigenvalues are 0 and never kept
+  std::vector<int> kept;
+  for (int k = 0; k < n; ++k)
+    if (diag[size_t(k) * n + k] > kRiTooLowEigval) kept.push_back(k);
+  const int nkept = int(kept.size());
+  RIGW_TRY(upload(c, b_kept, kept, "ri kept eigenpairs", s));
+  // sqrtinv [naux][nkept padded to even]
+  const int ldk = nkept + (nkept & 1);
+  DeviceBuffer b_si;
+  RIGW_TRY(b_si.allocate(&c, size_t(b.naux) * ldk * 8, "ri (P|Q)^-1/2"));
+  double* si = reinterpret_cast<double*>(b_si.data());
+  RIGW_CUDA_TRY(cudaMemsetAsync(si, 0, size_t(b.naux) * ldk * 8, s));
+  if (nkept > 0)
+    ri_sqrtinv_kernel<<<nkept, 128, 0, s>>>(v2, vec, n, b.naux, reinterpret_cast<const int*>(b_kept.data()), nkept,
+                                            si, ldk);
+  // halve the diagonal pairs, then B[c][pair] = sum_P sqrtinv[P][c] raw[P][pair] (DMMA)
+  RIGW_TRY(upload(c, b_diag, b.diag, "ri diagonal pairs", s));
+  if (!b.diag.empty())
+    ri_halve_diag_kernel<<<dim3(unsigned((b.diag.size() + 255) / 256), unsigned(b.naux)), 256, 0, s>>>(
+        raw, b.naux, pr.npair, reinterpret_cast<const int*>(b_diag.data()), int(b.diag.size()));
+  RIGW_CUDA_TRY(cudaGetLastError());
+  // pairs padded to even for the product: copy raw into an even-strided buffer when npair is odd
+  const int npp = pr.npair + (pr.npair & 1);
+  DeviceBuffer b_rawp, b_res;
+  const double* rawp = raw;
+  if (npp != pr.npair) {
+    RIGW_TRY(b_rawp.allocate(&c, size_t(b.naux) * npp * 8, "ri (mu nu|P) padded"));
+    double* rp = reinterpret_cast<double*>(b_rawp.data());
+    RIGW_CUDA_TRY(cudaMemsetAsync(rp, 0, size_t(b.naux) * npp * 8, s));
+    RIGW_CUDA_TRY(cudaMemcpy2DAsync(rp, size_t(npp) * 8, raw, size_t(pr.npair) * 8, size_t(pr.npair) * 8, b.naux,
+                                    cudaMemcpyDeviceToDevice, s));
+    rawp = rp;
+  }
+  RIGW_TRY(b_res.allocate(&c, size_t(ldk) * npp * 8, "ri B"));
+  double* res = reinterpret_cast<double*>(b_res.data());
+  std::vector<GemmItem> items;
+  for (int i0 = 0; i0 < ldk; i0 += 128)
+    for (int j0 = 0; j0 < npp; j0 += 128) {
+      GemmItem g{};
+      g.A = si + i0;   // A[k = P][m = c]
+      g.lda = ldk;
+      g.B = rawp + j0;   // B[k = P][n = pair]
+      g.ldb = npp;
+      g.C = res + size_t(i0) * npp + j0;
+      g.ldc = npp;
+      g.m = std::min(128, ldk - i0);
+      g.n = std::min(128, npp - j0);
+      g.k = b.naux;
+      g.alpha = 1.0;
+      items.push_back(g);
+    }
+  RIGW_TRY(upload(c, b_items, items, "ri product items", s));
+  launch_dgemm_128x128(reinterpret_cast<const GemmItem*>(b_items.data()), int(items.size()), 1, s);
+  RIGW_CUDA_TRY(cudaGetLastError());
+  const cudaMemcpyKind kind = on_dev ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+  RIGW_CUDA_TRY(cudaMemcpy2DAsync(out, size_t(pr.npair) * 8, res, size_t(npp) * 8, size_t(pr.npair) * 8, nkept, kind,
+                                  s));
+  RIGW_CUDA_TRY(cudaStreamSynchronize(s));
+  if (nkept_out) *nkept_out = nkept;
+  return Status::ok();
+}
+
+}  // namespace rigw

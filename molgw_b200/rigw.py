@@ -91,6 +91,43 @@ class G3w2Problem(C.Structure):
     ]
 
 
+class RiShell(C.Structure):
+    _fields_ = [("center", C.c_double * 3), ("am", C.c_int), ("nprim", C.c_int), ("alpha", _dp), ("coeff", _dp)]
+
+
+class RiProblem(C.Structure):
+    _fields_ = [
+        ("nshell", C.c_int), ("shells", C.POINTER(RiShell)), ("pure", C.c_int), ("nshell_aux", C.c_int),
+        ("aux_shells", C.POINTER(RiShell)), ("pure_aux", C.c_int), ("npair", C.c_int),
+        ("index_basis", C.POINTER(C.c_int)), ("flags", C.c_int),
+    ]
+
+
+def shell_coefficients(am: int, alpha, coeff) -> np.ndarray:
+    """The reference's shell coefficients (src/m_basis_set.f90:332-333) from a
+    basis file's contraction (coefficients of normalized primitives): the
+    contraction normalized so that its x^l component has unit norm, each
+    coefficient times (2/pi)^{3/4} 2^l alpha^{(2l+3)/4}."""
+    a = np.asarray(alpha, dtype=np.float64)
+    c = np.asarray(coeff, dtype=np.float64)
+    dfact = float(np.prod(np.arange(2 * am - 1, 0, -2))) if am > 0 else 1.0
+    norm = np.sqrt((2.0 * a / np.pi) ** 1.5 * (4.0 * a) ** am / dfact)           # primitive norm of x^l
+    ab = a[:, None] + a[None, :]
+    ovl = dfact / (2.0 * ab) ** am * (np.pi / ab) ** 1.5                         # <x^l g_a | x^l g_b>
+    s = 1.0 / np.sqrt(float(np.sum(np.outer(c * norm, c * norm) * ovl)))
+    return c * s * (2.0 / np.pi) ** 0.75 * 2.0 ** am * a ** ((2 * am + 3) / 4.0)
+
+
+def _ri_shells(shells, keep):
+    arr = (RiShell * len(shells))()
+    for k, sh in enumerate(shells):
+        a = np.ascontiguousarray(sh.alpha, dtype=np.float64)
+        c = np.ascontiguousarray(shell_coefficients(sh.am, sh.alpha, sh.coeff))
+        keep += [a, c]
+        arr[k] = RiShell((C.c_double * 3)(*[float(x) for x in sh.center]), sh.am, len(a), _ptr(a), _ptr(c))
+    return arr
+
+
 class DmProblem(C.Structure):
     _fields_ = [
         ("naux", C.c_int), ("nstate", C.c_int), ("m_full", _dp), ("nsig", C.c_int), ("sig_first", C.c_int),
@@ -225,6 +262,9 @@ def load_library(path: Path | str = LIB_PATH) -> C.CDLL:
     lib.rigw_g3w2_selfenergy_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(G3w2Problem), _dp]
     lib.rigw_gw_selfenergy_contour.argtypes = [C.c_void_p, C.POINTER(ContourProblem), C.POINTER(ContourResult)]
     lib.rigw_gw_density_matrix_imag.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(DmProblem), _dp]
+    lib.rigw_eri_2center.argtypes = [C.c_void_p, C.POINTER(RiProblem), _dp]
+    lib.rigw_eri_3center_raw.argtypes = [C.c_void_p, C.POINTER(RiProblem), _dp]
+    lib.rigw_eri_3center.argtypes = [C.c_void_p, C.POINTER(RiProblem), _dp, C.POINTER(C.c_int)]
     lib.rigw_g0w0.argtypes = [C.c_void_p, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_g0w0_batch.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(Result)]
     lib.rigw_autotune.argtypes = [C.c_void_p, C.c_int, C.POINTER(Problem), C.POINTER(TuneReport)]
@@ -658,6 +698,54 @@ class Engine:
         self._check(self._lib.rigw_g3w2_selfenergy_imag(self._h, wpol.handle, C.byref(gp), _ptr(out)),
                     "rigw_g3w2_selfenergy_imag")
         return out[..., 0] + 1j * out[..., 1]
+
+    # ---------------------------------------------------------------- RI integrals
+    def _ri_problem(self, shells, aux_shells, pure: bool, pure_aux: bool, pairs, keep):
+        rp = RiProblem()
+        if shells is not None:
+            rp.nshell, rp.shells = len(shells), _ri_shells(shells, keep)
+        rp.nshell_aux, rp.aux_shells = len(aux_shells), _ri_shells(aux_shells, keep)
+        rp.pure, rp.pure_aux = int(pure), int(pure_aux)
+        if pairs is not None:
+            pr = np.ascontiguousarray(pairs, dtype=np.int32)
+            keep.append(pr)
+            rp.npair, rp.index_basis = pr.shape[0], pr.ctypes.data_as(C.POINTER(C.c_int))
+        keep.append(rp.shells)
+        keep.append(rp.aux_shells)
+        return rp
+
+    def eri_2center(self, aux_shells, pure_aux: bool = True) -> np.ndarray:
+        """(P|Q) over the auxiliary basis on the device (rigw_eri_2center).
+        Shells: objects with am, alpha, coeff (basis-file contraction on normalized
+        primitives) and center (Bohr), e.g. oracle or basis-file parsers' shells."""
+        keep = []
+        rp = self._ri_problem(None, aux_shells, True, pure_aux, None, keep)
+        n = sum((2 * s.am + 1) if pure_aux else (s.am + 1) * (s.am + 2) // 2 for s in aux_shells)
+        out = np.zeros((n, n))
+        self._check(self._lib.rigw_eri_2center(self._h, C.byref(rp), _ptr(out)), "rigw_eri_2center")
+        return out
+
+    def eri_3center_raw(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True) -> np.ndarray:
+        """(mu nu|P) [naux_basis, npair] on the device, no metric (rigw_eri_3center_raw);
+        ``pairs`` [npair, 2] 1-based basis-function indices."""
+        keep = []
+        rp = self._ri_problem(shells, aux_shells, pure, pure_aux, pairs, keep)
+        n = sum((2 * s.am + 1) if pure_aux else (s.am + 1) * (s.am + 2) // 2 for s in aux_shells)
+        out = np.zeros((n, rp.npair))
+        self._check(self._lib.rigw_eri_3center_raw(self._h, C.byref(rp), _ptr(out)), "rigw_eri_3center_raw")
+        return out
+
+    def eri_3center(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True) -> np.ndarray:
+        """eri_3center as the reference stores it (rigw_eri_3center): the metric
+        (P|Q)^-1/2 with eigenvalues <= 1e-6 dropped, diagonal pairs halved;
+        [nauxil_kept, npair], the rigw_eri_3center_mo input."""
+        keep = []
+        rp = self._ri_problem(shells, aux_shells, pure, pure_aux, pairs, keep)
+        n = sum((2 * s.am + 1) if pure_aux else (s.am + 1) * (s.am + 2) // 2 for s in aux_shells)
+        out = np.zeros((n, rp.npair))
+        nk = C.c_int()
+        self._check(self._lib.rigw_eri_3center(self._h, C.byref(rp), _ptr(out), C.byref(nk)), "rigw_eri_3center")
+        return out[:nk.value].copy()
 
     def gw_density_matrix_imag(self, inst, m_full, nomega_sigma: int, precision: int = RIGW_FP64,
                                spin_fact: float = 2.0):

@@ -197,6 +197,7 @@ def test_sosex_problem_layout_matches_ctypes(tmp_path):
 
 
 @pytest.mark.parametrize("cname,pyname", [("rigw_contour_problem", "ContourProblem"), ("rigw_dm_problem", "DmProblem"),
+                                          ("rigw_shell", "RiShell"), ("rigw_ri_problem", "RiProblem"),
                                           ("rigw_contour_result", "ContourResult")])
 def test_contour_layouts_match_ctypes(tmp_path, cname, pyname):
     from molgw_b200 import rigw
