@@ -8,7 +8,8 @@
 // E^{ij}_t of the Gaussian products and Hermite Coulomb integrals R_tuv from the
 // Boys function.  One CTA per (orbital shell pair, auxiliary shell) or (auxiliary
 // shell pair): for every primitive pair/triple the E tables and the R table
-// (level-by-level recursion in shared memory, two cubes) are built once and every
+// (level-by-level recursion in shared memory over the live (t, u, v) only, two
+// cubes) are built once and every
 // Cartesian component of the block reads them; the Cartesian block is then
 // transformed to pure functions (real solid harmonics) or normalized per
 // component (CART) in shared memory and stored.
@@ -72,16 +73,18 @@ RIGW_DEVICE_INLINE void cart_comp(int l, int c, int& nx, int& ny, int& nz) {
   nx = ny = nz = 0;
 }
 
-// Boys function F_m(T), m = 0..mmax: series for the highest order and downward
-// recursion; for large T the asymptotic F_0 and upward recursion.
+// Boys function F_m(T), m = 0..mmax: for T >= max(10, 2 mmax), F_0 =
+// sqrt(pi/T) erf(sqrt(T)) / 2 and the upward recursion (stable there: each step
+// damps errors by (2m+1)/(2T) < 1); else the series for the highest order and
+// the downward recursion.
 __device__ void boys(int mmax, double T, double* F) {
   if (T < 1.0e-14) {
     for (int m = 0; m <= mmax; ++m) F[m] = 1.0 / (2 * m + 1) - T / (2 * m + 3);
     return;
   }
   const double e = exp(-T);
-  if (T > 50.0 && T > 2.0 * mmax) {
-    F[0] = 0.5 * sqrt(3.14159265358979323846 / T);
+  if (T >= 10.0 && T >= 2.0 * mmax) {
+    F[0] = 0.5 * sqrt(3.14159265358979323846 / T) * erf(sqrt(T));
     for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
     return;
   }
@@ -123,6 +126,20 @@ __device__ void hermite_e(int imax, int jmax, double a, double b, double qx, dou
 
 RIGW_DEVICE_INLINE int ridx(int t, int u, int v) { return (t * kRiNR + u) * kRiNR + v; }
 
+// Tetrahedral index -> (t, u, v), ordered by s = t + u + v, then t, then u.
+RIGW_DEVICE_INLINE void tet_decode(int idx, int& t, int& u, int& v) {
+  int s = 0;
+  while ((s + 1) * (s + 2) * (s + 3) / 6 <= idx) ++s;
+  int r = idx - s * (s + 1) * (s + 2) / 6;   // position among the (t, u) with t + u <= s
+  t = 0;
+  while (r >= s - t + 1) {
+    r -= s - t + 1;
+    ++t;
+  }
+  u = r;
+  v = s - t - u;
+}
+
 // R_tuv of order 0 for t + u + v <= L into R0 (cube of kRiNR^3), the whole CTA
 // working level by level with two cubes; F holds F_0..F_L.
 __device__ void hermite_r(int L, double p, double X, double Y, double Z, const double* F, double* R0, double* R1) {
@@ -134,9 +151,10 @@ __device__ void hermite_r(int L, double p, double X, double Y, double Z, const d
     double* nxt = (cur == R0) ? R1 : R0;
     const int lim = L - n;
     const double fac = pow(-2.0 * p, n) * F[n];
-    for (int idx = threadIdx.x; idx < kRiNR * kRiNR * kRiNR; idx += blockDim.x) {
-      const int t = idx / (kRiNR * kRiNR), u = (idx / kRiNR) % kRiNR, v = idx % kRiNR;
-      if (t + u + v > lim) continue;
+    const int ntet = (lim + 1) * (lim + 2) * (lim + 3) / 6;   // (t, u, v) with t + u + v <= lim
+    for (int idx = threadIdx.x; idx < ntet; idx += blockDim.x) {
+      int t, u, v;
+      tet_decode(idx, t, u, v);
       double val;
       if (t + u + v == 0) {
         val = fac;
@@ -147,7 +165,7 @@ __device__ void hermite_r(int L, double p, double X, double Y, double Z, const d
       } else {
         val = Z * cur[ridx(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[ridx(t, u, v - 2)] : 0.0);
       }
-      nxt[idx] = val;
+      nxt[ridx(t, u, v)] = val;
     }
     __syncthreads();
     cur = nxt;
