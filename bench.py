@@ -538,6 +538,49 @@ def run_contour_block(reps: int = 3) -> dict:
             "homo_lumo_ev": [float(out.ehomo * HA_EV), float(out.elumo * HA_EV)], "_qp": out.energy_qp_g.tolist()}
 
 
+def ri_cluster(nwater: int):
+    """Shells of an nwater water cluster (3 Angstrom lattice) in cc-pVTZ with
+    cc-pVTZ-RI, from the basis texts of the H2O fixture, and all its pairs."""
+    from molgw_b200 import basis as B
+    d = np.load(ROOT / "tests" / "golden" / "h2o_ccpvdz.npz")
+    texts = json.loads(str(d["basis"]))
+    atoms = B.water_cluster(nwater)
+    sh = B.molecule_shells(atoms, {int(z): t for z, t in texts["cc-pVTZ"].items()})
+    ax = B.molecule_shells(atoms, {int(z): t for z, t in texts["cc-pVTZ-RI"].items()})
+    nbf = B.nfunctions(sh)
+    pairs = np.array([(k, l) for l in range(1, nbf + 1) for k in range(1, l + 1)], dtype=np.int32)
+    return sh, ax, pairs
+
+
+def run_ri_block(reps: int = 2) -> dict:
+    """RI integrals on the device (rigw_eri_3center_raw and rigw_eri_3center) for
+    water clusters in cc-pVTZ / cc-pVTZ-RI: wall time per call with the result in
+    host memory (median of ``reps`` after one untimed call)."""
+    import torch
+    from molgw_b200.rigw import Engine
+    eng = Engine(0)
+    out = {"workload": "(H2O)_n on a 3 Angstrom lattice, cc-pVTZ with cc-pVTZ-RI, all basis-function pairs, FP64",
+           "clusters": []}
+    for nw in (2, 8):
+        sh, ax, pairs = ri_cluster(nw)
+        eng.eri_3center_raw(sh, ax, pairs)
+        raw_t, full_t = [], []
+        for _ in range(reps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            eng.eri_3center_raw(sh, ax, pairs)
+            raw_t.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            e3 = eng.eri_3center(sh, ax, pairs)
+            full_t.append(time.perf_counter() - t0)
+        out["clusters"].append({"waters": nw, "nbf": int(sum(2 * x.am + 1 for x in sh)),
+                                "naux": int(sum(2 * x.am + 1 for x in ax)), "npair": int(len(pairs)),
+                                "nauxil_kept": int(e3.shape[0]), "raw_3center_s": float(np.median(raw_t)),
+                                "eri_3center_with_metric_s": float(np.median(full_t))})
+    eng.close()
+    return out
+
+
 def run_ao_to_qp_block(reps: int = 3) -> dict:
     """From the AO tensor to the QP energies for the 21/207/840/32 workload:
     B(mu nu, P) over all 26 106 pairs of nbf = 228 functions (N(0, s^2), s the
@@ -1093,7 +1136,7 @@ def main():
             batched = run_batched(eng, args.batch_count, args.batch_reps, flush_l2, args.batch_reps_fp64)
         except Exception as exc:    # reported, not hidden
             batched = {"error": str(exc)}
-    ao_to_qp = h2o = contour = None
+    ao_to_qp = h2o = contour = ri = None
     if world == 1:
         # the blocks below use their own contexts: release this one's plan arenas first
         eng.close()
@@ -1110,6 +1153,10 @@ def main():
             contour = run_contour_block()
         except Exception as exc:    # reported, not hidden
             contour = {"error": str(exc)}
+        try:
+            ri = run_ri_block()
+        except Exception as exc:    # reported, not hidden
+            ri = {"error": str(exc)}
     sweep = None
     if args.sweep_block and world == 1:
         eng.close()
@@ -1164,6 +1211,7 @@ def main():
             "ao_to_qp": ao_to_qp,
             "h2o": h2o,
             "contour": contour,
+            "ri_integrals": ri,
             "sweep": sweep,
             "serving": serving,
         }
@@ -1212,6 +1260,19 @@ def main():
                                                      "restatement (LAPACK DSYEV per frequency)"}
                 contour["qp_error_mev_vs_oracle"] = float(
                     np.abs(np.array(contour["_qp"]) - ref_c.energy_qp_g).max() * HA_EV * 1e3)
+            if ri and "error" not in ri:
+                from oracle import gaussian_ri as gri
+                sh, ax, _ = ri_cluster(2)
+                to_g = lambda shells: [gri.Shell(x.am, x.alpha, x.coeff, x.center) for x in shells]
+                bf_c, aux_c = gri.build_functions(to_g(sh)), gri.build_functions(to_g(ax))
+                t0 = time.perf_counter()
+                gri.coulomb_3center(bf_c, aux_c)
+                dt = time.perf_counter() - t0
+                gpu2 = ri["clusters"][0]["raw_3center_s"]
+                ri["cpu_baseline"] = {"value": dt, "unit": "s", "cores": 1, "kind": "port",
+                                      "sample": "(mu nu|P) of the 2-water cluster, the oracle's C McMurchie-Davidson "
+                                                "integrals (one thread) with the pure transform",
+                                      "gpu_s_same_sample": gpu2, "speedup": dt / gpu2}
         if isinstance(line.get("contour"), dict):
             line["contour"].pop("_qp", None)
         print(json.dumps(line), flush=True)
