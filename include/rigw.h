@@ -503,7 +503,7 @@ RIGW_API int rigw_server_destroy(rigw_server* srv);
  * device-resident scratch array that every GPU loading the library keeps until
  * exit; limits: nsig <= 64, nomega_sigma_calc <= 128, 2*(nomega_sigma/2)+1 <=
  * 1025 (larger sizes return RIGW_ERR_ARG).  The first call on a device looks up
- * the scratch address (make it before any stream capture).  Calls share the
+ * the scratch address.  Calls share the
  * scratch: calls that overlap on the GPU race.  The message of a failure is
  * written to errbuf (errlen bytes, may be NULL). */
 RIGW_API int rigw_qp_solve_noalloc(int device, int nsig, int nomega_sigma_calc, const double* omega_calc,

@@ -11,7 +11,7 @@
 // Every GPU that loads this library holds that array until the process exits.
 // The host-side symbol is only a stand-in; its device address is obtained with
 // cudaGetSymbolAddress, once per device, on the first call made on that device
-// (with the device current).  Make that first call before any stream capture.
+// (with the device current).
 // All calls share the array and it keeps the last call's contents: calls that
 // overlap on the GPU (different streams, different host threads) race on it.
 #include <cstdio>
