@@ -5,7 +5,7 @@
 //   W~_k = Y_k^T Y_k - 1 = v^1/2 chi(i w_k) v^1/2      (DMMA, every frequency; Y_k = U_k^-T)
 //   per Sigma state q:
 //     X_k[Q][m] = sum_P W~_k[P][Q] M(q, m, P)        (DMMA, every frequency in one launch)
-//     dm_contract_kernel, one block per (p >= q, k):
+//     dm_contract_kernel, one warp per (p >= q, k), lanes over m:
 //       v(m) = sum_Q M(p, m, Q) X_k[Q][m]
 //       F(m) = sum_s w_s Re{ [1/(i s - e~_m + i w_k) + 1/(i s - e~_m - i w_k)]
 //                            / ((i s - e~_p)(i s - e~_q)) }
@@ -56,49 +56,39 @@ struct DmArgs {
   const double* ws;     // [ns]
   double* partial;      // [ng][nw]
   long long ldm;
-  int ng, wq, naux, naux_e, nw, ns, q;
+  int ng, wq, naux, naux_e, nw, ns, q, pend;
   double mu;
 };
 
 __global__ void __launch_bounds__(kDmThreads) dm_contract_kernel(DmArgs a) {
-  const int p = a.q + blockIdx.x, k = blockIdx.y, tid = threadIdx.x;
-  __shared__ double s_oms[kDmMaxS], s_ws[kDmMaxS];
-  __shared__ double red[kDmThreads / 32];
-  for (int s = tid; s < a.ns; s += kDmThreads) {
-    s_oms[s] = a.oms[s];
-    s_ws[s] = a.ws[s];
-  }
-  __syncthreads();
-  const double y = a.om[k];
-  const double ep = a.e[p] - a.mu, eq = a.e[a.q] - a.mu;
+  const int warp = int((blockIdx.x * (unsigned)kDmThreads + threadIdx.x) >> 5), lane = threadIdx.x & 31;
+  const int np = a.pend - a.q;
+  if (warp >= np * a.nw) return;
+  const int p = a.q + warp % np, k = warp / np;
+  const double y = __ldg(a.om + k);
+  const double ep = __ldg(a.e + p) - a.mu, eq = __ldg(a.e + a.q) - a.mu;
   const double* xk = a.x + (size_t)k * a.naux_e * a.wq;
   double acc = 0.0;
-  for (int m = tid; m < a.ng; m += kDmThreads) {
+  for (int m = lane; m < a.ng; m += 32) {
     double v = 0.0;
     const double* mp = a.mft + (long long)p * a.wq + m;
     for (int Q = 0; Q < a.naux; ++Q) v += mp[(long long)Q * a.ldm] * xk[(size_t)Q * a.wq + m];
-    const double em = a.e[m] - a.mu;
+    const double em = __ldg(a.e + m) - a.mu;
     double f = 0.0;
     for (int s = 0; s < a.ns; ++s) {
-      const double z = s_oms[s];
+      const double z = __ldg(a.oms + s);
       // 1/(-em + i(z + y)) + 1/(-em + i(z - y))
       const double d1 = em * em + (z + y) * (z + y), d2 = em * em + (z - y) * (z - y);
       const double ar = -em / d1 - em / d2;
       const double ai = -(z + y) / d1 - (z - y) / d2;
       // b = (-ep + i z)(-eq + i z)
       const double br = ep * eq - z * z, bi = -z * (ep + eq);
-      f += s_ws[s] * (ar * br + ai * bi) / (br * br + bi * bi);
+      f += __ldg(a.ws + s) * (ar * br + ai * bi) / (br * br + bi * bi);
     }
     acc += v * f;
   }
   acc = warp_sum(acc);
-  if ((tid & 31) == 0) red[tid >> 5] = acc;
-  __syncthreads();
-  if (tid == 0) {
-    double s = 0.0;
-    for (int w = 0; w < kDmThreads / 32; ++w) s += red[w];
-    a.partial[(size_t)p * a.nw + k] = a.wt[k] * s;
-  }
+  if (lane == 0) a.partial[(size_t)p * a.nw + k] = __ldg(a.wt + k) * acc;
 }
 
 // P[p][q] = P[q][p] = factor * sum_k partial[p][k] for the p >= q of state q.
@@ -216,8 +206,7 @@ Status gw_density_matrix_imag(Context& c, const Wpol& w, const rigw_dm_problem& 
   size_t nx = 0;
   for (int q0 = 0; q0 < naux_e; q0 += 128)
     for (int u0 = 0; u0 < wq; u0 += 128) ++nx;
-  const size_t max_items = std::max(iw.size(), nx);
-  RIGW_TRY(b_items.allocate(&c, max_items * sizeof(GemmItem), "dm gemm items"));
+  RIGW_TRY(b_items.allocate(&c, iw.size() * sizeof(GemmItem), "dm W~ items"));
   GemmItem* d_items = reinterpret_cast<GemmItem*>(b_items.data());
   RIGW_CUDA_TRY(cudaMemcpyAsync(d_items, iw.data(), iw.size() * sizeof(GemmItem), cudaMemcpyHostToDevice, s));
   launch_dgemm_128x128(d_items, int(iw.size()), 1, s);
@@ -242,11 +231,11 @@ Status gw_density_matrix_imag(Context& c, const Wpol& w, const rigw_dm_problem& 
   a.ns = ns;
   a.mu = pr.mu;
   const double factor = -pr.spin_fact * 2.0 / ((2.0 * 3.14159265358979323) * (2.0 * 3.14159265358979323));
-  std::vector<GemmItem> ix;
+  // X_k[Q][u] = sum_P W~_k[P][Q] M(q, u, P), every frequency (grid y): one item list per state, uploaded once
   const int pend = pr.sig_first + nsig;
-  for (int q = pr.sig_first; q < pend; ++q) {
-    // X_k[Q][u] = sum_P W~_k[P][Q] M(q, u, P), every frequency (grid y)
-    ix.clear();
+  std::vector<GemmItem> ix;
+  ix.reserve(size_t(nsig) * nx);
+  for (int q = pr.sig_first; q < pend; ++q)
     for (int q0 = 0; q0 < naux_e; q0 += 128)
       for (int u0 = 0; u0 < wq; u0 += 128) {
         GemmItem g{};
@@ -265,15 +254,19 @@ Status gw_density_matrix_imag(Context& c, const Wpol& w, const rigw_dm_problem& 
         g.sC = (long long)naux_e * wq;
         ix.push_back(g);
       }
-    // the previous state's launches read the list: the copy is ordered after them on the stream
-    RIGW_CUDA_TRY(cudaMemcpyAsync(d_items, ix.data(), ix.size() * sizeof(GemmItem), cudaMemcpyHostToDevice, s));
-    launch_dgemm_128x128(d_items, int(ix.size()), nwp, s);
+  DeviceBuffer b_xitems;
+  RIGW_TRY(b_xitems.allocate(&c, ix.size() * sizeof(GemmItem), "dm X items"));
+  GemmItem* d_xitems = reinterpret_cast<GemmItem*>(b_xitems.data());
+  RIGW_CUDA_TRY(cudaMemcpyAsync(d_xitems, ix.data(), ix.size() * sizeof(GemmItem), cudaMemcpyHostToDevice, s));
+  a.pend = pend;
+  for (int q = pr.sig_first; q < pend; ++q) {
+    launch_dgemm_128x128(d_xitems + size_t(q - pr.sig_first) * nx, int(nx), nwp, s);
     a.q = q;
-    dm_contract_kernel<<<dim3(unsigned(pend - q), unsigned(nwp)), kDmThreads, 0, s>>>(a);
+    const long long nwarps = (long long)(pend - q) * nwp;
+    dm_contract_kernel<<<unsigned((nwarps * 32 + kDmThreads - 1) / kDmThreads), kDmThreads, 0, s>>>(a);
     dm_reduce_kernel<<<(pend - q + 127) / 128, 128, 0, s>>>(part, nwp, q, pend, factor, pm, ng);
     RIGW_CUDA_TRY(cudaGetLastError());
     launches += 3;
-    RIGW_CUDA_TRY(cudaStreamSynchronize(s));   // the host vector `ix` is reused for the next state
   }
   if (!on_dev) RIGW_CUDA_TRY(cudaMemcpyAsync(p_matrix, pm, size_t(ng) * ng * 8, cudaMemcpyDeviceToHost, s));
   RIGW_CUDA_TRY(cudaEventRecord(e1, s));

@@ -7,12 +7,14 @@
 // "Molecular Electronic-Structure Theory", ch. 9): Hermite expansion coefficients
 // E^{ij}_t of the Gaussian products and Hermite Coulomb integrals R_tuv from the
 // Boys function.  One CTA per (orbital shell pair, auxiliary shell) or (auxiliary
-// shell pair): for every primitive pair/triple the E tables and the R table
+// shell pair): for every primitive pair/triple the E tables, the Boys values
+// (one thread per order, from a table and its Taylor expansion) and the R table
 // (level-by-level recursion in shared memory over the live (t, u, v) only, two
-// cubes) are built once and every
-// Cartesian component of the block reads them; the Cartesian block is then
-// transformed to pure functions (real solid harmonics) or normalized per
-// component (CART) in shared memory and stored.
+// tetrahedral arrays) are built once and every Cartesian component of the block
+// reads them; the Cartesian block is then transformed to pure functions (real
+// solid harmonics) or normalized per component (CART) in shared memory and
+// stored.  Shared memory is laid out per launch for the highest angular momenta
+// of the basis at hand.
 //
 // The metric: (P|Q) is diagonalized by the device eigensolver (eigh_jacobi.cu),
 // eigenvalues <= 1e-6 are dropped (TOO_LOW_EIGENVAL, src/m_eri.f90:27) and
@@ -20,6 +22,7 @@
 // the eigensolver's order; B is defined up to that orthogonal transformation of
 // the auxiliary index, like the reference's (every product M M^T downstream is
 // invariant to it).
+#include <algorithm>
 #include <cmath>
 #include <vector>
 
@@ -29,11 +32,16 @@ namespace rigw {
 namespace {
 
 constexpr int kRiLmax = 4;                                   // highest angular momentum of a shell
-constexpr int kRiNc = (kRiLmax + 1) * (kRiLmax + 2) / 2;     // Cartesian components (15)
-constexpr int kRiL3 = 3 * kRiLmax;                           // highest Hermite order (12)
-constexpr int kRiNR = kRiL3 + 1;
 constexpr int kRiThreads = 128;
 constexpr double kRiTooLowEigval = 1.0e-6;
+// Boys table: F_m(T) at T_i = i * 0.1, i = 0..400, m = 0..19 (orders up to 3 kRiLmax
+// plus the 7 derivatives of the Taylor expansion).  Beyond T = 40, F_0 = sqrt(pi/T)/2
+// (erfc(sqrt(40)) < 1e-18) and the upward recursion.
+constexpr int kBoysOrders = 3 * kRiLmax + 8;
+constexpr int kBoysRows = 401;
+constexpr double kBoysStep = 0.1;
+constexpr double kBoysTmax = 40.0;
+constexpr double kTwoPi52 = 34.98683665524972569;            // 2 pi^(5/2)
 
 struct DevShell {
   double x, y, z;
@@ -49,9 +57,19 @@ struct RiArgs {
   const int* toff;
   const int* shellpair;   // [nsp][2] orbital shell pairs (A >= B)
   const int* pairmap;     // [nbf][nbf] pair index or -1
+  const double* boys;     // [kBoysRows][kBoysOrders]
+  const int* tet;         // (t, u, v) of each tetrahedral index, packed t | u << 8 | v << 16
   double* out;            // 3-center: [naux][npair]; 2-center: [naux][naux]
   int nbf, naux, npair;
   int pure_orb, pure_aux;
+  // shared-memory layout of the launch (doubles): two R arrays of ntet, the bra E
+  // tables (entry (i, j, t) of an axis at i * ld_ei + j * ld_ej + t, axis stride
+  // e_axis), the ket tables (i * ld_fk + t, axis stride f_axis), the Cartesian
+  // block (nacc) and its transform scratch, which also holds the ket-contracted
+  // Hermite integrals during the primitive loops, the scaled Boys values, 8 scalars,
+  // the packed Cartesian exponents of each component (nacc ints)
+  int ntet, ld_ei, ld_ej, e_axis, ld_fk, f_axis;
+  int off_e, off_f, off_acc, off_tmp, off_boys, off_scal, off_code, smem_doubles;
 };
 
 RIGW_DEVICE_INLINE int ncart(int l) { return (l + 1) * (l + 2) / 2; }
@@ -73,34 +91,44 @@ RIGW_DEVICE_INLINE void cart_comp(int l, int c, int& nx, int& ny, int& nz) {
   nx = ny = nz = 0;
 }
 
-// Boys function F_m(T), m = 0..mmax: for T >= max(10, 2 mmax), F_0 =
-// sqrt(pi/T) erf(sqrt(T)) / 2 and the upward recursion (stable there: each step
-// damps errors by (2m+1)/(2T) < 1); else the series for the highest order and
-// the downward recursion.
-__device__ void boys(int mmax, double T, double* F) {
-  if (T < 1.0e-14) {
-    for (int m = 0; m <= mmax; ++m) F[m] = 1.0 / (2 * m + 1) - T / (2 * m + 3);
+// (-2 al)^m F_m(T) for one order m <= mmax, into F[m].  T < 40: the Taylor
+// expansion about the nearest table point T_i (|T_i - T| <= 0.05), eight terms,
+// F_m(T) = sum_k F_{m+k}(T_i) (T_i - T)^k / k! (dF_m/dT = -F_{m+1}; the first
+// omitted term is below 1e-15 F_m).  T >= 40: thread m == 0 alone fills every
+// order with F_0 = sqrt(pi/T)/2 and F_{m+1} = ((2m+1) F_m - e^-T) / (2T), stable
+// there since (2m+1)/(2T) < 1.
+__device__ __forceinline__ void boys_scaled(int m, int mmax, double al, double T, const double* __restrict__ tab,
+                                            double* F) {
+  if (T < kBoysTmax) {
+    const int i = __double2int_rn(T * 10.0);
+    const double d = i * kBoysStep - T;
+    const double* r = tab + i * kBoysOrders + m;
+    double v = __ldg(r + 7);
+    v = __ldg(r + 6) + v * d * (1.0 / 7.0);
+    v = __ldg(r + 5) + v * d * (1.0 / 6.0);
+    v = __ldg(r + 4) + v * d * (1.0 / 5.0);
+    v = __ldg(r + 3) + v * d * (1.0 / 4.0);
+    v = __ldg(r + 2) + v * d * (1.0 / 3.0);
+    v = __ldg(r + 1) + v * d * 0.5;
+    v = __ldg(r) + v * d;
+    double sc = 1.0;
+    for (int k = 0; k < m; ++k) sc *= -2.0 * al;
+    F[m] = sc * v;
     return;
   }
-  const double e = exp(-T);
-  if (T >= 10.0 && T >= 2.0 * mmax) {
-    F[0] = 0.5 * sqrt(3.14159265358979323846 / T) * erf(sqrt(T));
-    for (int m = 0; m < mmax; ++m) F[m + 1] = ((2 * m + 1) * F[m] - e) / (2.0 * T);
-    return;
+  if (m != 0) return;
+  const double e = exp(-T), h = 0.5 / T;
+  double f = 0.5 * sqrt(3.14159265358979323846 / T), sc = 1.0;
+  for (int k = 0; k <= mmax; ++k) {
+    F[k] = sc * f;
+    f = ((2 * k + 1) * f - e) * h;
+    sc *= -2.0 * al;
   }
-  double term = 1.0 / (2 * mmax + 1), sum = term;
-  for (int k = 1; k < 4000; ++k) {
-    term *= 2.0 * T / (2 * mmax + 2 * k + 1);
-    sum += term;
-    if (term < 1.0e-17 * sum) break;
-  }
-  F[mmax] = e * sum;
-  for (int m = mmax; m > 0; --m) F[m - 1] = (2.0 * T * F[m] + e) / (2 * m - 1);
 }
 
-// E^{ij}_t along one axis for i <= imax, j <= jmax (Q = A - B), into E[(i * (kRiLmax+1) + j) * (2*kRiLmax+1) + t].
-constexpr int kEi = kRiLmax + 1, kEt = 2 * kRiLmax + 1;
-__device__ void hermite_e(int imax, int jmax, double a, double b, double qx, double* E) {
+// E^{ij}_t along one axis for i <= imax, j <= jmax (Q = A - B), into E[i * ld_i + j * ld_j + t].
+__device__ __forceinline__ void hermite_e(int imax, int jmax, double a, double b, double qx, double* E, int ld_i,
+                                          int ld_j) {
   const double p = a + b, mu = a * b / p;
   const double xpa = -b / p * qx, xpb = a / p * qx, h = 0.5 / p;
   E[0] = exp(-mu * qx * qx);
@@ -108,152 +136,170 @@ __device__ void hermite_e(int imax, int jmax, double a, double b, double qx, dou
     for (int j = 0; j <= jmax; ++j) {
       if (i == 0 && j == 0) continue;
       const int tp = i + j - 1;
+      const double* Ep = i > 0 ? E + (i - 1) * ld_i + j * ld_j : E + i * ld_i + (j - 1) * ld_j;
+      const double x = i > 0 ? xpa : xpb;
       for (int t = 0; t <= i + j; ++t) {
-        double v;
-        if (i > 0) {
-          const double* Ep = E + ((i - 1) * kEi + j) * kEt;
-          v = (t <= tp ? xpa * Ep[t] : 0.0) + (t + 1 <= tp ? (t + 1) * Ep[t + 1] : 0.0);
-          if (t > 0) v += h * Ep[t - 1];
-        } else {
-          const double* Ep = E + (i * kEi + j - 1) * kEt;
-          v = (t <= tp ? xpb * Ep[t] : 0.0) + (t + 1 <= tp ? (t + 1) * Ep[t + 1] : 0.0);
-          if (t > 0) v += h * Ep[t - 1];
-        }
-        E[(i * kEi + j) * kEt + t] = v;
+        double v = (t <= tp ? x * Ep[t] : 0.0) + (t + 1 <= tp ? (t + 1) * Ep[t + 1] : 0.0);
+        if (t > 0) v += h * Ep[t - 1];
+        E[i * ld_i + j * ld_j + t] = v;
       }
     }
 }
 
-RIGW_DEVICE_INLINE int ridx(int t, int u, int v) { return (t * kRiNR + u) * kRiNR + v; }
-
-// Tetrahedral index -> (t, u, v), ordered by s = t + u + v, then t, then u.
-RIGW_DEVICE_INLINE void tet_decode(int idx, int& t, int& u, int& v) {
-  int s = 0;
-  while ((s + 1) * (s + 2) * (s + 3) / 6 <= idx) ++s;
-  int r = idx - s * (s + 1) * (s + 2) / 6;   // position among the (t, u) with t + u <= s
-  t = 0;
-  while (r >= s - t + 1) {
-    r -= s - t + 1;
-    ++t;
-  }
-  u = r;
-  v = s - t - u;
+// Tetrahedral index of (t, u, v): ordered by s = t + u + v, then t, then u.
+RIGW_DEVICE_INLINE int tet(int t, int u, int v) {
+  const int s = t + u + v;
+  return s * (s + 1) * (s + 2) / 6 + t * (2 * s + 3 - t) / 2 + u;
 }
 
-// R_tuv of order 0 for t + u + v <= L into R0 (cube of kRiNR^3), the whole CTA
-// working level by level with two cubes; F holds F_0..F_L.
-__device__ void hermite_r(int L, double p, double X, double Y, double Z, const double* F, double* R0, double* R1) {
-  // level n = L: only R^{(L)}_000
-  double* cur = (L & 1) ? R1 : R0;   // ends in R0 at n = 0
-  if (threadIdx.x == 0) cur[0] = pow(-2.0 * p, L) * F[L];
-  __syncthreads();
+// R_tuv of order 0 for t + u + v <= L (tetrahedral), the whole CTA working level
+// by level between two arrays; F[n] = (-2 al)^n F_n(T) = R^{(n)}_000, so F + L is
+// level L.  Returns the array holding level 0 (F itself when L = 0).
+__device__ __forceinline__ const double* hermite_r(int L, double X, double Y, double Z, const double* F,
+                                                   const int* __restrict__ code, double* R0, double* R1) {
+  const double* cur = F + L;
   for (int n = L - 1; n >= 0; --n) {
-    double* nxt = (cur == R0) ? R1 : R0;
+    double* nxt = (n & 1) ? R1 : R0;
     const int lim = L - n;
-    const double fac = pow(-2.0 * p, n) * F[n];
     const int ntet = (lim + 1) * (lim + 2) * (lim + 3) / 6;   // (t, u, v) with t + u + v <= lim
     for (int idx = threadIdx.x; idx < ntet; idx += blockDim.x) {
-      int t, u, v;
-      tet_decode(idx, t, u, v);
+      const int c = __ldg(code + idx);
+      const int t = c & 255, u = (c >> 8) & 255, v = c >> 16;
       double val;
-      if (t + u + v == 0) {
-        val = fac;
+      if (idx == 0) {
+        val = F[n];
       } else if (t > 0) {
-        val = X * cur[ridx(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[ridx(t - 2, u, v)] : 0.0);
+        val = X * cur[tet(t - 1, u, v)] + (t > 1 ? (t - 1) * cur[tet(t - 2, u, v)] : 0.0);
       } else if (u > 0) {
-        val = Y * cur[ridx(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[ridx(t, u - 2, v)] : 0.0);
+        val = Y * cur[tet(t, u - 1, v)] + (u > 1 ? (u - 1) * cur[tet(t, u - 2, v)] : 0.0);
       } else {
-        val = Z * cur[ridx(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[ridx(t, u, v - 2)] : 0.0);
+        val = Z * cur[tet(t, u, v - 1)] + (v > 1 ? (v - 1) * cur[tet(t, u, v - 2)] : 0.0);
       }
-      nxt[ridx(t, u, v)] = val;
+      nxt[idx] = val;
     }
     __syncthreads();
     cur = nxt;
   }
+  return cur;
 }
 
-// Shared memory of the integral kernels (doubles).
-constexpr int kSmemR = 2 * kRiNR * kRiNR * kRiNR;           // two R cubes
-constexpr int kSmemE = 3 * kEi * kEi * kEt;                 // E tables of the bra pair
-constexpr int kSmemF = 3 * kEi * kEi * kEt;                 // E tables of the ket (single function: j = 0)
-constexpr int kSmemAcc = kRiNc * kRiNc * kRiNc;             // Cartesian block
-constexpr int kSmemBoys = kRiNR + 1;
-constexpr size_t kRiSmemBytes = size_t(kSmemR + kSmemE + kSmemF + 2 * kSmemAcc + kSmemBoys) * sizeof(double);
-
 // Cartesian block of one shell triple (bra A, B; ket Q, a single function) or,
-// with B == nullptr, one auxiliary pair (bra P as a single function, ket Q).
-__device__ void shell_block(const DevShell& A, const DevShell* B, const DevShell& Q, const double* alpha,
-                            const double* coeff, double* smem, int na, int nb, int nq) {
+// with B == nullptr, one auxiliary pair (bra P as a single function, ket Q), into
+// smem + off_acc.  Per primitive triple, in one phase: the bra E tables (threads
+// 0-2, for a new primitive pair), the ket tables (threads 32-34, for a new ket
+// primitive), the Boys values (threads 64.., one per order; thread 64 also
+// publishes the prefactor and P - Q); then the R recursion, the ket step and the
+// bra step.  The Cartesian exponents of every component are decoded once per block.
+__device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, const DevShell* B, const DevShell& Q,
+                                            double* smem, int na, int nb, int nq) {
   double* R0 = smem;
-  double* R1 = R0 + kRiNR * kRiNR * kRiNR;
-  double* E = R1 + kRiNR * kRiNR * kRiNR;
-  double* Fk = E + kSmemE;
-  double* acc = Fk + kSmemF;
-  double* F = acc + 2 * kSmemAcc;
+  double* R1 = smem + g.ntet;
+  double* E = smem + g.off_e;
+  double* Fk = smem + g.off_f;
+  double* acc = smem + g.off_acc;
+  double* F = smem + g.off_boys;
+  double* G = smem + g.off_tmp;     // ket-contracted Hermite integrals (the transform scratch until the end)
+  double* sc = smem + g.off_scal;   // pref, X, Y, Z of the triple
+  int* code = reinterpret_cast<int*>(smem + g.off_code);
+  const double* alpha = g.alpha;
+  const double* coeff = g.coeff;
   const int tid = threadIdx.x;
   const int lb = B ? B->l : 0;
   const int nblk = na * nb * nq;
-  for (int i = tid; i < nblk; i += blockDim.x) acc[i] = 0.0;
+  for (int o = tid; o < nblk; o += blockDim.x) {
+    acc[o] = 0.0;
+    const int i = o / (nb * nq), j = (o / nq) % nb, k = o % nq;
+    int ix, iy, iz, jx = 0, jy = 0, jz = 0, kx, ky, kz;
+    cart_comp(A.l, i, ix, iy, iz);
+    if (B) cart_comp(lb, j, jx, jy, jz);
+    cart_comp(Q.l, k, kx, ky, kz);
+    code[o] = ix | iy << 3 | iz << 6 | jx << 9 | jy << 12 | jz << 15 | kx << 18 | ky << 21 | kz << 24;
+  }
   const int L = A.l + lb + Q.l;
+  const int lab = A.l + lb, ntab = (lab + 1) * (lab + 2) * (lab + 3) / 6;
   const int pbn = B ? B->nprim : 1;
-  for (int pa = 0; pa < A.nprim; ++pa)
-    for (int pb = 0; pb < pbn; ++pb) {
-      const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0;
-      const double cab = coeff[A.p0 + pa] * (B ? coeff[B->p0 + pb] : 1.0);
-      const double XB[3] = {B ? B->x : A.x, B ? B->y : A.y, B ? B->z : A.z};
-      const double XA[3] = {A.x, A.y, A.z};
-      const double p = a + b;
-      const double P[3] = {(a * XA[0] + b * XB[0]) / p, (a * XA[1] + b * XB[1]) / p, (a * XA[2] + b * XB[2]) / p};
-      __syncthreads();   // the previous pair's E tables are no longer read
-      if (tid < 3) hermite_e(A.l, lb, a, b, XA[tid] - XB[tid], E + tid * kEi * kEi * kEt);
-      for (int pq = 0; pq < Q.nprim; ++pq) {
-        const double q = alpha[Q.p0 + pq];
-        const double pref = cab * coeff[Q.p0 + pq] * 2.0 * pow(3.14159265358979323846, 2.5) / (p * q * sqrt(p + q));
-        const double al = p * q / (p + q);
-        const double X = P[0] - Q.x, Y = P[1] - Q.y, Z = P[2] - Q.z;
-        __syncthreads();   // the previous triple's R and ket tables are no longer read
-        if (tid >= 32 && tid < 35) hermite_e(Q.l, 0, q, 0.0, 0.0, Fk + (tid - 32) * kEi * kEi * kEt);
-        if (tid == 64) boys(L, al * (X * X + Y * Y + Z * Z), F);
-        __syncthreads();
-        hermite_r(L, al, X, Y, Z, F, R0, R1);   // ends with a barrier, result in R0
-        for (int o = tid; o < nblk; o += blockDim.x) {
-          const int i = o / (nb * nq), j = (o / nq) % nb, k = o % nq;
-          int ix, iy, iz, jx = 0, jy = 0, jz = 0, kx, ky, kz;
-          cart_comp(A.l, i, ix, iy, iz);
-          if (B) cart_comp(lb, j, jx, jy, jz);
-          cart_comp(Q.l, k, kx, ky, kz);
-          const double* Ex = E + (ix * kEi + jx) * kEt;
-          const double* Ey = E + kEi * kEi * kEt + (iy * kEi + jy) * kEt;
-          const double* Ez = E + 2 * kEi * kEi * kEt + (iz * kEi + jz) * kEt;
-          const double* Fx = Fk + (kx * kEi) * kEt;
-          const double* Fy = Fk + kEi * kEi * kEt + (ky * kEi) * kEt;
-          const double* Fz = Fk + 2 * kEi * kEi * kEt + (kz * kEi) * kEt;
-          double tot = 0.0;
-          for (int t = 0; t <= ix + jx; ++t)
-            for (int u = 0; u <= iy + jy; ++u)
-              for (int v = 0; v <= iz + jz; ++v) {
-                const double e1 = Ex[t] * Ey[u] * Ez[v];
-                if (e1 == 0.0) continue;
-                double s = 0.0;
-                for (int t2 = 0; t2 <= kx; ++t2)
-                  for (int u2 = 0; u2 <= ky; ++u2)
-                    for (int v2 = 0; v2 <= kz; ++v2) {
-                      const double e2 = Fx[t2] * Fy[u2] * Fz[v2];
-                      s += (((t2 + u2 + v2) & 1) ? -e2 : e2) * R0[ridx(t + t2, u + u2, v + v2)];
-                    }
-                tot += e1 * s;
-              }
-          acc[o] += pref * tot;
-        }
+  const double bx = B ? B->x : A.x, by = B ? B->y : A.y, bz = B ? B->z : A.z;
+  const int ntri = A.nprim * pbn * Q.nprim;
+  for (int tr = 0; tr < ntri; ++tr) {
+    const int pq = tr % Q.nprim, pb = (tr / Q.nprim) % pbn, pa = tr / (Q.nprim * pbn);
+    __syncthreads();   // the previous triple's tables, R and Hermite integrals are no longer read
+    if (tid < 3) {
+      if (pq == 0) {   // a new primitive pair
+        const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0;
+        const double qx = tid == 0 ? A.x - bx : (tid == 1 ? A.y - by : A.z - bz);
+        hermite_e(A.l, lb, a, b, qx, E + tid * g.e_axis, g.ld_ei, g.ld_ej);
+      }
+    } else if (tid >= 32 && tid < 35) {
+      if (tr == 0 || Q.nprim > 1)
+        hermite_e(Q.l, 0, alpha[Q.p0 + pq], 0.0, 0.0, Fk + (tid - 32) * g.f_axis, g.ld_fk, 0);
+    } else if (tid >= 64 && tid <= 64 + L) {
+      const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0, q = alpha[Q.p0 + pq];
+      const double p = a + b, ip = 1.0 / p;
+      const double X = (a * A.x + b * bx) * ip - Q.x, Y = (a * A.y + b * by) * ip - Q.y,
+                   Z = (a * A.z + b * bz) * ip - Q.z;
+      const double ipq = 1.0 / (p + q), al = p * q * ipq;
+      boys_scaled(tid - 64, L, al, al * (X * X + Y * Y + Z * Z), g.boys, F);
+      if (tid == 64) {
+        const double cab = coeff[A.p0 + pa] * (B ? coeff[B->p0 + pb] : 1.0);
+        sc[0] = cab * coeff[Q.p0 + pq] * kTwoPi52 * sqrt(ipq) / (p * q);
+        sc[1] = X;
+        sc[2] = Y;
+        sc[3] = Z;
       }
     }
+    __syncthreads();
+    const double* R = hermite_r(L, sc[1], sc[2], sc[3], F, g.tet, R0, R1);   // ends with a barrier when L > 0
+    // ket step: G[k][tuv] = sum_{t2 u2 v2} E^k_t2 E^k_u2 E^k_v2 R_{t+t2, u+u2, v+v2} for t + u + v <= lab;
+    // the ket is a single centre, so E^{i0}_t vanishes unless t = i (mod 2) and the sign
+    // (-1)^(t2+u2+v2) of the ket's Hermite functions is (-1)^lq throughout (folded into pref)
+    for (int w = tid; w < nq * ntab; w += blockDim.x) {
+      const int k = w / ntab, idx = w - k * ntab;
+      const int tc = __ldg(g.tet + idx);
+      const int t = tc & 255, u = (tc >> 8) & 255, v = tc >> 16;
+      const int c = code[k];
+      const int kx = (c >> 18) & 7, ky = (c >> 21) & 7, kz = (c >> 24) & 7;
+      const double* Fx = Fk + kx * g.ld_fk;
+      const double* Fy = Fk + g.f_axis + ky * g.ld_fk;
+      const double* Fz = Fk + 2 * g.f_axis + kz * g.ld_fk;
+      double sum = 0.0;
+      for (int t2 = kx & 1; t2 <= kx; t2 += 2)
+        for (int u2 = ky & 1; u2 <= ky; u2 += 2) {
+          const double fxy = Fx[t2] * Fy[u2];
+          for (int v2 = kz & 1; v2 <= kz; v2 += 2) sum += fxy * Fz[v2] * R[tet(t + t2, u + u2, v + v2)];
+        }
+      G[w] = sum;
+    }
+    __syncthreads();
+    // bra step: acc[i][j][k] += pref sum_{tuv} E^{ij}_t E^{ij}_u E^{ij}_v G[k][tuv]
+    const double pref = (Q.l & 1) ? -sc[0] : sc[0];
+    for (int o = tid; o < nblk; o += blockDim.x) {
+      const int c = code[o];
+      const int ix = c & 7, iy = (c >> 3) & 7, iz = (c >> 6) & 7, jx = (c >> 9) & 7, jy = (c >> 12) & 7,
+                jz = (c >> 15) & 7;
+      const double* Ex = E + ix * g.ld_ei + jx * g.ld_ej;
+      const double* Ey = E + g.e_axis + iy * g.ld_ei + jy * g.ld_ej;
+      const double* Ez = E + 2 * g.e_axis + iz * g.ld_ei + jz * g.ld_ej;
+      const double* Gk = G + (o % nq) * ntab;
+      double tot = 0.0;
+      for (int t = 0; t <= ix + jx; ++t) {
+        const double ex = Ex[t];
+        if (ex == 0.0) continue;
+        for (int u = 0; u <= iy + jy; ++u) {
+          const double exy = ex * Ey[u];
+          if (exy == 0.0) continue;
+          for (int v = 0; v <= iz + jz; ++v) tot += exy * Ez[v] * Gk[tet(t, u, v)];
+        }
+      }
+      acc[o] += pref * tot;
+    }
+  }
   __syncthreads();
 }
 
 // Transform of the Cartesian block acc[na][nb][nq] to functions: out[fa][fb][fq]
 // = sum Ta[fa][i] Tb[fb][j] Tq[fq][k] acc[i][j][k] (three passes through tmp).
-__device__ void transform_block(const double* Ta, int fa, int na, const double* Tb, int fb, int nb, const double* Tq,
-                                int fq, int nq, double* acc, double* tmp) {
+__device__ __forceinline__ void transform_block(const double* Ta, int fa, int na, const double* Tb, int fb, int nb,
+                                                const double* Tq, int fq, int nq, double* acc, double* tmp) {
   const int tid = threadIdx.x;
   // k: tmp[i][j][q] = sum_k Tq[q][k] acc[i][j][k]
   for (int o = tid; o < na * nb * fq; o += blockDim.x) {
@@ -286,9 +332,9 @@ __global__ void __launch_bounds__(kRiThreads) ri_3center_kernel(RiArgs a) {
   const int sp = blockIdx.x, qs = blockIdx.y;
   const DevShell A = a.sh[a.shellpair[2 * sp]], B = a.sh[a.shellpair[2 * sp + 1]], Q = a.ax[qs];
   const int na = ncart(A.l), nb = ncart(B.l), nq = ncart(Q.l);
-  shell_block(A, &B, Q, a.alpha, a.coeff, smem, na, nb, nq);
-  double* acc = smem + kSmemR + kSmemE + kSmemF;
-  double* tmp = acc + kSmemAcc;
+  shell_block(a, A, &B, Q, smem, na, nb, nq);
+  double* acc = smem + a.off_acc;
+  double* tmp = smem + a.off_tmp;
   const int fa = nfun(A.l, a.pure_orb), fb = nfun(B.l, a.pure_orb), fq = nfun(Q.l, a.pure_aux);
   transform_block(a.trans + a.toff[A.l], fa, na, a.trans + a.toff[B.l], fb, nb, a.trans + a.toff[5 + Q.l], fq, nq,
                   acc, tmp);
@@ -307,9 +353,9 @@ __global__ void __launch_bounds__(kRiThreads) ri_2center_kernel(RiArgs a) {
   if (qs > ps) return;
   const DevShell P = a.ax[ps], Q = a.ax[qs];
   const int np = ncart(P.l), nq = ncart(Q.l);
-  shell_block(P, nullptr, Q, a.alpha, a.coeff, smem, np, 1, nq);
-  double* acc = smem + kSmemR + kSmemE + kSmemF;
-  double* tmp = acc + kSmemAcc;
+  shell_block(a, P, nullptr, Q, smem, np, 1, nq);
+  double* acc = smem + a.off_acc;
+  double* tmp = smem + a.off_tmp;
   const double one = 1.0;
   const int fp = nfun(P.l, a.pure_aux), fq = nfun(Q.l, a.pure_aux);
   transform_block(a.trans + a.toff[5 + P.l], fp, np, &one, 1, 1, a.trans + a.toff[5 + Q.l], fq, nq, acc, tmp);
@@ -463,6 +509,60 @@ Status build_basis(const rigw_ri_problem& pr, RiBasis& b) {
   return Status::ok();
 }
 
+// F_m(T_i) for the table points T_i = i * 0.1 (the double the device forms), from
+// the series e^-T sum_k (2T)^k / ((2m+1)(2m+3)...(2m+2k+1)) in extended precision.
+const std::vector<double>& boys_table() {
+  static const std::vector<double> tab = [] {
+    std::vector<double> t(size_t(kBoysRows) * kBoysOrders);
+    for (int i = 0; i < kBoysRows; ++i) {
+      const long double T = (long double)(i * kBoysStep);
+      const long double e = std::exp(-T);
+      for (int m = 0; m < kBoysOrders; ++m) {
+        long double term = 1.0L / (2 * m + 1), sum = term;
+        for (int k = 1; k < 2000; ++k) {
+          term *= 2.0L * T / (2 * m + 2 * k + 1);
+          sum += term;
+          if (term < 1.0e-21L * sum) break;
+        }
+        t[size_t(i) * kBoysOrders + m] = double(e * sum);
+      }
+    }
+    return t;
+  }();
+  return tab;
+}
+
+// (t, u, v) of every tetrahedral index up to t + u + v = 3 kRiLmax.
+std::vector<int> tet_codes() {
+  std::vector<int> c;
+  for (int s = 0; s <= 3 * kRiLmax; ++s)
+    for (int t = 0; t <= s; ++t)
+      for (int u = 0; u <= s - t; ++u) c.push_back(t | (u << 8) | ((s - t - u) << 16));
+  return c;
+}
+
+// Shared-memory layout for bra shells up to la and lb, ket shells up to lk.
+void set_layout(RiArgs& g, int la, int lb, int lk) {
+  const int L = la + lb + lk;
+  auto nc = [](int l) { return (l + 1) * (l + 2) / 2; };
+  g.ntet = (L + 1) * (L + 2) * (L + 3) / 6;
+  g.ld_ej = la + lb + 1;
+  g.ld_ei = (lb + 1) * g.ld_ej;
+  g.e_axis = (la + 1) * g.ld_ei;
+  g.ld_fk = lk + 1;
+  g.f_axis = (lk + 1) * g.ld_fk;
+  const int nacc = nc(la) * nc(lb) * nc(lk);
+  const int ntab = (la + lb + 1) * (la + lb + 2) * (la + lb + 3) / 6;
+  g.off_e = 2 * g.ntet;
+  g.off_f = g.off_e + 3 * g.e_axis;
+  g.off_acc = g.off_f + 3 * g.f_axis;
+  g.off_tmp = g.off_acc + nacc;
+  g.off_boys = g.off_tmp + std::max(nacc, nc(lk) * ntab);
+  g.off_scal = g.off_boys + L + 1;
+  g.off_code = g.off_scal + 8;
+  g.smem_doubles = g.off_code + (nacc + 1) / 2;
+}
+
 template <class T>
 Status upload(Context& c, DeviceBuffer& buf, const std::vector<T>& v, const char* name, cudaStream_t s) {
   RIGW_TRY(buf.allocate(&c, std::max<size_t>(v.size(), 1) * sizeof(T), name));
@@ -481,13 +581,16 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
   RIGW_TRY(build_basis(pr, b));
   cudaStream_t s = c.stream;
   const bool on_dev = (pr.flags & RIGW_PROBLEM_DEVICE_POINTERS) != 0;
-  DeviceBuffer b_sh, b_ax, b_al, b_co, b_tr, b_to, b_sp, b_pm, b_out, b_v2, b_vec, b_kept, b_diag, b_items;
+  DeviceBuffer b_sh, b_ax, b_al, b_co, b_tr, b_to, b_sp, b_pm, b_out, b_v2, b_vec, b_kept, b_diag, b_items, b_boys,
+      b_tet;
   RIGW_TRY(upload(c, b_sh, b.sh, "ri shells", s));
   RIGW_TRY(upload(c, b_ax, b.ax, "ri auxiliary shells", s));
   RIGW_TRY(upload(c, b_al, b.alpha, "ri exponents", s));
   RIGW_TRY(upload(c, b_co, b.coeff, "ri coefficients", s));
   RIGW_TRY(upload(c, b_tr, b.trans, "ri transforms", s));
   RIGW_TRY(upload(c, b_to, b.toff, "ri transform offsets", s));
+  RIGW_TRY(upload(c, b_boys, boys_table(), "ri Boys table", s));
+  RIGW_TRY(upload(c, b_tet, tet_codes(), "ri Hermite index table", s));
   RiArgs a{};
   a.sh = reinterpret_cast<const DevShell*>(b_sh.data());
   a.ax = reinterpret_cast<const DevShell*>(b_ax.data());
@@ -500,10 +603,11 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
   a.npair = pr.npair;
   a.pure_orb = pr.pure != 0;
   a.pure_aux = pr.pure_aux != 0;
-  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(kRiSmemBytes)));
-  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_2center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     int(kRiSmemBytes)));
+  a.boys = reinterpret_cast<const double*>(b_boys.data());
+  a.tet = reinterpret_cast<const int*>(b_tet.data());
+  int lorb = 0, laux = 0;
+  for (const DevShell& d : b.sh) lorb = std::max(lorb, d.l);
+  for (const DevShell& d : b.ax) laux = std::max(laux, d.l);
   const int nax = int(b.ax.size());
   if (what == 2 || what == 0) {
     // (P|Q); for the metric, into a matrix padded to a multiple of 64 for the eigensolver
@@ -519,7 +623,10 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
     RiArgs a2 = a;
     a2.out = v2;
     a2.naux = n;   // row stride
-    ri_2center_kernel<<<dim3(nax, nax), kRiThreads, kRiSmemBytes, s>>>(a2);
+    set_layout(a2, laux, 0, laux);
+    const size_t smem2 = size_t(a2.smem_doubles) * sizeof(double);
+    RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_2center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem2)));
+    ri_2center_kernel<<<dim3(nax, nax), kRiThreads, smem2, s>>>(a2);
     RIGW_CUDA_TRY(cudaGetLastError());
     if (what == 2) {
       if (!on_dev) RIGW_CUDA_TRY(cudaMemcpyAsync(out, v2, size_t(n) * n * 8, cudaMemcpyDeviceToHost, s));
@@ -541,7 +648,10 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
     raw = reinterpret_cast<double*>(b_out.data());
   }
   a.out = raw;
-  ri_3center_kernel<<<dim3(nsp, nax), kRiThreads, kRiSmemBytes, s>>>(a);
+  set_layout(a, lorb, lorb, laux);
+  const size_t smem3 = size_t(a.smem_doubles) * sizeof(double);
+  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
+  ri_3center_kernel<<<dim3(nsp, nax), kRiThreads, smem3, s>>>(a);
   RIGW_CUDA_TRY(cudaGetLastError());
   if (what == 3) {
     if (!on_dev)
