@@ -555,7 +555,8 @@ def ri_cluster(nwater: int):
 def run_ri_block(reps: int = 2) -> dict:
     """RI integrals on the device (rigw_eri_3center_raw and rigw_eri_3center) for
     water clusters in cc-pVTZ / cc-pVTZ-RI: wall time per call with the result in
-    host memory (median of ``reps`` after one untimed call)."""
+    host memory, and of the raw call writing into device memory (median of
+    ``reps`` after one untimed call)."""
     import torch
     from molgw_b200.rigw import Engine
     eng = Engine(0)
@@ -563,20 +564,27 @@ def run_ri_block(reps: int = 2) -> dict:
            "clusters": []}
     for nw in (2, 8):
         sh, ax, pairs = ri_cluster(nw)
+        naux = int(sum(2 * x.am + 1 for x in ax))
+        dev = torch.empty((naux, len(pairs)), dtype=torch.float64, device="cuda")
         eng.eri_3center_raw(sh, ax, pairs)
-        raw_t, full_t = [], []
+        raw_t, dev_t, full_t = [], [], []
         for _ in range(reps):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             eng.eri_3center_raw(sh, ax, pairs)
             raw_t.append(time.perf_counter() - t0)
             t0 = time.perf_counter()
+            eng.eri_3center_raw(sh, ax, pairs, out=dev)
+            dev_t.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
             e3 = eng.eri_3center(sh, ax, pairs)
             full_t.append(time.perf_counter() - t0)
-        out["clusters"].append({"waters": nw, "nbf": int(sum(2 * x.am + 1 for x in sh)),
-                                "naux": int(sum(2 * x.am + 1 for x in ax)), "npair": int(len(pairs)),
-                                "nauxil_kept": int(e3.shape[0]), "raw_3center_s": float(np.median(raw_t)),
+        out["clusters"].append({"waters": nw, "nbf": int(sum(2 * x.am + 1 for x in sh)), "naux": naux,
+                                "npair": int(len(pairs)), "nauxil_kept": int(e3.shape[0]),
+                                "raw_3center_s": float(np.median(raw_t)),
+                                "raw_3center_device_result_s": float(np.median(dev_t)),
                                 "eri_3center_with_metric_s": float(np.median(full_t))})
+        del dev
     eng.close()
     return out
 

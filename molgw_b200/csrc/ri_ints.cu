@@ -152,17 +152,28 @@ RIGW_DEVICE_INLINE int tet(int t, int u, int v) {
   return s * (s + 1) * (s + 2) / 6 + t * (2 * s + 3 - t) / 2 + u;
 }
 
-// R_tuv of order 0 for t + u + v <= L (tetrahedral), the whole CTA working level
+// Barrier of a team of NT threads: one warp (a team inside a larger CTA) or the CTA.
+template <int NT>
+RIGW_DEVICE_INLINE void team_sync() {
+  if constexpr (NT == 32)
+    __syncwarp();
+  else
+    __syncthreads();
+}
+
+// R_tuv of order 0 for t + u + v <= L (tetrahedral), the whole team working level
 // by level between two arrays; F[n] = (-2 al)^n F_n(T) = R^{(n)}_000, so F + L is
 // level L.  Returns the array holding level 0 (F itself when L = 0).
+template <int NT>
 __device__ __forceinline__ const double* hermite_r(int L, double X, double Y, double Z, const double* F,
                                                    const int* __restrict__ code, double* R0, double* R1) {
+  const int lane = threadIdx.x & (NT - 1);
   const double* cur = F + L;
   for (int n = L - 1; n >= 0; --n) {
     double* nxt = (n & 1) ? R1 : R0;
     const int lim = L - n;
     const int ntet = (lim + 1) * (lim + 2) * (lim + 3) / 6;   // (t, u, v) with t + u + v <= lim
-    for (int idx = threadIdx.x; idx < ntet; idx += blockDim.x) {
+    for (int idx = lane; idx < ntet; idx += NT) {
       const int c = __ldg(code + idx);
       const int t = c & 255, u = (c >> 8) & 255, v = c >> 16;
       double val;
@@ -177,7 +188,7 @@ __device__ __forceinline__ const double* hermite_r(int L, double X, double Y, do
       }
       nxt[idx] = val;
     }
-    __syncthreads();
+    team_sync<NT>();
     cur = nxt;
   }
   return cur;
@@ -185,13 +196,17 @@ __device__ __forceinline__ const double* hermite_r(int L, double X, double Y, do
 
 // Cartesian block of one shell triple (bra A, B; ket Q, a single function) or,
 // with B == nullptr, one auxiliary pair (bra P as a single function, ket Q), into
-// smem + off_acc.  Per primitive triple, in one phase: the bra E tables (threads
-// 0-2, for a new primitive pair), the ket tables (threads 32-34, for a new ket
-// primitive), the Boys values (threads 64.., one per order; thread 64 also
-// publishes the prefactor and P - Q); then the R recursion, the ket step and the
-// bra step.  The Cartesian exponents of every component are decoded once per block.
+// smem + off_acc, by a CTA of NT threads.  Per primitive triple, in one phase: the
+// bra E tables (threads 0-2, for a new primitive pair), the ket tables (three
+// threads from kKet, for a new ket primitive), the Boys values (one thread per
+// order from kBoys, the first also publishing the prefactor and P - Q); then the
+// R recursion, the ket step and the bra step.  The Cartesian exponents of every component are decoded once per block.
+template <int NT>
 __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, const DevShell* B, const DevShell& Q,
-                                            double* smem, int na, int nb, int nq) {
+                                            double* smem, int na, int nb, int nq, int tr0, int trstep) {
+  constexpr int kKet = NT >= 64 ? 32 : 3;    // first of the three threads building the ket tables
+  constexpr int kBoys = NT >= 128 ? 64 : 8;  // thread of Boys order 0 (orders up to 3 kRiLmax follow)
+  static_assert(kBoys + 3 * kRiLmax < NT, "a thread per Boys order");
   double* R0 = smem;
   double* R1 = smem + g.ntet;
   double* E = smem + g.off_e;
@@ -203,10 +218,10 @@ __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, 
   int* code = reinterpret_cast<int*>(smem + g.off_code);
   const double* alpha = g.alpha;
   const double* coeff = g.coeff;
-  const int tid = threadIdx.x;
+  const int tid = threadIdx.x & (NT - 1);
   const int lb = B ? B->l : 0;
   const int nblk = na * nb * nq;
-  for (int o = tid; o < nblk; o += blockDim.x) {
+  for (int o = tid; o < nblk; o += NT) {
     acc[o] = 0.0;
     const int i = o / (nb * nq), j = (o / nq) % nb, k = o % nq;
     int ix, iy, iz, jx = 0, jy = 0, jz = 0, kx, ky, kz;
@@ -220,26 +235,26 @@ __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, 
   const int pbn = B ? B->nprim : 1;
   const double bx = B ? B->x : A.x, by = B ? B->y : A.y, bz = B ? B->z : A.z;
   const int ntri = A.nprim * pbn * Q.nprim;
-  for (int tr = 0; tr < ntri; ++tr) {
-    const int pq = tr % Q.nprim, pb = (tr / Q.nprim) % pbn, pa = tr / (Q.nprim * pbn);
-    __syncthreads();   // the previous triple's tables, R and Hermite integrals are no longer read
+  int cur_pair = -1, cur_q = -1;   // primitive pair and ket primitive whose tables are in place
+  for (int tr = tr0; tr < ntri; tr += trstep) {
+    const int pq = tr % Q.nprim, pab = tr / Q.nprim, pb = pab % pbn, pa = pab / pbn;
+    team_sync<NT>();   // the previous triple's tables, R and Hermite integrals are no longer read
     if (tid < 3) {
-      if (pq == 0) {   // a new primitive pair
+      if (pab != cur_pair) {
         const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0;
         const double qx = tid == 0 ? A.x - bx : (tid == 1 ? A.y - by : A.z - bz);
         hermite_e(A.l, lb, a, b, qx, E + tid * g.e_axis, g.ld_ei, g.ld_ej);
       }
-    } else if (tid >= 32 && tid < 35) {
-      if (tr == 0 || Q.nprim > 1)
-        hermite_e(Q.l, 0, alpha[Q.p0 + pq], 0.0, 0.0, Fk + (tid - 32) * g.f_axis, g.ld_fk, 0);
-    } else if (tid >= 64 && tid <= 64 + L) {
+    } else if (tid >= kKet && tid < kKet + 3) {
+      if (pq != cur_q) hermite_e(Q.l, 0, alpha[Q.p0 + pq], 0.0, 0.0, Fk + (tid - kKet) * g.f_axis, g.ld_fk, 0);
+    } else if (tid >= kBoys && tid <= kBoys + L) {
       const double a = alpha[A.p0 + pa], b = B ? alpha[B->p0 + pb] : 0.0, q = alpha[Q.p0 + pq];
       const double p = a + b, ip = 1.0 / p;
       const double X = (a * A.x + b * bx) * ip - Q.x, Y = (a * A.y + b * by) * ip - Q.y,
                    Z = (a * A.z + b * bz) * ip - Q.z;
       const double ipq = 1.0 / (p + q), al = p * q * ipq;
-      boys_scaled(tid - 64, L, al, al * (X * X + Y * Y + Z * Z), g.boys, F);
-      if (tid == 64) {
+      boys_scaled(tid - kBoys, L, al, al * (X * X + Y * Y + Z * Z), g.boys, F);
+      if (tid == kBoys) {
         const double cab = coeff[A.p0 + pa] * (B ? coeff[B->p0 + pb] : 1.0);
         sc[0] = cab * coeff[Q.p0 + pq] * kTwoPi52 * sqrt(ipq) / (p * q);
         sc[1] = X;
@@ -247,12 +262,14 @@ __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, 
         sc[3] = Z;
       }
     }
-    __syncthreads();
-    const double* R = hermite_r(L, sc[1], sc[2], sc[3], F, g.tet, R0, R1);   // ends with a barrier when L > 0
+    cur_pair = pab;
+    cur_q = pq;
+    team_sync<NT>();
+    const double* R = hermite_r<NT>(L, sc[1], sc[2], sc[3], F, g.tet, R0, R1);   // ends with a barrier when L > 0
     // ket step: G[k][tuv] = sum_{t2 u2 v2} E^k_t2 E^k_u2 E^k_v2 R_{t+t2, u+u2, v+v2} for t + u + v <= lab;
     // the ket is a single centre, so E^{i0}_t vanishes unless t = i (mod 2) and the sign
     // (-1)^(t2+u2+v2) of the ket's Hermite functions is (-1)^lq throughout (folded into pref)
-    for (int w = tid; w < nq * ntab; w += blockDim.x) {
+    for (int w = tid; w < nq * ntab; w += NT) {
       const int k = w / ntab, idx = w - k * ntab;
       const int tc = __ldg(g.tet + idx);
       const int t = tc & 255, u = (tc >> 8) & 255, v = tc >> 16;
@@ -269,10 +286,10 @@ __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, 
         }
       G[w] = sum;
     }
-    __syncthreads();
+    team_sync<NT>();
     // bra step: acc[i][j][k] += pref sum_{tuv} E^{ij}_t E^{ij}_u E^{ij}_v G[k][tuv]
     const double pref = (Q.l & 1) ? -sc[0] : sc[0];
-    for (int o = tid; o < nblk; o += blockDim.x) {
+    for (int o = tid; o < nblk; o += NT) {
       const int c = code[o];
       const int ix = c & 7, iy = (c >> 3) & 7, iz = (c >> 6) & 7, jx = (c >> 9) & 7, jy = (c >> 12) & 7,
                 jz = (c >> 15) & 7;
@@ -293,7 +310,7 @@ __device__ __forceinline__ void shell_block(const RiArgs& g, const DevShell& A, 
       acc[o] += pref * tot;
     }
   }
-  __syncthreads();
+  team_sync<NT>();
 }
 
 // Transform of the Cartesian block acc[na][nb][nq] to functions: out[fa][fb][fq]
@@ -327,14 +344,31 @@ __device__ __forceinline__ void transform_block(const double* Ta, int fa, int na
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(kRiThreads) ri_3center_kernel(RiArgs a) {
+// One CTA per (orbital shell pair, auxiliary shell) of a block list: blocks[b] =
+// shell pair | auxiliary shell << 32.  W teams of NT threads share the primitive
+// triples (triple tr to team tr mod W), each in its own smem_doubles of shared
+// memory; their Cartesian blocks are summed in team order, then the CTA
+// transforms and stores the block.
+template <int NT, int W>
+__global__ void __launch_bounds__(NT * W) ri_3center_kernel(RiArgs a, const long long* __restrict__ blocks) {
   extern __shared__ double smem[];
-  const int sp = blockIdx.x, qs = blockIdx.y;
+  const long long code = __ldg(blocks + blockIdx.x);
+  const int sp = int(code & 0xFFFFFFFFLL), qs = int(code >> 32);
   const DevShell A = a.sh[a.shellpair[2 * sp]], B = a.sh[a.shellpair[2 * sp + 1]], Q = a.ax[qs];
   const int na = ncart(A.l), nb = ncart(B.l), nq = ncart(Q.l);
-  shell_block(a, A, &B, Q, smem, na, nb, nq);
+  const int team = W > 1 ? int(threadIdx.x) / NT : 0;
+  shell_block<NT>(a, A, &B, Q, smem + (size_t)team * a.smem_doubles, na, nb, nq, team, W);
   double* acc = smem + a.off_acc;
   double* tmp = smem + a.off_tmp;
+  if constexpr (W > 1) {
+    __syncthreads();
+    for (int o = threadIdx.x; o < na * nb * nq; o += NT * W) {
+      double v = acc[o];
+      for (int w = 1; w < W; ++w) v += acc[(size_t)w * a.smem_doubles + o];
+      acc[o] = v;
+    }
+    __syncthreads();
+  }
   const int fa = nfun(A.l, a.pure_orb), fb = nfun(B.l, a.pure_orb), fq = nfun(Q.l, a.pure_aux);
   transform_block(a.trans + a.toff[A.l], fa, na, a.trans + a.toff[B.l], fb, nb, a.trans + a.toff[5 + Q.l], fq, nq,
                   acc, tmp);
@@ -353,7 +387,7 @@ __global__ void __launch_bounds__(kRiThreads) ri_2center_kernel(RiArgs a) {
   if (qs > ps) return;
   const DevShell P = a.ax[ps], Q = a.ax[qs];
   const int np = ncart(P.l), nq = ncart(Q.l);
-  shell_block(a, P, nullptr, Q, smem, np, 1, nq);
+  shell_block<kRiThreads>(a, P, nullptr, Q, smem, np, 1, nq, 0, 1);
   double* acc = smem + a.off_acc;
   double* tmp = smem + a.off_tmp;
   const double one = 1.0;
@@ -541,27 +575,44 @@ std::vector<int> tet_codes() {
   return c;
 }
 
-// Shared-memory layout for bra shells up to la and lb, ket shells up to lk.
-void set_layout(RiArgs& g, int la, int lb, int lk) {
-  const int L = la + lb + lk;
-  auto nc = [](int l) { return (l + 1) * (l + 2) / 2; };
+// Shared-memory layout for bra shells up to la and lb, ket shells up to lk, blocks
+// of total angular momentum up to L, Cartesian blocks of up to nacc components and
+// ket-contracted Hermite tables of up to ngk entries.
+void set_layout(RiArgs& g, int la, int lb, int lk, int L, int nacc, int ngk) {
   g.ntet = (L + 1) * (L + 2) * (L + 3) / 6;
   g.ld_ej = la + lb + 1;
   g.ld_ei = (lb + 1) * g.ld_ej;
   g.e_axis = (la + 1) * g.ld_ei;
   g.ld_fk = lk + 1;
   g.f_axis = (lk + 1) * g.ld_fk;
-  const int nacc = nc(la) * nc(lb) * nc(lk);
-  const int ntab = (la + lb + 1) * (la + lb + 2) * (la + lb + 3) / 6;
   g.off_e = 2 * g.ntet;
   g.off_f = g.off_e + 3 * g.e_axis;
   g.off_acc = g.off_f + 3 * g.f_axis;
   g.off_tmp = g.off_acc + nacc;
-  g.off_boys = g.off_tmp + std::max(nacc, nc(lk) * ntab);
+  g.off_boys = g.off_tmp + std::max(nacc, ngk);
   g.off_scal = g.off_boys + L + 1;
   g.off_code = g.off_scal + 8;
   g.smem_doubles = g.off_code + (nacc + 1) / 2;
 }
+
+int ncart_host(int l) { return (l + 1) * (l + 2) / 2; }
+int ntet_host(int l) { return (l + 1) * (l + 2) * (l + 3) / 6; }
+
+// A class of 3-center blocks launched together: the block list and the layout maxima.
+struct BlockClass {
+  std::vector<long long> blocks;
+  int la = 0, lb = 0, lk = 0, L = 0, nacc = 1, ngk = 1;
+  void add(long long code, const DevShell& A, const DevShell& B, const DevShell& Q) {
+    blocks.push_back(code);
+    const int nblk = ncart_host(A.l) * ncart_host(B.l) * ncart_host(Q.l);
+    la = std::max(la, A.l);
+    lb = std::max(lb, B.l);
+    lk = std::max(lk, Q.l);
+    L = std::max(L, A.l + B.l + Q.l);
+    nacc = std::max(nacc, nblk);
+    ngk = std::max(ngk, ncart_host(Q.l) * ntet_host(A.l + B.l));
+  }
+};
 
 template <class T>
 Status upload(Context& c, DeviceBuffer& buf, const std::vector<T>& v, const char* name, cudaStream_t s) {
@@ -623,7 +674,7 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
     RiArgs a2 = a;
     a2.out = v2;
     a2.naux = n;   // row stride
-    set_layout(a2, laux, 0, laux);
+    set_layout(a2, laux, 0, laux, 2 * laux, ncart_host(laux) * ncart_host(laux), ncart_host(laux) * ntet_host(laux));
     const size_t smem2 = size_t(a2.smem_doubles) * sizeof(double);
     RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_2center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem2)));
     ri_2center_kernel<<<dim3(nax, nax), kRiThreads, smem2, s>>>(a2);
@@ -648,10 +699,68 @@ Status ri_integrals(Context& c, const rigw_ri_problem& pr, int what, double* out
     raw = reinterpret_cast<double*>(b_out.data());
   }
   a.out = raw;
-  set_layout(a, lorb, lorb, laux);
-  const size_t smem3 = size_t(a.smem_doubles) * sizeof(double);
-  RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
-  ri_3center_kernel<<<dim3(nsp, nax), kRiThreads, smem3, s>>>(a);
+  // Three classes of blocks: at least 20 primitive triples and up to 128 Cartesian
+  // components (contracted shells on both sides) run four one-warp teams per CTA
+  // that share the triples; the others up to 32 components (most blocks) one warp
+  // per CTA; the rest 128 threads per CTA.
+  // Shell pairs with the most primitive pairs come first, so that the last wave
+  // holds short blocks.
+  std::vector<int> order(nsp);
+  for (int i = 0; i < nsp; ++i) order[i] = i;
+  auto prims = [&](int sp) { return b.sh[b.shellpair[2 * sp]].nprim * b.sh[b.shellpair[2 * sp + 1]].nprim; };
+  std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return prims(x) > prims(y); });
+  constexpr int kTeams = 4;
+  BlockClass cls[3];   // warp CTAs, teams of warps, 128-thread CTAs
+  cls[0].blocks.reserve(size_t(nsp) * nax);
+  for (const int sp : order)
+    for (int qs = 0; qs < nax; ++qs) {
+      const DevShell& A = b.sh[b.shellpair[2 * sp]];
+      const DevShell& B = b.sh[b.shellpair[2 * sp + 1]];
+      const DevShell& Q = b.ax[qs];
+      const int nblk = ncart_host(A.l) * ncart_host(B.l) * ncart_host(Q.l);
+      const int ntri = A.nprim * B.nprim * Q.nprim;
+      const int k = ntri >= 20 && nblk <= 128 ? 1 : (nblk <= 32 ? 0 : 2);
+      cls[k].add((long long)sp | ((long long)qs << 32), A, B, Q);
+    }
+  DeviceBuffer b_list[3];
+  for (int k = 0; k < 3; ++k) RIGW_TRY(upload(c, b_list[k], cls[k].blocks, "ri block list", s));
+  // the three launches run concurrently (each fills the others' tails): classes 0 and 1
+  // on two side streams that fork from and join back into the call's stream
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> ev;
+  RIGW_TRY(c.borrow(2, 3, &side, &ev));
+  RIGW_CUDA_TRY(cudaEventRecord(ev[0], s));
+  for (int k = 0; k < 2; ++k) RIGW_CUDA_TRY(cudaStreamWaitEvent(side[k], ev[0], 0));
+  for (const int k : {2, 1, 0}) {
+    const BlockClass& bc = cls[k];
+    if (bc.blocks.empty()) continue;
+    RiArgs ak = a;
+    set_layout(ak, bc.la, bc.lb, bc.lk, bc.L, bc.nacc, bc.ngk);
+    const long long* list = reinterpret_cast<const long long*>(b_list[k].data());
+    const unsigned nb = unsigned(bc.blocks.size());
+    const cudaStream_t sk = k == 2 ? s : side[k];
+    if (k == 0) {
+      const size_t smem3 = size_t(ak.smem_doubles) * sizeof(double);
+      RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel<32, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         int(smem3)));
+      ri_3center_kernel<32, 1><<<nb, 32, smem3, sk>>>(ak, list);
+    } else if (k == 1) {
+      const size_t smem3 = size_t(kTeams) * ak.smem_doubles * sizeof(double);
+      RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel<32, kTeams>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
+      ri_3center_kernel<32, kTeams><<<nb, 32 * kTeams, smem3, sk>>>(ak, list);
+    } else {
+      const size_t smem3 = size_t(ak.smem_doubles) * sizeof(double);
+      RIGW_CUDA_TRY(cudaFuncSetAttribute(ri_3center_kernel<kRiThreads, 1>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem3)));
+      ri_3center_kernel<kRiThreads, 1><<<nb, kRiThreads, smem3, sk>>>(ak, list);
+    }
+    RIGW_CUDA_TRY(cudaGetLastError());
+  }
+  for (int k = 0; k < 2; ++k) {
+    RIGW_CUDA_TRY(cudaEventRecord(ev[1 + k], side[k]));
+    RIGW_CUDA_TRY(cudaStreamWaitEvent(s, ev[1 + k], 0));
+  }
   RIGW_CUDA_TRY(cudaGetLastError());
   if (what == 3) {
     if (!on_dev)

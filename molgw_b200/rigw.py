@@ -725,27 +725,43 @@ class Engine:
         self._check(self._lib.rigw_eri_2center(self._h, C.byref(rp), _ptr(out)), "rigw_eri_2center")
         return out
 
-    def eri_3center_raw(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True) -> np.ndarray:
+    @staticmethod
+    def _ri_out(rp, out, n):
+        """Host result array, or the caller's CUDA tensor [n, npair] (float64,
+        contiguous) with RIGW_PROBLEM_DEVICE_POINTERS set."""
+        if out is None:
+            return np.zeros((n, rp.npair))
+        if tuple(out.shape) != (n, rp.npair) or not out.is_cuda or not out.is_contiguous() or \
+                str(out.dtype) != "torch.float64":
+            raise ValueError(f"out must be a contiguous float64 CUDA tensor of shape {(n, rp.npair)}")
+        rp.flags = RIGW_PROBLEM_DEVICE_POINTERS
+        return out
+
+    def eri_3center_raw(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True, out=None):
         """(mu nu|P) [naux_basis, npair] on the device, no metric (rigw_eri_3center_raw);
-        ``pairs`` [npair, 2] 1-based basis-function indices."""
+        ``pairs`` [npair, 2] 1-based basis-function indices.  With ``out`` (a CUDA
+        tensor) the result stays in device memory."""
         keep = []
         rp = self._ri_problem(shells, aux_shells, pure, pure_aux, pairs, keep)
         n = sum((2 * s.am + 1) if pure_aux else (s.am + 1) * (s.am + 2) // 2 for s in aux_shells)
-        out = np.zeros((n, rp.npair))
+        out = self._ri_out(rp, out, n)
         self._check(self._lib.rigw_eri_3center_raw(self._h, C.byref(rp), _ptr(out)), "rigw_eri_3center_raw")
         return out
 
-    def eri_3center(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True) -> np.ndarray:
+    def eri_3center(self, shells, aux_shells, pairs, pure: bool = True, pure_aux: bool = True, out=None):
         """eri_3center as the reference stores it (rigw_eri_3center): the metric
         (P|Q)^-1/2 with eigenvalues <= 1e-6 dropped, diagonal pairs halved;
-        [nauxil_kept, npair], the rigw_eri_3center_mo input."""
+        [nauxil_kept, npair], the rigw_eri_3center_mo input.  With ``out`` (a CUDA
+        tensor [naux_basis, npair]) the result stays in device memory and the
+        first nauxil_kept rows are returned."""
         keep = []
         rp = self._ri_problem(shells, aux_shells, pure, pure_aux, pairs, keep)
         n = sum((2 * s.am + 1) if pure_aux else (s.am + 1) * (s.am + 2) // 2 for s in aux_shells)
-        out = np.zeros((n, rp.npair))
+        dev = out is not None
+        out = self._ri_out(rp, out, n)
         nk = C.c_int()
         self._check(self._lib.rigw_eri_3center(self._h, C.byref(rp), _ptr(out), C.byref(nk)), "rigw_eri_3center")
-        return out[:nk.value].copy()
+        return out[:nk.value] if dev else out[:nk.value].copy()
 
     def gw_density_matrix_imag(self, inst, m_full, nomega_sigma: int, precision: int = RIGW_FP64,
                                spin_fact: float = 2.0):

@@ -70,3 +70,18 @@ def test_h2o_workload_from_device_integrals(engine):
     ref_sig = d["oracle_sigma_calc"]
     assert np.abs(out.sigma_calc - ref_sig.T).max() < 1e-9 * np.abs(ref_sig).max()
     assert np.abs(out.energy_qp_g - d["oracle_qp"]).max() * HA_EV < 1e-4
+
+
+def test_device_output_equals_host_output(engine):
+    import torch
+    d = h2o_case.load()
+    scf, m, det = h2o_case.front_end(d)
+    pairs = _pairs(det["nbf"])
+    bf, aux = det["bf"].shells, det["aux"].shells
+    host = engine.eri_3center_raw(bf, aux, pairs)
+    dev = torch.empty(host.shape, dtype=torch.float64, device="cuda")
+    assert engine.eri_3center_raw(bf, aux, pairs, out=dev) is dev
+    assert np.array_equal(dev.cpu().numpy(), host)
+    host_b = engine.eri_3center(bf, aux, pairs)
+    dev_b = engine.eri_3center(bf, aux, pairs, out=torch.empty(host.shape, dtype=torch.float64, device="cuda"))
+    assert np.array_equal(dev_b.cpu().numpy(), host_b)
