@@ -36,8 +36,9 @@ constexpr int kLd = kS + 1;       // shared-memory row stride (conflict-free col
 constexpr int kThreads = 256;
 constexpr int kOuterMaxSweeps = 60;
 constexpr double kRelTol = 1.0e-14;
-constexpr size_t kPairSmem = size_t(2 * kS * kLd + kS + kS / 2) * sizeof(double);   // S, Q, rotations, pairs
-constexpr size_t kApplySmem = size_t(3 * kS * kLd) * sizeof(double);                // tile, two rotations
+// S, Q, rotations, pairs (as doubles), the 528-entry block-pair table (as ints)
+constexpr size_t kPairSmem = size_t(2 * kS * kLd + kS + kS / 2) * sizeof(double) + (kS / 2) * (kS / 2 + 1) / 2 * 4;
+constexpr size_t kApplySmem = size_t(3 * kS * (kS + 4)) * sizeof(double);           // tile, two rotations
 
 // Pair k of round r of the round-robin ordering over m (even) indices.
 RIGW_DEVICE_INLINE void rr_pair(int r, int k, int m, int& a, int& b) {
@@ -77,58 +78,75 @@ __global__ void __launch_bounds__(1024) eigh_init_kernel(const double* __restric
 }
 
 // One cyclic Jacobi sweep on the 64 x 64 symmetric S (stride kLd) in shared
-// memory, accumulating the rotations into Q (starts as the identity).  Thread t owns
-// pair t % 32 of every round and the strip of 8 rows / columns t / 32: warp 0
-// sets the round's pairs and rotations; then rows a, b of S and columns a, b of
-// Q are rotated, and after a barrier columns a, b of S.
-__device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn, int* pab, double tau) {
+// memory, accumulating the rotations into Q (starts as the identity).  Per round:
+// warp 0 forms the round's 32 rotations (lane k: pair k); then, after one barrier,
+// the whole round is applied in one pass: thread t updates the 2 x 2 blocks
+// G_k S[{a_k,b_k},{a_l,b_l}] G_l^T for the upper block pairs k <= l of the table
+// blk (writing (l, k) as the transpose, so S stays exactly symmetric) and 8 rows
+// of columns a_k, b_k of Q.  Rotation: t = p2 / (d + sign(d) sqrt(d^2 + p2^2))
+// with d = S_bb - S_aa, p2 = 2 S_ab (Rutishauser's tan of the rotation angle,
+// |t| <= 1), c = 1/sqrt(1 + t^2), s = t c.
+__device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn, int* pab, const int* blk,
+                                   double tau) {
   const int tid = threadIdx.x;
-  const int kq = tid & 31, g = tid >> 5;   // pair, strip (8 warps x 8 = 64)
-  {
-    for (int r = 0; r < kS - 1; ++r) {
-      if (g == 0) {
-        int a, b;
-        rr_pair(r, kq, kS, a, b);
-        const double apq = S[a * kLd + b];
-        double c = 1.0, s = 0.0;
-        if (fabs(apq) > tau) {
-          const double th = (S[b * kLd + b] - S[a * kLd + a]) / (2.0 * apq);
-          const double t = fabs(th) < 1.0e150 ? copysign(1.0, th) / (fabs(th) + sqrt(th * th + 1.0)) : 0.5 / th;
-          c = 1.0 / sqrt(t * t + 1.0);
-          s = t * c;
-        }
-        cs[kq] = c;
-        sn[kq] = s;
-        pab[kq] = a | (b << 8);
+  constexpr int kNblk = (kS / 2) * (kS / 2 + 1) / 2;   // upper 2 x 2 block pairs (528)
+  for (int r = 0; r < kS - 1; ++r) {
+    if (tid < 32) {
+      int a, b;
+      rr_pair(r, tid, kS, a, b);
+      const double apq = S[a * kLd + b];
+      double c = 1.0, s = 0.0;
+      if (fabs(apq) > tau) {
+        const double d = S[b * kLd + b] - S[a * kLd + a], p2 = 2.0 * apq;
+        const double t = p2 / (d + copysign(sqrt(d * d + p2 * p2), d));
+        c = rsqrt(t * t + 1.0);
+        s = t * c;
       }
-      __syncthreads();
-      const double s = sn[kq];
-      const double c = cs[kq];
-      const int a = pab[kq] & 0xff, b = pab[kq] >> 8;
+      cs[tid] = c;
+      sn[tid] = s;
+      pab[tid] = a | (b << 8);
+    }
+    __syncthreads();
+    for (int e = tid; e < kNblk; e += kThreads) {
+      const int kl = blk[e], k = kl & 0xff, l = kl >> 8;
+      const double sk = sn[k], sl = sn[l];
+      if (sk == 0.0 && sl == 0.0) continue;
+      const double ck = cs[k], cl = cs[l];
+      const int ak = pab[k] & 0xff, bk = pab[k] >> 8, al = pab[l] & 0xff, bl = pab[l] >> 8;
+      const double x00 = S[ak * kLd + al], x01 = S[ak * kLd + bl], x10 = S[bk * kLd + al], x11 = S[bk * kLd + bl];
+      // rows: G_k = [[c, -s], [s, c]]
+      const double y00 = ck * x00 - sk * x10, y01 = ck * x01 - sk * x11;
+      const double y10 = sk * x00 + ck * x10, y11 = sk * x01 + ck * x11;
+      // columns: times G_l^T
+      const double z00 = cl * y00 - sl * y01, z01 = sl * y00 + cl * y01;
+      const double z10 = cl * y10 - sl * y11, z11 = sl * y10 + cl * y11;
+      S[ak * kLd + al] = z00;
+      S[ak * kLd + bl] = z01;
+      S[bk * kLd + al] = z10;
+      S[bk * kLd + bl] = z11;
+      if (k != l) {
+        S[al * kLd + ak] = z00;
+        S[bl * kLd + ak] = z01;
+        S[al * kLd + bk] = z10;
+        S[bl * kLd + bk] = z11;
+      }
+    }
+    {
+      const int k = tid & 31, g = tid >> 5;   // pair k, rows 8 g .. 8 g + 7 of Q
+      const double s = sn[k];
       if (s != 0.0) {
+        const double c = cs[k];
+        const int a = pab[k] & 0xff, b = pab[k] >> 8;
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {   // rows a, b of S; columns a, b of Q
+        for (int jj = 0; jj < 8; ++jj) {
           const int j = g * 8 + jj;
-          const double xa = S[a * kLd + j], xb = S[b * kLd + j];
-          S[a * kLd + j] = c * xa - s * xb;
-          S[b * kLd + j] = s * xa + c * xb;
           const double qa = Q[j * kLd + a], qb = Q[j * kLd + b];
           Q[j * kLd + a] = c * qa - s * qb;
           Q[j * kLd + b] = s * qa + c * qb;
         }
       }
-      __syncthreads();
-      if (s != 0.0) {
-#pragma unroll
-        for (int ii = 0; ii < 8; ++ii) {   // columns a, b of S
-          const int i = g * 8 + ii;
-          const double xa = S[i * kLd + a], xb = S[i * kLd + b];
-          S[i * kLd + a] = c * xa - s * xb;
-          S[i * kLd + b] = s * xa + c * xb;
-        }
-      }
-      __syncthreads();
     }
+    __syncthreads();
   }
 }
 
@@ -145,6 +163,7 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __res
   double* cs = Q + kS * kLd;
   double* sn = cs + kS / 2;
   int* pab = reinterpret_cast<int*>(sn + kS / 2);
+  int* blk = pab + kS;   // pab takes kS / 2 doubles = kS ints
   const int w = blockIdx.y, k = blockIdx.x, tid = threadIdx.x;
   const int nb = n / kB, npairs = nb / 2;
   const double* A = Aall + size_t(w) * sA;
@@ -166,7 +185,12 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __res
   // hysteresis: inside a flagged subproblem rotate down to tau/4, so that an
   // entry just above tau is not left just below it by the other rotations and
   // recreated above it by the rounding of the 64-wide updates
-  inner_jacobi_sweep(S, Q, cs, sn, pab, 0.25 * tw);
+  for (int e = tid; e < kS / 2; e += kThreads) {   // block pairs (k, l), k <= l, row by row
+    const int row0 = e * (kS / 2) - e * (e - 1) / 2;
+    for (int l = e; l < kS / 2; ++l) blk[row0 + l - e] = e | (l << 8);
+  }
+  __syncthreads();
+  inner_jacobi_sweep(S, Q, cs, sn, pab, blk, 0.25 * tw);
   if (tid == 0) {
     flags[w * npairs + k] = 1;
     atomicOr(rot + w, 1);
@@ -175,34 +199,49 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __res
   for (int idx = tid; idx < kS * kS; idx += kThreads) qg[idx] = Q[(idx / kS) * kLd + idx % kS];
 }
 
-// out = X^T T (transpose_x) or T X, 64 x 64 in shared memory, 4 x 4 outputs per
-// thread (rows ty + 16 ii, columns tx + 16 jj); the result goes back into T.
+// Tiles of the update pass: 64 x 64 with row stride kLdT = 68 (= 4 mod 16 doubles,
+// so that the DMMA fragment loads below hit 16 distinct 8-byte banks per half warp).
+constexpr int kLdT = kS + 4;
+
+// out = X^T T (transpose_x) or T X, 64 x 64 in shared memory (stride kLdT), on the
+// FP64 tensor cores (mma m8n8k4): warp w computes rows 32 (w & 1) .. + 31 and
+// columns 16 (w >> 1) .. + 15 as 4 x 2 fragments of 8 x 8; the result goes back into T.
 RIGW_DEVICE_INLINE void tile_product(double* T, const double* X, bool transpose_x) {
-  const int tid = threadIdx.x, ty = tid / 16, tx = tid % 16;
-  double acc[4][4] = {};
-  for (int kk = 0; kk < kS; ++kk) {
-    double u[4], v[4];
-    if (transpose_x) {   // sum_k X[k][i] T[k][j]
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int q = lane >> 2, r = lane & 3;
+  const int wm0 = (w & 1) * 32, wn0 = (w >> 1) * 16;
+  double acc[4][2][2];
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii) u[ii] = X[kk * kLd + ty + 16 * ii];
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) v[jj] = T[kk * kLd + tx + 16 * jj];
-    } else {             // sum_k T[i][k] X[k][j]
+    for (int j = 0; j < 2; ++j) acc[i][j][0] = acc[i][j][1] = 0.0;
+#pragma unroll 4
+  for (int k4 = 0; k4 < kS / 4; ++k4) {
+    const int k = 4 * k4 + r;
+    double a[4], b[2];
 #pragma unroll
-      for (int ii = 0; ii < 4; ++ii) u[ii] = T[(ty + 16 * ii) * kLd + kk];
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) v[jj] = X[kk * kLd + tx + 16 * jj];
+    for (int i = 0; i < 4; ++i) {
+      const int row = wm0 + 8 * i + q;
+      a[i] = transpose_x ? X[k * kLdT + row] : T[row * kLdT + k];
     }
 #pragma unroll
-    for (int ii = 0; ii < 4; ++ii)
+    for (int j = 0; j < 2; ++j) {
+      const int col = wn0 + 8 * j + q;
+      b[j] = transpose_x ? T[k * kLdT + col] : X[k * kLdT + col];
+    }
 #pragma unroll
-      for (int jj = 0; jj < 4; ++jj) acc[ii][jj] = fma(u[ii], v[jj], acc[ii][jj]);
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 2; ++j) dmma_8x8x4(acc[i][j][0], acc[i][j][1], a[i], b[j]);
   }
   __syncthreads();   // every read of T is done
 #pragma unroll
-  for (int ii = 0; ii < 4; ++ii)
+  for (int i = 0; i < 4; ++i)
 #pragma unroll
-    for (int jj = 0; jj < 4; ++jj) T[(ty + 16 * ii) * kLd + tx + 16 * jj] = acc[ii][jj];
+    for (int j = 0; j < 2; ++j) {
+      const int row = wm0 + 8 * i + q, col = wn0 + 8 * j + 2 * r;
+      *reinterpret_cast<double2*>(T + row * kLdT + col) = make_double2(acc[i][j][0], acc[i][j][1]);
+    }
   __syncthreads();
 }
 
@@ -219,8 +258,8 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
                                                               int r) {
   extern __shared__ double smem[];
   double* T = smem;
-  double* Qa = T + kS * kLd;
-  double* Qb = Qa + kS * kLd;
+  double* Qa = T + kS * kLdT;
+  double* Qb = Qa + kS * kLdT;
   const int nb = n / kB, npairs = nb / 2, ntri = npairs * (npairs + 1) / 2;
   const int w = blockIdx.y, tid = threadIdx.x;
   const int* fl = flags + w * npairs;
@@ -241,9 +280,9 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
     double* A = Aall + size_t(w) * sA;
     for (int idx = tid; idx < kS * kS; idx += kThreads) {
       const int i = idx / kS, j = idx % kS;
-      T[i * kLd + j] = A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)];
-      if (fp) Qa[i * kLd + j] = qw[size_t(p) * kS * kS + idx];
-      if (fq) Qb[i * kLd + j] = qw[size_t(q) * kS * kS + idx];
+      T[i * kLdT + j] = A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)];
+      if (fp) Qa[i * kLdT + j] = qw[size_t(p) * kS * kS + idx];
+      if (fq) Qb[i * kLdT + j] = qw[size_t(q) * kS * kS + idx];
     }
     __syncthreads();
     if (fp) tile_product(T, Qa, true);
@@ -251,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
     for (int idx = tid; idx < kS * kS; idx += kThreads) {
       const int i = idx / kS, j = idx % kS;
       // diagonal tile: the upper half mirrored, so the tile stays exactly symmetric
-      const double x = (p == q && i > j) ? T[j * kLd + i] : T[i * kLd + j];
+      const double x = (p == q && i > j) ? T[j * kLdT + i] : T[i * kLdT + j];
       A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)] = x;
       if (p != q) A[size_t(sub_index(j, Iq, Jq)) * n + sub_index(i, Ip, Jp)] = x;
     }
@@ -266,14 +305,14 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
   const int i0 = chunk * kS;
   for (int idx = tid; idx < kS * kS; idx += kThreads) {
     const int i = idx / kS, j = idx % kS;
-    T[i * kLd + j] = V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)];
-    Qb[i * kLd + j] = qw[size_t(q) * kS * kS + idx];
+    T[i * kLdT + j] = V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)];
+    Qb[i * kLdT + j] = qw[size_t(q) * kS * kS + idx];
   }
   __syncthreads();
   tile_product(T, Qb, false);
   for (int idx = tid; idx < kS * kS; idx += kThreads) {
     const int i = idx / kS, j = idx % kS;
-    V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)] = T[i * kLd + j];
+    V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)] = T[i * kLdT + j];
   }
 }
 
