@@ -278,12 +278,15 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
     rr_pair(r, p, nb, Ip, Jp);
     rr_pair(r, q, nb, Iq, Jq);
     double* A = Aall + size_t(w) * sA;
-    for (int idx = tid; idx < kS * kS; idx += kThreads) {
-      const int i = idx / kS, j = idx % kS;
-      T[i * kLdT + j] = A[size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq)];
-      if (fp) Qa[i * kLdT + j] = qw[size_t(p) * kS * kS + idx];
-      if (fq) Qb[i * kLdT + j] = qw[size_t(q) * kS * kS + idx];
+    // 16-byte asynchronous copies (two doubles; a pair never straddles a 32-wide block)
+    for (int c = tid; c < kS * kS / 2; c += kThreads) {
+      const int i = c / (kS / 2), j = 2 * (c % (kS / 2));
+      cp_async16(T + i * kLdT + j, A + size_t(sub_index(i, Ip, Jp)) * n + sub_index(j, Iq, Jq), 16);
+      if (fp) cp_async16(Qa + i * kLdT + j, qw + size_t(p) * kS * kS + i * kS + j, 16);
+      if (fq) cp_async16(Qb + i * kLdT + j, qw + size_t(q) * kS * kS + i * kS + j, 16);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
     __syncthreads();
     if (fp) tile_product(T, Qa, true);
     if (fq) tile_product(T, Qb, false);
@@ -303,11 +306,13 @@ __global__ void __launch_bounds__(kThreads) eigh_apply_kernel(double* __restrict
   rr_pair(r, q, nb, Iq, Jq);
   double* V = Vall + size_t(w) * sA;
   const int i0 = chunk * kS;
-  for (int idx = tid; idx < kS * kS; idx += kThreads) {
-    const int i = idx / kS, j = idx % kS;
-    T[i * kLdT + j] = V[size_t(i0 + i) * n + sub_index(j, Iq, Jq)];
-    Qb[i * kLdT + j] = qw[size_t(q) * kS * kS + idx];
+  for (int c = tid; c < kS * kS / 2; c += kThreads) {
+    const int i = c / (kS / 2), j = 2 * (c % (kS / 2));
+    cp_async16(T + i * kLdT + j, V + size_t(i0 + i) * n + sub_index(j, Iq, Jq), 16);
+    cp_async16(Qb + i * kLdT + j, qw + size_t(q) * kS * kS + i * kS + j, 16);
   }
+  cp_async_commit();
+  cp_async_wait<0>();
   __syncthreads();
   tile_product(T, Qb, false);
   for (int idx = tid; idx < kS * kS; idx += kThreads) {
