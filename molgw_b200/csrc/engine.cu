@@ -535,6 +535,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   const int nlists = nchains_ * std::max(max_panels, 1);
   wl_diag_.assign(nlists, {});
   gl_k2_.assign(nlists, {});
+  gl_k2n_.assign(nlists, {});
   gl_k3_.assign(nlists, {});
   gl_k3d_.assign(nlists, {});
   gl_k3a_.assign(nlists, {});
@@ -709,7 +710,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           g.sA = sW;
           g.sB = g.sC = (X == E) ? sE : sR;
           g.sQ = sQ;
-          gl_k2_[li].push_back(g);
+          // the column block of the next panel goes first (the next diagonal block needs it)
+          (X == E && c0 == r0 ? gl_k2n_[li] : gl_k2_[li]).push_back(g);
         };
         if (factor)
           for (int c0 = r0; c0 < npad; c0 += BMN) k2(E, npad, c0, std::min(BMN, npad - c0), nullptr);
@@ -721,8 +723,8 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
         // updated, with the U rows of panels kp .. k (K = (j+1) 128); after the last
         // panel of the group every row below it is updated once with the U rows of
         // the whole group, so each trailing tile is read and written once per group.
-        // Items of the next diagonal block go to their own list so that its
-        // factorization can start while the rest of the update runs (lookahead).
+        // Items of the next diagonal block go to their own list (in both forms) so that
+        // its factorization can start while the rest of the update runs (lookahead).
         const int jg = k % group_;
         const bool first_of_pair = jg != group_ - 1;           // not the group's last panel
         const int kp = k - jg;                                  // first panel of the U rows used
@@ -754,7 +756,7 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
           const int m = std::min(BM, iend - i0);
           if (factor)
             for (int j0 = i0 / BMN * BMN; j0 < npad; j0 += BMN) {
-              const bool next_diag = !first_of_pair && i0 < r0 + kPanel && j0 == r0;
+              const bool next_diag = i0 < r0 + kPanel && j0 == r0;
               k3(E, npad, E, npad, i0, j0, m, std::min(BMN, npad - j0), next_diag ? gl_k3d_[li] : rest);
             }
           // I block: columns below r0 only (the U rows of panel kp have zeros beyond it there)
@@ -841,11 +843,14 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
   }
   add(16, wl_pad_.data(), sizeof(WorkItem), wl_pad_.size(), 0);
   add(15, wl_trace_.data(), sizeof(WorkItem), wl_trace_.size(), 0);
-  // Panel loop of each chain with a one-panel lookahead: the update of the next
-  // diagonal block (K3d) goes first, then its factorization runs on the chain's
-  // lookahead stream while the rest of the trailing update (K3) runs on the
-  // chain's main stream.  Streams: chain c uses 2c (main) and 2c+1 (lookahead);
-  // stream 0 is the plan's own stream.  Kind -1 launches nothing (event marker).
+  // Panel loop of each chain with a one-panel lookahead.  After the diagonal block
+  // of panel k: on the chain's main stream the panel solve of the next panel's
+  // column block (K2n), then on the lookahead stream the update of the next
+  // diagonal block (K3d) and its factorization, while the main stream solves the
+  // rest of panel k (K2) and runs the rest of the trailing update (K3a / K3).  The
+  // next panel's solve waits for both.  Streams: chain c uses 2c (main) and 2c+1
+  // (lookahead); stream 0 is the plan's own stream.  Kind -1 launches nothing
+  // (event marker).
   int nev = 0;
   const int fork_ev = nchains_ > 1 ? nev++ : -1;
   if (fork_ev >= 0) pend.push_back({-1, nullptr, 0, 0, 0, 0, -1, fork_ev, 1});
@@ -857,25 +862,27 @@ Status Plan::build(Context* ctx, PlanMode mode, const std::vector<Shape>& shapes
     for (int k = 0; k < max_panels; ++k) {
       if (k == 0 && add(4, wl_diag_[L(0)].data(), sizeof(WorkItem), wl_diag_[L(0)].size(), 0, sm, pending))
         pending = -1;
-      if (add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm, pending)) pending = -1;
       const bool next = k + 1 < max_panels && !wl_diag_[L(k + 1)].empty();
-      if (k % group_ != group_ - 1) {
-        // not the last panel of its group: the rows of panel k + 1, then its diagonal block
-        if (add(6, gl_k3a_[L(k)].data(), sizeof(GemmItem), gl_k3a_[L(k)].size(), k, sm, pending)) pending = -1;
-        if (next && add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sm,
-                        pending))
-          pending = -1;
+      std::vector<GemmItem>& rest3 = k % group_ != group_ - 1 ? gl_k3a_[L(k)] : gl_k3_[L(k)];
+      if (next && !gl_k2n_[L(k)].empty() && !gl_k3d_[L(k)].empty()) {
+        const int ea = nev++, eb = nev++;
+        add(5, gl_k2n_[L(k)].data(), sizeof(GemmItem), gl_k2n_[L(k)].size(), k, sm, pending, ea);
+        pending = -1;
+        add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sl, ea);
+        add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sl, -1, eb);
+        add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm);
+        add(6, rest3.data(), sizeof(GemmItem), rest3.size(), k, sm);
+        pending = eb;
         continue;
       }
-      const int ea = next ? nev++ : -1, eb = next ? nev++ : -1;
-      if (next && !gl_k3d_[L(k)].empty()) {
-        add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm, -1, ea);
-        add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sl, ea, eb);
-        pending = eb;
-      } else {
-        add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm);
-      }
-      add(6, gl_k3_[L(k)].data(), sizeof(GemmItem), gl_k3_[L(k)].size(), k, sm);
+      // no next panel (or nothing to update ahead of it): everything on the main stream
+      if (add(5, gl_k2n_[L(k)].data(), sizeof(GemmItem), gl_k2n_[L(k)].size(), k, sm, pending)) pending = -1;
+      if (add(5, gl_k2_[L(k)].data(), sizeof(GemmItem), gl_k2_[L(k)].size(), k, sm, pending)) pending = -1;
+      if (add(14, gl_k3d_[L(k)].data(), sizeof(GemmItem), gl_k3d_[L(k)].size(), k, sm, pending)) pending = -1;
+      if (add(6, rest3.data(), sizeof(GemmItem), rest3.size(), k, sm, pending)) pending = -1;
+      if (next && add(4, wl_diag_[L(k + 1)].data(), sizeof(WorkItem), wl_diag_[L(k + 1)].size(), k + 1, sm,
+                      pending))
+        pending = -1;
     }
     if (ch > 0) {
       const int ej = nev++;

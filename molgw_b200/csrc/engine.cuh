@@ -174,7 +174,7 @@ class Plan {
   std::vector<WorkItem> wl_ozzero_, wl_rowmax_;    // Ozaki: row maxima over every frequency
   std::vector<std::vector<WorkItem>> wl_slice_;   // Ozaki: per frequency group
   std::vector<std::vector<TcItem>> tl_ozaki_, tl_ozaki4_;   // s >= 5 / s <= 4 (fused slice pairs)
-  std::vector<std::vector<GemmItem>> gl_k2_, gl_k3_, gl_k3d_, gl_k3a_;
+  std::vector<std::vector<GemmItem>> gl_k2_, gl_k2n_, gl_k3_, gl_k3d_, gl_k3a_;
   std::vector<WorkItem> wl_trace_, wl_pad_;
   struct Launch {
     int kind;        // see Plan::record
