@@ -36,7 +36,7 @@ constexpr int kLd = kS + 1;       // shared-memory row stride (conflict-free col
 constexpr int kThreads = 256;
 constexpr int kOuterMaxSweeps = 60;
 constexpr double kRelTol = 1.0e-14;
-// S, Q, rotations, pairs (as doubles), the 528-entry block-pair table (as ints)
+// S, Q, rotations, kS / 2 spare doubles, the 528-entry block-pair table (as ints)
 constexpr size_t kPairSmem = size_t(2 * kS * kLd + kS + kS / 2) * sizeof(double) + (kS / 2) * (kS / 2 + 1) / 2 * 4;
 constexpr size_t kApplySmem = size_t(3 * kS * (kS + 4)) * sizeof(double);           // tile, two rotations
 
@@ -86,10 +86,42 @@ __global__ void __launch_bounds__(1024) eigh_init_kernel(const double* __restric
 // of columns a_k, b_k of Q.  Rotation: t = p2 / (d + sign(d) sqrt(d^2 + p2^2))
 // with d = S_bb - S_aa, p2 = 2 S_ab (Rutishauser's tan of the rotation angle,
 // |t| <= 1), c = 1/sqrt(1 + t^2), s = t c.
-__device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn, int* pab, const int* blk,
-                                   double tau) {
+// G_k X G_l^T for the 2 x 2 block of pairs (k, l) of round r, written at (k, l)
+// and, for k != l, transposed at (l, k).
+RIGW_DEVICE_INLINE void rotate_block(double* S, int ak, int bk, int al, int bl, bool mirror, double ck, double sk,
+                                     double cl, double sl, double x00, double x01, double x10, double x11) {
+  // rows: G_k = [[c, -s], [s, c]]; columns: times G_l^T
+  const double y00 = ck * x00 - sk * x10, y01 = ck * x01 - sk * x11;
+  const double y10 = sk * x00 + ck * x10, y11 = sk * x01 + ck * x11;
+  const double z00 = cl * y00 - sl * y01, z01 = sl * y00 + cl * y01;
+  const double z10 = cl * y10 - sl * y11, z11 = sl * y10 + cl * y11;
+  S[ak * kLd + al] = z00;
+  S[ak * kLd + bl] = z01;
+  S[bk * kLd + al] = z10;
+  S[bk * kLd + bl] = z11;
+  if (mirror) {
+    S[al * kLd + ak] = z00;
+    S[bl * kLd + ak] = z01;
+    S[al * kLd + bk] = z10;
+    S[bl * kLd + bk] = z11;
+  }
+}
+
+__device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn, const int* blk, double tau) {
   const int tid = threadIdx.x;
   constexpr int kNblk = (kS / 2) * (kS / 2 + 1) / 2;   // upper 2 x 2 block pairs (528)
+  static_assert(kNblk > 2 * kThreads && kNblk <= 3 * kThreads, "two block pairs per thread plus a tail");
+  // this thread's block pairs e = tid and tid + kThreads (both loaded before either is
+  // stored), and e = tid + 2 kThreads for the first kNblk - 2 kThreads threads; decoded once
+  int bk[3], bl[3];
+#pragma unroll
+  for (int m = 0; m < 3; ++m) {
+    const int e = tid + m * kThreads;
+    const int kl = e < kNblk ? blk[e] : 0;
+    bk[m] = e < kNblk ? (kl & 0xff) : -1;
+    bl[m] = kl >> 8;
+  }
+  const int kq = tid & 31, g = tid >> 5;   // Q: pair kq, rows 8 g .. 8 g + 7
   for (int r = 0; r < kS - 1; ++r) {
     if (tid < 32) {
       int a, b;
@@ -104,46 +136,53 @@ __device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn,
       }
       cs[tid] = c;
       sn[tid] = s;
-      pab[tid] = a | (b << 8);
     }
     __syncthreads();
-    for (int e = tid; e < kNblk; e += kThreads) {
-      const int kl = blk[e], k = kl & 0xff, l = kl >> 8;
-      const double sk = sn[k], sl = sn[l];
-      if (sk == 0.0 && sl == 0.0) continue;
-      const double ck = cs[k], cl = cs[l];
-      const int ak = pab[k] & 0xff, bk = pab[k] >> 8, al = pab[l] & 0xff, bl = pab[l] >> 8;
-      const double x00 = S[ak * kLd + al], x01 = S[ak * kLd + bl], x10 = S[bk * kLd + al], x11 = S[bk * kLd + bl];
-      // rows: G_k = [[c, -s], [s, c]]
-      const double y00 = ck * x00 - sk * x10, y01 = ck * x01 - sk * x11;
-      const double y10 = sk * x00 + ck * x10, y11 = sk * x01 + ck * x11;
-      // columns: times G_l^T
-      const double z00 = cl * y00 - sl * y01, z01 = sl * y00 + cl * y01;
-      const double z10 = cl * y10 - sl * y11, z11 = sl * y10 + cl * y11;
-      S[ak * kLd + al] = z00;
-      S[ak * kLd + bl] = z01;
-      S[bk * kLd + al] = z10;
-      S[bk * kLd + bl] = z11;
-      if (k != l) {
-        S[al * kLd + ak] = z00;
-        S[bl * kLd + ak] = z01;
-        S[al * kLd + bk] = z10;
-        S[bl * kLd + bk] = z11;
-      }
-    }
     {
-      const int k = tid & 31, g = tid >> 5;   // pair k, rows 8 g .. 8 g + 7 of Q
-      const double s = sn[k];
-      if (s != 0.0) {
-        const double c = cs[k];
-        const int a = pab[k] & 0xff, b = pab[k] >> 8;
+      double x[2][4];
+      int ia[2][4];
+      bool act[2];
 #pragma unroll
-        for (int jj = 0; jj < 8; ++jj) {
-          const int j = g * 8 + jj;
-          const double qa = Q[j * kLd + a], qb = Q[j * kLd + b];
-          Q[j * kLd + a] = c * qa - s * qb;
-          Q[j * kLd + b] = s * qa + c * qb;
-        }
+      for (int m = 0; m < 2; ++m) {
+        act[m] = sn[bk[m]] != 0.0 || sn[bl[m]] != 0.0;
+        rr_pair(r, bk[m], kS, ia[m][0], ia[m][1]);
+        rr_pair(r, bl[m], kS, ia[m][2], ia[m][3]);
+        if (!act[m]) continue;
+        x[m][0] = S[ia[m][0] * kLd + ia[m][2]];
+        x[m][1] = S[ia[m][0] * kLd + ia[m][3]];
+        x[m][2] = S[ia[m][1] * kLd + ia[m][2]];
+        x[m][3] = S[ia[m][1] * kLd + ia[m][3]];
+      }
+#pragma unroll
+      for (int m = 0; m < 2; ++m)
+        if (act[m])
+          rotate_block(S, ia[m][0], ia[m][1], ia[m][2], ia[m][3], bk[m] != bl[m], cs[bk[m]], sn[bk[m]], cs[bl[m]],
+                       sn[bl[m]], x[m][0], x[m][1], x[m][2], x[m][3]);
+    }
+    if (bk[2] >= 0 && (sn[bk[2]] != 0.0 || sn[bl[2]] != 0.0)) {
+      int ak, bkk, al, bll;
+      rr_pair(r, bk[2], kS, ak, bkk);
+      rr_pair(r, bl[2], kS, al, bll);
+      const double x00 = S[ak * kLd + al], x01 = S[ak * kLd + bll], x10 = S[bkk * kLd + al], x11 = S[bkk * kLd + bll];
+      rotate_block(S, ak, bkk, al, bll, bk[2] != bl[2], cs[bk[2]], sn[bk[2]], cs[bl[2]], sn[bl[2]], x00, x01, x10,
+                   x11);
+    }
+    // Q: columns a, b of pair kq, rows 8 g .. 8 g + 7, loaded before they are stored
+    const double sq = sn[kq];
+    if (sq != 0.0) {
+      const double cq = cs[kq];
+      int qa_i, qb_i;
+      rr_pair(r, kq, kS, qa_i, qb_i);
+      double qa[8], qb[8];
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        qa[jj] = Q[(g * 8 + jj) * kLd + qa_i];
+        qb[jj] = Q[(g * 8 + jj) * kLd + qb_i];
+      }
+#pragma unroll
+      for (int jj = 0; jj < 8; ++jj) {
+        Q[(g * 8 + jj) * kLd + qa_i] = cq * qa[jj] - sq * qb[jj];
+        Q[(g * 8 + jj) * kLd + qb_i] = sq * qa[jj] + cq * qb[jj];
       }
     }
     __syncthreads();
@@ -153,7 +192,7 @@ __device__ void inner_jacobi_sweep(double* S, double* Q, double* cs, double* sn,
 // One CTA per (pair k of round r, matrix w = blockIdx.y): one sweep on the
 // subproblem, its Q to Qbuf.  flags[w][k] says whether the pair rotated;
 // rot[w] whether any pair of matrix w did.
-__global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __restrict__ Aall,
+__global__ void __launch_bounds__(kThreads, 3) eigh_pair_kernel(const double* __restrict__ Aall,
                                                              double* __restrict__ Qbuf, int* __restrict__ flags,
                                                              int* __restrict__ rot, const double* __restrict__ tau,
                                                              int n, long long sA, int r) {
@@ -162,8 +201,7 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __res
   double* Q = S + kS * kLd;
   double* cs = Q + kS * kLd;
   double* sn = cs + kS / 2;
-  int* pab = reinterpret_cast<int*>(sn + kS / 2);
-  int* blk = pab + kS;   // pab takes kS / 2 doubles = kS ints
+  int* blk = reinterpret_cast<int*>(sn + kS / 2) + kS;   // after kS / 2 spare doubles
   const int w = blockIdx.y, k = blockIdx.x, tid = threadIdx.x;
   const int nb = n / kB, npairs = nb / 2;
   const double* A = Aall + size_t(w) * sA;
@@ -190,7 +228,7 @@ __global__ void __launch_bounds__(kThreads) eigh_pair_kernel(const double* __res
     for (int l = e; l < kS / 2; ++l) blk[row0 + l - e] = e | (l << 8);
   }
   __syncthreads();
-  inner_jacobi_sweep(S, Q, cs, sn, pab, blk, 0.25 * tw);
+  inner_jacobi_sweep(S, Q, cs, sn, blk, 0.25 * tw);
   if (tid == 0) {
     flags[w * npairs + k] = 1;
     atomicOr(rot + w, 1);
