@@ -6,15 +6,19 @@
 // The integrals follow the McMurchie-Davidson scheme (Helgaker, Jorgensen, Olsen,
 // "Molecular Electronic-Structure Theory", ch. 9): Hermite expansion coefficients
 // E^{ij}_t of the Gaussian products and Hermite Coulomb integrals R_tuv from the
-// Boys function.  One CTA per (orbital shell pair, auxiliary shell) or (auxiliary
-// shell pair): for every primitive pair/triple the E tables, the Boys values
-// (one thread per order, from a table and its Taylor expansion) and the R table
-// (level-by-level recursion in shared memory over the live (t, u, v) only, two
-// tetrahedral arrays) are built once and every Cartesian component of the block
-// reads them; the Cartesian block is then transformed to pure functions (real
-// solid harmonics) or normalized per component (CART) in shared memory and
-// stored.  Shared memory is laid out per launch for the highest angular momenta
-// of the basis at hand.
+// Boys function.  A block is one (orbital shell pair, auxiliary shell) or one
+// auxiliary shell pair.  The 3-center blocks come in three classes, launched
+// together on three streams: up to 32 Cartesian components and 4 primitive
+// triples on one warp per CTA, contracted blocks (>= 20 triples, <= 128
+// components) on four warp teams per CTA that share the triples, the rest on
+// 128 threads per CTA.  For every primitive pair/triple the E tables, the Boys
+// values (one thread per order, from a table and its Taylor expansion) and the
+// R table (level-by-level recursion in shared memory over the live (t, u, v)
+// only, two tetrahedral arrays) are built once; the ket step and the bra step
+// contract them into the Cartesian block, which is then transformed to pure
+// functions (real solid harmonics) or normalized per component (CART) in shared
+// memory and stored.  Shared memory is laid out per class for the angular
+// momenta it holds.
 //
 // The metric: (P|Q) is diagonalized by the device eigensolver (eigh_jacobi.cu),
 // eigenvalues <= 1e-6 are dropped (TOO_LOW_EIGENVAL, src/m_eri.f90:27) and
