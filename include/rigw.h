@@ -450,7 +450,10 @@ RIGW_API int rigw_autotune(rigw_ctx* ctx, int nprob, const rigw_problem* probs, 
  * others run are admitted as workers and memory free up, and batches of
  * different workers overlap on the GPU.  Small requests go first; one large
  * request runs at a time, started when no small request waits or when the
- * oldest has waited 5 s.  The caller keeps the
+ * oldest has waited 5 s.  With two or more workers, worker 0 takes only small
+ * requests, on high-priority streams, and the others run on low-priority
+ * streams, so that a large request's kernels do not hold up small batches.  The
+ * caller keeps the
  * arrays of a submitted problem and its result buffers alive until
  * rigw_server_wait returned for its ticket. */
 typedef struct rigw_server rigw_server;

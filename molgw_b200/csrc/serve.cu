@@ -8,7 +8,12 @@
 // larger than the share is split into frequency chunks by the scheduler), and
 // runs them as one batch.  Small requests go first; at most one large request
 // runs at a time, and it starts when no small request waits or when the oldest
-// large request has waited kLargeAgeNs (so neither lane starves).  Requests
+// large request has waited kLargeAgeNs (so neither lane starves).  With two or
+// more workers, worker 0 takes only small batches and runs on high-priority
+// streams, the others on low-priority ones.  A large batch
+// that finds no memory while other workers hold theirs goes back to the front of
+// its lane; no new small batch starts until it is taken again, which happens as
+// soon as another batch completes.  Requests
 // that arrive meanwhile wait for the next free worker; batches of different
 // workers run concurrently on the GPU on their own streams.  Waits are bounded
 // by the caller's timeout.
@@ -50,6 +55,7 @@ struct Server {
   int device = 0;
   int max_batch = 64;
   size_t share = 0;
+  bool small_lane_worker = false;   // worker 0 takes only small batches (two or more workers)
   std::vector<std::unique_ptr<Context>> ctx;
   std::vector<std::thread> threads;
   std::mutex mu;
@@ -78,7 +84,9 @@ struct Server {
         auto pick = [&]() -> int {
           const bool large_ready = !queue[1].empty() && large_busy == 0;
           const bool large_aged = large_ready && steady_ns() - queue[1].front()->t_submit_ns > kLargeAgeNs;
-          if (large_ready && (large_aged || queue[0].empty())) return 1;
+          if (w == 0 && small_lane_worker) return (hold_small || queue[0].empty()) ? -1 : 0;
+          // a large request sent back for memory goes next: the small lane holds for it
+          if (large_ready && (large_aged || queue[0].empty() || hold_small)) return 1;
           if (hold_small) return -1;
           return queue[0].empty() ? -1 : 0;
         };
@@ -96,7 +104,13 @@ struct Server {
           q.pop_front();
         }
         ++busy;
-        if (lane == 1) ++large_busy;
+        if (lane == 1) {
+          ++large_busy;
+          if (hold_small) {   // the large request is on its way: small batches may start again
+            hold_small = false;
+            st.hold_ns += steady_ns() - hold_since;
+          }
+        }
         st.batches[lane]++;
       }
       const int64_t t_start = steady_ns();
@@ -198,9 +212,14 @@ RIGW_API int rigw_server_create(rigw_server** srv, int device, size_t hbm_budget
   S.device = device;
   S.max_batch = max_batch;
   S.share = budget / size_t(workers);
+  S.small_lane_worker = workers > 1;
   for (int w = 0; w < workers; ++w) {
     S.ctx.emplace_back(new rigw::Context());
-    rigw::Status st = S.ctx.back()->init(device, S.share, 0, /*blocking_waits=*/true);
+    // with two or more workers, worker 0 serves the small lane on high-priority streams
+    // and the others run on low-priority ones: the block scheduler then hands free SM
+    // slots to small batches first, so a large request's long kernels do not hold them up
+    const int priority = workers > 1 ? (w == 0 ? 1 : -1) : 0;
+    rigw::Status st = S.ctx.back()->init(device, S.share, priority, /*blocking_waits=*/true);
     // the worker's device memory is reserved once: batch plans take their arena
     // from it, so no batch waits for the memory pool to grow
     if (st.good() && S.share > (size_t(2) << 30)) st = S.ctx.back()->reserve(S.share - (size_t(1) << 30));
